@@ -1,0 +1,887 @@
+/*
+ * CPU restatement of the FluidSim UniformCPU pressure projection (FP64, single thread).
+ *
+ * TEST INFRASTRUCTURE ONLY: the parity oracle for the CUDA backend. Only tests/, the smoke
+ * check and the cpu_baseline leg of bench.py load it. Each function names the reference
+ * code it follows (paths inside the FluidSim project).
+ *
+ * Additions that have no reference counterpart (solid obstacle cells, the L2 stop rule,
+ * the cell classification mask) are marked as such; with no solid cells and the max-norm
+ * rule the arithmetic is the reference's.
+ */
+#include "fluid_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* ------------------------------------------------------------------------------------------ */
+/* Materials and coefficients                                                                  */
+/* ------------------------------------------------------------------------------------------ */
+
+/* Density = total component mass / cell area. FluidGridCPU.cpp:1399-1423 (rebuildDensity). */
+void or_density(int cells, int components, const double* const* masses, double cell_size, double* density)
+{
+    const double inverse_area = 1.0 / (cell_size * cell_size);
+    for (int i = 0; i < cells; ++i)
+    {
+        double total = 0.0;
+        for (int k = 0; k < components; ++k)
+            total += masses[k][i];
+        density[i] = total * inverse_area;
+    }
+}
+
+/* Face weights 2/(rho_a + rho_b), zero on the four walls, and the inverse diagonal.
+ * FluidGridCPU.cpp:1154-1205 (rebuildPressureCoefficients). u faces are (w+1) x h, row-major
+ * with index y*(w+1)+x; v faces are w x (h+1) with index y*w+x. */
+void or_coefficients(int w, int h, const double* rho, double* inv_u, double* inv_v, double* inv_diagonal)
+{
+    for (int y = 0; y < h; ++y)
+    {
+        double* hu = inv_u + (size_t)y * (w + 1);
+        hu[0] = 0.0;
+        hu[w] = 0.0;
+        for (int x = 1; x < w; ++x)
+            hu[x] = 2.0 / (rho[y * w + x - 1] + rho[y * w + x]);
+        for (int x = 0; x < w; ++x)
+            inv_v[(size_t)y * w + x] = y == 0 ? 0.0 : 2.0 / (rho[(y - 1) * w + x] + rho[y * w + x]);
+    }
+    for (int x = 0; x < w; ++x)
+        inv_v[(size_t)h * w + x] = 0.0;
+
+    if (!inv_diagonal)
+        return;
+    for (int y = 0; y < h; ++y)
+    {
+        for (int x = 0; x < w; ++x)
+        {
+            const double sum = inv_u[(size_t)y * (w + 1) + x] + inv_u[(size_t)y * (w + 1) + x + 1] +
+                               inv_v[(size_t)y * w + x] + inv_v[(size_t)(y + 1) * w + x];
+            inv_diagonal[(size_t)y * w + x] = sum > 0.0 ? 1.0 / sum : 0.0;
+        }
+    }
+}
+
+/* Solid obstacle cells close their four faces, as the reference closes its outer walls
+ * (FluidGridCPU.cpp:1170-1185). No reference counterpart: the reference has no obstacles. */
+void or_face_flags(int w, int h, const unsigned char* solid, double* inv_u, double* inv_v)
+{
+    if (!solid)
+        return;
+    for (int y = 0; y < h; ++y)
+    {
+        for (int x = 0; x < w; ++x)
+        {
+            if (!solid[y * w + x])
+                continue;
+            inv_u[(size_t)y * (w + 1) + x] = 0.0;
+            inv_u[(size_t)y * (w + 1) + x + 1] = 0.0;
+            inv_v[(size_t)y * w + x] = 0.0;
+            inv_v[(size_t)(y + 1) * w + x] = 0.0;
+        }
+    }
+}
+
+/* Cell classes from the reference thresholds: liquid phase f > 0.5 (FluidGridCPU.cpp:1321-1322),
+ * interface 0 < f < 1 (FluidGridCPU.cpp:531-533); solid from the obstacle mask (no reference
+ * counterpart). Bits: 1 liquid, 2 interface, 4 solid; a solid cell carries only bit 4. */
+void or_classify(int cells, const double* f, const unsigned char* solid, unsigned char* mask)
+{
+    for (int i = 0; i < cells; ++i)
+    {
+        if (solid && solid[i])
+        {
+            mask[i] = 4;
+            continue;
+        }
+        unsigned char m = 0;
+        if (f[i] > 0.5)
+            m |= 1;
+        if (f[i] > 0.0 && f[i] < 1.0)
+            m |= 2;
+        mask[i] = m;
+    }
+}
+
+/* (A x)_i = sum over the cell's faces of weight * (x_i - x_neighbour); returns x . Ax.
+ * FluidGridCPU.cpp:1507-1598 (applyPressureOperator); same pairing of the four terms. */
+double or_operator(int w, int h, const double* inv_u, const double* inv_v, const double* x, double* y)
+{
+    double dot = 0.0;
+    for (int j = 0; j < h; ++j)
+    {
+        for (int i = 0; i < w; ++i)
+        {
+            const int c = j * w + i;
+            const double center = x[c];
+            const double wl = inv_u[(size_t)j * (w + 1) + i];
+            const double wr = inv_u[(size_t)j * (w + 1) + i + 1];
+            const double wu = inv_v[(size_t)j * w + i];
+            const double wd = inv_v[(size_t)(j + 1) * w + i];
+            const double xl = i > 0 ? x[c - 1] : center;
+            const double xr = i + 1 < w ? x[c + 1] : center;
+            const double xu = j > 0 ? x[c - w] : center;
+            const double xd = j + 1 < h ? x[c + w] : center;
+            const double value = (wl * (center - xl) + wr * (center - xr)) + (wu * (center - xu) + wd * (center - xd));
+            y[c] = value;
+            dot += center * value;
+        }
+    }
+    return dot;
+}
+
+/* Zero the wall normal velocities and form b = -(du + dv)/dx * dx^2/dt (not yet mean-free).
+ * FluidGridCPU.cpp:1050-1083. */
+void or_rhs(int w, int h, double dx, double dt, double* u, double* v, double* b)
+{
+    const double scale = dx * dx / dt;
+    for (int y = 0; y < h; ++y)
+    {
+        u[(size_t)y * (w + 1)] = 0.0;
+        u[(size_t)y * (w + 1) + w] = 0.0;
+    }
+    for (int x = 0; x < w; ++x)
+    {
+        v[x] = 0.0;
+        v[(size_t)h * w + x] = 0.0;
+    }
+    for (int y = 0; y < h; ++y)
+    {
+        for (int x = 0; x < w; ++x)
+        {
+            const double du = u[(size_t)y * (w + 1) + x + 1] - u[(size_t)y * (w + 1) + x];
+            const double dv = v[(size_t)(y + 1) * w + x] - v[(size_t)y * w + x];
+            b[y * w + x] = -(du + dv) / dx * scale;
+        }
+    }
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* Multigrid preconditioner: PressureMultigrid.cpp                                              */
+/* ------------------------------------------------------------------------------------------ */
+
+typedef struct
+{
+    int first, second;
+    double weight; /* weight of `second`; `first` gets 1 - weight */
+} or_interp;
+
+typedef struct
+{
+    int count;
+    int index[4];
+    double weight[4];
+} or_gather;
+
+typedef struct
+{
+    int w, h, s; /* s = w + 2: one zero halo cell on every side */
+    double *cx, *cy;
+    double *right, *down, *invd, *rhs, *sol, *res;
+    or_interp *px, *py;  /* fine cell -> two coarse cells (used on the fine level) */
+    or_gather *rx, *ry;  /* coarse cell -> fine cells: the transpose of px, py */
+} or_level;
+
+struct or_mg
+{
+    int count;
+    or_level* lev;
+    int n;          /* coarsest unknowns: cells - 1 (cell 0 pinned) */
+    double* factor; /* dense n x n Cholesky factor, lower triangle */
+    double* work;
+};
+
+/* Level geometry; cell centres with a shorter last cell on odd sizes. PressureMultigrid.cpp:24-36. */
+static void level_init(or_level* l, int w, int h, int spacing, int domain_w, int domain_h)
+{
+    memset(l, 0, sizeof(*l));
+    l->w = w;
+    l->h = h;
+    l->s = w + 2;
+    const size_t count = (size_t)l->s * (h + 2);
+    double** arrays[] = {&l->right, &l->down, &l->invd, &l->rhs, &l->sol, &l->res};
+    for (int a = 0; a < 6; ++a)
+        *arrays[a] = (double*)calloc(count, sizeof(double));
+    l->cx = (double*)calloc(w, sizeof(double));
+    l->cy = (double*)calloc(h, sizeof(double));
+    for (int x = 0; x < w; ++x)
+    {
+        const int end = (x + 1) * spacing < domain_w ? (x + 1) * spacing : domain_w;
+        l->cx[x] = 0.5 * (x * spacing + end);
+    }
+    for (int y = 0; y < h; ++y)
+    {
+        const int end = (y + 1) * spacing < domain_h ? (y + 1) * spacing : domain_h;
+        l->cy[y] = 0.5 * (y * spacing + end);
+    }
+}
+
+/* Linear interpolation between the two nearest coarse centres, clamped at the ends; the
+ * restriction is its exact transpose. PressureMultigrid.cpp:64-102 (buildTransfers). */
+static void build_axis(int nf, const double* fc, int nc, const double* cc, or_interp* p, or_gather* r)
+{
+    for (int c = 0; c < nc; ++c)
+        r[c].count = 0;
+    for (int f = 0; f < nf; ++f)
+    {
+        const int parent = f / 2;
+        int first = parent - (fc[f] < cc[parent] ? 1 : 0);
+        if (first < 0)
+            first = 0;
+        const int second = first + 1 < nc ? first + 1 : nc - 1;
+        double weight = 0.0;
+        if (first != second)
+        {
+            weight = (fc[f] - cc[first]) / (cc[second] - cc[first]);
+            weight = weight < 0.0 ? 0.0 : (weight > 1.0 ? 1.0 : weight);
+        }
+        p[f].first = first;
+        p[f].second = second;
+        p[f].weight = weight;
+        const int targets[2] = {first, second};
+        const double values[2] = {1.0 - weight, weight};
+        for (int k = 0; k < 2; ++k)
+        {
+            if (values[k] == 0.0)
+                continue;
+            or_gather* g = &r[targets[k]];
+            g->index[g->count] = f;
+            g->weight[g->count] = values[k];
+            g->count++;
+        }
+    }
+}
+
+/* Halve (rounding up) until the level has at most 64 cells. PressureMultigrid.cpp:38-62. */
+or_mg* or_mg_create(int width, int height)
+{
+    or_mg* mg = (or_mg*)calloc(1, sizeof(or_mg));
+    int w = width, h = height, spacing = 1, count = 0, cap = 4;
+    mg->lev = (or_level*)calloc(cap, sizeof(or_level));
+    for (;;)
+    {
+        if (count == cap)
+        {
+            cap *= 2;
+            mg->lev = (or_level*)realloc(mg->lev, cap * sizeof(or_level));
+        }
+        level_init(&mg->lev[count++], w, h, spacing, width, height);
+        if (w * h <= 64)
+            break;
+        w = (w + 1) / 2;
+        h = (h + 1) / 2;
+        spacing *= 2;
+    }
+    mg->count = count;
+    for (int i = 0; i + 1 < count; ++i)
+    {
+        or_level* f = &mg->lev[i];
+        or_level* c = &mg->lev[i + 1];
+        f->px = (or_interp*)calloc(f->w, sizeof(or_interp));
+        f->py = (or_interp*)calloc(f->h, sizeof(or_interp));
+        f->rx = (or_gather*)calloc(c->w, sizeof(or_gather));
+        f->ry = (or_gather*)calloc(c->h, sizeof(or_gather));
+        build_axis(f->w, f->cx, c->w, c->cx, f->px, f->rx);
+        build_axis(f->h, f->cy, c->h, c->cy, f->py, f->ry);
+    }
+    const or_level* last = &mg->lev[count - 1];
+    mg->n = last->w * last->h - 1;
+    mg->factor = (double*)calloc((size_t)(mg->n > 0 ? mg->n : 1) * (mg->n > 0 ? mg->n : 1), sizeof(double));
+    mg->work = (double*)calloc(mg->n > 0 ? mg->n : 1, sizeof(double));
+    return mg;
+}
+
+void or_mg_destroy(or_mg* mg)
+{
+    if (!mg)
+        return;
+    for (int i = 0; i < mg->count; ++i)
+    {
+        or_level* l = &mg->lev[i];
+        free(l->right), free(l->down), free(l->invd), free(l->rhs), free(l->sol), free(l->res);
+        free(l->cx), free(l->cy), free(l->px), free(l->py), free(l->rx), free(l->ry);
+    }
+    free(mg->lev);
+    free(mg->factor);
+    free(mg->work);
+    free(mg);
+}
+
+int or_mg_levels(const or_mg* mg) { return mg->count; }
+
+/* PressureMultigrid.cpp:104-117 (rebuildDiagonal). */
+static void level_diagonal(or_level* l)
+{
+    for (int y = 0; y < l->h; ++y)
+    {
+        for (int x = 0; x < l->w; ++x)
+        {
+            const int i = (y + 1) * l->s + x + 1;
+            const double d = l->right[i - 1] + l->right[i] + l->down[i - l->s] + l->down[i];
+            l->invd[i] = d > 0.0 ? 1.0 / d : 0.0;
+        }
+    }
+}
+
+/* Coarse conductances: fine faces crossing a coarse face add in parallel; along the path
+ * between coarse centres each crossed fine face adds in series, weighted by the fraction of
+ * the fine spacing that the path covers. PressureMultigrid.cpp:142-202 (coarsen). */
+static void level_coarsen(const or_level* f, or_level* c)
+{
+    for (int y = 0; y < c->h; ++y)
+    {
+        for (int x = 0; x + 1 < c->w; ++x)
+        {
+            const int e = 2 * x + 2;
+            const double a = (f->cx[e - 1] - c->cx[x]) / (f->cx[e - 1] - f->cx[e - 2]);
+            const double b = e + 1 < f->w ? (c->cx[x + 1] - f->cx[e]) / (f->cx[e + 1] - f->cx[e]) : 0.0;
+            double g = 0.0;
+            const int fy_end = 2 * y + 2 < f->h ? 2 * y + 2 : f->h;
+            for (int fy = 2 * y; fy < fy_end; ++fy)
+            {
+                const int i = (fy + 1) * f->s + e;
+                double resistance = a / f->right[i - 1] + 1.0 / f->right[i];
+                if (b != 0.0)
+                    resistance += b / f->right[i + 1];
+                g += 1.0 / resistance;
+            }
+            c->right[(y + 1) * c->s + x + 1] = g;
+        }
+    }
+    for (int y = 0; y + 1 < c->h; ++y)
+    {
+        for (int x = 0; x < c->w; ++x)
+        {
+            const int e = 2 * y + 2;
+            const double a = (f->cy[e - 1] - c->cy[y]) / (f->cy[e - 1] - f->cy[e - 2]);
+            const double b = e + 1 < f->h ? (c->cy[y + 1] - f->cy[e]) / (f->cy[e + 1] - f->cy[e]) : 0.0;
+            double g = 0.0;
+            const int fx_end = 2 * x + 2 < f->w ? 2 * x + 2 : f->w;
+            for (int fx = 2 * x; fx < fx_end; ++fx)
+            {
+                const int i = e * f->s + fx + 1;
+                double resistance = a / f->down[i - f->s] + 1.0 / f->down[i];
+                if (b != 0.0)
+                    resistance += b / f->down[i + f->s];
+                g += 1.0 / resistance;
+            }
+            c->down[(y + 1) * c->s + x + 1] = g;
+        }
+    }
+    level_diagonal(c);
+}
+
+/* Dense Cholesky of the coarsest operator with cell 0 pinned to zero.
+ * PressureMultigrid.cpp:300-345 (factorCoarsest). Returns 0 on a non-positive pivot. */
+static int factor_coarsest(or_mg* mg)
+{
+    const or_level* l = &mg->lev[mg->count - 1];
+    const int n = mg->n;
+    double* a = mg->factor;
+    if (n <= 0)
+        return 1;
+    memset(a, 0, sizeof(double) * (size_t)n * n);
+    for (int cell = 1; cell <= n; ++cell)
+    {
+        const int x = cell % l->w, y = cell / l->w;
+        const int i = (y + 1) * l->s + x + 1;
+        const int row = cell - 1;
+        a[row * n + row] = l->right[i - 1] + l->right[i] + l->down[i - l->s] + l->down[i];
+        if (x > 0 && cell - 1 > 0)
+            a[row * n + row - 1] = -l->right[i - 1];
+        if (y > 0 && cell - l->w > 0)
+            a[row * n + row - l->w] = -l->down[i - l->s];
+    }
+    for (int row = 0; row < n; ++row)
+    {
+        for (int col = 0; col <= row; ++col)
+        {
+            double value = a[row * n + col];
+            for (int k = 0; k < col; ++k)
+                value -= a[row * n + k] * a[col * n + k];
+            if (row == col)
+            {
+                if (!(value > 0.0) || !isfinite(value))
+                    return 0;
+                a[row * n + col] = sqrt(value);
+            }
+            else
+                a[row * n + col] = value / a[col * n + col];
+        }
+    }
+    return 1;
+}
+
+/* PressureMultigrid.cpp:119-140 (rebuild). */
+int or_mg_rebuild(or_mg* mg, const double* inv_u, const double* inv_v)
+{
+    or_level* f = &mg->lev[0];
+    for (int y = 0; y < f->h; ++y)
+    {
+        for (int x = 0; x < f->w; ++x)
+        {
+            const int i = (y + 1) * f->s + x + 1;
+            f->right[i] = inv_u[(size_t)y * (f->w + 1) + x + 1];
+            f->down[i] = inv_v[(size_t)(y + 1) * f->w + x];
+        }
+    }
+    level_diagonal(f);
+    for (int i = 0; i + 1 < mg->count; ++i)
+        level_coarsen(&mg->lev[i], &mg->lev[i + 1]);
+    return factor_coarsest(mg);
+}
+
+/* One red-black Gauss-Seidel sweep: colour (x + y) & 1 == c is updated from the other
+ * colour; `reverse` runs colour 1 first; `from_zero` treats the first colour's neighbours as
+ * zero. PressureMultigrid.cpp:204-231 (smooth). */
+static void level_smooth(or_level* l, int reverse, int from_zero)
+{
+    const int s = l->s;
+    for (int pass = 0; pass < 2; ++pass)
+    {
+        const int colour = reverse ? 1 - pass : pass;
+        for (int y = 0; y < l->h; ++y)
+        {
+            for (int x = (colour ^ (y & 1)); x < l->w; x += 2)
+            {
+                const int i = (y + 1) * s + x + 1;
+                double value = l->rhs[i];
+                if (!(from_zero && pass == 0))
+                    value += (l->right[i - 1] * l->sol[i - 1] + l->right[i] * l->sol[i + 1]) +
+                             (l->down[i - s] * l->sol[i - s] + l->down[i] * l->sol[i + s]);
+                l->sol[i] = value * l->invd[i];
+            }
+        }
+    }
+}
+
+/* Fine residual, then its transpose-interpolation onto the coarse rhs.
+ * PressureMultigrid.cpp:233-276 (restrictResidual). */
+static void level_restrict(or_level* f, or_level* c)
+{
+    const int s = f->s;
+    for (int y = 0; y < f->h; ++y)
+    {
+        for (int x = 0; x < f->w; ++x)
+        {
+            const int i = (y + 1) * s + x + 1;
+            const double center = f->sol[i];
+            const double product = (f->right[i - 1] * (center - f->sol[i - 1]) + f->right[i] * (center - f->sol[i + 1])) +
+                                   (f->down[i - s] * (center - f->sol[i - s]) + f->down[i] * (center - f->sol[i + s]));
+            f->res[i] = f->rhs[i] - product;
+        }
+    }
+    for (int y = 0; y < c->h; ++y)
+    {
+        for (int x = 0; x < c->w; ++x)
+        {
+            const or_gather* gx = &f->rx[x];
+            const or_gather* gy = &f->ry[y];
+            double value = 0.0;
+            for (int j = 0; j < gy->count; ++j)
+            {
+                const double* row = f->res + (size_t)(gy->index[j] + 1) * s + 1;
+                double line = 0.0;
+                for (int k = 0; k < gx->count; ++k)
+                    line += gx->weight[k] * row[gx->index[k]];
+                value += gy->weight[j] * line;
+            }
+            c->rhs[(y + 1) * c->s + x + 1] = value;
+        }
+    }
+}
+
+/* Bilinear interpolation of the coarse correction, added to the fine solution.
+ * PressureMultigrid.cpp:278-298 (prolongCorrection). */
+static void level_prolong(const or_level* c, or_level* f)
+{
+    for (int y = 0; y < f->h; ++y)
+    {
+        const or_interp* py = &f->py[y];
+        const double* top = c->sol + (size_t)(py->first + 1) * c->s + 1;
+        const double* bottom = c->sol + (size_t)(py->second + 1) * c->s + 1;
+        for (int x = 0; x < f->w; ++x)
+        {
+            const or_interp* px = &f->px[x];
+            const double a = (1.0 - px->weight) * top[px->first] + px->weight * top[px->second];
+            const double b = (1.0 - px->weight) * bottom[px->first] + px->weight * bottom[px->second];
+            f->sol[(y + 1) * f->s + x + 1] += (1.0 - py->weight) * a + py->weight * b;
+        }
+    }
+}
+
+/* Forward/back substitution on the mean-free coarse rhs, then a mean-zero gauge.
+ * PressureMultigrid.cpp:347-384 (solveCoarsest). */
+static void solve_coarsest(or_mg* mg)
+{
+    or_level* l = &mg->lev[mg->count - 1];
+    const int n = mg->n;
+    const double* a = mg->factor;
+    double* z = mg->work;
+    double mean = 0.0;
+    for (int y = 0; y < l->h; ++y)
+        for (int x = 0; x < l->w; ++x)
+            mean += l->rhs[(y + 1) * l->s + x + 1];
+    mean /= n + 1;
+    for (int row = 0; row < n; ++row)
+    {
+        const int cell = row + 1;
+        double value = l->rhs[(cell / l->w + 1) * l->s + cell % l->w + 1] - mean;
+        for (int col = 0; col < row; ++col)
+            value -= a[row * n + col] * z[col];
+        z[row] = value / a[row * n + row];
+    }
+    for (int row = n - 1; row >= 0; --row)
+    {
+        double value = z[row];
+        for (int col = row + 1; col < n; ++col)
+            value -= a[col * n + row] * z[col];
+        z[row] = value / a[row * n + row];
+    }
+    double sum = 0.0;
+    for (int k = 0; k < n; ++k)
+        sum += z[k];
+    mean = sum / (n + 1);
+    l->sol[l->s + 1] = -mean;
+    for (int cell = 1; cell <= n; ++cell)
+        l->sol[(cell / l->w + 1) * l->s + cell % l->w + 1] = z[cell - 1] - mean;
+}
+
+/* Four pre-sweeps (the first from zero), restrict, recurse, prolong, four post-sweeps in the
+ * reversed colour order. PressureMultigrid.cpp:386-408 (cycle). */
+static void mg_cycle(or_mg* mg, int index)
+{
+    if (index + 1 == mg->count)
+    {
+        solve_coarsest(mg);
+        return;
+    }
+    or_level* f = &mg->lev[index];
+    or_level* c = &mg->lev[index + 1];
+    level_smooth(f, 0, 1);
+    for (int sweep = 1; sweep < 4; ++sweep)
+        level_smooth(f, 0, 0);
+    level_restrict(f, c);
+    mg_cycle(mg, index + 1);
+    level_prolong(c, f);
+    for (int sweep = 0; sweep < 4; ++sweep)
+        level_smooth(f, 1, 0);
+}
+
+/* PressureMultigrid.cpp:410-434 (apply). */
+void or_mg_apply(or_mg* mg, const double* residual, double* correction, double residual_mean)
+{
+    or_level* f = &mg->lev[0];
+    for (int y = 0; y < f->h; ++y)
+        for (int x = 0; x < f->w; ++x)
+            f->rhs[(y + 1) * f->s + x + 1] = residual[y * f->w + x] - residual_mean;
+    mg_cycle(mg, 0);
+    for (int y = 0; y < f->h; ++y)
+        memcpy(correction + (size_t)y * f->w, f->sol + (size_t)(y + 1) * f->s + 1, sizeof(double) * f->w);
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* Grid and projection: FluidGridCPU.cpp                                                        */
+/* ------------------------------------------------------------------------------------------ */
+
+struct or_grid
+{
+    int w, h, n;
+    double dx;
+    int preconditioner;
+    double *density, *u, *v, *p, *p_prev;
+    double *inv_u, *inv_v, *inv_diag;
+    double *b, *r, *z, *d, *q;
+    or_mg* mg;
+    int mg_valid;
+};
+
+or_grid* or_grid_create(int width, int height, double cell_size)
+{
+    or_grid* g = (or_grid*)calloc(1, sizeof(or_grid));
+    g->w = width;
+    g->h = height;
+    g->n = width * height;
+    g->dx = cell_size;
+    g->preconditioner = OR_PRECONDITIONER_MULTIGRID;
+    const size_t n = (size_t)g->n, nu = (size_t)(width + 1) * height, nv = (size_t)width * (height + 1);
+    g->density = (double*)calloc(n, sizeof(double));
+    g->u = (double*)calloc(nu, sizeof(double));
+    g->v = (double*)calloc(nv, sizeof(double));
+    g->p = (double*)calloc(n, sizeof(double));
+    g->p_prev = (double*)calloc(n, sizeof(double));
+    g->inv_u = (double*)calloc(nu, sizeof(double));
+    g->inv_v = (double*)calloc(nv, sizeof(double));
+    g->inv_diag = (double*)calloc(n, sizeof(double));
+    double** vectors[] = {&g->b, &g->r, &g->z, &g->d, &g->q};
+    for (int k = 0; k < 5; ++k)
+        *vectors[k] = (double*)calloc(n, sizeof(double));
+    g->mg = or_mg_create(width, height);
+    return g;
+}
+
+void or_grid_destroy(or_grid* g)
+{
+    if (!g)
+        return;
+    free(g->density), free(g->u), free(g->v), free(g->p), free(g->p_prev);
+    free(g->inv_u), free(g->inv_v), free(g->inv_diag);
+    free(g->b), free(g->r), free(g->z), free(g->d), free(g->q);
+    or_mg_destroy(g->mg);
+    free(g);
+}
+
+void or_grid_set_preconditioner(or_grid* g, int which) { g->preconditioner = which; }
+
+/* FluidGridCPU.cpp:198-254 (upload): fields replaced, history reset, caches invalidated. */
+void or_grid_upload(or_grid* g, const double* density, const double* u, const double* v, const double* p)
+{
+    const size_t n = (size_t)g->n, nu = (size_t)(g->w + 1) * g->h, nv = (size_t)g->w * (g->h + 1);
+    if (density)
+        memcpy(g->density, density, n * sizeof(double));
+    else
+        memset(g->density, 0, n * sizeof(double));
+    if (u)
+        memcpy(g->u, u, nu * sizeof(double));
+    else
+        memset(g->u, 0, nu * sizeof(double));
+    if (v)
+        memcpy(g->v, v, nv * sizeof(double));
+    else
+        memset(g->v, 0, nv * sizeof(double));
+    if (p)
+        memcpy(g->p, p, n * sizeof(double));
+    else
+        memset(g->p, 0, n * sizeof(double));
+    memcpy(g->p_prev, g->p, n * sizeof(double));
+    or_coefficients(g->w, g->h, g->density, g->inv_u, g->inv_v, g->inv_diag);
+    g->mg_valid = 0;
+}
+
+void or_grid_download(const or_grid* g, double* u, double* v, double* p)
+{
+    if (u)
+        memcpy(u, g->u, (size_t)(g->w + 1) * g->h * sizeof(double));
+    if (v)
+        memcpy(v, g->v, (size_t)g->w * (g->h + 1) * sizeof(double));
+    if (p)
+        memcpy(p, g->p, (size_t)g->n * sizeof(double));
+}
+
+/* Interior horizontal faces only. FluidGridCPU.cpp:987-996 (applyGravity). */
+void or_grid_apply_gravity(or_grid* g, double gravity, double dt)
+{
+    for (int i = g->w; i < g->w * g->h; ++i)
+        g->v[i] += gravity * dt;
+}
+
+static double sum_of(const double* x, int n)
+{
+    double s = 0.0;
+    for (int i = 0; i < n; ++i)
+        s += x[i];
+    return s;
+}
+
+/* FluidGridCPU.cpp:1466-1474 (removeMean). */
+static void remove_mean(double* x, int n)
+{
+    const double mean = sum_of(x, n) / n;
+    for (int i = 0; i < n; ++i)
+        x[i] -= mean;
+}
+
+typedef struct
+{
+    double sum, max, sumsq;
+} or_stats;
+
+static or_stats stats_of(const double* r, int n)
+{
+    or_stats s = {0.0, 0.0, 0.0};
+    for (int i = 0; i < n; ++i)
+    {
+        s.sum += r[i];
+        const double a = fabs(r[i]);
+        if (a > s.max)
+            s.max = a;
+        s.sumsq += r[i] * r[i];
+    }
+    if (!isfinite(s.sum))
+        s.max = INFINITY;
+    return s;
+}
+
+/* r = b - A p with its stats. FluidGridCPU.cpp:1643-1683 (rebuildPressureResidual). */
+static or_stats true_residual(or_grid* g)
+{
+    or_operator(g->w, g->h, g->inv_u, g->inv_v, g->p, g->q);
+    for (int i = 0; i < g->n; ++i)
+        g->r[i] = g->b[i] - g->q[i];
+    return stats_of(g->r, g->n);
+}
+
+/* Preconditioner, then z's mean removed and r . z returned. FluidGridCPU.cpp:1685-1726. */
+static double precondition(or_grid* g, double residual_mean)
+{
+    if (g->preconditioner == OR_PRECONDITIONER_MULTIGRID)
+        or_mg_apply(g->mg, g->r, g->z, residual_mean);
+    else
+        for (int i = 0; i < g->n; ++i)
+            g->z[i] = (g->r[i] - residual_mean) * g->inv_diag[i];
+    const double mean = sum_of(g->z, g->n) / g->n;
+    double dot = 0.0;
+    for (int i = 0; i < g->n; ++i)
+    {
+        g->z[i] -= mean;
+        dot += g->r[i] * g->z[i];
+    }
+    return dot;
+}
+
+static int met(or_stats s, double tol_max, double tol_sumsq)
+{
+    return s.max <= tol_max && s.sumsq <= tol_sumsq;
+}
+
+/* PCG with warm start, lazy preconditioner, restart on drift.
+ * FluidGridCPU.cpp:1728-1824 (solvePressure). */
+static int solve_pressure(or_grid* g, int max_iterations, double tol_max, double tol_sumsq)
+{
+    const int n = g->n;
+    double bmax = 0.0, bsq = 0.0;
+    for (int i = 0; i < n; ++i)
+    {
+        const double a = isfinite(g->b[i]) ? fabs(g->b[i]) : INFINITY;
+        bmax = a > bmax ? a : bmax;
+        bsq += g->b[i] * g->b[i];
+    }
+    if (bmax <= tol_max && bsq <= tol_sumsq)
+    {
+        memset(g->p, 0, n * sizeof(double));
+        memset(g->p_prev, 0, n * sizeof(double));
+        return 0;
+    }
+    for (int i = 0; i < n; ++i)
+    {
+        const double latest = g->p[i];
+        g->p[i] = 2.0 * latest - g->p_prev[i];
+        g->p_prev[i] = latest;
+    }
+    remove_mean(g->p, n);
+    or_stats initial = true_residual(g);
+    if (met(initial, tol_max, tol_sumsq) || max_iterations == 0)
+        return 0;
+    if (g->preconditioner == OR_PRECONDITIONER_MULTIGRID && !g->mg_valid)
+    {
+        g->mg_valid = or_mg_rebuild(g->mg, g->inv_u, g->inv_v);
+        if (!g->mg_valid)
+            return -1;
+    }
+    double residual_mean = initial.sum / n;
+    double rz = precondition(g, residual_mean);
+    memcpy(g->d, g->z, n * sizeof(double));
+    int iterations = 0;
+    while (iterations < max_iterations && rz > 0.0 && isfinite(rz))
+    {
+        const double dq = or_operator(g->w, g->h, g->inv_u, g->inv_v, g->d, g->q);
+        if (dq <= 0.0 || !isfinite(dq))
+            break;
+        const double alpha = rz / dq;
+        if (!isfinite(alpha))
+            break;
+        for (int i = 0; i < n; ++i)
+        {
+            g->p[i] += alpha * g->d[i];
+            g->r[i] -= alpha * g->q[i];
+        }
+        or_stats s = stats_of(g->r, n);
+        residual_mean = s.sum / n;
+        ++iterations;
+        int restart = 0;
+        if (met(s, tol_max, tol_sumsq))
+        {
+            const or_stats actual = true_residual(g);
+            if (met(actual, tol_max, tol_sumsq))
+                break;
+            residual_mean = actual.sum / n;
+            restart = 1;
+        }
+        const double next = precondition(g, residual_mean);
+        const double beta = restart ? 0.0 : next / rz;
+        if (!isfinite(beta))
+            break;
+        for (int i = 0; i < n; ++i)
+            g->d[i] = g->z[i] + beta * g->d[i];
+        rz = next;
+    }
+    remove_mean(g->p, n);
+    return iterations;
+}
+
+/* FluidGridCPU.cpp:1126-1152 (maxDivergence). */
+double or_grid_max_divergence(const or_grid* g)
+{
+    double maximum = 0.0;
+    for (int y = 0; y < g->h; ++y)
+    {
+        for (int x = 0; x < g->w; ++x)
+        {
+            const double div = ((g->u[(size_t)y * (g->w + 1) + x + 1] - g->u[(size_t)y * (g->w + 1) + x]) +
+                                   (g->v[(size_t)(y + 1) * g->w + x] - g->v[(size_t)y * g->w + x])) /
+                               g->dx;
+            if (!isfinite(div))
+                return INFINITY;
+            if (fabs(div) > maximum)
+                maximum = fabs(div);
+        }
+    }
+    return maximum;
+}
+
+/* FluidGridCPU.cpp:1030-1124 (project). */
+or_result or_grid_project(
+    or_grid* g, double dt, int max_iterations, double divergence_tolerance, double relative_tolerance)
+{
+    or_result result = {0, 0, INFINITY, 0.0, 0.0, 0.0};
+    if (dt <= 0.0 || g->w <= 0 || g->h <= 0 || max_iterations < 0)
+        return result;
+    const int w = g->w, h = g->h, n = g->n;
+    const double scale = g->dx * g->dx / dt;
+    or_rhs(w, h, g->dx, dt, g->u, g->v, g->b);
+    remove_mean(g->b, n);
+    double bsq = 0.0;
+    for (int i = 0; i < n; ++i)
+        bsq += g->b[i] * g->b[i];
+    result.rhs_l2 = sqrt(bsq);
+
+    double tol_max = divergence_tolerance * scale, tol_sumsq = INFINITY;
+    if (relative_tolerance > 0.0)
+    {
+        tol_max = INFINITY;
+        tol_sumsq = relative_tolerance * relative_tolerance * bsq;
+    }
+    result.iterations = solve_pressure(g, max_iterations, tol_max, tol_sumsq);
+    if (result.iterations < 0)
+        return result;
+
+    const or_stats final_residual = true_residual(g);
+    result.residual_max = final_residual.max;
+    result.residual_l2 = sqrt(final_residual.sumsq);
+
+    /* u -= dp/dx * dt * w on interior faces. FluidGridCPU.cpp:1098-1118. */
+    for (int y = 0; y < h; ++y)
+    {
+        const double* row = g->p + (size_t)y * w;
+        for (int x = 1; x < w; ++x)
+            g->u[(size_t)y * (w + 1) + x] -= ((row[x] - row[x - 1]) / g->dx) * dt * g->inv_u[(size_t)y * (w + 1) + x];
+        if (y == 0)
+            continue;
+        for (int x = 0; x < w; ++x)
+            g->v[(size_t)y * w + x] -= ((row[x] - row[x - w]) / g->dx) * dt * g->inv_v[(size_t)y * w + x];
+    }
+    result.max_divergence = or_grid_max_divergence(g);
+    result.converged = result.max_divergence <= divergence_tolerance;
+    return result;
+}

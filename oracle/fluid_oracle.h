@@ -1,0 +1,73 @@
+/*
+ * CPU restatement of the FluidSim UniformCPU pressure projection, in plain C and FP64.
+ *
+ * TEST INFRASTRUCTURE ONLY. This is the parity oracle for the CUDA backend: it is linked by
+ * tests/, __graft_entry__.smoke() and the cpu_baseline leg of bench.py, never by the product.
+ * It is pinned against the reference engine itself (oracle/_ref, compiled from the reference
+ * sources by oracle/Makefile) and against the golden fixtures in tests/golden/.
+ *
+ * Reference files (paths inside the FluidSim project):
+ *   FluidSim/UniformCPU/FluidGridCPU.cpp   project, coefficients, operator, PCG driver
+ *   FluidSim/UniformCPU/PressureMultigrid.cpp  V-cycle preconditioner
+ */
+#ifndef FLUID_ORACLE_H
+#define FLUID_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct or_grid or_grid;
+typedef struct or_mg or_mg;
+
+typedef struct or_result
+{
+    int iterations;        /* PCG iterations; -1 on coarse factor breakdown */
+    int converged;         /* max |div u| <= tolerance after the update */
+    double max_divergence; /* max |(du + dv)/dx| over cells, 1/s; +inf if non-finite */
+    double residual_max;   /* final true residual, max norm (pressure units) */
+    double residual_l2;    /* final true residual, L2 norm */
+    double rhs_l2;         /* L2 norm of the mean-free right-hand side */
+} or_result;
+
+enum { OR_PRECONDITIONER_DIAGONAL = 0, OR_PRECONDITIONER_MULTIGRID = 1 };
+
+/* Grid lifecycle. The grid owns u ((w+1)*h), v (w*(h+1)), pressure and previous pressure (w*h). */
+or_grid* or_grid_create(int width, int height, double cell_size);
+void or_grid_destroy(or_grid* grid);
+void or_grid_set_preconditioner(or_grid* grid, int which);
+
+/* Upload: density per cell, face velocities and pressure (null = zero). Resets the warm-start
+ * history to the uploaded pressure, like FluidGridCPU::upload. */
+void or_grid_upload(or_grid* grid, const double* density, const double* u, const double* v, const double* pressure);
+void or_grid_download(const or_grid* grid, double* u, double* v, double* pressure);
+
+/* v += g*dt on interior horizontal faces (FluidGridCPU::applyGravity). */
+void or_grid_apply_gravity(or_grid* grid, double gravity, double dt);
+
+/* One projection (FluidGridCPU::project). Stop rule: when relative_tolerance > 0, the L2 rule
+ * ||r|| <= relative_tolerance * ||b|| is used, else the reference's max-norm rule
+ * max |r| <= divergence_tolerance * dx^2 / dt. */
+or_result or_grid_project(
+    or_grid* grid, double dt, int max_iterations, double divergence_tolerance, double relative_tolerance);
+double or_grid_max_divergence(const or_grid* grid);
+
+/* Stand-alone pieces, used by the unit tests. */
+void or_density(int cells, int components, const double* const* masses, double cell_size, double* density);
+void or_coefficients(int width, int height, const double* density, double* inv_u, double* inv_v, double* inv_diagonal);
+double or_operator(int width, int height, const double* inv_u, const double* inv_v, const double* x, double* y);
+void or_rhs(int width, int height, double cell_size, double dt, double* u, double* v, double* rhs);
+void or_face_flags(int width, int height, const unsigned char* solid, double* inv_u, double* inv_v);
+void or_classify(int cells, const double* fraction, const unsigned char* solid, unsigned char* mask);
+
+/* Multigrid preconditioner (PressureMultigrid). */
+or_mg* or_mg_create(int width, int height);
+void or_mg_destroy(or_mg* mg);
+int or_mg_levels(const or_mg* mg);
+int or_mg_rebuild(or_mg* mg, const double* inv_u, const double* inv_v); /* 1 ok, 0 breakdown */
+void or_mg_apply(or_mg* mg, const double* residual, double* correction, double residual_mean);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,310 @@
+"""ctypes access to the CPU oracle (test infrastructure only).
+
+Two libraries, both FP64 on the host:
+
+* ``_build/liboracle.so``: the C restatement of the UniformCPU projection (fluid_oracle.c).
+* ``_ref/libfluidref.so``: the reference engine itself (FluidSim/UniformCPU/FluidGridCPU.cpp and
+  PressureMultigrid.cpp), compiled from the reference sources by oracle/Makefile when the
+  reference checkout is present. It travels with the repository snapshot as a built file.
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg import this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "_build", "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libfluidref.so")
+
+_dp = C.POINTER(C.c_double)
+_u8p = C.POINTER(C.c_uint8)
+
+
+def build(reference: bool = True) -> None:
+    """Compile the restatement, and the reference engine when its sources are present."""
+    targets = ["all"] if reference else ["oracle"]
+    subprocess.run(["make", "-s", "-f", os.path.join(HERE, "Makefile")] + targets, check=True)
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    return a.ctypes.data_as(_dp)
+
+
+def _f64(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+
+
+class _OrResult(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("converged", C.c_int), ("max_divergence", C.c_double),
+                ("residual_max", C.c_double), ("residual_l2", C.c_double), ("rhs_l2", C.c_double)]
+
+
+class _RefResult(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("converged", C.c_int), ("max_divergence", C.c_double),
+                ("elapsed_ms", C.c_double)]
+
+
+@dataclass
+class ProjectionResult:
+    iterations: int
+    converged: bool
+    max_divergence: float
+    residual_max: float = float("nan")
+    residual_l2: float = float("nan")
+    rhs_l2: float = float("nan")
+    elapsed_ms: float = float("nan")
+
+
+_lib = None
+_ref = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(ORACLE_SO):
+            build(reference=False)
+        L = C.CDLL(ORACLE_SO)
+        L.or_grid_create.restype = C.c_void_p
+        L.or_grid_create.argtypes = [C.c_int, C.c_int, C.c_double]
+        L.or_grid_destroy.argtypes = [C.c_void_p]
+        L.or_grid_set_preconditioner.argtypes = [C.c_void_p, C.c_int]
+        L.or_grid_upload.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp]
+        L.or_grid_download.argtypes = [C.c_void_p, _dp, _dp, _dp]
+        L.or_grid_apply_gravity.argtypes = [C.c_void_p, C.c_double, C.c_double]
+        L.or_grid_project.restype = _OrResult
+        L.or_grid_project.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_double, C.c_double]
+        L.or_grid_max_divergence.restype = C.c_double
+        L.or_grid_max_divergence.argtypes = [C.c_void_p]
+        L.or_coefficients.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp, _dp]
+        L.or_operator.restype = C.c_double
+        L.or_operator.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp, _dp]
+        L.or_rhs.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, _dp, _dp, _dp]
+        L.or_classify.argtypes = [C.c_int, _dp, _u8p, _u8p]
+        L.or_face_flags.argtypes = [C.c_int, C.c_int, _u8p, _dp, _dp]
+        L.or_mg_create.restype = C.c_void_p
+        L.or_mg_create.argtypes = [C.c_int, C.c_int]
+        L.or_mg_destroy.argtypes = [C.c_void_p]
+        L.or_mg_levels.restype = C.c_int
+        L.or_mg_levels.argtypes = [C.c_void_p]
+        L.or_mg_rebuild.restype = C.c_int
+        L.or_mg_rebuild.argtypes = [C.c_void_p, _dp, _dp]
+        L.or_mg_apply.argtypes = [C.c_void_p, _dp, _dp, C.c_double]
+        _lib = L
+    return _lib
+
+
+def reference_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref():
+    global _ref
+    if _ref is None:
+        if not os.path.exists(REF_SO):
+            raise FileNotFoundError("reference engine not built: " + REF_SO)
+        L = C.CDLL(REF_SO)
+        L.ref_create.restype = C.c_void_p
+        L.ref_create.argtypes = [C.c_int, C.c_int, C.c_double]
+        L.ref_destroy.argtypes = [C.c_void_p]
+        L.ref_set_threads.argtypes = [C.c_int]
+        L.ref_configure.argtypes = [C.c_void_p, C.c_double, C.c_double]
+        L.ref_set_gravity.argtypes = [C.c_void_p, C.c_double]
+        L.ref_set_preconditioner.argtypes = [C.c_void_p, C.c_int]
+        L.ref_upload.restype = C.c_int
+        L.ref_upload.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp, _dp, _dp]
+        L.ref_download.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp]
+        L.ref_project.restype = _RefResult
+        L.ref_project.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_double]
+        L.ref_step.restype = _RefResult
+        L.ref_step.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_double]
+        L.ref_apply_gravity.argtypes = [C.c_void_p, C.c_double]
+        L.ref_max_divergence.restype = C.c_double
+        L.ref_max_divergence.argtypes = [C.c_void_p]
+        L.ref_coefficients.argtypes = [C.c_void_p, _dp, _dp, _dp]
+        L.ref_mg_apply.restype = C.c_int
+        L.ref_mg_apply.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp, C.c_double, _dp]
+        _ref = L
+    return _ref
+
+
+# --------------------------------------------------------------------------------------------
+# Restatement
+# --------------------------------------------------------------------------------------------
+
+def coefficients(density):
+    """Face weights (inv_u, inv_v, inv_diagonal) of a h x w density field."""
+    density = _f64(density)
+    h, w = density.shape
+    inv_u = np.zeros((h, w + 1))
+    inv_v = np.zeros((h + 1, w))
+    inv_d = np.zeros((h, w))
+    lib().or_coefficients(w, h, _ptr(density), _ptr(inv_u), _ptr(inv_v), _ptr(inv_d))
+    return inv_u, inv_v, inv_d
+
+
+def apply_operator(inv_u, inv_v, x):
+    inv_u, inv_v, x = _f64(inv_u), _f64(inv_v), _f64(x)
+    h, w = x.shape
+    y = np.zeros_like(x)
+    dot = lib().or_operator(w, h, _ptr(inv_u), _ptr(inv_v), _ptr(x), _ptr(y))
+    return y, dot
+
+
+def classify(fraction, solid=None):
+    f = _f64(fraction)
+    mask = np.zeros(f.shape, dtype=np.uint8)
+    s = None if solid is None else np.ascontiguousarray(solid, dtype=np.uint8)
+    lib().or_classify(f.size, _ptr(f), None if s is None else s.ctypes.data_as(_u8p), mask.ctypes.data_as(_u8p))
+    return mask
+
+
+def close_solid_faces(inv_u, inv_v, solid):
+    """Zero the face weights around solid cells (in place)."""
+    s = np.ascontiguousarray(solid, dtype=np.uint8)
+    h, w = s.shape
+    lib().or_face_flags(w, h, s.ctypes.data_as(_u8p), _ptr(inv_u), _ptr(inv_v))
+
+
+class Multigrid:
+    """PressureMultigrid restated: rebuild from face weights, apply one V-cycle."""
+
+    def __init__(self, width, height):
+        self.w, self.h = width, height
+        self.handle = lib().or_mg_create(width, height)
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            lib().or_mg_destroy(self.handle)
+            self.handle = None
+
+    @property
+    def levels(self):
+        return lib().or_mg_levels(self.handle)
+
+    def rebuild(self, inv_u, inv_v) -> bool:
+        self._u, self._v = _f64(inv_u), _f64(inv_v)
+        return bool(lib().or_mg_rebuild(self.handle, _ptr(self._u), _ptr(self._v)))
+
+    def apply(self, residual, residual_mean=0.0):
+        r = _f64(residual)
+        z = np.zeros((self.h, self.w))
+        lib().or_mg_apply(self.handle, _ptr(r), _ptr(z), float(residual_mean))
+        return z
+
+
+class OracleGrid:
+    """FP64 restatement of FluidGridCPU's projection for one grid."""
+
+    def __init__(self, width, height, cell_size):
+        self.w, self.h, self.dx = width, height, cell_size
+        self.handle = lib().or_grid_create(width, height, cell_size)
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            lib().or_grid_destroy(self.handle)
+            self.handle = None
+
+    def set_preconditioner(self, multigrid: bool):
+        lib().or_grid_set_preconditioner(self.handle, 1 if multigrid else 0)
+
+    def upload(self, density, u, v, pressure=None):
+        lib().or_grid_upload(self.handle, _ptr(_f64(density)), _ptr(_f64(u)), _ptr(_f64(v)), _ptr(_f64(pressure)))
+
+    def download(self):
+        u = np.zeros((self.h, self.w + 1))
+        v = np.zeros((self.h + 1, self.w))
+        p = np.zeros((self.h, self.w))
+        lib().or_grid_download(self.handle, _ptr(u), _ptr(v), _ptr(p))
+        return u, v, p
+
+    def apply_gravity(self, gravity, dt):
+        lib().or_grid_apply_gravity(self.handle, gravity, dt)
+
+    def project(self, dt, max_iterations=200, tolerance=1e-6, relative_tolerance=0.0):
+        r = lib().or_grid_project(self.handle, dt, max_iterations, tolerance, relative_tolerance)
+        return ProjectionResult(r.iterations, bool(r.converged), r.max_divergence, r.residual_max,
+                                r.residual_l2, r.rhs_l2)
+
+    def max_divergence(self):
+        return lib().or_grid_max_divergence(self.handle)
+
+
+# --------------------------------------------------------------------------------------------
+# Reference engine
+# --------------------------------------------------------------------------------------------
+
+class ReferenceGrid:
+    """The reference FluidGridCPU (two components: one liquid, one gas)."""
+
+    def __init__(self, width, height, cell_size, liquid_density=100.0, gas_density=0.1):
+        self.w, self.h, self.dx = width, height, cell_size
+        self.handle = ref().ref_create(width, height, cell_size)
+        ref().ref_configure(self.handle, liquid_density, gas_density)
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            ref().ref_destroy(self.handle)
+            self.handle = None
+
+    def set_preconditioner(self, multigrid: bool):
+        ref().ref_set_preconditioner(self.handle, 1 if multigrid else 0)
+
+    def set_gravity(self, g):
+        ref().ref_set_gravity(self.handle, g)
+
+    def upload(self, fraction=None, u=None, v=None, pressure=None, liquid_mass=None, gas_mass=None):
+        rc = ref().ref_upload(self.handle, *(_ptr(_f64(a)) for a in (fraction, u, v, pressure, liquid_mass, gas_mass)))
+        if rc != 0:
+            raise ValueError("reference rejected the upload")
+
+    def download(self):
+        f = np.zeros((self.h, self.w))
+        u = np.zeros((self.h, self.w + 1))
+        v = np.zeros((self.h + 1, self.w))
+        p = np.zeros((self.h, self.w))
+        ref().ref_download(self.handle, _ptr(f), _ptr(u), _ptr(v), _ptr(p))
+        return f, u, v, p
+
+    def coefficients(self):
+        inv_u = np.zeros((self.h, self.w + 1))
+        inv_v = np.zeros((self.h + 1, self.w))
+        inv_d = np.zeros((self.h, self.w))
+        ref().ref_coefficients(self.handle, _ptr(inv_u), _ptr(inv_v), _ptr(inv_d))
+        return inv_u, inv_v, inv_d
+
+    def project(self, dt, max_iterations=200, tolerance=1e-6):
+        r = ref().ref_project(self.handle, dt, max_iterations, tolerance)
+        return ProjectionResult(r.iterations, bool(r.converged), r.max_divergence, elapsed_ms=r.elapsed_ms)
+
+    def step(self, dt, max_iterations=200, tolerance=1e-6):
+        r = ref().ref_step(self.handle, dt, max_iterations, tolerance)
+        return ProjectionResult(r.iterations, bool(r.converged), r.max_divergence, elapsed_ms=r.elapsed_ms)
+
+    def apply_gravity(self, dt):
+        ref().ref_apply_gravity(self.handle, dt)
+
+    def max_divergence(self):
+        return ref().ref_max_divergence(self.handle)
+
+
+def reference_mg_apply(inv_u, inv_v, residual, residual_mean=0.0):
+    inv_u, inv_v, r = _f64(inv_u), _f64(inv_v), _f64(residual)
+    h, w = r.shape
+    z = np.zeros((h, w))
+    rc = ref().ref_mg_apply(w, h, _ptr(inv_u), _ptr(inv_v), _ptr(r), float(residual_mean), _ptr(z))
+    if rc != 0:
+        raise RuntimeError("reference multigrid breakdown")
+    return z
+
+
+def set_reference_threads(n: int):
+    ref().ref_set_threads(int(n))

@@ -1,0 +1,428 @@
+"""Benchmark of the UniformCUDA projection: MAC cells projected per second at a 1e-6 residual.
+
+Workload (one step): a 2048 x 2048 two-phase dam break (liquid 1000 / gas 1, liquid below half
+height plus a seeded 200x300 block, face velocities U[-1, 1] in FP32), gravity -9.8 applied,
+then one pressure projection (coefficients and multigrid rebuilt from the step's masses, PCG
+to ||r|| <= 1e-6 ||b||, velocity update, divergence check). Inputs are seeded synthetic data;
+the reference publishes no dataset for this path.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuda|reference]
+
+N > 1 runs under torchrun, one rank per GPU, each projecting its own grid (independent
+replicas: the path has no exchange step). Rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "MAC cells projected/s at 1e-6 residual"
+UNIT = "cells/s"
+L2_FLUSH_BYTES = 256 << 20
+# Algorithmic bytes per fine cell of the two fused fine-level smoothing kernels (FP32):
+# pre reads r, right, down and writes the pre-smoothed solution plus a quarter cell of coarse
+# rhs; post reads the pre-smoothed solution, a quarter cell of coarse solution, r, right, down
+# and writes z.
+ALGORITHMIC_BYTES = {0: 4 + 4 + 4 + 4 + 1, 1: 4 + 1 + 4 + 4 + 4 + 4}
+KERNEL_NAMES = {0: "k_mg_pre<float,8> (fine level)", 1: "k_mg_post<float,8> (fine level)"}
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["cuda", "reference"], default="cuda")
+    p.add_argument("--size", type=int, default=2048)
+    p.add_argument("--tolerance", type=float, default=1e-6)
+    p.add_argument("--no-batched", action="store_true", help="skip the batched uneven-grid measurement")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def scene_for(size, rank):
+    from fluidsim_b200 import scenes
+
+    return scenes.dam_break(size, size, seed=1234 + rank, obstacles=0, velocity=1.0)
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per fine cell of the fused smoothing kernels, from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+    if not os.path.exists(path):
+        return {}
+    with open(path) as f:
+        return {int(k): float(v) for k, v in json.load(f).get("dram_bytes_per_cell", {}).items()}
+
+
+class ClockSampler:
+    """nvidia-smi clock and throttle-reason samples during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.device = device_index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{device_index}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.file = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.file.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------------------------
+# CPU legs (the reference engine compiled from its own sources, else the C restatement)
+# ---------------------------------------------------------------------------------------------
+
+def cpu_projection(scene, tolerance, threads):
+    """Runs one step of the workload on the host; returns (seconds, iterations, kind)."""
+    from oracle import oracle
+
+    if oracle.reference_available():
+        oracle.set_reference_threads(threads)
+        g = oracle.ReferenceGrid(scene.width, scene.height, scene.cell_size, scene.liquid_density, scene.gas_density)
+        g.set_gravity(scene.gravity)
+        g.upload(scene.fraction, scene.u, scene.v, None, scene.liquid_mass[0], scene.gas_mass[0])
+        t = time.perf_counter()
+        g.apply_gravity(scene.dt)
+        # The reference runs its own stop rule, max |div u| <= tol (FluidGridCPU.cpp:1093).
+        r = g.project(scene.dt, 200, tolerance)
+        return time.perf_counter() - t, r.iterations, "reference"
+    oracle.build(reference=False)
+    g = oracle.OracleGrid(scene.width, scene.height, scene.cell_size)
+    g.upload(scene.density(), scene.u, scene.v)
+    t = time.perf_counter()
+    g.apply_gravity(scene.gravity, scene.dt)
+    r = g.project(scene.dt, 200, tolerance, relative_tolerance=tolerance)
+    return time.perf_counter() - t, r.iterations, "port"
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return None
+    size = args.size
+    scene = scene_for(size, 0)
+    threads = min(8, host_threads())
+    times, iters, kind = [], [], "reference"
+    for i in range(args.warmup + args.steps):
+        seconds, it, kind = cpu_projection(scene, args.tolerance, threads)
+        if i >= args.warmup:
+            times.append(seconds)
+            iters.append(it)
+    per_step = statistics.mean(times)
+    value = scene.cells / per_step
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_step * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"dam_break_{size}x{size} projection", "cells": scene.cells,
+                   "tolerance": args.tolerance, "l2": "inputs larger than L2 on the host"},
+        "iterations": statistics.mean(iters),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+                         "sample": f"{args.steps} projections of the {size}x{size} workload, FluidGridCPU::project"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    return line
+
+
+# ---------------------------------------------------------------------------------------------
+# CUDA arm
+# ---------------------------------------------------------------------------------------------
+
+def run_cuda(args, world, rank, local_rank):
+    import torch
+
+    from fluidsim_b200 import FluidGrid, FluidGridState, ProjectionBatch, kernel_launches, scenes
+
+    torch.cuda.set_device(local_rank)
+    size = args.size
+    scene = scene_for(size, rank)
+    pristine = FluidGrid(size, size, scene.cell_size, "fp32")
+    scenes.upload_scene(pristine, scene)
+    work = FluidGrid(size, size, scene.cell_size, "fp32")
+    work.configureMaterials([scene.liquid_density], [scene.gas_density])
+    work.setGravityY(scene.gravity)
+    stream = torch.cuda.ExternalStream(work.stream())
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    def one_step(timed):
+        work.copyStateFrom(pristine)
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)
+            start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            start.record(stream)
+        work.applyGravity(scene.dt)
+        r = work.project(scene.dt, 200, args.tolerance, relative_tolerance=args.tolerance)
+        stop.record(stream)
+        stop.synchronize()
+        return start.elapsed_time(stop), r
+
+    for _ in range(args.warmup):
+        one_step(False)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    results, times = [], []
+    launches_before = kernel_launches()
+    with ClockSampler(local_rank) as clocks:
+        for _ in range(args.steps):
+            ms, r = one_step(True)
+            times.append(ms)
+            results.append(r)
+    torch.cuda.synchronize()
+    launches = kernel_launches() - launches_before
+    total_ms = sum(times)
+    if world > 1:
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * scene.cells * args.steps / (total_ms / 1e3)
+    converged = all(r.solve_status == "converged" and r.residual_l2 <= args.tolerance * r.rhs_l2 * 1.0001
+                    for r in results)
+
+    # Live roofline of the fused fine-level smoothing kernels (CUDA events on the grid stream).
+    peak, peak_kind = measured_peaks()
+    traffic_per_cell = profiled_traffic()
+    kernel_ms = {k: work.timeKernel(k, 20) for k in (0, 1)}
+    dominant = max(kernel_ms, key=kernel_ms.get)
+    algorithmic = ALGORITHMIC_BYTES[dominant] * scene.cells
+    achieved = algorithmic / (kernel_ms[dominant] / 1e3) / 1e9
+    traffic = traffic_per_cell.get(dominant)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": None if traffic is None else traffic * scene.cells,
+                "kernel": KERNEL_NAMES[dominant], "kernel_ms": kernel_ms[dominant],
+                "algorithmic_bytes": algorithmic, "peak_source": f"{peak_kind} hbm_gbs (copy, burst)"}
+    # Whole-projection bandwidth against the survey's per-iteration byte model (306 B/cell per
+    # PCG iteration plus 70 B/cell of set-up), for reference beside the kernel figure.
+    mean_iters = statistics.mean(r.iterations for r in results)
+    model_bytes = scene.cells * (70 + 306 * mean_iters)
+    projection_model = {"iterations": mean_iters, "bytes": model_bytes,
+                        "gbs": model_bytes / (total_ms / args.steps / 1e3) / 1e9 / (world if world > 1 else 1)}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"dam_break_{size}x{size} projection (gravity + PCG-MG to 1e-6 relative)",
+                   "cells": scene.cells, "tolerance": args.tolerance, "density_ratio": "1000:1",
+                   "l2": "flushed (256 MiB write) before every timed step", "parallelism": f"replicas x{world}"},
+        "iterations": mean_iters,
+        "converged": converged,
+        "relative_residual": max(r.relative_residual for r in results),
+        "restarts": max(r.restarts for r in results),
+        "roofline": roofline,
+        "projection_bandwidth_model": projection_model,
+        "clocks": clocks.summary(),
+        "gpu_launches": launches,
+    }
+
+    if rank == 0 and not args.no_e2e:
+        line["e2e"] = e2e_measure(args, scene, torch)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        seconds, it, kind = cpu_projection(scene, args.tolerance, min(8, host_threads()))
+        line["cpu_baseline"] = {"value": scene.cells / seconds, "unit": UNIT, "cores": min(8, host_threads()),
+                                "kind": kind, "iterations": it,
+                                "sample": f"1 projection of the {size}x{size} workload"}
+    if rank == 0 and not args.no_batched:
+        line["batched"] = batched_measure(args, torch)
+    return line
+
+
+def e2e_measure(args, scene, torch):
+    """The same step through the public API from pinned FP64 host buffers, copies included."""
+    from fluidsim_b200 import FluidGrid, FluidGridState
+
+    def pinned(a):
+        t = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
+        t.numpy()[...] = a
+        return t.numpy()
+
+    state = FluidGridState(pinned(scene.fraction), pinned(scene.u), pinned(scene.v),
+                           pinned(np.zeros_like(scene.fraction)),
+                           [pinned(scene.liquid_mass[0])], [pinned(scene.gas_mass[0])])
+    out = {k: pinned(np.zeros_like(a)) for k, a in (("u", scene.u), ("v", scene.v), ("p", scene.fraction))}
+    g = FluidGrid(scene.width, scene.height, scene.cell_size, "fp32")
+    g.configureMaterials([scene.liquid_density], [scene.gas_density])
+    g.setGravityY(scene.gravity)
+    stream = torch.cuda.ExternalStream(g.stream())
+    import ctypes as C
+    from fluidsim_b200 import _native as N
+
+    dp = C.POINTER(C.c_double)
+
+    def download_uvp():
+        N.check(N.lib().fc_download(g.handle, None, out["u"].ctypes.data_as(dp), out["v"].ctypes.data_as(dp),
+                                    out["p"].ctypes.data_as(dp), None, None))
+
+    times = []
+    for i in range(args.warmup + args.steps):
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        g.upload(state)
+        g.applyGravity(scene.dt)
+        g.project(scene.dt, 200, args.tolerance, relative_tolerance=args.tolerance)
+        download_uvp()
+        stop.record(stream)
+        stop.synchronize()
+        if i >= args.warmup:
+            times.append(start.elapsed_time(stop))
+    n, nu, nv = scene.cells, scene.u.size, scene.v.size
+    h2d = 8 * (n + nu + nv + n + 2 * n)
+    d2h = 8 * (nu + nv + n)
+    ms = statistics.mean(times)
+    return {"value": scene.cells / (ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+            "ms_per_step": ms}
+
+
+def batched_measure(args, torch, count=256):
+    """Uneven grids (sides log-uniform 64..1024, aspect <= 2:1, fill 0.3-0.9, 0-8 obstacles)
+    projected together, against the same grids projected one at a time."""
+    from fluidsim_b200 import FluidGrid, ProjectionBatch, scenes
+
+    batch_scenes = scenes.uneven_batch(count, seed=7)
+    grids, pristine = [], []
+    for s in batch_scenes:
+        p = FluidGrid(s.width, s.height, s.cell_size, "fp32")
+        scenes.upload_scene(p, s)
+        g = FluidGrid(s.width, s.height, s.cell_size, "fp32")
+        g.configureMaterials([s.liquid_density], [s.gas_density])
+        g.setObstacles(s.solid)
+        pristine.append(p)
+        grids.append(g)
+    cells = sum(s.cells for s in batch_scenes)
+    batch = ProjectionBatch(grids)
+    dts = [s.dt for s in batch_scenes]
+
+    def restore():
+        for g, p in zip(grids, pristine):
+            g.copyStateFrom(p)
+
+    stream = torch.cuda.ExternalStream(batch.stream())
+    times = []
+    for i in range(2 + 3):
+        restore()
+        torch.cuda.synchronize()
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        res = batch.project(dts, 300, args.tolerance, relative_tolerance=args.tolerance)
+        stop.record(stream)
+        stop.synchronize()
+        if i >= 2:
+            times.append(start.elapsed_time(stop))
+    batched_ms = statistics.mean(times)
+    ok = all(r.solve_status in ("converged", "no_work") for r in res)
+    # One grid at a time through the same engine (the plain path).
+    restore()
+    torch.cuda.synchronize()
+    plain_ms = 0.0
+    for g in grids:
+        gs = torch.cuda.ExternalStream(g.stream())
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(gs)
+        g.project(dts[grids.index(g)], 300, args.tolerance, relative_tolerance=args.tolerance)
+        stop.record(gs)
+        stop.synchronize()
+        plain_ms += start.elapsed_time(stop)
+    batch.destroy()
+    return {"value": cells / (batched_ms / 1e3), "unit": UNIT, "grids": count, "cells": cells,
+            "ms_per_batch": batched_ms, "plain_one_at_a_time_cells_per_s": cells / (plain_ms / 1e3),
+            "speedup_vs_plain": plain_ms / batched_ms, "all_converged": ok,
+            "max_iterations": max(r.iterations for r in res)}
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        line = run_reference(args, world, rank)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    line = run_cuda(args, world, rank, local_rank)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch
+
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,142 @@
+"""ctypes binding of libfluidcuda.so (the C ABI declared in include/fluidcuda.h).
+
+The library is built in place by fluidsim_b200/build.py. There is no fallback: if the library
+is missing or cannot be loaded, importing the product raises, so no caller ever runs a silent
+CPU substitute.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBRARY = os.path.join(HERE, "libfluidcuda.so")
+
+FC_OK = 0
+STATUS_NAMES = {
+    0: "ok", 1: "invalid argument", 2: "lifecycle", 3: "cuda", 4: "out of memory",
+    5: "non-finite", 6: "breakdown", 7: "unsupported", 8: "timeout",
+}
+
+PRECISION = {"fp32": 0, "fp64": 1, "mixed": 2}
+PRECONDITIONER = {"diagonal": 0, "multigrid": 1}
+SOLVE_STATUS = {0: "running", 1: "converged", 2: "iteration_limit", 3: "stalled", 4: "no_work", 5: "breakdown"}
+
+
+class FcResult(C.Structure):
+    """Mirror of fc_result (fluid::FluidProjectionResult plus solver measurements)."""
+    _fields_ = [
+        ("iterations", C.c_int),
+        ("max_divergence", C.c_double),
+        ("converged", C.c_int),
+        ("physical_steps", C.c_int),
+        ("transport_steps", C.c_int),
+        ("relaxed", C.c_int),
+        ("max_volume_error", C.c_double),
+        ("rms_volume_error", C.c_double),
+        ("viscosity_iterations", C.c_int),
+        ("precision_limited", C.c_int),
+        ("solve_status", C.c_int),
+        ("residual_max", C.c_double),
+        ("residual_l2", C.c_double),
+        ("rhs_l2", C.c_double),
+        ("divergence_excess", C.c_double),
+        ("divergence_l2", C.c_double),
+        ("restarts", C.c_int),
+        ("kernels", C.c_int),
+    ]
+
+
+class FcTimings(C.Structure):
+    _fields_ = [(name, C.c_double) for name in
+                ("transport_ms", "viscosity_ms", "forces_ms", "pressure_ms", "selection_ms", "regrid_ms")]
+
+
+_dp = C.POINTER(C.c_double)
+_dpp = C.POINTER(_dp)
+_vp = C.c_void_p
+_int = C.c_int
+_dbl = C.c_double
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "fc_abi_version": (_int, []),
+    "fc_last_error": (C.c_char_p, []),
+    "fc_status_string": (C.c_char_p, [_int]),
+    "fc_kernel_launches": (C.c_longlong, []),
+    "fc_create": (_int, [_int, _int, _dbl, _int, C.POINTER(_vp)]),
+    "fc_destroy": (_int, [_vp]),
+    "fc_get_geometry": (_int, [_vp, C.POINTER(_int), C.POINTER(_int), _dp]),
+    "fc_get_origin": (_int, [_vp, _dp, _dp]),
+    "fc_set_origin": (_int, [_vp, _dbl, _dbl]),
+    "fc_get_precision": (_int, [_vp, C.POINTER(_int)]),
+    "fc_configure_materials": (_int, [_vp, _int, _dp, _dp, _int, _dp, _dp]),
+    "fc_get_gravity": (_int, [_vp, _dp]),
+    "fc_set_gravity": (_int, [_vp, _dbl]),
+    "fc_set_preconditioner": (_int, [_vp, _int]),
+    "fc_set_obstacles": (_int, [_vp, C.POINTER(C.c_uint8)]),
+    "fc_upload": (_int, [_vp, _dp, _dp, _dp, _dp, _dpp, _dpp]),
+    "fc_download": (_int, [_vp, _dp, _dp, _dp, _dp, _dpp, _dpp]),
+    "fc_copy_state": (_int, [_vp, _vp]),
+    "fc_project": (_int, [_vp, _dbl, _int, _dbl, C.POINTER(FcResult)]),
+    "fc_project_relative": (_int, [_vp, _dbl, _int, _dbl, _dbl, C.POINTER(FcResult)]),
+    "fc_step": (_int, [_vp, _dbl, _int, _dbl, C.POINTER(FcResult), C.POINTER(FcTimings)]),
+    "fc_apply_gravity": (_int, [_vp, _dbl]),
+    "fc_max_divergence": (_int, [_vp, _dp]),
+    "fc_classify": (_int, [_vp, C.POINTER(C.c_uint8)]),
+    "fc_apply_preconditioner": (_int, [_vp, _dp, _dbl, _dp]),
+    "fc_time_kernel": (_int, [_vp, _int, _int, _dp]),
+    "fc_velocity_pointers": (_int, [_vp, C.POINTER(_vp), C.POINTER(_vp)]),
+    "fc_get_stream": (_int, [_vp, C.POINTER(_vp)]),
+    "fc_synchronize": (_int, [_vp]),
+    "fc_batch_create": (_int, [C.POINTER(_vp), _int, C.POINTER(_vp)]),
+    "fc_batch_destroy": (_int, [_vp]),
+    "fc_batch_project": (_int, [_vp, _dp, _int, _dbl, _dbl, C.POINTER(FcResult)]),
+    "fc_batch_get_stream": (_int, [_vp, C.POINTER(_vp)]),
+}
+
+_lib = None
+
+
+class FluidCudaError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+class FluidInvalidArgument(FluidCudaError, ValueError):
+    """The reference throws std::invalid_argument for these."""
+
+
+class FluidLifecycleError(FluidCudaError):
+    """The reference throws std::logic_error for these."""
+
+
+def lib():
+    """Loads libfluidcuda.so, failing loudly when it is absent."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIBRARY):
+            raise ImportError(f"libfluidcuda.so is not built ({LIBRARY}); run fluidsim_b200/build.py")
+        L = C.CDLL(LIBRARY)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(status: int):
+    if status == FC_OK:
+        return
+    message = lib().fc_last_error().decode(errors="replace")
+    if status == 1:
+        raise FluidInvalidArgument(status, message)
+    if status == 2:
+        raise FluidLifecycleError(status, message)
+    raise FluidCudaError(status, message)
+
+
+def kernel_launches() -> int:
+    return int(lib().fc_kernel_launches())

@@ -1,0 +1,255 @@
+// Device-side layout, descriptors and reduction helpers of the UniformCUDA backend.
+//
+// Layout in HBM. Every cell-centred array of a grid level (face weights, multigrid rhs and
+// solution, and on the fine level the PCG vectors r, z, d, q, p) is stored padded: cell (x, y)
+// lives at index (y + 1) * S + (x + 2), with S = round_up(w + 3, 8) elements per row and
+// h + 2 rows. Row 0, row h + 1 and the columns left of x = 0 and right of x = w - 1 stay zero,
+// so stencils need no bounds tests and a closed wall reads as a zero weight.
+//
+// A cell stores the weight of its right face ("right", the u face at x + 1) and of its lower
+// face ("down", the v face at y + 1). The left weight of a cell is right[i - 1] and its upper
+// weight down[i - S]. On the fine level these are the reference's inv_density_u/v
+// (FluidGridCPU.cpp:1154-1205); coarse levels hold the multigrid conductances
+// (PressureMultigrid.cpp:142-202).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace fc
+{
+
+constexpr int kMaxLevels = 16;
+constexpr int kPadX = 2;   // column of x = 0 inside a padded row
+constexpr int kVecTileX = 32;
+constexpr int kVecTileY = 32;
+constexpr int kVecThreads = 256;
+
+__host__ __device__ inline int padded_stride(int w) { return ((w + 3) + 7) / 8 * 8; }
+__host__ __device__ inline long long padded_index(int S, int x, int y) { return (long long)(y + 1) * S + x + kPadX; }
+
+// Solver status codes shared with the C ABI (fc_result.status).
+enum SolveStatus : int
+{
+    kRunning = 0,
+    kConverged = 1,        // stop rule met on the true residual
+    kIterationLimit = 2,   // max_iterations reached
+    kStalled = 3,          // r.z or d.Ad lost positivity / finiteness (reference loop exit)
+    kNoWork = 4,           // right-hand side already below tolerance
+    kBreakdown = 5,        // coarsest factorisation failed
+};
+
+// Per-grid PCG scalars, resident on the device for the whole solve.
+struct SolveState
+{
+    double rz;          // r . z of the current direction
+    double dq;          // d . A d
+    double beta;
+    double mean_b;      // mean of the raw right-hand side
+    double mean_r;      // mean of the current residual
+    double mean_z;
+    double mean_p;
+    double sum_r, max_r, sumsq_r;
+    double bmax, bsumsq;
+    double tol_max;     // max-norm stop rule (pressure units); +inf when unused
+    double tol_sumsq;   // L2 stop rule, squared; +inf when unused
+    double inv_cells;   // 1 / cell count
+    double div_max;     // post-projection max |div u|
+    double div_excess;  // max(0, |div u| - local float rounding allowance)
+    double div_sumsq;   // sum of div^2
+    double res_max, res_sumsq;
+    double dt;          // time step of the projection in flight
+    int iterations;
+    int restarts;       // true-residual checks that failed and restarted the directions
+    int max_iterations;
+    int done;
+    int status;
+    int verify;
+    int restart;
+    int mg_valid;       // multigrid hierarchy and coarsest inverse are usable
+    int use_mg;         // multigrid (1) or diagonal (0) preconditioner
+    int nonfinite;
+};
+
+// Linear interpolation from a fine axis position to the two nearest coarse centres
+// (PressureMultigrid.cpp:64-102). weight belongs to `second`.
+struct Interp
+{
+    int first;
+    int second;
+    double weight;
+};
+
+// Transpose of Interp: the fine cells that a coarse cell gathers from.
+struct Gather
+{
+    int count;
+    int index[4];
+    double weight[4];
+};
+
+// Unknowns of the coarsest direct solve: every cell with an open face except the first one,
+// which is pinned (the reference pins cell 0, PressureMultigrid.cpp:306-320; with no obstacle
+// the two are the same). Written by the rebuild, read by every V-cycle.
+struct CoarseInfo
+{
+    int n;       // unknowns
+    int pinned;  // pinned cell, -1 when no cell is open
+    int open;    // open cells (n + 1, or 0)
+    int map[64]; // cell -> unknown index, -1 for the pinned and the closed cells
+};
+
+struct LevelDesc
+{
+    int w, h, S;
+    void* right;
+    void* down;
+    void* rhs;           // levels >= 1 (level 0 reads the PCG residual minus its mean)
+    void* pre;           // pre-smoothed solution, read by the post-smoothing of the same level
+    void* sol;           // final solution of the level (level 0: the PCG vector z)
+    const double* cx;    // cell centres, in fine cells
+    const double* cy;
+    const Interp* px;    // fine level -> this level's coarse parent (valid for l < last)
+    const Interp* py;
+    const Gather* rx;    // coarse (l+1) cell -> fine cells of l
+    const Gather* ry;
+};
+
+struct GridDesc
+{
+    int W, H, S;
+    int levels;          // multigrid levels, the last one solved directly
+    int tail;            // first level handled by the one-block coarse tail
+    int ncoarse;         // unknowns of the coarsest solve (cells - 1)
+    double dx;
+    LevelDesc lev[kMaxLevels];
+    // fine-level vectors (padded layout)
+    void* r;
+    void* z;
+    void* d[2];
+    void* q;
+    double* p;
+    double* p_prev;
+    double* b;
+    // face velocities, unpadded: u is (W+1) x H, v is W x (H+1), row-major
+    void* u;
+    void* v;
+    // coarsest inverse, up to ncoarse x ncoarse, row-major FP64, and its unknown map
+    double* coarse_inverse;
+    CoarseInfo* coarse;
+    SolveState* state;
+    double4* partial;        // one slot per tile of the largest reduction
+    unsigned int* counter;   // arrival counter of the reduction in flight
+    int vec_tiles;           // tiles of the fine vector kernels
+    int post_tiles;          // tiles of the level-0 post-smoothing kernel (0 when tail == 0)
+    unsigned char* solid;    // optional obstacle mask, W x H, unpadded (null: none)
+    double* density;         // W x H, unpadded
+    double* const* masses;   // device array of `components` W x H mass fields
+    int components;
+};
+
+// One CTA of work: grid index, tile origin in cells, and the tile's index within its grid.
+struct Tile
+{
+    int grid;
+    int x0;
+    int y0;
+    int index;
+};
+
+template <typename T> __device__ __forceinline__ T load_as(const void* base, long long i)
+{
+    return static_cast<const T*>(base)[i];
+}
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+    for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ double warp_max(double v)
+{
+    for (int o = 16; o > 0; o >>= 1)
+        v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Block reduction of up to four doubles; lane (component) c is summed, or maxed when
+// (max_mask >> c) & 1. Result valid in thread 0. Fixed order: deterministic.
+template <int NT> __device__ double4 block_reduce4(double4 v, int max_mask)
+{
+    __shared__ double4 slots[NT / 32];
+    double a[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int c = 0; c < 4; ++c)
+        a[c] = ((max_mask >> c) & 1) ? warp_max(a[c]) : warp_sum(a[c]);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __syncthreads();
+    if (lane == 0)
+        slots[warp] = make_double4(a[0], a[1], a[2], a[3]);
+    __syncthreads();
+    double4 out = make_double4(0, 0, 0, 0);
+    if (threadIdx.x == 0)
+    {
+        out = slots[0];
+        for (int w = 1; w < NT / 32; ++w)
+        {
+            const double4 s = slots[w];
+            out.x = (max_mask & 1) ? fmax(out.x, s.x) : out.x + s.x;
+            out.y = (max_mask & 2) ? fmax(out.y, s.y) : out.y + s.y;
+            out.z = (max_mask & 4) ? fmax(out.z, s.z) : out.z + s.z;
+            out.w = (max_mask & 8) ? fmax(out.w, s.w) : out.w + s.w;
+        }
+    }
+    return out;
+}
+
+// Publishes this tile's partial and reports whether this block is the last of its grid to
+// arrive; the last block then reads every partial in tile order (deterministic) and resets
+// the counter. Must be called by all threads of the block.
+template <int NT>
+__device__ bool arrive_last(const GridDesc& g, int tile_index, int tiles, double4 mine, double4* total, int max_mask)
+{
+    __shared__ int is_last;
+    if (threadIdx.x == 0)
+    {
+        g.partial[tile_index] = mine;
+        __threadfence();
+        const unsigned int ticket = atomicAdd(g.counter, 1u);
+        is_last = ticket == unsigned(tiles - 1);
+    }
+    __syncthreads();
+    if (!is_last)
+        return false;
+    __threadfence();
+    // The last block folds the partials in fixed order.
+    double4 acc = make_double4(0, 0, 0, 0);
+    // Each thread folds a contiguous run, then runs are combined in order.
+    const int per = (tiles + NT - 1) / NT;
+    const int first = threadIdx.x * per;
+    const int last = min(tiles, first + per);
+    for (int t = first; t < last; ++t)
+    {
+        const volatile double* slot = reinterpret_cast<const volatile double*>(&g.partial[t]);
+        const double4 s = make_double4(slot[0], slot[1], slot[2], slot[3]);
+        acc.x = (max_mask & 1) ? fmax(acc.x, s.x) : acc.x + s.x;
+        acc.y = (max_mask & 2) ? fmax(acc.y, s.y) : acc.y + s.y;
+        acc.z = (max_mask & 4) ? fmax(acc.z, s.z) : acc.z + s.z;
+        acc.w = (max_mask & 8) ? fmax(acc.w, s.w) : acc.w + s.w;
+    }
+    const double4 out = block_reduce4<NT>(acc, max_mask);
+    if (threadIdx.x == 0)
+    {
+        *total = out;
+        *g.counter = 0u;
+        __threadfence();
+    }
+    __syncthreads();
+    return true;
+}
+
+__device__ __forceinline__ bool finite_d(double v) { return isfinite(v); }
+
+} // namespace fc

@@ -1,0 +1,1691 @@
+// UniformCUDA engine: device memory, multigrid hierarchy, launch plans, CUDA graphs, C ABI.
+//
+// One grid = one arena of device memory holding every field of the projection. A Plan is the
+// launch schedule of a set of grids (one grid, or a batch of uneven grids): tile tables per
+// kernel and level, a device array of grid descriptors, and one CUDA graph that runs a whole
+// projection: set-up, a conditional WHILE node around the PCG iterations, the velocity update
+// and the divergence check. The loop condition is computed on the device, so a projection is
+// one graph launch plus one small read-back of the per-grid results.
+#include "fc_device.cuh"
+#include "fc_multigrid.cuh"
+#include "fc_pcg.cuh"
+
+#include "../../include/fluidcuda.h"
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+namespace fc
+{
+
+// ------------------------------------------------------------------------------------------
+// Errors and launches
+// ------------------------------------------------------------------------------------------
+
+thread_local std::string last_error;
+std::atomic<long long> launch_count{0};
+
+struct Failure
+{
+    int status;
+};
+
+[[noreturn]] void fail(int status, const char* format, ...)
+{
+    char buffer[512];
+    va_list args;
+    va_start(args, format);
+    vsnprintf(buffer, sizeof(buffer), format, args);
+    va_end(args);
+    last_error = buffer;
+    throw Failure{status};
+}
+
+void check(cudaError_t err, const char* what)
+{
+    if (err != cudaSuccess)
+    {
+        cudaGetLastError();
+        fail(err == cudaErrorMemoryAllocation ? FC_ERR_OUT_OF_MEMORY : FC_ERR_CUDA, "%s: %s", what,
+            cudaGetErrorString(err));
+    }
+}
+
+template <typename F> int guarded(F&& body)
+{
+    try
+    {
+        body();
+        return FC_OK;
+    }
+    catch (const Failure& f)
+    {
+        return f.status;
+    }
+    catch (const std::bad_alloc&)
+    {
+        last_error = "host allocation failed";
+        return FC_ERR_OUT_OF_MEMORY;
+    }
+    catch (...)
+    {
+        last_error = "unexpected exception";
+        return FC_ERR_CUDA;
+    }
+}
+
+#define FC_LAUNCH(kernel, blocks, threads, smem, stream, ...)                                      \
+    do                                                                                             \
+    {                                                                                              \
+        if ((blocks) > 0)                                                                          \
+        {                                                                                          \
+            kernel<<<(blocks), (threads), (smem), (stream)>>>(__VA_ARGS__);                        \
+            check(cudaGetLastError(), #kernel);                                                    \
+            ::fc::launch_count.fetch_add(1, std::memory_order_relaxed);                            \
+        }                                                                                          \
+    } while (0)
+
+int ceil_div(int a, int b) { return (a + b - 1) / b; }
+
+// ------------------------------------------------------------------------------------------
+// Multigrid hierarchy (host side)
+// ------------------------------------------------------------------------------------------
+
+struct HostLevel
+{
+    int w = 0, h = 0, S = 0;
+    std::vector<double> cx, cy;
+    std::vector<Interp> px, py; // this level -> next
+    std::vector<Gather> rx, ry; // next level's cells -> this level
+};
+
+// Halving until at most 64 cells; cell centres keep a shorter last cell on odd sizes.
+// PressureMultigrid.cpp:24-62.
+std::vector<HostLevel> build_levels(int W, int H)
+{
+    std::vector<HostLevel> levels;
+    int w = W, h = H, spacing = 1;
+    for (;;)
+    {
+        HostLevel l;
+        l.w = w;
+        l.h = h;
+        l.S = padded_stride(w);
+        l.cx.resize(w);
+        l.cy.resize(h);
+        for (int x = 0; x < w; ++x)
+            l.cx[x] = 0.5 * (double(x) * spacing + std::min((x + 1) * spacing, W));
+        for (int y = 0; y < h; ++y)
+            l.cy[y] = 0.5 * (double(y) * spacing + std::min((y + 1) * spacing, H));
+        levels.push_back(std::move(l));
+        if (w * h <= 64)
+            break;
+        w = (w + 1) / 2;
+        h = (h + 1) / 2;
+        spacing *= 2;
+    }
+    if (int(levels.size()) > kMaxLevels)
+        fail(FC_ERR_INVALID_ARGUMENT, "grid %dx%d needs more than %d multigrid levels", W, H, kMaxLevels);
+    // Linear interpolation between neighbouring coarse centres, clamped at the ends; the
+    // restriction is its transpose. PressureMultigrid.cpp:64-102.
+    auto axis = [](const std::vector<double>& fine, const std::vector<double>& coarse, std::vector<Interp>& p,
+                    std::vector<Gather>& r)
+    {
+        const int nf = int(fine.size()), nc = int(coarse.size());
+        p.assign(nf, Interp{});
+        r.assign(nc, Gather{});
+        for (int f = 0; f < nf; ++f)
+        {
+            const int parent = f / 2;
+            const int first = std::max(0, parent - int(fine[f] < coarse[parent]));
+            const int second = std::min(first + 1, nc - 1);
+            const double weight =
+                first == second ? 0.0 : std::clamp((fine[f] - coarse[first]) / (coarse[second] - coarse[first]), 0.0, 1.0);
+            p[f] = {first, second, weight};
+            const int target[2] = {first, second};
+            const double value[2] = {1.0 - weight, weight};
+            for (int k = 0; k < 2; ++k)
+            {
+                if (value[k] == 0.0)
+                    continue;
+                Gather& g = r[target[k]];
+                if (g.count >= 4)
+                    fail(FC_ERR_CUDA, "restriction stencil overflow");
+                g.index[g.count] = f;
+                g.weight[g.count] = value[k];
+                ++g.count;
+            }
+        }
+    };
+    for (size_t i = 0; i + 1 < levels.size(); ++i)
+    {
+        axis(levels[i].cx, levels[i + 1].cx, levels[i].px, levels[i].rx);
+        axis(levels[i].cy, levels[i + 1].cy, levels[i].py, levels[i].ry);
+    }
+    return levels;
+}
+
+// ------------------------------------------------------------------------------------------
+// Grid
+// ------------------------------------------------------------------------------------------
+
+struct Plan;
+
+struct Grid
+{
+    int W = 0, H = 0, S = 0;
+    double dx = 1.0;
+    double origin_x = 0.0, origin_y = 0.0;
+    int precision = FC_PRECISION_FP32;
+    size_t elem = 4;
+    int device = 0;
+    int preconditioner = FC_PRECONDITIONER_MULTIGRID;
+    double gravity_y = 100.0; // FluidGridCPU.h:37
+    std::vector<double> liquid_density, gas_density, liquid_viscosity, gas_viscosity;
+    bool configured = false;
+    bool uploaded = false;
+    bool coefficients_dirty = true;
+    bool has_solid = false;
+
+    std::vector<HostLevel> levels;
+    int tail = 0;
+    size_t tail_smem = 0;
+
+    cudaStream_t stream = nullptr;
+    char* arena = nullptr;
+    size_t arena_bytes = 0;
+    GridDesc desc{};
+    double* fraction = nullptr;
+    double* masses = nullptr;     // components x W*H
+    double** mass_ptrs = nullptr; // device array of component pointers
+    double* staging = nullptr;    // FP64 staging for upload/download conversions
+    size_t staging_count = 0;
+    unsigned char* solid = nullptr;
+    unsigned char* mask = nullptr;
+    size_t cells = 0, faces_u = 0, faces_v = 0;
+    int mass_capacity = 0;
+
+    std::unique_ptr<Plan> plan; // single-grid plan, built lazily
+
+    int components() const { return int(liquid_density.size() + gas_density.size()); }
+    ~Grid();
+};
+
+template <typename T> struct Tiling;
+template <> struct Tiling<float>
+{
+    static constexpr int K = 8;
+};
+template <> struct Tiling<double>
+{
+    static constexpr int K = 6;
+};
+
+struct TileSizes
+{
+    int pre_x, pre_y, post_x, post_y;
+};
+
+TileSizes tile_sizes(int precision)
+{
+    if (precision == FC_PRECISION_FP64)
+        return {TileShape<double, 6, true>::OX, TileShape<double, 6, true>::OY, TileShape<double, 6, false>::OX,
+            TileShape<double, 6, false>::OY};
+    return {TileShape<float, 8, true>::OX, TileShape<float, 8, true>::OY, TileShape<float, 8, false>::OX,
+        TileShape<float, 8, false>::OY};
+}
+
+// The coarse tail starts at the first level whose cells and shared-memory footprint fit one CTA.
+void choose_tail(Grid& g)
+{
+    const int limit_cells = g.elem == 4 ? 4096 : 1024;
+    const size_t limit_bytes = 200 * 1024;
+    std::vector<int> w, h;
+    for (auto& l : g.levels)
+        w.push_back(l.w), h.push_back(l.h);
+    const int n = int(g.levels.size());
+    for (int l = 0; l < n; ++l)
+    {
+        const size_t bytes = tail_bytes(w.data(), h.data(), l, n, g.elem);
+        if (w[l] * h[l] <= limit_cells && bytes <= limit_bytes)
+        {
+            g.tail = l;
+            g.tail_smem = bytes;
+            return;
+        }
+    }
+    g.tail = n - 1;
+    g.tail_smem = tail_bytes(w.data(), h.data(), n - 1, n, g.elem);
+}
+
+// Lays out every device field of a grid in one allocation and fills the descriptor.
+void allocate_grid(Grid& g)
+{
+    const int W = g.W, H = g.H;
+    g.levels = build_levels(W, H);
+    choose_tail(g);
+    g.S = g.levels[0].S;
+    g.cells = size_t(W) * H;
+    g.faces_u = size_t(W + 1) * H;
+    g.faces_v = size_t(W) * (H + 1);
+    g.staging_count = std::max(g.faces_u, g.faces_v);
+
+    struct Slot
+    {
+        void** where;
+        size_t bytes;
+    };
+    std::vector<Slot> slots;
+    const size_t elem = g.elem;
+    GridDesc& d = g.desc;
+    d = GridDesc{};
+    d.W = W;
+    d.H = H;
+    d.S = g.S;
+    d.dx = g.dx;
+    d.levels = int(g.levels.size());
+    d.tail = g.tail;
+    const HostLevel& last = g.levels.back();
+    d.ncoarse = last.w * last.h - 1;
+    d.vec_tiles = ceil_div(W, kVecTileX) * ceil_div(H, kVecTileY);
+    const TileSizes ts = tile_sizes(g.precision);
+    d.post_tiles = g.tail > 0 ? ceil_div(W, ts.post_x) * ceil_div(H, ts.post_y) : 0;
+
+    const size_t padded0 = size_t(g.S) * (H + 2);
+    auto add = [&](void** where, size_t bytes) { slots.push_back({where, bytes}); };
+    add(&d.r, padded0 * elem);
+    add(&d.z, padded0 * elem);
+    add(&d.d[0], padded0 * elem);
+    add(&d.d[1], padded0 * elem);
+    add(&d.q, padded0 * elem);
+    add((void**)&d.p, padded0 * sizeof(double));
+    add((void**)&d.p_prev, padded0 * sizeof(double));
+    add((void**)&d.b, padded0 * sizeof(double));
+    add(&d.u, g.faces_u * elem);
+    add(&d.v, g.faces_v * elem);
+    add((void**)&d.coarse_inverse, size_t(std::max(1, d.ncoarse * d.ncoarse)) * sizeof(double));
+    add((void**)&d.coarse, sizeof(CoarseInfo));
+    add((void**)&d.state, sizeof(SolveState));
+    add((void**)&d.partial, size_t(std::max(std::max(d.vec_tiles, d.post_tiles), 1)) * sizeof(double4));
+    add((void**)&d.counter, sizeof(unsigned int) * 4);
+    add((void**)&d.density, g.cells * sizeof(double));
+    add((void**)&g.fraction, g.cells * sizeof(double));
+    add((void**)&g.staging, g.staging_count * sizeof(double));
+    add((void**)&g.solid, g.cells);
+    add((void**)&g.mask, g.cells);
+    add((void**)&d.lev[0].pre, padded0 * elem);
+    std::vector<void*> cx(g.levels.size()), cy(g.levels.size()), px(g.levels.size()), py(g.levels.size()),
+        rx(g.levels.size()), ry(g.levels.size());
+    for (size_t l = 0; l < g.levels.size(); ++l)
+    {
+        const HostLevel& L = g.levels[l];
+        LevelDesc& ld = d.lev[l];
+        ld.w = L.w;
+        ld.h = L.h;
+        ld.S = L.S;
+        const size_t padded = size_t(L.S) * (L.h + 2);
+        add(&ld.right, padded * elem);
+        add(&ld.down, padded * elem);
+        if (l > 0)
+        {
+            add(&ld.rhs, padded * elem);
+            add(&ld.pre, padded * elem);
+            add(&ld.sol, padded * elem);
+        }
+        add(&cx[l], L.cx.size() * sizeof(double));
+        add(&cy[l], L.cy.size() * sizeof(double));
+        if (l + 1 < g.levels.size())
+        {
+            add(&px[l], L.px.size() * sizeof(Interp));
+            add(&py[l], L.py.size() * sizeof(Interp));
+            add(&rx[l], L.rx.size() * sizeof(Gather));
+            add(&ry[l], L.ry.size() * sizeof(Gather));
+        }
+    }
+    size_t total = 0;
+    std::vector<size_t> offsets;
+    for (auto& s : slots)
+    {
+        offsets.push_back(total);
+        total += (s.bytes + 255) / 256 * 256;
+    }
+    check(cudaMalloc(&g.arena, total), "grid allocation");
+    g.arena_bytes = total;
+    check(cudaMemsetAsync(g.arena, 0, total, g.stream), "grid clear");
+    for (size_t i = 0; i < slots.size(); ++i)
+        *slots[i].where = g.arena + offsets[i];
+    d.lev[0].sol = d.z;
+    for (size_t l = 0; l < g.levels.size(); ++l)
+    {
+        const HostLevel& L = g.levels[l];
+        LevelDesc& ld = d.lev[l];
+        check(cudaMemcpyAsync(cx[l], L.cx.data(), L.cx.size() * sizeof(double), cudaMemcpyHostToDevice, g.stream), "centres");
+        check(cudaMemcpyAsync(cy[l], L.cy.data(), L.cy.size() * sizeof(double), cudaMemcpyHostToDevice, g.stream), "centres");
+        ld.cx = static_cast<const double*>(cx[l]);
+        ld.cy = static_cast<const double*>(cy[l]);
+        if (l + 1 < g.levels.size())
+        {
+            check(cudaMemcpyAsync(px[l], L.px.data(), L.px.size() * sizeof(Interp), cudaMemcpyHostToDevice, g.stream), "tables");
+            check(cudaMemcpyAsync(py[l], L.py.data(), L.py.size() * sizeof(Interp), cudaMemcpyHostToDevice, g.stream), "tables");
+            check(cudaMemcpyAsync(rx[l], L.rx.data(), L.rx.size() * sizeof(Gather), cudaMemcpyHostToDevice, g.stream), "tables");
+            check(cudaMemcpyAsync(ry[l], L.ry.data(), L.ry.size() * sizeof(Gather), cudaMemcpyHostToDevice, g.stream), "tables");
+            ld.px = static_cast<const Interp*>(px[l]);
+            ld.py = static_cast<const Interp*>(py[l]);
+            ld.rx = static_cast<const Gather*>(rx[l]);
+            ld.ry = static_cast<const Gather*>(ry[l]);
+        }
+    }
+    d.solid = nullptr;
+    check(cudaStreamSynchronize(g.stream), "grid set-up");
+}
+
+// Component masses live in their own allocation (their count follows configureMaterials).
+void allocate_masses(Grid& g)
+{
+    const int k = g.components();
+    if (k == g.mass_capacity && g.masses)
+        return;
+    cudaFree(g.masses);
+    cudaFree(g.mass_ptrs);
+    g.masses = nullptr;
+    g.mass_ptrs = nullptr;
+    g.mass_capacity = k;
+    if (k > 0)
+    {
+        check(cudaMalloc(&g.masses, size_t(k) * g.cells * sizeof(double)), "mass allocation");
+        check(cudaMalloc(&g.mass_ptrs, size_t(k) * sizeof(double*)), "mass pointers");
+        std::vector<double*> ptrs(k);
+        for (int i = 0; i < k; ++i)
+            ptrs[i] = g.masses + size_t(i) * g.cells;
+        check(cudaMemcpy(g.mass_ptrs, ptrs.data(), k * sizeof(double*), cudaMemcpyHostToDevice), "mass pointers");
+        check(cudaMemset(g.masses, 0, size_t(k) * g.cells * sizeof(double)), "mass clear");
+    }
+    g.desc.masses = g.mass_ptrs;
+    g.desc.components = k;
+}
+
+// ------------------------------------------------------------------------------------------
+// Plan: tile tables + descriptors + graph for a set of grids
+// ------------------------------------------------------------------------------------------
+
+struct Range
+{
+    int offset = 0;
+    int count = 0;
+};
+
+struct ProjectParams
+{
+    double dt;
+    double tol_max;
+    double tol_sumsq; // negative: relative rule carrying -tol^2
+    int max_iterations;
+    int use_mg;
+};
+
+__global__ void k_init_states(const GridDesc* grids, int n, const ProjectParams* params, int* body_count)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0)
+        *body_count = 0;
+    if (i >= n)
+        return;
+    const GridDesc& g = grids[i];
+    SolveState& s = *g.state;
+    const ProjectParams p = params[i];
+    const int mg_valid = s.mg_valid;
+    s = SolveState{};
+    s.mg_valid = mg_valid;
+    s.use_mg = p.use_mg;
+    s.tol_max = p.tol_max;
+    s.tol_sumsq = p.tol_sumsq;
+    s.max_iterations = p.max_iterations;
+    s.restart = 1;
+    s.rz = 1.0;
+    s.dq = 1.0;
+    s.dt = p.dt;
+    s.inv_cells = 1.0 / (double(g.W) * double(g.H));
+    g.counter[0] = 0u;
+}
+
+// Open (non-solid) cells define the mean-free subspace of the solve.
+__global__ void __launch_bounds__(kVecThreads) k_count_open(const GridDesc* grids, const Tile* tiles)
+{
+    const Tile t = tiles[blockIdx.x];
+    const GridDesc& g = grids[t.grid];
+    if (!g.solid)
+        return;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    double open = 0.0;
+    for (int k = 0; k < 4; ++k)
+    {
+        const int x = t.x0 + tx, y = t.y0 + ty + 8 * k;
+        if (x >= g.W || y >= g.H)
+            continue;
+        open += g.solid[(long long)y * g.W + x] ? 0.0 : 1.0;
+    }
+    __shared__ double4 total;
+    if (arrive_last<kVecThreads>(g, t.index, g.vec_tiles, block_reduce4<kVecThreads>(make_double4(open, 0, 0, 0), 0), &total, 0))
+    {
+        if (threadIdx.x == 0)
+            g.state->inv_cells = total.x > 0.0 ? 1.0 / total.x : 0.0;
+    }
+}
+
+__global__ void k_loop_condition(const GridDesc* grids, int n, int* body_count, int cap, cudaGraphConditionalHandle handle)
+{
+    int running = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+        running |= grids[i].state->done == 0;
+    running = __syncthreads_or(running);
+    if (threadIdx.x == 0)
+    {
+        const int bodies = ++*body_count;
+        cudaGraphSetConditional(handle, (running && bodies < cap) ? 1u : 0u);
+    }
+}
+
+__global__ void k_gather_states(const GridDesc* grids, int n, SolveState* out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        out[i] = *grids[i].state;
+}
+
+// v += g dt on interior horizontal faces (FluidGridCPU.cpp:987-996): every cell below the top
+// row updates its upper face.
+template <typename T> __global__ void k_gravity(const GridDesc* grids, const Tile* tiles, double increment)
+{
+    const Tile t = tiles[blockIdx.x];
+    const GridDesc& g = grids[t.grid];
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    T* v = static_cast<T*>(g.v);
+    for (int k = 0; k < 4; ++k)
+    {
+        const int x = t.x0 + tx, y = t.y0 + ty + 8 * k;
+        if (x >= g.W || y >= g.H || y == 0)
+            continue;
+        const long long f = (long long)y * g.W + x;
+        v[f] = T(double(v[f]) + increment);
+    }
+}
+
+__global__ void k_classify(const GridDesc* grids, const Tile* tiles, const double* fraction, unsigned char* mask)
+{
+    const Tile t = tiles[blockIdx.x];
+    const GridDesc& g = grids[t.grid];
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (int k = 0; k < 4; ++k)
+    {
+        const int x = t.x0 + tx, y = t.y0 + ty + 8 * k;
+        if (x >= g.W || y >= g.H)
+            continue;
+        const long long i = (long long)y * g.W + x;
+        unsigned char m = 0;
+        if (g.solid && g.solid[i])
+            m = 4;
+        else
+        {
+            const double f = fraction[i];
+            if (f > 0.5)
+                m |= 1;
+            if (f > 0.0 && f < 1.0)
+                m |= 2;
+        }
+        mask[i] = m;
+    }
+}
+
+struct Plan
+{
+    std::vector<Grid*> grids;
+    int precision = FC_PRECISION_FP32;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    GridDesc* d_desc = nullptr;
+    Tile* d_tiles = nullptr;
+    ProjectParams* d_params = nullptr;
+    ProjectParams* h_params = nullptr; // pinned
+    SolveState* d_states = nullptr;
+    SolveState* h_states = nullptr;    // pinned
+    int* d_body_count = nullptr;
+    Range vec;
+    Range coarsen[kMaxLevels];
+    Range pre[kMaxLevels];
+    Range post[kMaxLevels];
+    int max_levels = 0;
+    int max_tail = 0;
+    size_t tail_smem = 0;
+    cudaGraphExec_t exec = nullptr;
+    cudaGraph_t graph = nullptr;
+    int graph_cap = -1;
+    int graph_use_mg = -1;
+    int h_bodies = 0;       // loop bodies the last projection ran
+    int setup_kernels = 0;  // kernels outside the loop in the captured graph
+    int body_kernels = 0;   // kernels of one loop body
+    int rebuild_kernels = 0;
+
+    ~Plan()
+    {
+        if (exec)
+            cudaGraphExecDestroy(exec);
+        if (graph)
+            cudaGraphDestroy(graph);
+        cudaFree(d_desc);
+        cudaFree(d_tiles);
+        cudaFree(d_params);
+        cudaFree(d_states);
+        cudaFree(d_body_count);
+        cudaFreeHost(h_params);
+        cudaFreeHost(h_states);
+        if (own_stream && stream)
+            cudaStreamDestroy(stream);
+    }
+
+    const Tile* at(const Range& r) const { return d_tiles + r.offset; }
+    int n() const { return int(grids.size()); }
+};
+
+Grid::~Grid()
+{
+    plan.reset();
+    cudaFree(masses);
+    cudaFree(mass_ptrs);
+    cudaFree(arena);
+    if (stream)
+        cudaStreamDestroy(stream);
+}
+
+void append_tiles(std::vector<Tile>& tiles, int grid, int w, int h, int tx, int ty)
+{
+    int index = 0;
+    for (int y = 0; y < h; y += ty)
+        for (int x = 0; x < w; x += tx)
+            tiles.push_back({grid, x, y, index++});
+}
+
+void upload_descriptors(Plan& plan)
+{
+    std::vector<GridDesc> descs(plan.n());
+    for (int i = 0; i < plan.n(); ++i)
+        descs[i] = plan.grids[i]->desc;
+    check(cudaMemcpyAsync(plan.d_desc, descs.data(), descs.size() * sizeof(GridDesc), cudaMemcpyHostToDevice, plan.stream),
+        "plan descriptors");
+    check(cudaStreamSynchronize(plan.stream), "plan descriptors");
+}
+
+std::unique_ptr<Plan> make_plan(const std::vector<Grid*>& grids, cudaStream_t stream)
+{
+    auto plan = std::make_unique<Plan>();
+    plan->grids = grids;
+    plan->precision = grids.front()->precision;
+    if (stream)
+        plan->stream = stream;
+    else
+    {
+        check(cudaStreamCreateWithFlags(&plan->stream, cudaStreamNonBlocking), "plan stream");
+        plan->own_stream = true;
+    }
+    const int n = plan->n();
+    const TileSizes ts = tile_sizes(plan->precision);
+    std::vector<Tile> tiles;
+    auto add = [&](Range& r, auto&& body)
+    {
+        r.offset = int(tiles.size());
+        body();
+        r.count = int(tiles.size()) - r.offset;
+    };
+    add(plan->vec, [&]
+    {
+        for (int i = 0; i < n; ++i)
+            append_tiles(tiles, i, grids[i]->W, grids[i]->H, kVecTileX, kVecTileY);
+    });
+    for (Grid* g : grids)
+    {
+        plan->max_levels = std::max(plan->max_levels, int(g->levels.size()));
+        plan->max_tail = std::max(plan->max_tail, g->tail);
+        plan->tail_smem = std::max(plan->tail_smem, g->tail_smem);
+    }
+    for (int l = 0; l + 1 < plan->max_levels; ++l)
+    {
+        add(plan->coarsen[l], [&]
+        {
+            for (int i = 0; i < n; ++i)
+            {
+                const auto& L = grids[i]->levels;
+                if (l + 1 < int(L.size()))
+                    append_tiles(tiles, i, L[l + 1].w, L[l + 1].h, kVecTileX, kVecTileY);
+            }
+        });
+    }
+    for (int l = 0; l < plan->max_tail; ++l)
+    {
+        add(plan->pre[l], [&]
+        {
+            for (int i = 0; i < n; ++i)
+                if (l < grids[i]->tail)
+                    append_tiles(tiles, i, grids[i]->levels[l].w, grids[i]->levels[l].h, ts.pre_x, ts.pre_y);
+        });
+        add(plan->post[l], [&]
+        {
+            for (int i = 0; i < n; ++i)
+                if (l < grids[i]->tail)
+                    append_tiles(tiles, i, grids[i]->levels[l].w, grids[i]->levels[l].h, ts.post_x, ts.post_y);
+        });
+    }
+    check(cudaMalloc(&plan->d_tiles, std::max<size_t>(1, tiles.size()) * sizeof(Tile)), "plan tiles");
+    check(cudaMemcpy(plan->d_tiles, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice), "plan tiles");
+    check(cudaMalloc(&plan->d_desc, n * sizeof(GridDesc)), "plan descriptors");
+    check(cudaMalloc(&plan->d_params, n * sizeof(ProjectParams)), "plan params");
+    check(cudaMalloc(&plan->d_states, n * sizeof(SolveState)), "plan states");
+    check(cudaMalloc(&plan->d_body_count, sizeof(int)), "plan counter");
+    check(cudaHostAlloc(&plan->h_params, n * sizeof(ProjectParams), cudaHostAllocDefault), "plan params");
+    check(cudaHostAlloc(&plan->h_states, n * sizeof(SolveState), cudaHostAllocDefault), "plan states");
+    upload_descriptors(*plan);
+    return plan;
+}
+
+// ------------------------------------------------------------------------------------------
+// Launch sequences
+// ------------------------------------------------------------------------------------------
+
+// Density, face weights, multigrid conductances and the coarsest inverse of every grid.
+template <typename T> void launch_rebuild(Plan& p)
+{
+    cudaStream_t s = p.stream;
+    FC_LAUNCH(k_density, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
+    FC_LAUNCH(k_coefficients<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
+    for (int l = 0; l + 1 < p.max_levels; ++l)
+        FC_LAUNCH(k_coarsen<T>, p.coarsen[l].count, kVecThreads, 0, s, p.d_desc, p.at(p.coarsen[l]), l);
+    FC_LAUNCH(k_coarse_inverse<T>, p.n(), 256, 0, s, p.d_desc);
+}
+
+// One application of the preconditioner to r: z, mean z, r.z and beta.
+template <typename T> void launch_precondition(Plan& p, bool use_mg)
+{
+    cudaStream_t s = p.stream;
+    if (!use_mg)
+    {
+        FC_LAUNCH(k_precondition_diagonal<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
+        return;
+    }
+    constexpr int K = Tiling<T>::K;
+    for (int l = 0; l < p.max_tail; ++l)
+        FC_LAUNCH((k_mg_pre<T, K>), p.pre[l].count, 256, 0, s, p.d_desc, p.at(p.pre[l]), l);
+    FC_LAUNCH(k_mg_tail<T>, p.n(), kTailThreads, p.tail_smem, s, p.d_desc);
+    for (int l = p.max_tail - 1; l >= 0; --l)
+        FC_LAUNCH((k_mg_post<T, K>), p.post[l].count, 256, 0, s, p.d_desc, p.at(p.post[l]), l);
+}
+
+template <typename T> void launch_iteration(Plan& p, bool use_mg, int parity)
+{
+    cudaStream_t s = p.stream;
+    FC_LAUNCH(k_direction_operator<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec), parity);
+    FC_LAUNCH(k_update<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec), parity);
+    FC_LAUNCH(k_true_residual<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec), 0);
+    launch_precondition<T>(p, use_mg);
+}
+
+template <typename T> void set_kernel_attributes(Plan& p)
+{
+    if (p.tail_smem > 48 * 1024)
+        check(cudaFuncSetAttribute(k_mg_tail<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(p.tail_smem)),
+            "tail shared memory");
+}
+
+// Captures the projection: set-up, WHILE { 2 iterations, condition }, velocity, divergence.
+template <typename T> void capture_projection(Plan& p, bool use_mg, int cap)
+{
+    if (p.exec)
+    {
+        cudaGraphExecDestroy(p.exec);
+        p.exec = nullptr;
+    }
+    if (p.graph)
+    {
+        cudaGraphDestroy(p.graph);
+        p.graph = nullptr;
+    }
+    set_kernel_attributes<T>(p);
+    cudaStream_t s = p.stream;
+    cudaGraph_t graph;
+    check(cudaGraphCreate(&graph, 0), "graph create");
+    p.graph = graph;
+
+    // Set-up, captured into the outer graph.
+    const long long before_setup = launch_count.load();
+    check(cudaStreamBeginCaptureToGraph(s, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal), "capture");
+    FC_LAUNCH(k_init_states, ceil_div(p.n(), 128), 128, 0, s, p.d_desc, p.n(), p.d_params, p.d_body_count);
+    FC_LAUNCH(k_count_open, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
+    FC_LAUNCH(k_rhs<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
+    FC_LAUNCH(k_rhs_stats<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
+    FC_LAUNCH(k_warm_start, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
+    FC_LAUNCH(k_remove_pressure_mean, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
+    FC_LAUNCH(k_true_residual<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec), 1);
+    launch_precondition<T>(p, use_mg);
+
+    // The conditional node depends on everything captured so far.
+    cudaStreamCaptureStatus status;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    check(cudaStreamGetCaptureInfo(s, &status, nullptr, nullptr, &deps, &ndeps), "capture info");
+    std::vector<cudaGraphNode_t> dependencies(deps, deps + ndeps);
+    cudaGraphConditionalHandle handle;
+    check(cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault), "conditional handle");
+    cudaGraphNodeParams params = {};
+    params.type = cudaGraphNodeTypeConditional;
+    params.conditional.handle = handle;
+    params.conditional.type = cudaGraphCondTypeWhile;
+    params.conditional.size = 1;
+    cudaGraphNode_t loop;
+    check(cudaGraphAddNode(&loop, graph, dependencies.data(), dependencies.size(), &params), "while node");
+    cudaGraph_t body = params.conditional.phGraph_out[0];
+    check(cudaStreamUpdateCaptureDependencies(s, &loop, 1, cudaStreamSetCaptureDependencies), "capture deps");
+
+    // Finishing kernels after the loop, in the outer graph.
+    FC_LAUNCH(k_pressure_sum, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
+    FC_LAUNCH(k_velocity_update<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
+    FC_LAUNCH(k_remove_pressure_mean, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
+    FC_LAUNCH(k_divergence<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
+    FC_LAUNCH(k_gather_states, ceil_div(p.n(), 128), 128, 0, s, p.d_desc, p.n(), p.d_states);
+    cudaGraph_t captured;
+    check(cudaStreamEndCapture(s, &captured), "end capture");
+    p.setup_kernels = int(launch_count.load() - before_setup);
+    const long long before_body = launch_count.load();
+
+    // Loop body: two iterations (the direction buffers alternate) and the condition.
+    cudaStream_t side;
+    check(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking), "body stream");
+    check(cudaStreamBeginCaptureToGraph(side, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal), "body capture");
+    {
+        Plan& q = p;
+        cudaStream_t saved = q.stream;
+        q.stream = side;
+        launch_iteration<T>(q, use_mg, 0);
+        launch_iteration<T>(q, use_mg, 1);
+        FC_LAUNCH(k_loop_condition, 1, 256, 0, side, q.d_desc, q.n(), q.d_body_count, cap, handle);
+        q.stream = saved;
+    }
+    cudaGraph_t body_captured;
+    check(cudaStreamEndCapture(side, &body_captured), "body end capture");
+    cudaStreamDestroy(side);
+    p.body_kernels = int(launch_count.load() - before_body);
+    // Captured launches are not executions: take them back out of the process counter, which
+    // then advances by the executed kernels after each projection.
+    launch_count.fetch_sub(p.setup_kernels + p.body_kernels);
+
+    check(cudaGraphInstantiate(&p.exec, graph, 0), "graph instantiate");
+    p.graph_cap = cap;
+    p.graph_use_mg = use_mg ? 1 : 0;
+}
+
+template <typename T> void run_projection(Plan& p, bool use_mg, int max_iterations)
+{
+    const int cap = (std::max(max_iterations, 0) + 1) / 2 + 8;
+    if (!p.exec || p.graph_cap != cap || p.graph_use_mg != (use_mg ? 1 : 0))
+        capture_projection<T>(p, use_mg, cap);
+    check(cudaMemcpyAsync(p.d_params, p.h_params, p.n() * sizeof(ProjectParams), cudaMemcpyHostToDevice, p.stream),
+        "params");
+    check(cudaGraphLaunch(p.exec, p.stream), "graph launch");
+    check(cudaMemcpyAsync(p.h_states, p.d_states, p.n() * sizeof(SolveState), cudaMemcpyDeviceToHost, p.stream),
+        "results");
+    check(cudaMemcpyAsync(&p.h_bodies, p.d_body_count, sizeof(int), cudaMemcpyDeviceToHost, p.stream), "results");
+    check(cudaStreamSynchronize(p.stream), "projection");
+}
+
+void fill_result(const Grid& g, const SolveState& s, double divergence_tolerance, fc_result* out)
+{
+    fc_result r{};
+    r.physical_steps = 1;
+    r.solve_status = s.status;
+    if (s.status == kBreakdown)
+    {
+        // The reference returns a default result on a coarse breakdown (FluidGridCPU.cpp:1095-1096).
+        r.iterations = 0;
+        r.max_divergence = INFINITY;
+        r.converged = 0;
+    }
+    else
+    {
+        r.iterations = s.iterations;
+        r.max_divergence = s.div_max;
+        r.converged = s.div_max <= divergence_tolerance;
+        r.precision_limited =
+            !r.converged && (s.status == kConverged || s.status == kNoWork) && s.div_excess <= divergence_tolerance;
+    }
+    r.residual_max = s.res_max;
+    r.residual_l2 = std::sqrt(s.res_sumsq);
+    r.rhs_l2 = std::sqrt(s.bsumsq);
+    r.divergence_excess = s.div_excess;
+    r.divergence_l2 = std::sqrt(s.div_sumsq);
+    r.restarts = s.restarts;
+    if (s.status == kNoWork)
+    {
+        r.residual_max = s.bmax;
+        r.residual_l2 = std::sqrt(s.bsumsq);
+    }
+    *out = r;
+}
+
+// ------------------------------------------------------------------------------------------
+// Grid operations
+// ------------------------------------------------------------------------------------------
+
+Plan& single_plan(Grid& g)
+{
+    if (!g.plan)
+        g.plan = make_plan({&g}, g.stream);
+    return *g.plan;
+}
+
+template <typename F> void dispatch(int precision, F&& body)
+{
+    if (precision == FC_PRECISION_FP64)
+        body(double{});
+    else
+        body(float{});
+}
+
+void refresh_descriptor(Grid& g)
+{
+    g.desc.solid = g.has_solid ? g.solid : nullptr;
+    g.desc.masses = g.mass_ptrs;
+    g.desc.components = g.components();
+    if (g.plan)
+        upload_descriptors(*g.plan);
+}
+
+void rebuild_if_dirty(Plan& p)
+{
+    bool dirty = false;
+    for (Grid* g : p.grids)
+        dirty |= g->coefficients_dirty;
+    if (!dirty)
+        return;
+    const long long before = launch_count.load();
+    dispatch(p.precision, [&](auto zero)
+    {
+        using T = decltype(zero);
+        launch_rebuild<T>(p);
+    });
+    p.rebuild_kernels = int(launch_count.load() - before);
+    for (Grid* g : p.grids)
+        g->coefficients_dirty = false;
+}
+
+void require_uploaded(const Grid& g)
+{
+    if (!g.uploaded)
+        fail(FC_ERR_LIFECYCLE, "upload the grid state before stepping");
+}
+
+void project_plan(Plan& p, const double* dts, int max_iterations, double divergence_tolerance, double relative_tolerance,
+    fc_result* results)
+{
+    p.rebuild_kernels = 0;
+    for (Grid* g : p.grids)
+        require_uploaded(*g);
+    const bool use_mg = p.grids.front()->preconditioner == FC_PRECONDITIONER_MULTIGRID;
+    for (Grid* g : p.grids)
+        if ((g->preconditioner == FC_PRECONDITIONER_MULTIGRID) != use_mg)
+            fail(FC_ERR_INVALID_ARGUMENT, "a batch needs one preconditioner for all grids");
+    rebuild_if_dirty(p);
+    for (int i = 0; i < p.n(); ++i)
+    {
+        const Grid& g = *p.grids[i];
+        ProjectParams& q = p.h_params[i];
+        q.dt = dts[i];
+        const double scale = g.dx * g.dx / dts[i];
+        if (relative_tolerance > 0.0)
+        {
+            q.tol_max = INFINITY;
+            q.tol_sumsq = -(relative_tolerance * relative_tolerance);
+        }
+        else
+        {
+            q.tol_max = divergence_tolerance * scale;
+            q.tol_sumsq = INFINITY;
+        }
+        q.max_iterations = max_iterations;
+        q.use_mg = use_mg ? 1 : 0;
+    }
+    dispatch(p.precision, [&](auto zero)
+    {
+        using T = decltype(zero);
+        run_projection<T>(p, use_mg, max_iterations);
+    });
+    const int executed = p.rebuild_kernels + p.setup_kernels + p.h_bodies * p.body_kernels;
+    launch_count.fetch_add(p.setup_kernels + p.h_bodies * p.body_kernels);
+    for (int i = 0; i < p.n(); ++i)
+    {
+        const SolveState& s = p.h_states[i];
+        if (!s.done)
+            fail(FC_ERR_TIMEOUT, "pressure loop stopped at its iteration cap before grid %d finished", i);
+        fill_result(*p.grids[i], s, divergence_tolerance, &results[i]);
+        results[i].kernels = executed;
+    }
+}
+
+int project_one(Grid& g, double dt, int max_iterations, double divergence_tolerance, double relative_tolerance,
+    fc_result* out)
+{
+    return guarded([&]
+    {
+        if (!out)
+            fail(FC_ERR_INVALID_ARGUMENT, "null result");
+        // FluidGridCPU::project returns a default result for these (FluidGridCPU.cpp:1032-1035).
+        if (!(dt > 0.0) || max_iterations < 0)
+        {
+            *out = fc_result{};
+            out->max_divergence = INFINITY;
+            out->physical_steps = 1;
+            return;
+        }
+        project_plan(single_plan(g), &dt, max_iterations, divergence_tolerance, relative_tolerance, out);
+    });
+}
+
+template <typename T> void upload_velocity(Grid& g, const double* host, void* device, size_t count)
+{
+    if (!host)
+    {
+        check(cudaMemsetAsync(device, 0, count * sizeof(T), g.stream), "upload clear");
+        return;
+    }
+    check(cudaMemcpyAsync(g.staging, host, count * sizeof(double), cudaMemcpyHostToDevice, g.stream), "upload");
+    FC_LAUNCH(k_from_f64<T>, std::min<int>(ceil_div(int(std::min<size_t>(count, 1 << 30)), 256), 4096), 256, 0, g.stream,
+        g.staging, static_cast<T*>(device), (long long)count);
+}
+
+template <typename T> void download_velocity(Grid& g, double* host, const void* device, size_t count)
+{
+    if (!host)
+        return;
+    FC_LAUNCH(k_to_f64<T>, std::min<int>(ceil_div(int(std::min<size_t>(count, 1 << 30)), 256), 4096), 256, 0, g.stream,
+        static_cast<const T*>(device), g.staging, (long long)count);
+    check(cudaMemcpyAsync(host, g.staging, count * sizeof(double), cudaMemcpyDeviceToHost, g.stream), "download");
+    check(cudaStreamSynchronize(g.stream), "download");
+}
+
+int blocks_for(size_t n) { return int(std::min<size_t>((n + 255) / 256, 4096)); }
+
+void upload(Grid& g, const double* fraction, const double* u, const double* v, const double* pressure,
+    const double* const* liquid_mass, const double* const* gas_mass)
+{
+    if (!g.configured)
+        fail(FC_ERR_LIFECYCLE, "configure materials before uploading");
+    allocate_masses(g);
+    refresh_descriptor(g);
+    const size_t n = g.cells;
+    if (fraction)
+        check(cudaMemcpyAsync(g.fraction, fraction, n * sizeof(double), cudaMemcpyHostToDevice, g.stream), "fraction");
+    else
+        check(cudaMemsetAsync(g.fraction, 0, n * sizeof(double), g.stream), "fraction");
+    const int nl = int(g.liquid_density.size()), ng = int(g.gas_density.size());
+    for (int k = 0; k < nl + ng; ++k)
+    {
+        const double* src = k < nl ? (liquid_mass ? liquid_mass[k] : nullptr) : (gas_mass ? gas_mass[k - nl] : nullptr);
+        double* dst = g.masses + size_t(k) * n;
+        if (src)
+            check(cudaMemcpyAsync(dst, src, n * sizeof(double), cudaMemcpyHostToDevice, g.stream), "masses");
+        else
+            check(cudaMemsetAsync(dst, 0, n * sizeof(double), g.stream), "masses");
+    }
+    dispatch(g.precision, [&](auto zero)
+    {
+        using T = decltype(zero);
+        upload_velocity<T>(g, u, g.desc.u, g.faces_u);
+        upload_velocity<T>(g, v, g.desc.v, g.faces_v);
+    });
+    const size_t padded = size_t(g.S) * (g.H + 2);
+    check(cudaMemsetAsync(g.desc.p, 0, padded * sizeof(double), g.stream), "pressure");
+    if (pressure)
+    {
+        check(cudaMemcpyAsync(g.staging, pressure, n * sizeof(double), cudaMemcpyHostToDevice, g.stream), "pressure");
+        FC_LAUNCH(k_pad_f64, blocks_for(n), 256, 0, g.stream, g.staging, g.desc.p, g.W, g.H, g.S);
+    }
+    // The warm-start history restarts from the uploaded pressure (FluidGridCPU.cpp:251).
+    check(cudaMemcpyAsync(g.desc.p_prev, g.desc.p, padded * sizeof(double), cudaMemcpyDeviceToDevice, g.stream), "history");
+    check(cudaStreamSynchronize(g.stream), "upload");
+    g.uploaded = true;
+    g.coefficients_dirty = true;
+}
+
+void download(Grid& g, double* fraction, double* u, double* v, double* pressure, double* const* liquid_mass,
+    double* const* gas_mass)
+{
+    require_uploaded(g);
+    const size_t n = g.cells;
+    if (fraction)
+        check(cudaMemcpyAsync(fraction, g.fraction, n * sizeof(double), cudaMemcpyDeviceToHost, g.stream), "fraction");
+    const int nl = int(g.liquid_density.size()), ng = int(g.gas_density.size());
+    for (int k = 0; k < nl + ng; ++k)
+    {
+        double* dst = k < nl ? (liquid_mass ? liquid_mass[k] : nullptr) : (gas_mass ? gas_mass[k - nl] : nullptr);
+        if (dst)
+            check(cudaMemcpyAsync(dst, g.masses + size_t(k) * n, n * sizeof(double), cudaMemcpyDeviceToHost, g.stream), "masses");
+    }
+    check(cudaStreamSynchronize(g.stream), "download");
+    dispatch(g.precision, [&](auto zero)
+    {
+        using T = decltype(zero);
+        download_velocity<T>(g, u, g.desc.u, g.faces_u);
+        download_velocity<T>(g, v, g.desc.v, g.faces_v);
+    });
+    if (pressure)
+    {
+        FC_LAUNCH(k_unpad_f64, blocks_for(n), 256, 0, g.stream, g.desc.p, g.staging, g.W, g.H, g.S);
+        check(cudaMemcpyAsync(pressure, g.staging, n * sizeof(double), cudaMemcpyDeviceToHost, g.stream), "pressure");
+    }
+    check(cudaStreamSynchronize(g.stream), "download");
+}
+
+// One preconditioner application to a given residual (PressureMultigrid::apply,
+// PressureMultigrid.cpp:410-434, or the diagonal at FluidGridCPU.cpp:1691-1698); the
+// correction is returned without its mean removed, as the reference's apply returns it.
+void apply_preconditioner(Grid& g, const double* residual, double residual_mean, double* correction)
+{
+    require_uploaded(g);
+    Plan& p = single_plan(g);
+    rebuild_if_dirty(p);
+    const bool use_mg = g.preconditioner == FC_PRECONDITIONER_MULTIGRID;
+    SolveState s;
+    check(cudaMemcpyAsync(&s, g.desc.state, sizeof(s), cudaMemcpyDeviceToHost, p.stream), "state");
+    check(cudaStreamSynchronize(p.stream), "state");
+    if (use_mg && !s.mg_valid)
+        fail(FC_ERR_BREAKDOWN, "coarsest multigrid factorisation failed");
+    const int mg_valid = s.mg_valid;
+    s = SolveState{};
+    s.mg_valid = mg_valid;
+    s.use_mg = use_mg ? 1 : 0;
+    s.mean_r = residual_mean;
+    s.restart = 1;
+    s.rz = 1.0;
+    s.inv_cells = 1.0 / double(g.cells);
+    check(cudaMemcpyAsync(g.desc.state, &s, sizeof(s), cudaMemcpyHostToDevice, p.stream), "state");
+    check(cudaMemcpyAsync(g.staging, residual, g.cells * sizeof(double), cudaMemcpyHostToDevice, p.stream), "residual");
+    dispatch(g.precision, [&](auto zero)
+    {
+        using T = decltype(zero);
+        set_kernel_attributes<T>(p);
+        FC_LAUNCH(k_pad_t<T>, blocks_for(g.cells), 256, 0, p.stream, g.staging, g.desc.r, g.W, g.H, g.S);
+        launch_precondition<T>(p, use_mg);
+        FC_LAUNCH(k_unpad_t<T>, blocks_for(g.cells), 256, 0, p.stream, g.desc.z, g.staging, g.W, g.H, g.S);
+    });
+    check(cudaMemcpyAsync(correction, g.staging, g.cells * sizeof(double), cudaMemcpyDeviceToHost, p.stream), "correction");
+    check(cudaStreamSynchronize(p.stream), "preconditioner");
+}
+
+double time_kernel(Grid& g, int kernel, int repeats)
+{
+    require_uploaded(g);
+    Plan& p = single_plan(g);
+    if (kernel < 0 || kernel > 3 || repeats <= 0)
+        fail(FC_ERR_INVALID_ARGUMENT, "unknown kernel or repeat count");
+    if ((kernel == 0 || kernel == 1) && g.tail == 0)
+        fail(FC_ERR_INVALID_ARGUMENT, "grid too small for the fine-level smoothing kernels");
+    rebuild_if_dirty(p);
+    SolveState saved;
+    check(cudaMemcpyAsync(&saved, g.desc.state, sizeof(saved), cudaMemcpyDeviceToHost, p.stream), "state");
+    check(cudaStreamSynchronize(p.stream), "state");
+    SolveState running = saved;
+    running.done = 0;
+    running.restart = 1;
+    check(cudaMemcpyAsync(g.desc.state, &running, sizeof(running), cudaMemcpyHostToDevice, p.stream), "state");
+    cudaEvent_t start, stop;
+    check(cudaEventCreate(&start), "event");
+    check(cudaEventCreate(&stop), "event");
+    float ms = 0.0f;
+    dispatch(g.precision, [&](auto zero)
+    {
+        using T = decltype(zero);
+        constexpr int K = Tiling<T>::K;
+        set_kernel_attributes<T>(p);
+        auto launch = [&]
+        {
+            switch (kernel)
+            {
+            case 0: FC_LAUNCH((k_mg_pre<T, K>), p.pre[0].count, 256, 0, p.stream, p.d_desc, p.at(p.pre[0]), 0); break;
+            case 1: FC_LAUNCH((k_mg_post<T, K>), p.post[0].count, 256, 0, p.stream, p.d_desc, p.at(p.post[0]), 0); break;
+            case 2: FC_LAUNCH(k_direction_operator<T>, p.vec.count, kVecThreads, 0, p.stream, p.d_desc, p.at(p.vec), 0); break;
+            default: FC_LAUNCH(k_mg_tail<T>, p.n(), kTailThreads, p.tail_smem, p.stream, p.d_desc); break;
+            }
+        };
+        launch(); // warm
+        check(cudaEventRecord(start, p.stream), "event");
+        for (int i = 0; i < repeats; ++i)
+        {
+            // The level-0 post kernel folds a reduction that may mark the solve done.
+            check(cudaMemcpyAsync(&g.desc.state->done, &running.done, sizeof(int), cudaMemcpyHostToDevice, p.stream), "state");
+            launch();
+        }
+        check(cudaEventRecord(stop, p.stream), "event");
+    });
+    check(cudaEventSynchronize(stop), "event");
+    check(cudaEventElapsedTime(&ms, start, stop), "event");
+    cudaEventDestroy(start);
+    cudaEventDestroy(stop);
+    check(cudaMemcpyAsync(g.desc.state, &saved, sizeof(saved), cudaMemcpyHostToDevice, p.stream), "state");
+    check(cudaStreamSynchronize(p.stream), "state");
+    return double(ms) / repeats;
+}
+
+} // namespace fc
+
+// ==========================================================================================
+// C ABI
+// ==========================================================================================
+
+using fc::Grid;
+using fc::guarded;
+using fc::fail;
+using fc::check;
+
+struct fc_grid
+{
+    Grid impl;
+};
+
+struct fc_batch
+{
+    std::vector<fc_grid*> grids;
+    std::unique_ptr<fc::Plan> plan;
+};
+
+extern "C" {
+
+int fc_abi_version(void) { return FC_ABI_VERSION; }
+
+const char* fc_last_error(void) { return fc::last_error.c_str(); }
+
+const char* fc_status_string(int status)
+{
+    switch (status)
+    {
+    case FC_OK: return "ok";
+    case FC_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case FC_ERR_LIFECYCLE: return "lifecycle";
+    case FC_ERR_CUDA: return "cuda";
+    case FC_ERR_OUT_OF_MEMORY: return "out of memory";
+    case FC_ERR_NONFINITE: return "non-finite";
+    case FC_ERR_BREAKDOWN: return "breakdown";
+    case FC_ERR_UNSUPPORTED: return "unsupported";
+    case FC_ERR_TIMEOUT: return "timeout";
+    default: return "unknown";
+    }
+}
+
+long long fc_kernel_launches(void) { return fc::launch_count.load(); }
+
+int fc_create(int width, int height, double cell_size, int precision, fc_grid** out)
+{
+    return guarded([&]
+    {
+        if (!out)
+            fail(FC_ERR_INVALID_ARGUMENT, "null output handle");
+        *out = nullptr;
+        if (width <= 0 || height <= 0 || !(cell_size > 0.0) || !std::isfinite(cell_size))
+            fail(FC_ERR_INVALID_ARGUMENT, "grid geometry must be positive and finite");
+        if ((long long)width * height > (1ll << 30))
+            fail(FC_ERR_INVALID_ARGUMENT, "grid too large");
+        if (precision == FC_PRECISION_MIXED)
+            fail(FC_ERR_UNSUPPORTED, "mixed precision is not available in this build");
+        if (precision != FC_PRECISION_FP32 && precision != FC_PRECISION_FP64)
+            fail(FC_ERR_INVALID_ARGUMENT, "unknown precision %d", precision);
+        auto handle = std::make_unique<fc_grid>();
+        Grid& g = handle->impl;
+        g.W = width;
+        g.H = height;
+        g.dx = cell_size;
+        g.precision = precision;
+        g.elem = precision == FC_PRECISION_FP64 ? 8 : 4;
+        check(cudaGetDevice(&g.device), "device");
+        check(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking), "stream");
+        fc::allocate_grid(g);
+        *out = handle.release();
+    });
+}
+
+int fc_destroy(fc_grid* grid)
+{
+    return guarded([&]
+    {
+        if (grid)
+        {
+            cudaStreamSynchronize(grid->impl.stream);
+            delete grid;
+        }
+    });
+}
+
+int fc_get_geometry(const fc_grid* grid, int* width, int* height, double* cell_size)
+{
+    return guarded([&]
+    {
+        if (!grid)
+            fail(FC_ERR_INVALID_ARGUMENT, "null grid");
+        if (width)
+            *width = grid->impl.W;
+        if (height)
+            *height = grid->impl.H;
+        if (cell_size)
+            *cell_size = grid->impl.dx;
+    });
+}
+
+int fc_get_origin(const fc_grid* grid, double* x, double* y)
+{
+    return guarded([&]
+    {
+        if (!grid || !x || !y)
+            fail(FC_ERR_INVALID_ARGUMENT, "null argument");
+        *x = grid->impl.origin_x;
+        *y = grid->impl.origin_y;
+    });
+}
+
+int fc_set_origin(fc_grid* grid, double x, double y)
+{
+    return guarded([&]
+    {
+        if (!grid)
+            fail(FC_ERR_INVALID_ARGUMENT, "null grid");
+        grid->impl.origin_x = x;
+        grid->impl.origin_y = y;
+    });
+}
+
+int fc_get_precision(const fc_grid* grid, int* precision)
+{
+    return guarded([&]
+    {
+        if (!grid || !precision)
+            fail(FC_ERR_INVALID_ARGUMENT, "null argument");
+        *precision = grid->impl.precision;
+    });
+}
+
+int fc_configure_materials(fc_grid* grid, int liquid_count, const double* liquid_densities,
+    const double* liquid_viscosities, int gas_count, const double* gas_densities, const double* gas_viscosities)
+{
+    return guarded([&]
+    {
+        if (!grid || liquid_count < 0 || gas_count < 0 || (liquid_count && !liquid_densities) || (gas_count && !gas_densities))
+            fail(FC_ERR_INVALID_ARGUMENT, "invalid material description");
+        Grid& g = grid->impl;
+        auto take = [](std::vector<double>& out, int n, const double* values)
+        {
+            out.assign(n, 0.0);
+            for (int i = 0; i < n && values; ++i)
+                out[i] = values[i];
+        };
+        for (int i = 0; i < liquid_count; ++i)
+            if (!(liquid_densities[i] > 0.0) || !std::isfinite(liquid_densities[i]))
+                fail(FC_ERR_INVALID_ARGUMENT, "component densities must be positive and finite");
+        for (int i = 0; i < gas_count; ++i)
+            if (!(gas_densities[i] > 0.0) || !std::isfinite(gas_densities[i]))
+                fail(FC_ERR_INVALID_ARGUMENT, "component densities must be positive and finite");
+        for (int i = 0; i < liquid_count && liquid_viscosities; ++i)
+            if (liquid_viscosities[i] != 0.0)
+                fail(FC_ERR_UNSUPPORTED, "viscosity is not available in this build");
+        for (int i = 0; i < gas_count && gas_viscosities; ++i)
+            if (gas_viscosities[i] != 0.0)
+                fail(FC_ERR_UNSUPPORTED, "viscosity is not available in this build");
+        take(g.liquid_density, liquid_count, liquid_densities);
+        take(g.gas_density, gas_count, gas_densities);
+        take(g.liquid_viscosity, liquid_count, liquid_viscosities);
+        take(g.gas_viscosity, gas_count, gas_viscosities);
+        g.configured = true;
+        // Changing mixtures requires another upload (FluidGridBase.h:41).
+        g.uploaded = false;
+    });
+}
+
+int fc_get_gravity(const fc_grid* grid, double* gravity_y)
+{
+    return guarded([&]
+    {
+        if (!grid || !gravity_y)
+            fail(FC_ERR_INVALID_ARGUMENT, "null argument");
+        *gravity_y = grid->impl.gravity_y;
+    });
+}
+
+int fc_set_gravity(fc_grid* grid, double gravity_y)
+{
+    return guarded([&]
+    {
+        if (!grid)
+            fail(FC_ERR_INVALID_ARGUMENT, "null grid");
+        grid->impl.gravity_y = gravity_y;
+    });
+}
+
+int fc_set_preconditioner(fc_grid* grid, int preconditioner)
+{
+    return guarded([&]
+    {
+        if (!grid || (preconditioner != FC_PRECONDITIONER_DIAGONAL && preconditioner != FC_PRECONDITIONER_MULTIGRID))
+            fail(FC_ERR_INVALID_ARGUMENT, "unknown preconditioner");
+        grid->impl.preconditioner = preconditioner;
+    });
+}
+
+int fc_set_obstacles(fc_grid* grid, const unsigned char* solid)
+{
+    return guarded([&]
+    {
+        if (!grid)
+            fail(FC_ERR_INVALID_ARGUMENT, "null grid");
+        Grid& g = grid->impl;
+        if (solid)
+        {
+            std::vector<unsigned char> flags(g.cells);
+            for (size_t i = 0; i < g.cells; ++i)
+                flags[i] = solid[i] ? 1 : 0;
+            check(cudaMemcpyAsync(g.solid, flags.data(), g.cells, cudaMemcpyHostToDevice, g.stream), "obstacles");
+            check(cudaStreamSynchronize(g.stream), "obstacles");
+            g.has_solid = true;
+        }
+        else
+            g.has_solid = false;
+        fc::refresh_descriptor(g);
+        g.coefficients_dirty = true;
+    });
+}
+
+int fc_upload(fc_grid* grid, const double* liquid_fraction, const double* u, const double* v, const double* pressure,
+    const double* const* liquid_mass, const double* const* gas_mass)
+{
+    return guarded([&]
+    {
+        if (!grid)
+            fail(FC_ERR_INVALID_ARGUMENT, "null grid");
+        fc::upload(grid->impl, liquid_fraction, u, v, pressure, liquid_mass, gas_mass);
+    });
+}
+
+int fc_download(fc_grid* grid, double* liquid_fraction, double* u, double* v, double* pressure,
+    double* const* liquid_mass, double* const* gas_mass)
+{
+    return guarded([&]
+    {
+        if (!grid)
+            fail(FC_ERR_INVALID_ARGUMENT, "null grid");
+        fc::download(grid->impl, liquid_fraction, u, v, pressure, liquid_mass, gas_mass);
+    });
+}
+
+int fc_copy_state(fc_grid* dst, const fc_grid* src)
+{
+    return guarded([&]
+    {
+        if (!dst || !src)
+            fail(FC_ERR_INVALID_ARGUMENT, "null grid");
+        Grid& d = dst->impl;
+        const Grid& s = src->impl;
+        if (d.W != s.W || d.H != s.H || d.precision != s.precision || d.components() != s.components())
+            fail(FC_ERR_INVALID_ARGUMENT, "grids differ in geometry, precision or materials");
+        fc::require_uploaded(s);
+        if (!d.configured)
+            fail(FC_ERR_LIFECYCLE, "configure the destination's materials first");
+        fc::allocate_masses(d);
+        fc::refresh_descriptor(d);
+        const size_t padded = size_t(d.S) * (d.H + 2);
+        check(cudaStreamSynchronize(s.stream), "copy source");
+        auto copy = [&](void* to, const void* from, size_t bytes)
+        { check(cudaMemcpyAsync(to, from, bytes, cudaMemcpyDeviceToDevice, d.stream), "state copy"); };
+        copy(d.fraction, s.fraction, d.cells * sizeof(double));
+        if (d.components() > 0)
+            copy(d.masses, s.masses, size_t(d.components()) * d.cells * sizeof(double));
+        copy(d.desc.u, s.desc.u, d.faces_u * d.elem);
+        copy(d.desc.v, s.desc.v, d.faces_v * d.elem);
+        copy(d.desc.p, s.desc.p, padded * sizeof(double));
+        copy(d.desc.p_prev, s.desc.p_prev, padded * sizeof(double));
+        check(cudaStreamSynchronize(d.stream), "state copy");
+        d.uploaded = true;
+        d.coefficients_dirty = true;
+    });
+}
+
+int fc_project(fc_grid* grid, double dt, int max_iterations, double divergence_tolerance, fc_result* result)
+{
+    if (!grid)
+        return FC_ERR_INVALID_ARGUMENT;
+    return fc::project_one(grid->impl, dt, max_iterations, divergence_tolerance, 0.0, result);
+}
+
+int fc_project_relative(fc_grid* grid, double dt, int max_iterations, double relative_tolerance,
+    double divergence_tolerance, fc_result* result)
+{
+    if (!grid || !(relative_tolerance > 0.0))
+        return FC_ERR_INVALID_ARGUMENT;
+    return fc::project_one(grid->impl, dt, max_iterations, divergence_tolerance, relative_tolerance, result);
+}
+
+int fc_apply_gravity(fc_grid* grid, double dt)
+{
+    return guarded([&]
+    {
+        if (!grid)
+            fail(FC_ERR_INVALID_ARGUMENT, "null grid");
+        Grid& g = grid->impl;
+        fc::require_uploaded(g);
+        fc::Plan& p = fc::single_plan(g);
+        fc::dispatch(g.precision, [&](auto zero)
+        {
+            using T = decltype(zero);
+            FC_LAUNCH(fc::k_gravity<T>, p.vec.count, fc::kVecThreads, 0, p.stream, p.d_desc, p.at(p.vec), g.gravity_y * dt);
+        });
+        check(cudaStreamSynchronize(p.stream), "gravity");
+    });
+}
+
+int fc_step(fc_grid* grid, double dt, int max_iterations, double divergence_tolerance, fc_result* result,
+    fc_timings* timings)
+{
+    if (!grid)
+        return FC_ERR_INVALID_ARGUMENT;
+    using Clock = std::chrono::steady_clock;
+    if (timings)
+        *timings = fc_timings{};
+    if (!(dt > 0.0))
+    {
+        // FluidGridCPU::step: dt <= 0 returns {0, inf, false, 0, 0} (FluidGridCPU.cpp:306-307).
+        if (result)
+        {
+            *result = fc_result{};
+            result->max_divergence = INFINITY;
+        }
+        return FC_OK;
+    }
+    const auto t0 = Clock::now();
+    int status = fc_apply_gravity(grid, dt);
+    if (status != FC_OK)
+        return status;
+    const auto t1 = Clock::now();
+    status = fc_project(grid, dt, max_iterations, divergence_tolerance, result);
+    const auto t2 = Clock::now();
+    if (timings)
+    {
+        timings->forces_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+        timings->pressure_ms = std::chrono::duration<double, std::milli>(t2 - t1).count();
+    }
+    if (result)
+        result->physical_steps = 1;
+    return status;
+}
+
+int fc_max_divergence(fc_grid* grid, double* out)
+{
+    return guarded([&]
+    {
+        if (!grid || !out)
+            fail(FC_ERR_INVALID_ARGUMENT, "null argument");
+        Grid& g = grid->impl;
+        fc::require_uploaded(g);
+        fc::Plan& p = fc::single_plan(g);
+        fc::dispatch(g.precision, [&](auto zero)
+        {
+            using T = decltype(zero);
+            FC_LAUNCH(fc::k_divergence<T>, p.vec.count, fc::kVecThreads, 0, p.stream, p.d_desc, p.at(p.vec));
+        });
+        fc::SolveState s;
+        check(cudaMemcpyAsync(&s, g.desc.state, sizeof(s), cudaMemcpyDeviceToHost, p.stream), "divergence");
+        check(cudaStreamSynchronize(p.stream), "divergence");
+        *out = s.div_max;
+    });
+}
+
+int fc_classify(fc_grid* grid, unsigned char* mask)
+{
+    return guarded([&]
+    {
+        if (!grid || !mask)
+            fail(FC_ERR_INVALID_ARGUMENT, "null argument");
+        Grid& g = grid->impl;
+        fc::require_uploaded(g);
+        fc::Plan& p = fc::single_plan(g);
+        FC_LAUNCH(fc::k_classify, p.vec.count, fc::kVecThreads, 0, p.stream, p.d_desc, p.at(p.vec), g.fraction, g.mask);
+        check(cudaMemcpyAsync(mask, g.mask, g.cells, cudaMemcpyDeviceToHost, p.stream), "classify");
+        check(cudaStreamSynchronize(p.stream), "classify");
+    });
+}
+
+int fc_time_kernel(fc_grid* grid, int kernel, int repeats, double* mean_ms)
+{
+    return guarded([&]
+    {
+        if (!grid || !mean_ms)
+            fail(FC_ERR_INVALID_ARGUMENT, "null argument");
+        *mean_ms = fc::time_kernel(grid->impl, kernel, repeats);
+    });
+}
+
+int fc_velocity_pointers(fc_grid* grid, void** u, void** v)
+{
+    return guarded([&]
+    {
+        if (!grid)
+            fail(FC_ERR_INVALID_ARGUMENT, "null grid");
+        if (u)
+            *u = grid->impl.desc.u;
+        if (v)
+            *v = grid->impl.desc.v;
+    });
+}
+
+int fc_get_stream(const fc_grid* grid, void** stream)
+{
+    return guarded([&]
+    {
+        if (!grid || !stream)
+            fail(FC_ERR_INVALID_ARGUMENT, "null argument");
+        *stream = grid->impl.stream;
+    });
+}
+
+int fc_synchronize(fc_grid* grid)
+{
+    return guarded([&]
+    {
+        if (!grid)
+            fail(FC_ERR_INVALID_ARGUMENT, "null grid");
+        check(cudaStreamSynchronize(grid->impl.stream), "synchronize");
+    });
+}
+
+int fc_apply_preconditioner(fc_grid* grid, const double* residual, double residual_mean, double* correction)
+{
+    return guarded([&]
+    {
+        if (!grid || !residual || !correction)
+            fail(FC_ERR_INVALID_ARGUMENT, "null argument");
+        fc::apply_preconditioner(grid->impl, residual, residual_mean, correction);
+    });
+}
+
+int fc_batch_create(fc_grid* const* grids, int count, fc_batch** out)
+{
+    return guarded([&]
+    {
+        if (!grids || count <= 0 || !out)
+            fail(FC_ERR_INVALID_ARGUMENT, "empty batch");
+        *out = nullptr;
+        std::vector<Grid*> members;
+        for (int i = 0; i < count; ++i)
+        {
+            if (!grids[i])
+                fail(FC_ERR_INVALID_ARGUMENT, "null grid in batch");
+            if (grids[i]->impl.precision != grids[0]->impl.precision)
+                fail(FC_ERR_INVALID_ARGUMENT, "a batch needs one precision");
+            for (int j = 0; j < i; ++j)
+                if (grids[j] == grids[i])
+                    fail(FC_ERR_INVALID_ARGUMENT, "grid listed twice in a batch");
+            members.push_back(&grids[i]->impl);
+        }
+        auto batch = std::make_unique<fc_batch>();
+        batch->grids.assign(grids, grids + count);
+        batch->plan = fc::make_plan(members, nullptr);
+        *out = batch.release();
+    });
+}
+
+int fc_batch_destroy(fc_batch* batch)
+{
+    return guarded([&]
+    {
+        if (batch)
+        {
+            cudaStreamSynchronize(batch->plan->stream);
+            delete batch;
+        }
+    });
+}
+
+int fc_batch_project(fc_batch* batch, const double* dts, int max_iterations, double divergence_tolerance,
+    double relative_tolerance, fc_result* results)
+{
+    return guarded([&]
+    {
+        if (!batch || !dts || !results)
+            fail(FC_ERR_INVALID_ARGUMENT, "null argument");
+        if (max_iterations < 0)
+            fail(FC_ERR_INVALID_ARGUMENT, "max_iterations must be non-negative");
+        for (size_t i = 0; i < batch->grids.size(); ++i)
+            if (!(dts[i] > 0.0))
+                fail(FC_ERR_INVALID_ARGUMENT, "time steps must be positive");
+        fc::Plan& p = *batch->plan;
+        // Grids may have changed (obstacles, materials) since the batch was made.
+        for (Grid* g : p.grids)
+        {
+            g->desc.solid = g->has_solid ? g->solid : nullptr;
+            g->desc.masses = g->mass_ptrs;
+            g->desc.components = g->components();
+            check(cudaStreamSynchronize(g->stream), "batch member");
+        }
+        fc::upload_descriptors(p);
+        fc::project_plan(p, dts, max_iterations, divergence_tolerance, relative_tolerance, results);
+    });
+}
+
+int fc_batch_get_stream(const fc_batch* batch, void** stream)
+{
+    return guarded([&]
+    {
+        if (!batch || !stream)
+            fail(FC_ERR_INVALID_ARGUMENT, "null argument");
+        *stream = batch->plan->stream;
+    });
+}
+
+} // extern "C"

@@ -1,0 +1,592 @@
+// Fine-level PCG kernels of the UniformCUDA projection.
+//
+// Every kernel takes the grid descriptors and a tile table, so one launch serves one grid or a
+// batch of independent grids of uneven sizes (each CTA looks up its grid). A tile is 32 x 32
+// cells worked by 256 threads, 4 rows each. Reductions are folded in FP64: each CTA writes one
+// partial and the last CTA of a grid to arrive folds them in tile order, so results do not
+// depend on which other grids share the launch.
+//
+// The per-iteration schedule follows FluidGridCPU::solvePressure (FluidGridCPU.cpp:1728-1824):
+//   dir_op   d = (z - mean z) + beta d ; q = A d ; d.q            (operator :1507-1598)
+//   update   p += alpha d ; r -= alpha q ; sum r, max |r|, sum r^2  (:1600-1641)
+//   verify   on a met stop rule: r = b - A p, accept or restart     (:1795-1804, :1643-1683)
+//   V-cycle  z = M r (fc_multigrid.cuh), then r.z and beta          (:1685-1726)
+#pragma once
+
+#include "fc_device.cuh"
+
+namespace fc
+{
+
+template <typename T> __device__ __forceinline__ double dd(T v) { return double(v); }
+
+// Arithmetic of the stop rule: max-norm (the reference rule) and/or squared L2 norm.
+__device__ __forceinline__ bool stop_rule_met(const SolveState& s, double maximum, double sumsq)
+{
+    return maximum <= s.tol_max && sumsq <= s.tol_sumsq;
+}
+
+__device__ __forceinline__ bool cell_solid(const GridDesc& g, int x, int y)
+{
+    return g.solid && g.solid[(long long)y * g.W + x];
+}
+
+#define FC_VEC_TILE_PROLOGUE                                                                       \
+    const Tile t = tiles[blockIdx.x];                                                              \
+    const GridDesc& g = grids[t.grid];                                                             \
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+
+// Density from component masses: sum of liquid then gas masses, times 1/dx^2.
+// FluidGridCPU.cpp:1399-1423 (rebuildDensity).
+__global__ void k_density(const GridDesc* grids, const Tile* tiles)
+{
+    FC_VEC_TILE_PROLOGUE
+    const double inv_area = 1.0 / (g.dx * g.dx);
+    for (int k = 0; k < 4; ++k)
+    {
+        const int x = t.x0 + tx, y = t.y0 + ty + 8 * k;
+        if (x >= g.W || y >= g.H)
+            continue;
+        const long long i = (long long)y * g.W + x;
+        double total = 0.0;
+        for (int m = 0; m < g.components; ++m)
+            total += g.masses[m][i];
+        g.density[i] = total * inv_area;
+    }
+}
+
+// Face weights 2/(rho_a + rho_b), zero on walls and around solid cells.
+// FluidGridCPU.cpp:1154-1205 (rebuildPressureCoefficients).
+template <typename T> __global__ void k_coefficients(const GridDesc* grids, const Tile* tiles)
+{
+    FC_VEC_TILE_PROLOGUE
+    const double* density = g.density;
+    T* right = static_cast<T*>(g.lev[0].right);
+    T* down = static_cast<T*>(g.lev[0].down);
+    for (int k = 0; k < 4; ++k)
+    {
+        const int x = t.x0 + tx, y = t.y0 + ty + 8 * k;
+        if (x >= g.W || y >= g.H)
+            continue;
+        const long long c = (long long)y * g.W + x;
+        const long long i = padded_index(g.S, x, y);
+        const bool solid = cell_solid(g, x, y);
+        double wr = 0.0, wd = 0.0;
+        if (x + 1 < g.W && !solid && !cell_solid(g, x + 1, y))
+            wr = 2.0 / (density[c] + density[c + 1]);
+        if (y + 1 < g.H && !solid && !cell_solid(g, x, y + 1))
+            wd = 2.0 / (density[c] + density[c + g.W]);
+        right[i] = T(wr);
+        down[i] = T(wd);
+    }
+}
+
+// Closed faces (outer walls, and faces of solid cells) read as zero; the thread of the cell on
+// the low side of a face writes the zero. Returns the four face velocities of cell (x, y).
+template <typename T>
+__device__ __forceinline__ void cell_faces(const GridDesc& g, int x, int y, bool write_closed, double& ul, double& ur,
+    double& vu, double& vd)
+{
+    T* u = static_cast<T*>(g.u);
+    T* v = static_cast<T*>(g.v);
+    const long long iu = (long long)y * (g.W + 1) + x;
+    const long long iv = (long long)y * g.W + x;
+    const bool solid = cell_solid(g, x, y);
+    const bool closed_l = x == 0 || solid || cell_solid(g, x - 1, y);
+    const bool closed_r = x + 1 == g.W || solid || cell_solid(g, x + 1, y);
+    const bool closed_u = y == 0 || solid || cell_solid(g, x, y - 1);
+    const bool closed_d = y + 1 == g.H || solid || cell_solid(g, x, y + 1);
+    ul = closed_l ? 0.0 : dd(u[iu]);
+    ur = closed_r ? 0.0 : dd(u[iu + 1]);
+    vu = closed_u ? 0.0 : dd(v[iv]);
+    vd = closed_d ? 0.0 : dd(v[iv + g.W]);
+    if (write_closed)
+    {
+        // Each closed face is zeroed by exactly one cell: the left/upper face by this cell when
+        // it is the outer wall or this cell is solid; the right/lower face when it is the wall.
+        if (closed_r)
+            u[iu + 1] = T(0);
+        if (closed_d)
+            v[iv + g.W] = T(0);
+        if (x == 0)
+            u[iu] = T(0);
+        if (y == 0)
+            v[iv] = T(0);
+    }
+}
+
+// b = -(du + dv)/dx * dx^2/dt with closed faces zeroed; sums b over open cells.
+// FluidGridCPU.cpp:1050-1083.
+template <typename T> __global__ void __launch_bounds__(kVecThreads) k_rhs(const GridDesc* grids, const Tile* tiles)
+{
+    FC_VEC_TILE_PROLOGUE
+    const double dt = g.state->dt;
+    const double scale = g.dx * g.dx / dt;
+    double sum = 0.0;
+    for (int k = 0; k < 4; ++k)
+    {
+        const int x = t.x0 + tx, y = t.y0 + ty + 8 * k;
+        if (x >= g.W || y >= g.H)
+            continue;
+        double ul, ur, vu, vd;
+        cell_faces<T>(g, x, y, true, ul, ur, vu, vd);
+        const double du = ur - ul;
+        const double dv = vd - vu;
+        double b = -(du + dv) / g.dx * scale;
+        if (cell_solid(g, x, y))
+            b = 0.0;
+        g.b[padded_index(g.S, x, y)] = b;
+        sum += b;
+    }
+    __shared__ double4 total;
+    if (arrive_last<kVecThreads>(g, t.index, g.vec_tiles, block_reduce4<kVecThreads>(make_double4(sum, 0, 0, 0), 0), &total, 0))
+    {
+        if (threadIdx.x == 0)
+            g.state->mean_b = total.x * g.state->inv_cells;
+    }
+}
+
+// max |b - mean| and sum (b - mean)^2; decides the early exit (FluidGridCPU.cpp:1731-1740).
+template <typename T> __global__ void __launch_bounds__(kVecThreads) k_rhs_stats(const GridDesc* grids, const Tile* tiles)
+{
+    FC_VEC_TILE_PROLOGUE
+    const double mean = g.state->mean_b;
+    double mx = 0.0, sq = 0.0;
+    for (int k = 0; k < 4; ++k)
+    {
+        const int x = t.x0 + tx, y = t.y0 + ty + 8 * k;
+        if (x >= g.W || y >= g.H || cell_solid(g, x, y))
+            continue;
+        const double b = g.b[padded_index(g.S, x, y)] - mean;
+        mx = fmax(mx, isfinite(b) ? fabs(b) : INFINITY);
+        sq += b * b;
+    }
+    __shared__ double4 total;
+    if (arrive_last<kVecThreads>(g, t.index, g.vec_tiles, block_reduce4<kVecThreads>(make_double4(mx, sq, 0, 0), 1), &total, 1))
+    {
+        if (threadIdx.x == 0)
+        {
+            SolveState& s = *g.state;
+            s.bmax = total.x;
+            s.bsumsq = total.y;
+            if (s.tol_sumsq < 0.0) // relative rule requested: -tol_sumsq carries tol^2
+                s.tol_sumsq = -s.tol_sumsq * total.y;
+            if (stop_rule_met(s, total.x, total.y))
+            {
+                s.status = kNoWork;
+                s.done = 1;
+            }
+        }
+    }
+}
+
+// Warm start p = 2p - p_prev, or clear both when no solve is needed; sums the prediction.
+// FluidGridCPU.cpp:1731-1753.
+__global__ void __launch_bounds__(kVecThreads) k_warm_start(const GridDesc* grids, const Tile* tiles)
+{
+    FC_VEC_TILE_PROLOGUE
+    const bool clear = g.state->status == kNoWork;
+    double sum = 0.0;
+    for (int k = 0; k < 4; ++k)
+    {
+        const int x = t.x0 + tx, y = t.y0 + ty + 8 * k;
+        if (x >= g.W || y >= g.H)
+            continue;
+        const long long i = padded_index(g.S, x, y);
+        if (clear || cell_solid(g, x, y))
+        {
+            g.p[i] = 0.0;
+            g.p_prev[i] = 0.0;
+            continue;
+        }
+        const double latest = g.p[i];
+        const double predicted = 2.0 * latest - g.p_prev[i];
+        g.p[i] = predicted;
+        g.p_prev[i] = latest;
+        sum += predicted;
+    }
+    __shared__ double4 total;
+    if (arrive_last<kVecThreads>(g, t.index, g.vec_tiles, block_reduce4<kVecThreads>(make_double4(sum, 0, 0, 0), 0), &total, 0))
+    {
+        if (threadIdx.x == 0)
+            g.state->mean_p = total.x * g.state->inv_cells;
+    }
+}
+
+// Pressure sum for the final mean removal.
+__global__ void __launch_bounds__(kVecThreads) k_pressure_sum(const GridDesc* grids, const Tile* tiles)
+{
+    FC_VEC_TILE_PROLOGUE
+    if (g.state->status == kBreakdown)
+        return;
+    double sum = 0.0;
+    for (int k = 0; k < 4; ++k)
+    {
+        const int x = t.x0 + tx, y = t.y0 + ty + 8 * k;
+        if (x >= g.W || y >= g.H || cell_solid(g, x, y))
+            continue;
+        sum += g.p[padded_index(g.S, x, y)];
+    }
+    __shared__ double4 total;
+    if (arrive_last<kVecThreads>(g, t.index, g.vec_tiles, block_reduce4<kVecThreads>(make_double4(sum, 0, 0, 0), 0), &total, 0))
+    {
+        if (threadIdx.x == 0)
+            g.state->mean_p = total.x * g.state->inv_cells;
+    }
+}
+
+// p -= mean_p over open cells (FluidGridCPU.cpp:1466-1474, removeMean).
+__global__ void k_remove_pressure_mean(const GridDesc* grids, const Tile* tiles)
+{
+    FC_VEC_TILE_PROLOGUE
+    if (g.state->status == kBreakdown)
+        return;
+    const double mean = g.state->mean_p;
+    for (int k = 0; k < 4; ++k)
+    {
+        const int x = t.x0 + tx, y = t.y0 + ty + 8 * k;
+        if (x >= g.W || y >= g.H)
+            continue;
+        const long long i = padded_index(g.S, x, y);
+        // Pressure inside obstacles is held at zero.
+        g.p[i] = cell_solid(g, x, y) ? 0.0 : g.p[i] - mean;
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ double apply_cell_fp64(const T* right, const T* down, const double* x, long long i, int S)
+{
+    const double c = x[i];
+    return (dd(right[i - 1]) * (c - x[i - 1]) + dd(right[i]) * (c - x[i + 1])) +
+           (dd(down[i - S]) * (c - x[i - S]) + dd(down[i]) * (c - x[i + S]));
+}
+
+// True residual r = (b - mean b) - A p in FP64, stored in the working type, with its stats.
+// `initial` selects the solve's first residual (FluidGridCPU.cpp:1754-1757) versus the
+// convergence check inside the loop (:1795-1804).
+template <typename T>
+__global__ void __launch_bounds__(kVecThreads) k_true_residual(const GridDesc* grids, const Tile* tiles, int initial)
+{
+    FC_VEC_TILE_PROLOGUE
+    SolveState& s = *g.state;
+    if (s.done || (!initial && !s.verify))
+        return;
+    const T* right = static_cast<const T*>(g.lev[0].right);
+    const T* down = static_cast<const T*>(g.lev[0].down);
+    T* r = static_cast<T*>(g.r);
+    const double mean_b = s.mean_b;
+    double sum = 0.0, mx = 0.0, sq = 0.0;
+    for (int k = 0; k < 4; ++k)
+    {
+        const int x = t.x0 + tx, y = t.y0 + ty + 8 * k;
+        if (x >= g.W || y >= g.H)
+            continue;
+        const long long i = padded_index(g.S, x, y);
+        double value = 0.0;
+        if (!cell_solid(g, x, y))
+            value = (g.b[i] - mean_b) - apply_cell_fp64(right, down, g.p, i, g.S);
+        const T stored = T(value);
+        r[i] = stored;
+        const double rv = dd(stored);
+        sum += rv;
+        mx = fmax(mx, fabs(rv));
+        sq += rv * rv;
+    }
+    __shared__ double4 total;
+    if (arrive_last<kVecThreads>(g, t.index, g.vec_tiles, block_reduce4<kVecThreads>(make_double4(sum, mx, sq, 0), 2), &total, 2))
+    {
+        if (threadIdx.x == 0)
+        {
+            const double maximum = isfinite(total.x) ? total.y : INFINITY;
+            s.sum_r = total.x;
+            s.max_r = maximum;
+            s.sumsq_r = total.z;
+            s.res_max = maximum;
+            s.res_sumsq = total.z;
+            s.mean_r = total.x * s.inv_cells;
+            s.verify = 0;
+            if (stop_rule_met(s, maximum, total.z))
+            {
+                s.status = kConverged;
+                s.done = 1;
+            }
+            else if (s.iterations >= s.max_iterations)
+            {
+                s.status = kIterationLimit;
+                s.done = 1;
+            }
+            else if (s.use_mg && !s.mg_valid)
+            {
+                s.status = kBreakdown;
+                s.done = 1;
+            }
+            else
+            {
+                s.restart = 1;
+                s.restarts += initial ? 0 : 1;
+            }
+        }
+    }
+}
+
+// d_new = (z - mean z) + beta d_old at one cell (the reference's direction update, :1812-1816,
+// after the correction's mean removal at :1712-1722).
+template <typename T>
+__device__ __forceinline__ double direction_at(const T* z, const T* d_old, long long i, double mean_z, double beta)
+{
+    return (dd(z[i]) - mean_z) + beta * dd(d_old[i]);
+}
+
+// d = (z - mean z) + beta d_old; q = A d; returns d.q through the grid's reduction.
+template <typename T>
+__global__ void __launch_bounds__(kVecThreads) k_direction_operator(const GridDesc* grids, const Tile* tiles, int parity)
+{
+    FC_VEC_TILE_PROLOGUE
+    SolveState& s = *g.state;
+    if (s.done)
+        return;
+    const T* right = static_cast<const T*>(g.lev[0].right);
+    const T* down = static_cast<const T*>(g.lev[0].down);
+    const T* z = static_cast<const T*>(g.z);
+    const T* d_old = static_cast<const T*>(g.d[parity]);
+    T* d_new = static_cast<T*>(g.d[parity ^ 1]);
+    T* q = static_cast<T*>(g.q);
+    const double mean_z = s.mean_z, beta = s.beta;
+    const int S = g.S;
+    double dot = 0.0;
+    for (int k = 0; k < 4; ++k)
+    {
+        const int x = t.x0 + tx, y = t.y0 + ty + 8 * k;
+        if (x >= g.W || y >= g.H)
+            continue;
+        const long long i = padded_index(S, x, y);
+        // Direction values are rounded to the working type before the operator reads them, so
+        // that q = A d uses exactly the stored d (the p update reads the same stored d).
+        const T c = T(direction_at(z, d_old, i, mean_z, beta));
+        const T l = T(direction_at(z, d_old, i - 1, mean_z, beta));
+        const T rr = T(direction_at(z, d_old, i + 1, mean_z, beta));
+        const T u = T(direction_at(z, d_old, i - S, mean_z, beta));
+        const T dn = T(direction_at(z, d_old, i + S, mean_z, beta));
+        const T value = (right[i - 1] * (c - l) + right[i] * (c - rr)) + (down[i - S] * (c - u) + down[i] * (c - dn));
+        d_new[i] = c;
+        q[i] = value;
+        dot += dd(c) * dd(value);
+    }
+    __shared__ double4 total;
+    if (arrive_last<kVecThreads>(g, t.index, g.vec_tiles, block_reduce4<kVecThreads>(make_double4(dot, 0, 0, 0), 0), &total, 0))
+    {
+        if (threadIdx.x == 0)
+        {
+            s.dq = total.x;
+            const double alpha = s.rz / total.x;
+            if (!(total.x > 0.0) || !isfinite(total.x) || !isfinite(alpha))
+            {
+                s.status = kStalled;
+                s.done = 1;
+            }
+        }
+    }
+}
+
+// p += alpha d ; r -= alpha q ; residual stats. FluidGridCPU.cpp:1600-1641.
+template <typename T>
+__global__ void __launch_bounds__(kVecThreads) k_update(const GridDesc* grids, const Tile* tiles, int parity)
+{
+    FC_VEC_TILE_PROLOGUE
+    SolveState& s = *g.state;
+    if (s.done)
+        return;
+    const T* d = static_cast<const T*>(g.d[parity ^ 1]);
+    const T* q = static_cast<const T*>(g.q);
+    T* r = static_cast<T*>(g.r);
+    const double alpha = s.rz / s.dq;
+    double sum = 0.0, mx = 0.0, sq = 0.0;
+    for (int k = 0; k < 4; ++k)
+    {
+        const int x = t.x0 + tx, y = t.y0 + ty + 8 * k;
+        if (x >= g.W || y >= g.H)
+            continue;
+        const long long i = padded_index(g.S, x, y);
+        g.p[i] += alpha * dd(d[i]);
+        const T value = T(dd(r[i]) - alpha * dd(q[i]));
+        r[i] = value;
+        const double rv = dd(value);
+        sum += rv;
+        mx = fmax(mx, fabs(rv));
+        sq += rv * rv;
+    }
+    __shared__ double4 total;
+    if (arrive_last<kVecThreads>(g, t.index, g.vec_tiles, block_reduce4<kVecThreads>(make_double4(sum, mx, sq, 0), 2), &total, 2))
+    {
+        if (threadIdx.x == 0)
+        {
+            s.iterations += 1;
+            const double maximum = isfinite(total.x) ? total.y : INFINITY;
+            s.sum_r = total.x;
+            s.max_r = maximum;
+            s.sumsq_r = total.z;
+            s.mean_r = total.x * s.inv_cells;
+            if (stop_rule_met(s, maximum, total.z))
+                s.verify = 1;
+            else if (s.iterations >= s.max_iterations)
+            {
+                s.status = kIterationLimit;
+                s.done = 1;
+            }
+        }
+    }
+}
+
+// u -= (dp/dx) dt w on open interior faces; each cell updates its left and upper face.
+// FluidGridCPU.cpp:1098-1118.
+template <typename T> __global__ void k_velocity_update(const GridDesc* grids, const Tile* tiles)
+{
+    FC_VEC_TILE_PROLOGUE
+    if (g.state->status == kBreakdown)
+        return;
+    const double dt = g.state->dt;
+    T* u = static_cast<T*>(g.u);
+    T* v = static_cast<T*>(g.v);
+    const T* right = static_cast<const T*>(g.lev[0].right);
+    const T* down = static_cast<const T*>(g.lev[0].down);
+    for (int k = 0; k < 4; ++k)
+    {
+        const int x = t.x0 + tx, y = t.y0 + ty + 8 * k;
+        if (x >= g.W || y >= g.H)
+            continue;
+        const long long i = padded_index(g.S, x, y);
+        const double pc = g.p[i];
+        if (x > 0)
+        {
+            const double w = dd(right[i - 1]);
+            if (w != 0.0)
+            {
+                const long long f = (long long)y * (g.W + 1) + x;
+                u[f] = T(dd(u[f]) - ((pc - g.p[i - 1]) / g.dx) * dt * w);
+            }
+        }
+        if (y > 0)
+        {
+            const double w = dd(down[i - g.S]);
+            if (w != 0.0)
+            {
+                const long long f = (long long)y * g.W + x;
+                v[f] = T(dd(v[f]) - ((pc - g.p[i - g.S]) / g.dx) * dt * w);
+            }
+        }
+    }
+}
+
+// Storage rounding of one face velocity: one unit in the last place of the working type.
+__device__ __forceinline__ double face_ulp(float value)
+{
+    const unsigned int bits = __float_as_uint(fabsf(value)) & 0x7f800000u;
+    return double(__uint_as_float(bits)) * 1.1920928955078125e-7;
+}
+
+__device__ __forceinline__ double face_ulp(double value)
+{
+    const unsigned long long bits = __double_as_longlong(fabs(value)) & 0x7ff0000000000000ull;
+    return __longlong_as_double(bits) * 2.220446049250313e-16;
+}
+
+// max |div u| (FluidGridCPU.cpp:1126-1152), its excess over the float rounding allowance of the
+// four faces (as UniformWebGPU's velocity_stats, FluidUniformWebGPUKernels.h:166-213), and the
+// sum of squares.
+template <typename T> __global__ void __launch_bounds__(kVecThreads) k_divergence(const GridDesc* grids, const Tile* tiles)
+{
+    FC_VEC_TILE_PROLOGUE
+    const T* u = static_cast<const T*>(g.u);
+    const T* v = static_cast<const T*>(g.v);
+    double mx = 0.0, excess = 0.0, sq = 0.0;
+    int nonfinite = 0;
+    for (int k = 0; k < 4; ++k)
+    {
+        const int x = t.x0 + tx, y = t.y0 + ty + 8 * k;
+        if (x >= g.W || y >= g.H)
+            continue;
+        const long long iu = (long long)y * (g.W + 1) + x;
+        const long long iv = (long long)y * g.W + x;
+        const T ul = u[iu], ur = u[iu + 1], vu = v[iv], vd = v[iv + g.W];
+        const double div = ((dd(ur) - dd(ul)) + (dd(vd) - dd(vu))) / g.dx;
+        if (!isfinite(div))
+        {
+            nonfinite = 1;
+            continue;
+        }
+        const double rounding = (face_ulp(ul) + face_ulp(ur) + face_ulp(vu) + face_ulp(vd)) / g.dx;
+        mx = fmax(mx, fabs(div));
+        excess = fmax(excess, fmax(0.0, fabs(div) - rounding));
+        sq += div * div;
+    }
+    __shared__ double4 total;
+    const double4 mine = make_double4(mx, excess, sq, double(nonfinite));
+    if (arrive_last<kVecThreads>(g, t.index, g.vec_tiles, block_reduce4<kVecThreads>(mine, 1 | 2 | 8), &total, 1 | 2 | 8))
+    {
+        if (threadIdx.x == 0)
+        {
+            SolveState& s = *g.state;
+            s.nonfinite = total.w != 0.0;
+            s.div_max = s.nonfinite ? INFINITY : total.x;
+            s.div_excess = s.nonfinite ? INFINITY : total.y;
+            s.div_sumsq = total.z;
+        }
+    }
+}
+
+// Converts FP64 host-layout fields into the device working type (upload) ...
+template <typename T> __global__ void k_from_f64(const double* src, T* dst, long long n)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        dst[i] = T(src[i]);
+}
+
+// ... and back (download).
+template <typename T> __global__ void k_to_f64(const T* src, double* dst, long long n)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        dst[i] = double(src[i]);
+}
+
+// Unpadded W x H FP64 field <-> padded FP64 field (pressure).
+__global__ void k_pad_f64(const double* src, double* dst, int W, int H, int S)
+{
+    const long long n = (long long)W * H;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    {
+        const int x = int(i % W), y = int(i / W);
+        dst[padded_index(S, x, y)] = src[i];
+    }
+}
+
+__global__ void k_unpad_f64(const double* src, double* dst, int W, int H, int S)
+{
+    const long long n = (long long)W * H;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    {
+        const int x = int(i % W), y = int(i / W);
+        dst[i] = src[padded_index(S, x, y)];
+    }
+}
+
+template <typename T> __global__ void k_unpad_t(const void* src, double* dst, int W, int H, int S)
+{
+    const long long n = (long long)W * H;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    {
+        const int x = int(i % W), y = int(i / W);
+        dst[i] = double(static_cast<const T*>(src)[padded_index(S, x, y)]);
+    }
+}
+
+template <typename T> __global__ void k_pad_t(const double* src, void* dst, int W, int H, int S)
+{
+    const long long n = (long long)W * H;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    {
+        const int x = int(i % W), y = int(i / W);
+        static_cast<T*>(dst)[padded_index(S, x, y)] = T(src[i]);
+    }
+}
+
+} // namespace fc

@@ -1,0 +1,276 @@
+// fluid::FluidGridCUDA: the UniformCUDA engine behind FluidSim's engine contract.
+//
+// Header-only adapter from fluid::FluidGridBase (FluidSim/FluidGridBase.h:20-147) to the C ABI
+// in fluidcuda.h. A FluidSim build adds it as one more backend of FluidGrid::selectBackend
+// (FluidSim/FluidGrid.cpp:37-90); see INTEGRATION.md for the selection branch. Status codes
+// become the reference's exception types: std::invalid_argument, std::logic_error,
+// std::runtime_error; a non-converged projection is a result, not an exception.
+#pragma once
+
+#include "FluidGridBase.h"
+#include "fluidcuda.h"
+
+#include <cmath>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+namespace fluid
+{
+
+class FluidGridCUDA final : public FluidGridBase
+{
+public:
+    // Identifies the backend kind for selection code (0 = unknown, 1 = UniformCUDA).
+    static constexpr int kind() { return 1; }
+
+    FluidGridCUDA(int width, int height, double cell_size, int precision = FC_PRECISION_FP32)
+        : width(width), height(height), cell_size(cell_size)
+    {
+        check(fc_create(width, height, cell_size, precision, &grid));
+    }
+
+    ~FluidGridCUDA() override
+    {
+        if (grid)
+            fc_destroy(grid);
+    }
+
+    FluidGridCUDA(const FluidGridCUDA&) = delete;
+    FluidGridCUDA& operator=(const FluidGridCUDA&) = delete;
+
+    int getWidth() const override { return width; }
+
+    int getHeight() const override { return height; }
+
+    double getCellSize() const override { return cell_size; }
+
+    bl::DVec2 getOrigin() const override { return origin; }
+
+    void setOrigin(bl::DVec2 position) override
+    {
+        origin = position;
+        check(fc_set_origin(live(), position.x, position.y));
+    }
+
+    bool requiresRenderThread() const override { return false; }
+
+    void configureMaterials(SubstanceCatalogue catalogue, FluidMixture liquid, FluidMixture gas) override
+    {
+        std::vector<double> ld, lv, gd, gv;
+        for (const auto& c : liquid.components)
+            ld.push_back(c.density), lv.push_back(c.dynamic_viscosity);
+        for (const auto& c : gas.components)
+            gd.push_back(c.density), gv.push_back(c.dynamic_viscosity);
+        check(fc_configure_materials(live(), int(ld.size()), ld.data(), lv.data(), int(gd.size()), gd.data(), gv.data()));
+        substances = std::move(catalogue);
+        liquid_mixture = std::move(liquid);
+        gas_mixture = std::move(gas);
+    }
+
+    const SubstanceCatalogue& getSubstances() const override { return substances; }
+
+    const FluidMixture& getLiquidMixture() const override { return liquid_mixture; }
+
+    const FluidMixture& getGasMixture() const override { return gas_mixture; }
+
+    double getGravityY() const override
+    {
+        double g = 0.0;
+        check(fc_get_gravity(grid, &g));
+        return g;
+    }
+
+    void setGravityY(double acceleration) override { check(fc_set_gravity(live(), acceleration)); }
+
+    void upload(const State& state) override
+    {
+        const size_t cells = size_t(width) * height;
+        auto sized = [](const std::vector<double>& values, size_t count)
+        {
+            if (!values.empty() && values.size() != count)
+                throw std::invalid_argument("FluidGridCUDA upload dimensions do not match the grid");
+            return values.empty() ? nullptr : values.data();
+        };
+        const double* f = sized(state.liquid_fraction, cells);
+        const double* u = sized(state.u, size_t(width + 1) * height);
+        const double* v = sized(state.v, size_t(width) * (height + 1));
+        const double* p = sized(state.pressure, cells);
+        auto components = [&](const std::vector<std::vector<double>>& masses, size_t expected)
+        {
+            std::vector<const double*> ptrs;
+            if (masses.empty())
+                return ptrs;
+            if (masses.size() != expected)
+                throw std::invalid_argument("FluidGridCUDA upload component count does not match the mixture");
+            for (const auto& m : masses)
+                ptrs.push_back(sized(m, cells));
+            return ptrs;
+        };
+        const auto lm = components(state.liquid_mass, liquid_mixture.components.size());
+        const auto gm = components(state.gas_mass, gas_mixture.components.size());
+        check(fc_upload(live(), f, u, v, p, lm.empty() ? nullptr : lm.data(), gm.empty() ? nullptr : gm.data()));
+    }
+
+    State download() const override
+    {
+        const size_t cells = size_t(width) * height;
+        State s;
+        s.liquid_fraction.resize(cells);
+        s.u.resize(size_t(width + 1) * height);
+        s.v.resize(size_t(width) * (height + 1));
+        s.pressure.resize(cells);
+        s.liquid_mass.assign(liquid_mixture.components.size(), std::vector<double>(cells));
+        s.gas_mass.assign(gas_mixture.components.size(), std::vector<double>(cells));
+        std::vector<double*> lm, gm;
+        for (auto& m : s.liquid_mass)
+            lm.push_back(m.data());
+        for (auto& m : s.gas_mass)
+            gm.push_back(m.data());
+        check(fc_download(grid, s.liquid_fraction.data(), s.u.data(), s.v.data(), s.pressure.data(),
+            lm.empty() ? nullptr : lm.data(), gm.empty() ? nullptr : gm.data()));
+        return s;
+    }
+
+    void destroy() override
+    {
+        if (grid)
+            fc_destroy(grid);
+        grid = nullptr;
+    }
+
+    ProjectionResult step(double dt, int max_iterations = 200, double divergence_tolerance = 1e-6,
+        StepTimings* timings = nullptr) override
+    {
+        fc_result r{};
+        fc_timings t{};
+        check(fc_step(live(), dt, max_iterations, divergence_tolerance, &r, &t));
+        if (timings)
+        {
+            *timings = {};
+            timings->transport_ms = t.transport_ms;
+            timings->viscosity_ms = t.viscosity_ms;
+            timings->forces_ms = t.forces_ms;
+            timings->pressure_ms = t.pressure_ms;
+        }
+        return convert(r);
+    }
+
+    // FluidGridCPU::project (UniformCPU/FluidGridCPU.h:125): one projection without forces.
+    ProjectionResult project(double dt, int max_iterations = 200, double divergence_tolerance = 1e-6)
+    {
+        fc_result r{};
+        check(fc_project(live(), dt, max_iterations, divergence_tolerance, &r));
+        return convert(r);
+    }
+
+    double maxDivergence() const override
+    {
+        double value = 0.0;
+        check(fc_max_divergence(grid, &value));
+        return value;
+    }
+
+    // Display colour of each cell from its component volumes (FluidGridCPU.cpp:1826-1860).
+    void writeColorPixels(std::vector<float>& pixels, bool liquid_fraction_alpha = false) const override
+    {
+        const State s = download();
+        const size_t cells = size_t(width) * height;
+        const double volume = cell_size * cell_size;
+        pixels.assign(cells * 4, 0.0f);
+        for (size_t i = 0; i < cells; ++i)
+        {
+            float* pixel = pixels.data() + i * 4;
+            pixel[3] = liquid_fraction_alpha ? float(s.liquid_fraction[i]) : 1.0f;
+            auto add = [&](const FluidMixture& mixture, const std::vector<std::vector<double>>& masses)
+            {
+                for (size_t k = 0; k < mixture.components.size(); ++k)
+                {
+                    const auto& component = mixture.components[k];
+                    const auto& color = substances[component.substance].color;
+                    const double fraction = masses[k][i] / (component.density * volume);
+                    for (int c = 0; c < 3; ++c)
+                        pixel[c] += float(fraction * color[c]);
+                }
+            };
+            add(liquid_mixture, s.liquid_mass);
+            add(gas_mixture, s.gas_mass);
+        }
+    }
+
+    fc_grid* native() const { return grid; }
+
+protected:
+    // Material replacements (FluidGridCPU.cpp:256-290): a host round trip; edits are rare.
+    void commitEdits(detail::CellEditBatch& batch) override
+    {
+        if (batch.velocity)
+            throw std::invalid_argument("Material edit velocity requires uniform WebGPU");
+        batch.prepare(width, height, cell_size * cell_size, liquid_mixture, gas_mixture);
+        State s = download();
+        const size_t liquids = s.liquid_mass.size();
+        for (const auto& cell : batch.cells)
+        {
+            const size_t i = size_t(cell.y) * width + cell.x;
+            const bool liquid = cell.component < liquids;
+            s.liquid_fraction[i] = liquid ? 1.0 : 0.0;
+            for (auto& m : s.liquid_mass)
+                m[i] = 0.0;
+            for (auto& m : s.gas_mass)
+                m[i] = 0.0;
+            if (liquid)
+                s.liquid_mass[cell.component][i] = cell.mass;
+            else
+                s.gas_mass[cell.component - liquids][i] = cell.mass;
+        }
+        upload(s);
+    }
+
+private:
+    static void check(int status)
+    {
+        if (status == FC_OK)
+            return;
+        const std::string message = fc_last_error();
+        if (status == FC_ERR_INVALID_ARGUMENT)
+            throw std::invalid_argument(message);
+        if (status == FC_ERR_LIFECYCLE)
+            throw std::logic_error(message);
+        throw std::runtime_error(message);
+    }
+
+    fc_grid* live() const
+    {
+        if (!grid)
+            throw std::logic_error("FluidGridCUDA used after destroy()");
+        return grid;
+    }
+
+    static ProjectionResult convert(const fc_result& r)
+    {
+        ProjectionResult out;
+        out.iterations = r.iterations;
+        out.max_divergence = r.max_divergence;
+        out.converged = r.converged != 0;
+        out.physical_steps = r.physical_steps;
+        out.transport_steps = r.transport_steps;
+        out.relaxed = r.relaxed != 0;
+        out.max_volume_error = r.max_volume_error;
+        out.rms_volume_error = r.rms_volume_error;
+        out.viscosity_iterations = r.viscosity_iterations;
+        out.precision_limited = r.precision_limited != 0;
+        return out;
+    }
+
+    fc_grid* grid = nullptr;
+    int width;
+    int height;
+    double cell_size;
+    bl::DVec2 origin{};
+    SubstanceCatalogue substances;
+    FluidMixture liquid_mixture;
+    FluidMixture gas_mixture;
+};
+
+}

@@ -1,0 +1,209 @@
+/*
+ * fluidcuda: C ABI of the UniformCUDA backend for FluidSim's uniform MAC grid (B200, sm_100a).
+ *
+ * This is the drop-in boundary for FluidSim's engine contract fluid::FluidGridBase
+ * (FluidSim/FluidGridBase.h:20-147), reached through FluidGrid::selectBackend
+ * (FluidSim/FluidGrid.cpp:37-90). include/FluidGridCUDA.h wraps these functions into a
+ * FluidGridBase implementation; each entry point below names the reference member it replaces.
+ *
+ * Conventions
+ *  - Every function returns an fc_status code; 0 is success. No C++ exception crosses the ABI.
+ *    fc_last_error() returns a message for the last failure on the calling thread.
+ *  - Host arrays are FP64 in the reference's layouts (FluidSim/FluidGridTypes.h:10-20):
+ *    cell fields are width*height, row-major (index y*width + x); u faces are (width+1)*height
+ *    (index y*(width+1) + x); v faces are width*(height+1) (index y*width + x).
+ *  - A grid owns its device memory and one CUDA stream; calls on one grid come from one thread
+ *    (the reference's simulation-owner rule, FluidGridBase.h:37-39).
+ *  - Device state is converted to the working precision on upload and back to FP64 on download
+ *    (the reference converts the same way, UniformWebGPU/FluidGridWebGPU.cpp:134-137).
+ */
+#ifndef FLUIDCUDA_H
+#define FLUIDCUDA_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FC_ABI_VERSION 1
+
+typedef enum fc_status
+{
+    FC_OK = 0,
+    FC_ERR_INVALID_ARGUMENT = 1, /* the reference throws std::invalid_argument */
+    FC_ERR_LIFECYCLE = 2,        /* std::logic_error: wrong call order (e.g. step before upload) */
+    FC_ERR_CUDA = 3,             /* std::runtime_error: device failure */
+    FC_ERR_OUT_OF_MEMORY = 4,
+    FC_ERR_NONFINITE = 5,
+    FC_ERR_BREAKDOWN = 6,
+    FC_ERR_UNSUPPORTED = 7,
+    FC_ERR_TIMEOUT = 8           /* a device loop hit its iteration cap without finishing */
+} fc_status;
+
+typedef enum fc_precision
+{
+    FC_PRECISION_FP32 = 0,  /* plain FP32 working arrays; FP64 pressure, dots and coarse solve */
+    FC_PRECISION_FP64 = 1,  /* everything FP64: the reference's arithmetic */
+    FC_PRECISION_MIXED = 2  /* FP32 fine level, FP16-stored coarse multigrid levels */
+} fc_precision;
+
+typedef enum fc_preconditioner
+{
+    FC_PRECONDITIONER_DIAGONAL = 0, /* FluidGridCPU::PressurePreconditioner::Diagonal */
+    FC_PRECONDITIONER_MULTIGRID = 1 /* ::Multigrid (default) */
+} fc_preconditioner;
+
+/* Why a pressure solve stopped. */
+typedef enum fc_solve_status
+{
+    FC_SOLVE_RUNNING = 0,
+    FC_SOLVE_CONVERGED = 1,       /* stop rule met on the true residual */
+    FC_SOLVE_ITERATION_LIMIT = 2,
+    FC_SOLVE_STALLED = 3,         /* r.z or d.Ad lost positivity or finiteness */
+    FC_SOLVE_NO_WORK = 4,         /* right-hand side already below tolerance */
+    FC_SOLVE_BREAKDOWN = 5        /* coarsest factorisation failed */
+} fc_solve_status;
+
+/* Mirrors fluid::FluidProjectionResult field for field (FluidSim/FluidGridTypes.h:59-79), then
+ * adds the solver's own measurements. */
+typedef struct fc_result
+{
+    int iterations;
+    double max_divergence; /* max |div u| over cells, 1/s; +inf when non-finite */
+    int converged;         /* max_divergence <= divergence tolerance */
+    int physical_steps;
+    int transport_steps;
+    int relaxed;
+    double max_volume_error;
+    double rms_volume_error;
+    int viscosity_iterations;
+    int precision_limited; /* solve converged; only float velocity rounding exceeds tolerance */
+    /* additions */
+    int solve_status;          /* fc_solve_status */
+    double residual_max;       /* final true residual b - A p, max norm (pressure units) */
+    double residual_l2;        /* its L2 norm */
+    double rhs_l2;             /* L2 norm of the mean-free right-hand side */
+    double divergence_excess;  /* max over cells of |div u| minus its float rounding allowance */
+    double divergence_l2;      /* L2 norm of div u over cells */
+    int restarts;              /* recurrences that drifted and were restarted from b - A p */
+    int kernels;               /* kernels the projection launched on the device */
+} fc_result;
+
+/* Mirrors fluid::FluidStepTimings (FluidSim/FluidGridTypes.h:49-57); milliseconds. */
+typedef struct fc_timings
+{
+    double transport_ms;
+    double viscosity_ms;
+    double forces_ms;
+    double pressure_ms;
+    double selection_ms;
+    double regrid_ms;
+} fc_timings;
+
+typedef struct fc_grid fc_grid;
+typedef struct fc_batch fc_batch;
+
+int fc_abi_version(void);
+const char* fc_last_error(void);
+const char* fc_status_string(int status);
+/* Number of kernels this library has launched in the calling process (a launch counter). */
+long long fc_kernel_launches(void);
+
+/* FluidGridCPU::FluidGridCPU(w, h, cell_size) (UniformCPU/FluidGridCPU.h:63); the device is
+ * the calling thread's current CUDA device. */
+int fc_create(int width, int height, double cell_size, int precision, fc_grid** out);
+/* FluidGridBase::destroy (FluidGridBase.h:129) and the destructor. */
+int fc_destroy(fc_grid* grid);
+
+/* getWidth/getHeight/getCellSize (FluidGridBase.h:31-33). */
+int fc_get_geometry(const fc_grid* grid, int* width, int* height, double* cell_size);
+/* getOrigin/setOrigin (FluidGridBase.h:34-35). */
+int fc_get_origin(const fc_grid* grid, double* x, double* y);
+int fc_set_origin(fc_grid* grid, double x, double y);
+int fc_get_precision(const fc_grid* grid, int* precision);
+
+/* configureMaterials (FluidGridBase.h:42): component densities of the liquid and the gas
+ * mixture, in order. Viscosities may be null (all zero). Must precede fc_upload. */
+int fc_configure_materials(fc_grid* grid, int liquid_count, const double* liquid_densities,
+    const double* liquid_viscosities, int gas_count, const double* gas_densities, const double* gas_viscosities);
+
+/* getGravityY/setGravityY (FluidGridBase.h:70-71). */
+int fc_get_gravity(const fc_grid* grid, double* gravity_y);
+int fc_set_gravity(fc_grid* grid, double gravity_y);
+
+/* FluidGridCPU::pressure_preconditioner (UniformCPU/FluidGridCPU.h:39-44). */
+int fc_set_preconditioner(fc_grid* grid, int preconditioner);
+
+/* Solid obstacle cells (width*height bytes, nonzero = solid; null clears). Their faces close
+ * like the outer walls. No reference counterpart: the reference has only the four walls. */
+int fc_set_obstacles(fc_grid* grid, const unsigned char* solid);
+
+/* upload (FluidGridBase.h:118; FluidGridCPU.cpp:198-254). Null arrays mean zero. liquid_mass
+ * and gas_mass point to one array per configured component (may be null: all zero). */
+int fc_upload(fc_grid* grid, const double* liquid_fraction, const double* u, const double* v, const double* pressure,
+    const double* const* liquid_mass, const double* const* gas_mass);
+/* download (FluidGridBase.h:119). Null outputs are skipped. */
+int fc_download(fc_grid* grid, double* liquid_fraction, double* u, double* v, double* pressure,
+    double* const* liquid_mass, double* const* gas_mass);
+
+/* Device-side copy of the complete physical state and solver history between two grids of
+ * the same geometry, precision and materials (no host traffic). */
+int fc_copy_state(fc_grid* dst, const fc_grid* src);
+
+/* FluidGridCPU::project(dt, max_iterations, tolerance) (FluidGridCPU.cpp:1030-1124): closes the
+ * walls, forms the mean-free divergence, solves the pressure by PCG to the reference's rule
+ * max |r| <= tolerance * dx^2 / dt, updates the face velocities. */
+int fc_project(fc_grid* grid, double dt, int max_iterations, double divergence_tolerance, fc_result* result);
+/* The same projection stopped by the relative rule ||r||_2 <= relative_tolerance * ||b||_2. */
+int fc_project_relative(fc_grid* grid, double dt, int max_iterations, double relative_tolerance, double divergence_tolerance,
+    fc_result* result);
+
+/* step (FluidGridBase.h:133-134): forces (gravity on interior v faces,
+ * FluidGridCPU.cpp:987-996), then the projection. */
+int fc_step(fc_grid* grid, double dt, int max_iterations, double divergence_tolerance, fc_result* result,
+    fc_timings* timings);
+/* FluidGridCPU::applyGravity (FluidGridCPU.cpp:987-996). */
+int fc_apply_gravity(fc_grid* grid, double dt);
+
+/* maxDivergence (FluidGridBase.h:135; FluidGridCPU.cpp:1126-1152). */
+int fc_max_divergence(fc_grid* grid, double* out);
+
+/* Cell classes from the reference thresholds (liquid f > 0.5, FluidGridCPU.cpp:1321-1322;
+ * interface 0 < f < 1, FluidGridCPU.cpp:531-533) and the obstacle mask: bit 1 liquid,
+ * bit 2 interface, bit 4 solid (a solid cell carries only bit 4). width*height bytes. */
+int fc_classify(fc_grid* grid, unsigned char* mask);
+
+/* One application of the grid's pressure preconditioner to `residual` (width*height, minus
+ * residual_mean), as PressureMultigrid::apply (UniformCPU/PressureMultigrid.h:43,
+ * PressureMultigrid.cpp:410-434) or the diagonal (FluidGridCPU.cpp:1691-1698). The correction
+ * keeps its constant component, like the reference's apply. Rebuilds coefficients if needed. */
+int fc_apply_preconditioner(fc_grid* grid, const double* residual, double residual_mean, double* correction);
+
+/* Times one kernel of the projection with CUDA events on the grid's stream, on the grid's
+ * current data, and returns the mean duration of `repeats` launches in milliseconds. Kernels:
+ * 0 fine-level pre-smoothing + restriction, 1 fine-level prolongation + post-smoothing,
+ * 2 direction update + operator, 3 coarse tail. They write only solver scratch (the multigrid
+ * levels, z, d, q), so the physical state is unchanged. Profiling aid. */
+int fc_time_kernel(fc_grid* grid, int kernel, int repeats, double* mean_ms);
+
+/* Device pointers of the face velocities (working precision), for zero-copy producers. */
+int fc_velocity_pointers(fc_grid* grid, void** u, void** v);
+/* The grid's stream (cudaStream_t) and a wait for all of its work. */
+int fc_get_stream(const fc_grid* grid, void** stream);
+int fc_synchronize(fc_grid* grid);
+
+/* Batched projection: many independent grids of one precision, uneven sizes allowed, solved
+ * together (one launch per kernel for all grids; per-grid convergence). No reference
+ * counterpart: the reference steps scenes one after another (FluidSim.cpp:90-93, 120-131). */
+int fc_batch_create(fc_grid* const* grids, int count, fc_batch** out);
+int fc_batch_destroy(fc_batch* batch);
+/* dts: one time step per grid. relative_tolerance > 0 selects the relative rule. */
+int fc_batch_project(fc_batch* batch, const double* dts, int max_iterations, double divergence_tolerance,
+    double relative_tolerance, fc_result* results);
+int fc_batch_get_stream(const fc_batch* batch, void** stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -63,6 +63,20 @@ void or_coefficients(int w, int h, const double* rho, double* inv_u, double* inv
     }
 }
 
+/* Inverse diagonal from face weights (the second pass of FluidGridCPU.cpp:1188-1202). */
+void or_diagonal(int w, int h, const double* inv_u, const double* inv_v, double* inv_diagonal)
+{
+    for (int y = 0; y < h; ++y)
+    {
+        for (int x = 0; x < w; ++x)
+        {
+            const double sum = inv_u[(size_t)y * (w + 1) + x] + inv_u[(size_t)y * (w + 1) + x + 1] +
+                               inv_v[(size_t)y * w + x] + inv_v[(size_t)(y + 1) * w + x];
+            inv_diagonal[(size_t)y * w + x] = sum > 0.0 ? 1.0 / sum : 0.0;
+        }
+    }
+}
+
 /* Solid obstacle cells close their four faces, as the reference closes its outer walls
  * (FluidGridCPU.cpp:1170-1185). No reference counterpart: the reference has no obstacles. */
 void or_face_flags(int w, int h, const unsigned char* solid, double* inv_u, double* inv_v)
@@ -187,7 +201,9 @@ struct or_mg
 {
     int count;
     or_level* lev;
-    int n;          /* coarsest unknowns: cells - 1 (cell 0 pinned) */
+    int n;          /* coarsest unknowns: open cells - 1 (one pinned) */
+    int pinned;     /* the pinned cell, -1 when no cell is open */
+    int* map;       /* coarsest cell -> unknown index, -1 when pinned or closed */
     double* factor; /* dense n x n Cholesky factor, lower triangle */
     double* work;
 };
@@ -286,9 +302,11 @@ or_mg* or_mg_create(int width, int height)
         build_axis(f->h, f->cy, c->h, c->cy, f->py, f->ry);
     }
     const or_level* last = &mg->lev[count - 1];
-    mg->n = last->w * last->h - 1;
-    mg->factor = (double*)calloc((size_t)(mg->n > 0 ? mg->n : 1) * (mg->n > 0 ? mg->n : 1), sizeof(double));
-    mg->work = (double*)calloc(mg->n > 0 ? mg->n : 1, sizeof(double));
+    const int cells = last->w * last->h;
+    mg->n = cells - 1;
+    mg->map = (int*)calloc(cells, sizeof(int));
+    mg->factor = (double*)calloc((size_t)cells * cells, sizeof(double));
+    mg->work = (double*)calloc(cells, sizeof(double));
     return mg;
 }
 
@@ -303,6 +321,7 @@ void or_mg_destroy(or_mg* mg)
         free(l->cx), free(l->cy), free(l->px), free(l->py), free(l->rx), free(l->ry);
     }
     free(mg->lev);
+    free(mg->map);
     free(mg->factor);
     free(mg->work);
     free(mg);
@@ -372,26 +391,48 @@ static void level_coarsen(const or_level* f, or_level* c)
     level_diagonal(c);
 }
 
-/* Dense Cholesky of the coarsest operator with cell 0 pinned to zero.
- * PressureMultigrid.cpp:300-345 (factorCoarsest). Returns 0 on a non-positive pivot. */
+/* Dense Cholesky of the coarsest operator with one cell pinned to zero.
+ * PressureMultigrid.cpp:300-345 (factorCoarsest). The reference pins cell 0; here the pinned
+ * cell is the first cell with an open face and cells without one (inside obstacles) are left
+ * out of the system, which is the same system when no cell is closed. Returns 0 on a
+ * non-positive pivot. */
 static int factor_coarsest(or_mg* mg)
 {
     const or_level* l = &mg->lev[mg->count - 1];
-    const int n = mg->n;
+    const int cells = l->w * l->h;
+    int* map = mg->map;
+    int n = 0;
+    mg->pinned = -1;
+    for (int cell = 0; cell < cells; ++cell)
+    {
+        const int x = cell % l->w, y = cell / l->w;
+        const int i = (y + 1) * l->s + x + 1;
+        const double diag = l->right[i - 1] + l->right[i] + l->down[i - l->s] + l->down[i];
+        map[cell] = -1;
+        if (!(diag > 0.0))
+            continue;
+        if (mg->pinned < 0)
+            mg->pinned = cell;
+        else
+            map[cell] = n++;
+    }
+    mg->n = n;
     double* a = mg->factor;
     if (n <= 0)
         return 1;
     memset(a, 0, sizeof(double) * (size_t)n * n);
-    for (int cell = 1; cell <= n; ++cell)
+    for (int cell = 0; cell < cells; ++cell)
     {
+        const int row = map[cell];
+        if (row < 0)
+            continue;
         const int x = cell % l->w, y = cell / l->w;
         const int i = (y + 1) * l->s + x + 1;
-        const int row = cell - 1;
         a[row * n + row] = l->right[i - 1] + l->right[i] + l->down[i - l->s] + l->down[i];
-        if (x > 0 && cell - 1 > 0)
-            a[row * n + row - 1] = -l->right[i - 1];
-        if (y > 0 && cell - l->w > 0)
-            a[row * n + row - l->w] = -l->down[i - l->s];
+        if (x > 0 && map[cell - 1] >= 0)
+            a[row * n + map[cell - 1]] = -l->right[i - 1];
+        if (y > 0 && map[cell - l->w] >= 0)
+            a[row * n + map[cell - l->w]] = -l->down[i - l->s];
     }
     for (int row = 0; row < n; ++row)
     {
@@ -469,7 +510,9 @@ static void level_restrict(or_level* f, or_level* c)
             const double center = f->sol[i];
             const double product = (f->right[i - 1] * (center - f->sol[i - 1]) + f->right[i] * (center - f->sol[i + 1])) +
                                    (f->down[i - s] * (center - f->sol[i - s]) + f->down[i] * (center - f->sol[i + s]));
-            f->res[i] = f->rhs[i] - product;
+            /* A cell without an open face (possible only inside obstacles) passes no residual
+             * down, which keeps the cycle symmetric; otherwise this is the reference's residual. */
+            f->res[i] = f->invd[i] > 0.0 ? f->rhs[i] - product : 0.0;
         }
     }
     for (int y = 0; y < c->h; ++y)
@@ -512,21 +555,32 @@ static void level_prolong(const or_level* c, or_level* f)
 }
 
 /* Forward/back substitution on the mean-free coarse rhs, then a mean-zero gauge.
- * PressureMultigrid.cpp:347-384 (solveCoarsest). */
+ * PressureMultigrid.cpp:347-384 (solveCoarsest); means run over the open cells. */
 static void solve_coarsest(or_mg* mg)
 {
     or_level* l = &mg->lev[mg->count - 1];
-    const int n = mg->n;
+    const int n = mg->n, cells = l->w * l->h;
     const double* a = mg->factor;
     double* z = mg->work;
     double mean = 0.0;
-    for (int y = 0; y < l->h; ++y)
-        for (int x = 0; x < l->w; ++x)
-            mean += l->rhs[(y + 1) * l->s + x + 1];
-    mean /= n + 1;
-    for (int row = 0; row < n; ++row)
+    int open = 0;
+    for (int cell = 0; cell < cells; ++cell)
     {
-        const int cell = row + 1;
+        if (cell != mg->pinned && mg->map[cell] < 0)
+            continue;
+        mean += l->rhs[(cell / l->w + 1) * l->s + cell % l->w + 1];
+        ++open;
+    }
+    for (int cell = 0; cell < cells; ++cell)
+        l->sol[(cell / l->w + 1) * l->s + cell % l->w + 1] = 0.0;
+    if (open == 0)
+        return;
+    mean /= open;
+    for (int cell = 0; cell < cells; ++cell)
+    {
+        const int row = mg->map[cell];
+        if (row < 0)
+            continue;
         double value = l->rhs[(cell / l->w + 1) * l->s + cell % l->w + 1] - mean;
         for (int col = 0; col < row; ++col)
             value -= a[row * n + col] * z[col];
@@ -542,10 +596,11 @@ static void solve_coarsest(or_mg* mg)
     double sum = 0.0;
     for (int k = 0; k < n; ++k)
         sum += z[k];
-    mean = sum / (n + 1);
-    l->sol[l->s + 1] = -mean;
-    for (int cell = 1; cell <= n; ++cell)
-        l->sol[(cell / l->w + 1) * l->s + cell % l->w + 1] = z[cell - 1] - mean;
+    mean = sum / open;
+    l->sol[(mg->pinned / l->w + 1) * l->s + mg->pinned % l->w + 1] = -mean;
+    for (int cell = 0; cell < cells; ++cell)
+        if (mg->map[cell] >= 0)
+            l->sol[(cell / l->w + 1) * l->s + cell % l->w + 1] = z[mg->map[cell]] - mean;
 }
 
 /* Four pre-sweeps (the first from zero), restrict, recurse, prolong, four post-sweeps in the
@@ -573,9 +628,14 @@ static void mg_cycle(or_mg* mg, int index)
 void or_mg_apply(or_mg* mg, const double* residual, double* correction, double residual_mean)
 {
     or_level* f = &mg->lev[0];
+    /* Cells without an open face (inside obstacles) take no part; with none closed this is
+     * the reference's rhs = residual - mean. */
     for (int y = 0; y < f->h; ++y)
         for (int x = 0; x < f->w; ++x)
-            f->rhs[(y + 1) * f->s + x + 1] = residual[y * f->w + x] - residual_mean;
+        {
+            const int i = (y + 1) * f->s + x + 1;
+            f->rhs[i] = f->invd[i] > 0.0 ? residual[y * f->w + x] - residual_mean : 0.0;
+        }
     mg_cycle(mg, 0);
     for (int y = 0; y < f->h; ++y)
         memcpy(correction + (size_t)y * f->w, f->sol + (size_t)(y + 1) * f->s + 1, sizeof(double) * f->w);
@@ -588,6 +648,8 @@ void or_mg_apply(or_mg* mg, const double* residual, double* correction, double r
 struct or_grid
 {
     int w, h, n;
+    int open;              /* cells outside obstacles */
+    unsigned char* solid;  /* obstacle mask or NULL (no reference counterpart) */
     double dx;
     int preconditioner;
     double *density, *u, *v, *p, *p_prev;
@@ -604,6 +666,7 @@ or_grid* or_grid_create(int width, int height, double cell_size)
     g->h = height;
     g->n = width * height;
     g->dx = cell_size;
+    g->open = g->n;
     g->preconditioner = OR_PRECONDITIONER_MULTIGRID;
     const size_t n = (size_t)g->n, nu = (size_t)(width + 1) * height, nv = (size_t)width * (height + 1);
     g->density = (double*)calloc(n, sizeof(double));
@@ -621,10 +684,32 @@ or_grid* or_grid_create(int width, int height, double cell_size)
     return g;
 }
 
+void or_grid_set_solid(or_grid* g, const unsigned char* solid)
+{
+    free(g->solid);
+    g->solid = NULL;
+    g->open = g->n;
+    if (solid)
+    {
+        g->solid = (unsigned char*)malloc((size_t)g->n);
+        g->open = 0;
+        for (int i = 0; i < g->n; ++i)
+        {
+            g->solid[i] = solid[i] ? 1 : 0;
+            g->open += !g->solid[i];
+        }
+    }
+    or_coefficients(g->w, g->h, g->density, g->inv_u, g->inv_v, g->inv_diag);
+    or_face_flags(g->w, g->h, g->solid, g->inv_u, g->inv_v);
+    or_diagonal(g->w, g->h, g->inv_u, g->inv_v, g->inv_diag);
+    g->mg_valid = 0;
+}
+
 void or_grid_destroy(or_grid* g)
 {
     if (!g)
         return;
+    free(g->solid);
     free(g->density), free(g->u), free(g->v), free(g->p), free(g->p_prev);
     free(g->inv_u), free(g->inv_v), free(g->inv_diag);
     free(g->b), free(g->r), free(g->z), free(g->d), free(g->q);
@@ -656,6 +741,11 @@ void or_grid_upload(or_grid* g, const double* density, const double* u, const do
         memset(g->p, 0, n * sizeof(double));
     memcpy(g->p_prev, g->p, n * sizeof(double));
     or_coefficients(g->w, g->h, g->density, g->inv_u, g->inv_v, g->inv_diag);
+    if (g->solid)
+    {
+        or_face_flags(g->w, g->h, g->solid, g->inv_u, g->inv_v);
+        or_diagonal(g->w, g->h, g->inv_u, g->inv_v, g->inv_diag);
+    }
     g->mg_valid = 0;
 }
 
@@ -684,12 +774,16 @@ static double sum_of(const double* x, int n)
     return s;
 }
 
-/* FluidGridCPU.cpp:1466-1474 (removeMean). */
-static void remove_mean(double* x, int n)
+/* FluidGridCPU.cpp:1466-1474 (removeMean); obstacle cells are held at zero and excluded. */
+static void remove_mean(const or_grid* g, double* x)
 {
-    const double mean = sum_of(x, n) / n;
-    for (int i = 0; i < n; ++i)
-        x[i] -= mean;
+    double sum = 0.0;
+    for (int i = 0; i < g->n; ++i)
+        if (!g->solid || !g->solid[i])
+            sum += x[i];
+    const double mean = sum / g->open;
+    for (int i = 0; i < g->n; ++i)
+        x[i] = (g->solid && g->solid[i]) ? 0.0 : x[i] - mean;
 }
 
 typedef struct
@@ -730,11 +824,15 @@ static double precondition(or_grid* g, double residual_mean)
     else
         for (int i = 0; i < g->n; ++i)
             g->z[i] = (g->r[i] - residual_mean) * g->inv_diag[i];
-    const double mean = sum_of(g->z, g->n) / g->n;
+    double zsum = 0.0;
+    for (int i = 0; i < g->n; ++i)
+        if (!g->solid || !g->solid[i])
+            zsum += g->z[i];
+    const double mean = zsum / g->open;
     double dot = 0.0;
     for (int i = 0; i < g->n; ++i)
     {
-        g->z[i] -= mean;
+        g->z[i] = (g->solid && g->solid[i]) ? 0.0 : g->z[i] - mean;
         dot += g->r[i] * g->z[i];
     }
     return dot;
@@ -769,7 +867,7 @@ static int solve_pressure(or_grid* g, int max_iterations, double tol_max, double
         g->p[i] = 2.0 * latest - g->p_prev[i];
         g->p_prev[i] = latest;
     }
-    remove_mean(g->p, n);
+    remove_mean(g, g->p);
     or_stats initial = true_residual(g);
     if (met(initial, tol_max, tol_sumsq) || max_iterations == 0)
         return 0;
@@ -779,7 +877,7 @@ static int solve_pressure(or_grid* g, int max_iterations, double tol_max, double
         if (!g->mg_valid)
             return -1;
     }
-    double residual_mean = initial.sum / n;
+    double residual_mean = initial.sum / g->open;
     double rz = precondition(g, residual_mean);
     memcpy(g->d, g->z, n * sizeof(double));
     int iterations = 0;
@@ -797,7 +895,7 @@ static int solve_pressure(or_grid* g, int max_iterations, double tol_max, double
             g->r[i] -= alpha * g->q[i];
         }
         or_stats s = stats_of(g->r, n);
-        residual_mean = s.sum / n;
+        residual_mean = s.sum / g->open;
         ++iterations;
         int restart = 0;
         if (met(s, tol_max, tol_sumsq))
@@ -805,7 +903,7 @@ static int solve_pressure(or_grid* g, int max_iterations, double tol_max, double
             const or_stats actual = true_residual(g);
             if (met(actual, tol_max, tol_sumsq))
                 break;
-            residual_mean = actual.sum / n;
+            residual_mean = actual.sum / g->open;
             restart = 1;
         }
         const double next = precondition(g, residual_mean);
@@ -816,7 +914,7 @@ static int solve_pressure(or_grid* g, int max_iterations, double tol_max, double
             g->d[i] = g->z[i] + beta * g->d[i];
         rz = next;
     }
-    remove_mean(g->p, n);
+    remove_mean(g, g->p);
     return iterations;
 }
 
@@ -849,8 +947,21 @@ or_result or_grid_project(
         return result;
     const int w = g->w, h = g->h, n = g->n;
     const double scale = g->dx * g->dx / dt;
+    if (g->solid)
+    {
+        /* Faces of obstacle cells close like walls (no reference counterpart). */
+        for (int y = 0; y < h; ++y)
+            for (int x = 0; x < w; ++x)
+                if (g->solid[y * w + x])
+                {
+                    g->u[(size_t)y * (w + 1) + x] = 0.0;
+                    g->u[(size_t)y * (w + 1) + x + 1] = 0.0;
+                    g->v[(size_t)y * w + x] = 0.0;
+                    g->v[(size_t)(y + 1) * w + x] = 0.0;
+                }
+    }
     or_rhs(w, h, g->dx, dt, g->u, g->v, g->b);
-    remove_mean(g->b, n);
+    remove_mean(g, g->b);
     double bsq = 0.0;
     for (int i = 0; i < n; ++i)
         bsq += g->b[i] * g->b[i];

@@ -36,6 +36,9 @@ enum { OR_PRECONDITIONER_DIAGONAL = 0, OR_PRECONDITIONER_MULTIGRID = 1 };
 or_grid* or_grid_create(int width, int height, double cell_size);
 void or_grid_destroy(or_grid* grid);
 void or_grid_set_preconditioner(or_grid* grid, int which);
+/* Solid obstacle cells (no reference counterpart): their faces close like walls and they are
+ * excluded from every mean. NULL clears. Call after upload (it rebuilds the coefficients). */
+void or_grid_set_solid(or_grid* grid, const unsigned char* solid);
 
 /* Upload: density per cell, face velocities and pressure (null = zero). Resets the warm-start
  * history to the uploaded pressure, like FluidGridCPU::upload. */
@@ -55,6 +58,7 @@ double or_grid_max_divergence(const or_grid* grid);
 /* Stand-alone pieces, used by the unit tests. */
 void or_density(int cells, int components, const double* const* masses, double cell_size, double* density);
 void or_coefficients(int width, int height, const double* density, double* inv_u, double* inv_v, double* inv_diagonal);
+void or_diagonal(int width, int height, const double* inv_u, const double* inv_v, double* inv_diagonal);
 double or_operator(int width, int height, const double* inv_u, const double* inv_v, const double* x, double* y);
 void or_rhs(int width, int height, double cell_size, double dt, double* u, double* v, double* rhs);
 void or_face_flags(int width, int height, const unsigned char* solid, double* inv_u, double* inv_v);

@@ -77,6 +77,7 @@ def lib():
         L.or_grid_create.argtypes = [C.c_int, C.c_int, C.c_double]
         L.or_grid_destroy.argtypes = [C.c_void_p]
         L.or_grid_set_preconditioner.argtypes = [C.c_void_p, C.c_int]
+        L.or_grid_set_solid.argtypes = [C.c_void_p, _u8p]
         L.or_grid_upload.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp]
         L.or_grid_download.argtypes = [C.c_void_p, _dp, _dp, _dp]
         L.or_grid_apply_gravity.argtypes = [C.c_void_p, C.c_double, C.c_double]
@@ -216,8 +217,11 @@ class OracleGrid:
     def set_preconditioner(self, multigrid: bool):
         lib().or_grid_set_preconditioner(self.handle, 1 if multigrid else 0)
 
-    def upload(self, density, u, v, pressure=None):
+    def upload(self, density, u, v, pressure=None, solid=None):
         lib().or_grid_upload(self.handle, _ptr(_f64(density)), _ptr(_f64(u)), _ptr(_f64(v)), _ptr(_f64(pressure)))
+        if solid is not None:
+            s = np.ascontiguousarray(solid, dtype=np.uint8)
+            lib().or_grid_set_solid(self.handle, s.ctypes.data_as(_u8p))
 
     def download(self):
         u = np.zeros((self.h, self.w + 1))

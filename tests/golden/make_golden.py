@@ -1,0 +1,88 @@
+"""Generates the golden fixtures of the projection from the reference engine itself.
+
+Runs FluidSim's own UniformCPU code (FluidSim/UniformCPU/FluidGridCPU.cpp and
+PressureMultigrid.cpp, compiled from the reference sources into oracle/_ref/libfluidref.so by
+oracle/Makefile) on seeded inputs and stores inputs and outputs as .npz files next to this
+script. Needs the reference checkout, so it runs only where that exists:
+
+    make -C oracle && python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle import oracle as O  # noqa: E402
+from fluidsim_b200 import scenes  # noqa: E402
+
+
+def projection_case(name, scene, max_iterations, tolerance, preconditioner="multigrid"):
+    g = O.ReferenceGrid(scene.width, scene.height, scene.cell_size, scene.liquid_density, scene.gas_density)
+    g.set_preconditioner(preconditioner == "multigrid")
+    g.upload(scene.fraction, scene.u, scene.v, None, scene.liquid_mass[0], scene.gas_mass[0])
+    # Inputs that are exact in FP32 (the seeded scenes) are stored in FP32.
+    exact32 = all(np.array_equal(a.astype(np.float32).astype(np.float64), a) for a in (scene.u, scene.v))
+    store = (lambda a: a.astype(np.float32)) if exact32 else (lambda a: a)
+    r = g.project(scene.dt, max_iterations, tolerance)
+    _, u, v, p = g.download()
+    inv_u, inv_v, inv_d = g.coefficients()
+    np.savez_compressed(
+        os.path.join(HERE, f"project_{name}.npz"),
+        width=scene.width, height=scene.height, cell_size=scene.cell_size, dt=scene.dt,
+        liquid_density=scene.liquid_density, gas_density=scene.gas_density,
+        fraction=scene.fraction, u_in=store(scene.u), v_in=store(scene.v),
+        max_iterations=max_iterations, tolerance=tolerance, preconditioner=preconditioner,
+        iterations=r.iterations, converged=r.converged, max_divergence=r.max_divergence,
+        u=u, v=v, p=p, inv_u=inv_u, inv_v=inv_v, inv_diagonal=inv_d)
+    print(name, scene.width, scene.height, "iterations", r.iterations, "maxdiv", r.max_divergence)
+
+
+def multigrid_case(name, w, h):
+    """The reference test's checkerboard densities (tests/FluidGridTests.cpp:538-625)."""
+    y, x = np.mgrid[0:h, 0:w]
+    density = np.where(((x // 3 + y // 4) % 2) == 0, 0.1, 100.0)
+    inv_u, inv_v, _ = O.coefficients(density)
+    i = np.arange(w * h)
+    a = (np.sin(i * 0.31) + np.cos(i * 0.073)).reshape(h, w)
+    a -= a.mean()
+    z = O.reference_mg_apply(inv_u, inv_v, a, 0.0)
+    np.savez_compressed(os.path.join(HERE, f"multigrid_{name}.npz"), width=w, height=h, density=density,
+                        residual=a, correction=z)
+    print(name, w, h, "levels", O.Multigrid(w, h).levels)
+
+
+def hydrostatic_case():
+    """A full tank after one step with gravity (tests/FluidGridTests.cpp:140-160)."""
+    w, h, dx = 12, 10, 2.0
+    g = O.ReferenceGrid(w, h, dx, 100.0, 0.1)
+    f = np.ones((h, w))
+    g.upload(f, None, None, None, 100.0 * f * dx * dx, 0.1 * (1 - f) * dx * dx)
+    r = g.step(1.0 / 120.0, 2000, 1e-8)
+    _, u, v, p = g.download()
+    np.savez_compressed(os.path.join(HERE, "hydrostatic_12x10.npz"), width=w, height=h, cell_size=dx,
+                        dt=1.0 / 120.0, gravity=100.0, liquid_density=100.0, gas_density=0.1,
+                        iterations=r.iterations, converged=r.converged, u=u, v=v, p=p)
+    print("hydrostatic", r.iterations, "rise", p[h - 1, 0] - p[0, 0])
+
+
+def main():
+    O.build(reference=True)
+    O.set_reference_threads(1)
+    projection_case("box128", scenes.liquid_box(128, 128, seed=0), 200, 1e-6)
+    for (w, h) in [(13, 9), (65, 37), (2, 67), (1, 129), (131, 1)]:
+        projection_case(f"sloped{w}x{h}", scenes.sloped_pool(w, h), 4000, 1e-8)
+    projection_case("sloped65x37_diagonal", scenes.sloped_pool(65, 37), 4000, 1e-8, preconditioner="diagonal")
+    projection_case("pool64x48", scenes.random_pool(64, 48, seed=3, fill=0.6, cell_size=1.0 / 64), 200, 1e-6)
+    for (w, h) in [(1, 1), (13, 9), (65, 37)]:
+        multigrid_case(f"{w}x{h}", w, h)
+    hydrostatic_case()
+
+
+if __name__ == "__main__":
+    main()

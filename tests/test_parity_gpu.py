@@ -1,0 +1,301 @@
+"""Parity of the CUDA projection (through the C ABI) with the oracle.
+
+FP64 device arithmetic is compared tightly with the reference's fixtures and the C restatement;
+the FP32 drop-in is compared within stated tolerances. Tolerances are written in each test.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, golden
+from fluidsim_b200 import FluidGrid, FluidGridState, ProjectionBatch, scenes
+from fluidsim_b200 import FluidInvalidArgument, FluidLifecycleError, FluidCudaError
+
+pytestmark = pytest.mark.gpu
+
+FIXTURES = sorted(glob.glob(os.path.join(GOLDEN, "project_*.npz")))
+
+
+def fixture_scene(d):
+    w, h = int(d["width"]), int(d["height"])
+    s = scenes.Scene(w, h, float(d["cell_size"]), float(d["dt"]), float(d["liquid_density"]),
+                     float(d["gas_density"]), d["fraction"], d["u_in"].astype(np.float64), d["v_in"].astype(np.float64))
+    return s
+
+
+def gpu_grid(scene, precision="fp64", preconditioner="multigrid"):
+    g = FluidGrid(scene.width, scene.height, scene.cell_size, precision)
+    g.setPreconditioner(preconditioner)
+    scenes.upload_scene(g, scene)
+    return g
+
+
+def oracle_grid(oracle, scene, preconditioner="multigrid"):
+    g = oracle.OracleGrid(scene.width, scene.height, scene.cell_size)
+    g.set_preconditioner(preconditioner == "multigrid")
+    g.upload(scene.density(), scene.u, scene.v, None, solid=scene.solid)
+    return g
+
+
+def rel_err(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+# ---------------------------------------------------------------------------------------------
+# Golden fixtures made by the reference engine
+# ---------------------------------------------------------------------------------------------
+
+@pytest.mark.parametrize("path", FIXTURES, ids=os.path.basename)
+def test_fp64_matches_reference_fixture(path):
+    d = golden(os.path.basename(path))
+    s = fixture_scene(d)
+    g = gpu_grid(s, "fp64", str(d["preconditioner"]))
+    r = g.project(s.dt, int(d["max_iterations"]), float(d["tolerance"]))
+    out = g.download()
+    # Same algorithm in FP64; only reduction order differs. Tolerances: iterations within one,
+    # velocities 1e-8 of their scale, pressure 1e-8 relative.
+    assert abs(r.iterations - int(d["iterations"])) <= 1, (r.iterations, int(d["iterations"]))
+    assert r.converged == bool(d["converged"])
+    scale = max(1.0, np.abs(d["u"]).max(), np.abs(d["v"]).max())
+    assert np.abs(out.u - d["u"]).max() <= 1e-8 * scale
+    assert np.abs(out.v - d["v"]).max() <= 1e-8 * scale
+    assert rel_err(out.pressure, d["p"]) <= 1e-8
+
+
+@pytest.mark.parametrize("path", FIXTURES, ids=os.path.basename)
+def test_fp32_matches_reference_fixture(path):
+    d = golden(os.path.basename(path))
+    s = fixture_scene(d)
+    g = gpu_grid(s, "fp32", str(d["preconditioner"]))
+    r = g.project(s.dt, 4000, float(d["tolerance"]), relative_tolerance=1e-6)
+    out = g.download()
+    # FP32 working arrays solved to ||r|| <= 1e-6 ||b||: velocities within 1e-4 of their
+    # scale of the FP64 reference (the reference's own FP32-vs-FP64 precedent is 5e-3 absolute,
+    # tests/FluidGridWebGPUTests.cpp:270-305), pressure within 1e-4 relative.
+    assert r.solve_status in ("converged", "no_work")
+    assert r.residual_l2 <= 1e-6 * r.rhs_l2 * 1.0001 or r.solve_status == "no_work"
+    scale = max(1.0, np.abs(d["u"]).max(), np.abs(d["v"]).max())
+    assert np.abs(out.u - d["u"]).max() <= 1e-4 * scale
+    assert np.abs(out.v - d["v"]).max() <= 1e-4 * scale
+    assert rel_err(out.pressure, d["p"]) <= 1e-4
+
+
+@pytest.mark.parametrize("name", ["1x1", "13x9", "65x37"])
+def test_multigrid_apply_matches_reference_fixture(name):
+    d = golden(f"multigrid_{name}.npz")
+    w, h = int(d["width"]), int(d["height"])
+    density = d["density"]
+    s = scenes.Scene(w, h, 1.0, 1.0, 1.0, 1.0, np.ones((h, w)), np.zeros((h, w + 1)), np.zeros((h + 1, w)),
+                     liquid_mass=[density], gas_mass=[np.zeros((h, w))])
+    g = gpu_grid(s, "fp64")
+    z = g.applyPreconditioner(d["residual"], 0.0)
+    assert np.abs(z - d["correction"]).max() <= 1e-11 * max(1.0, np.abs(d["correction"]).max())
+
+
+# ---------------------------------------------------------------------------------------------
+# Seeded scenes against the C restatement
+# ---------------------------------------------------------------------------------------------
+
+SIZES = [(13, 9), (64, 64), (65, 37), (100, 70), (129, 65), (1, 129), (2, 67), (257, 193), (333, 251)]
+
+
+@pytest.mark.parametrize("size", SIZES)
+def test_fp64_matches_restatement(oracle, size):
+    w, h = size
+    s = scenes.random_pool(w, h, seed=w * 31 + h, fill=0.55, cell_size=1.0 / max(w, h))
+    o = oracle_grid(oracle, s)
+    ro = o.project(s.dt, 300, 1e-6)
+    uo, vo, po = o.download()
+    g = gpu_grid(s, "fp64")
+    r = g.project(s.dt, 300, 1e-6)
+    out = g.download()
+    # Reduction order differs from the host's, which can move a restart-on-drift by an
+    # iteration or two near the max-norm threshold; the solutions agree regardless.
+    assert abs(r.iterations - ro.iterations) <= 3
+    assert r.converged == ro.converged
+    scale = max(1.0, np.abs(uo).max(), np.abs(vo).max())
+    assert np.abs(out.u - uo).max() <= 1e-8 * scale
+    assert np.abs(out.v - vo).max() <= 1e-8 * scale
+    assert rel_err(out.pressure, po) <= 1e-7
+
+
+@pytest.mark.parametrize("size", [(64, 64), (129, 65), (257, 193), (333, 251)])
+def test_fp32_matches_restatement(oracle, size):
+    w, h = size
+    s = scenes.random_pool(w, h, seed=w * 17 + h, fill=0.55, cell_size=1.0 / max(w, h))
+    o = oracle_grid(oracle, s)
+    o.project(s.dt, 500, 1e-12, relative_tolerance=1e-12)
+    uo, vo, po = o.download()
+    g = gpu_grid(s, "fp32")
+    r = g.project(s.dt, 500, 1e-6, relative_tolerance=1e-6)
+    out = g.download()
+    assert r.solve_status == "converged"
+    assert r.residual_l2 <= 1.0001e-6 * r.rhs_l2
+    scale = max(np.abs(uo).max(), np.abs(vo).max())
+    # FP32 at a 1e-6 relative residual against the FP64 solution at 1e-12: 1e-4 of the velocity scale.
+    assert np.abs(out.u - uo).max() <= 1e-4 * scale
+    assert np.abs(out.v - vo).max() <= 1e-4 * scale
+    assert rel_err(out.pressure, po) <= 1e-4
+
+
+def test_diagonal_preconditioner_fp64(oracle):
+    s = scenes.random_pool(48, 40, seed=9, fill=0.5, cell_size=1.0 / 48)
+    o = oracle_grid(oracle, s, "diagonal")
+    ro = o.project(s.dt, 2000, 1e-7)
+    uo, vo, po = o.download()
+    g = gpu_grid(s, "fp64", "diagonal")
+    r = g.project(s.dt, 2000, 1e-7)
+    out = g.download()
+    assert abs(r.iterations - ro.iterations) <= 2
+    assert np.abs(out.u - uo).max() <= 1e-8 * max(1.0, np.abs(uo).max())
+
+
+def test_obstacles_fp64_match_restatement(oracle):
+    s = scenes.random_pool(150, 110, seed=11, fill=0.6, obstacles=6, cell_size=1.0 / 150)
+    o = oracle_grid(oracle, s)
+    ro = o.project(s.dt, 500, 1e-7)
+    uo, vo, po = o.download()
+    g = gpu_grid(s, "fp64")
+    r = g.project(s.dt, 500, 1e-7)
+    out = g.download()
+    assert ro.converged and r.converged
+    assert abs(r.iterations - ro.iterations) <= 1
+    assert np.abs(out.u - uo).max() <= 1e-8 * max(1.0, np.abs(uo).max())
+    assert np.abs(out.v - vo).max() <= 1e-8 * max(1.0, np.abs(vo).max())
+    assert np.all(out.pressure[s.solid != 0] == 0.0)
+
+
+def test_classification_bit_exact(oracle):
+    rng = np.random.default_rng(4)
+    w, h = 77, 53
+    f = rng.uniform(-0.2, 1.2, (h, w)).clip(0.0, 1.0)
+    f.flat[:8] = [0.0, 1.0, 0.5, np.nextafter(0.5, 1), np.nextafter(0.5, 0), 1e-300, np.nextafter(1.0, 0), 0.25]
+    solid = (rng.uniform(size=(h, w)) < 0.1).astype(np.uint8)
+    s = scenes.Scene(w, h, 1.0, 1.0, 1.0, 0.001, f, np.zeros((h, w + 1)), np.zeros((h + 1, w)), solid=solid)
+    g = gpu_grid(s, "fp32")
+    assert np.array_equal(g.classify(), oracle.classify(f, solid))
+
+
+# ---------------------------------------------------------------------------------------------
+# Multigrid contract on the device (FluidGridTests.cpp:538-625)
+# ---------------------------------------------------------------------------------------------
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-10), ("fp32", 5e-4)])
+@pytest.mark.parametrize("size", [(1, 1), (1, 129), (131, 1), (2, 67), (13, 9), (64, 64), (65, 37), (512, 512)])
+def test_multigrid_contract(precision, tol, size):
+    w, h = size
+    y, x = np.mgrid[0:h, 0:w]
+    density = np.where(((x // 3 + y // 4) % 2) == 0, 0.1, 100.0)
+    s = scenes.Scene(w, h, 1.0, 1.0, 1.0, 1.0, np.ones((h, w)), np.zeros((h, w + 1)), np.zeros((h + 1, w)),
+                     liquid_mass=[density], gas_mass=[np.zeros((h, w))])
+    g = gpu_grid(s, precision)
+    i = np.arange(w * h)
+    a = (np.sin(i * 0.31) + np.cos(i * 0.073)).reshape(h, w)
+    b = (np.cos(i * 0.17) - np.sin(i * 0.019)).reshape(h, w)
+    a -= a.mean()
+    b -= b.mean()
+    ma, mb, mc = g.applyPreconditioner(a), g.applyPreconditioner(b), g.applyPreconditioner(1.3 * a - 0.7 * b)
+    assert np.array_equal(ma, g.applyPreconditioner(a)), "preconditioner retained history"
+    ma, mb, mc = ma - ma.mean(), mb - mb.mean(), mc - mc.mean()
+    assert np.abs(mc - (1.3 * ma - 0.7 * mb)).max() <= tol * max(1.0, np.abs(mc).max())
+    ea, eb = float((a * ma).sum()), float((b * mb).sum())
+    assert abs(float((a * mb).sum()) - float((b * ma).sum())) <= tol * max(1.0, np.sqrt(abs(ea * eb)))
+    if w * h == 1:
+        assert ea == 0.0
+    else:
+        assert ea > 0.0 and eb > 0.0
+    assert np.all(g.applyPreconditioner(np.full((h, w), 7.0), 7.0) == 0.0)
+
+
+# ---------------------------------------------------------------------------------------------
+# Known answers, batching, determinism, edge cases
+# ---------------------------------------------------------------------------------------------
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_hydrostatic_known_answer(precision):
+    w, h, dx = 12, 10, 2.0
+    f = np.ones((h, w))
+    s = scenes.Scene(w, h, dx, 1.0 / 120.0, 100.0, 0.1, f, np.zeros((h, w + 1)), np.zeros((h + 1, w)), gravity=100.0)
+    g = gpu_grid(s, precision)
+    r = g.step(s.dt, 2000, 1e-8 if precision == "fp64" else 1e-5)
+    out = g.download()
+    expected = 100.0 * 100.0 * dx * (h - 1)
+    rise = out.pressure[h - 1, 0] - out.pressure[0, 0]
+    if precision == "fp64":
+        assert r.converged
+        assert np.abs(out.v).max() < 1e-7
+        assert abs(rise - expected) < expected * 1e-8
+    else:
+        assert r.accepted()
+        assert np.abs(out.v).max() < 1e-4
+        assert abs(rise - expected) < expected * 1e-5
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_batch_equals_single(precision):
+    batch_scenes = scenes.uneven_batch(6, seed=1, min_side=40, max_side=300)
+    singles, members = [], []
+    for s in batch_scenes:
+        g = gpu_grid(s, precision)
+        singles.append(g.project(s.dt, 300, 1e-6, relative_tolerance=1e-6))
+        singles[-1] = (singles[-1], g.download())
+        members.append(gpu_grid(s, precision))
+    b = ProjectionBatch(members)
+    results = b.project([s.dt for s in batch_scenes], 300, 1e-6, relative_tolerance=1e-6)
+    for (single, state), res, m in zip(singles, results, members):
+        out = m.download()
+        assert res.iterations == single.iterations
+        assert np.array_equal(out.u, state.u) and np.array_equal(out.v, state.v)
+        assert np.array_equal(out.pressure, state.pressure)
+    b.destroy()
+
+
+def test_deterministic_repeat():
+    s = scenes.dam_break(256, 256, seed=2, obstacles=4, velocity=1.0)
+    outs = []
+    for _ in range(2):
+        g = gpu_grid(s, "fp32")
+        g.applyGravity(s.dt)
+        r = g.project(s.dt, 200, 1e-6, relative_tolerance=1e-6)
+        outs.append((r.iterations, g.download()))
+    assert outs[0][0] == outs[1][0]
+    assert np.array_equal(outs[0][1].u, outs[1][1].u) and np.array_equal(outs[0][1].pressure, outs[1][1].pressure)
+
+
+def test_edge_cases():
+    s = scenes.liquid_box(1, 1)
+    g = gpu_grid(s, "fp32")
+    r = g.project(s.dt, 200, 1e-6)
+    assert r.converged and r.iterations == 0
+    g = gpu_grid(scenes.liquid_box(32, 24, seed=1), "fp32")
+    r0 = g.step(0.0)
+    assert r0.iterations == 0 and not r0.converged and r0.max_divergence == float("inf")
+    r1 = g.project(1.0 / 60, 0, 1e-6)
+    assert r1.iterations == 0 and not r1.converged
+    # A divergence-free field needs no work.
+    z = scenes.Scene(32, 24, 1.0, 0.01, 1.0, 0.001, np.ones((24, 32)), np.zeros((24, 33)), np.zeros((25, 32)))
+    gz = gpu_grid(z, "fp32")
+    rz = gz.project(0.01, 200, 1e-6)
+    assert rz.converged and rz.iterations == 0 and rz.solve_status == "no_work"
+    with pytest.raises(ValueError):
+        g.upload(FluidGridState(np.ones(5)))
+    fresh = FluidGrid(8, 8, 1.0)
+    fresh.configureMaterials([1.0], [0.001])
+    with pytest.raises(FluidLifecycleError):
+        fresh.step(0.01)
+    with pytest.raises(FluidCudaError):
+        fresh.configureMaterials([1.0], [0.001], liquid_viscosities=[1.0])
+
+
+def test_large_grid_converges_relative():
+    s = scenes.dam_break(1024, 1024, seed=0, obstacles=16, velocity=1.0)
+    g = gpu_grid(s, "fp32")
+    g.applyGravity(s.dt)
+    r = g.project(s.dt, 300, 1e-6, relative_tolerance=1e-6)
+    assert r.solve_status == "converged"
+    assert r.residual_l2 <= 1.0001e-6 * r.rhs_l2
+    assert r.iterations < 80
+    # divergence falls by orders of magnitude (FP32 velocity storage sets the floor)
+    assert r.divergence_l2 < 1e-3 * r.rhs_l2 / (s.cell_size * s.cell_size / s.dt) + 1e-3

@@ -86,6 +86,7 @@ SIGNATURES = {
     "fc_classify": (_int, [_vp, C.POINTER(C.c_uint8)]),
     "fc_apply_preconditioner": (_int, [_vp, _dp, _dbl, _dp]),
     "fc_time_kernel": (_int, [_vp, _int, _int, _dp]),
+    "fc_divergence_noalloc": (_int, [_vp, _vp, _int, _int, _dbl, _int, _vp, _vp]),
     "fc_velocity_pointers": (_int, [_vp, C.POINTER(_vp), C.POINTER(_vp)]),
     "fc_get_stream": (_int, [_vp, C.POINTER(_vp)]),
     "fc_synchronize": (_int, [_vp]),

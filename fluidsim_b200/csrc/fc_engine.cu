@@ -20,6 +20,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -1179,6 +1180,107 @@ double time_kernel(Grid& g, int kernel, int repeats)
     return double(ms) / repeats;
 }
 
+// ------------------------------------------------------------------------------------------
+// Divergence statistics for callers that cannot allocate device memory
+// ------------------------------------------------------------------------------------------
+//
+// Some callers cannot call cudaMalloc: a host whose allocator owns every byte of device memory
+// (a game engine or a simulation framework with its own pool), a process held to a fixed
+// device-memory budget, or a real-time loop that must never stall in the driver (cudaMalloc can
+// synchronise the device). fc_divergence_noalloc serves them: the caller passes the face
+// velocities and a device buffer for the result, and the reduction's scratch lives in the
+// fixed array below instead of a per-grid allocation. Every GPU that loads this library holds
+// the array until the process exits.
+
+constexpr int kNoAllocMaxTiles = 4096; // 32 x 32 cells per tile: at most 4,194,304 cells
+constexpr size_t kNoAllocCounterOffset = size_t(kNoAllocMaxTiles) * sizeof(double4);
+static __device__ __align__(256) unsigned char noalloc_scratch[kNoAllocCounterOffset + 256];
+
+// Same statistics as k_divergence, over a caller's unpadded face arrays; tile t covers the
+// 32 x 32 cells at (t % tiles_x, t / tiles_x). The last tile to arrive folds the partials in
+// tile order and resets the arrival counter.
+template <typename T>
+__global__ void __launch_bounds__(kVecThreads) k_divergence_noalloc(const T* u, const T* v, int W, int H, double dx,
+    unsigned char* scratch, double* out)
+{
+    double4* partial = reinterpret_cast<double4*>(scratch);
+    unsigned int* counter = reinterpret_cast<unsigned int*>(scratch + kNoAllocCounterOffset);
+    const int tiles_x = (W + kVecTileX - 1) / kVecTileX;
+    const int x0 = (blockIdx.x % tiles_x) * kVecTileX, y0 = (blockIdx.x / tiles_x) * kVecTileY;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    double mx = 0.0, excess = 0.0, sq = 0.0;
+    int nonfinite = 0;
+    for (int k = 0; k < 4; ++k)
+    {
+        const int x = x0 + tx, y = y0 + ty + 8 * k;
+        if (x >= W || y >= H)
+            continue;
+        const long long iu = (long long)y * (W + 1) + x;
+        const long long iv = (long long)y * W + x;
+        const T ul = u[iu], ur = u[iu + 1], vu = v[iv], vd = v[iv + W];
+        const double div = ((dd(ur) - dd(ul)) + (dd(vd) - dd(vu))) / dx;
+        if (!isfinite(div))
+        {
+            nonfinite = 1;
+            continue;
+        }
+        const double rounding = (face_ulp(ul) + face_ulp(ur) + face_ulp(vu) + face_ulp(vd)) / dx;
+        mx = fmax(mx, fabs(div));
+        excess = fmax(excess, fmax(0.0, fabs(div) - rounding));
+        sq += div * div;
+    }
+    const double4 mine = block_reduce4<kVecThreads>(make_double4(mx, excess, sq, double(nonfinite)), 1 | 2 | 8);
+    __shared__ int is_last;
+    if (threadIdx.x == 0)
+    {
+        partial[blockIdx.x] = mine;
+        __threadfence();
+        is_last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!is_last)
+        return;
+    __threadfence();
+    double4 acc = make_double4(0, 0, 0, 0);
+    const int per = (int(gridDim.x) + kVecThreads - 1) / kVecThreads;
+    const int first = threadIdx.x * per, last = min(int(gridDim.x), first + per);
+    for (int t = first; t < last; ++t)
+    {
+        const volatile double* slot = reinterpret_cast<const volatile double*>(&partial[t]);
+        acc.x = fmax(acc.x, slot[0]);
+        acc.y = fmax(acc.y, slot[1]);
+        acc.z += slot[2];
+        acc.w = fmax(acc.w, slot[3]);
+    }
+    const double4 total = block_reduce4<kVecThreads>(acc, 1 | 2 | 8);
+    if (threadIdx.x == 0)
+    {
+        out[0] = total.w != 0.0 ? INFINITY : total.x;
+        out[1] = total.w != 0.0 ? INFINITY : total.y;
+        out[2] = total.z;
+        *counter = 0u;
+    }
+}
+
+// Device address of the scratch array, looked up once per device (with that device current).
+void* noalloc_address()
+{
+    static std::mutex lock;
+    static void* addresses[64] = {};
+    int device = 0;
+    check(cudaGetDevice(&device), "current device");
+    if (device < 0 || device >= 64)
+        fail(FC_ERR_UNSUPPORTED, "device index %d out of range", device);
+    std::lock_guard<std::mutex> guard(lock);
+    if (!addresses[device])
+    {
+        void* address = nullptr;
+        check(cudaGetSymbolAddress(&address, noalloc_scratch), "scratch symbol address");
+        addresses[device] = address;
+    }
+    return addresses[device];
+}
+
 } // namespace fc
 
 // ==========================================================================================
@@ -1568,6 +1670,35 @@ int fc_time_kernel(fc_grid* grid, int kernel, int repeats, double* mean_ms)
         if (!grid || !mean_ms)
             fail(FC_ERR_INVALID_ARGUMENT, "null argument");
         *mean_ms = fc::time_kernel(grid->impl, kernel, repeats);
+    });
+}
+
+int fc_divergence_noalloc(const void* u, const void* v, int width, int height, double cell_size, int precision,
+    double* stats, void* stream)
+{
+    return guarded([&]
+    {
+        if (!u || !v || !stats)
+            fail(FC_ERR_INVALID_ARGUMENT, "null argument");
+        if (width <= 0 || height <= 0 || !(cell_size > 0.0) || !std::isfinite(cell_size))
+            fail(FC_ERR_INVALID_ARGUMENT, "grid geometry must be positive and finite");
+        if (precision != FC_PRECISION_FP32 && precision != FC_PRECISION_FP64)
+            fail(FC_ERR_INVALID_ARGUMENT, "precision must be FP32 or FP64");
+        const long long tiles = (long long)fc::ceil_div(width, fc::kVecTileX) * fc::ceil_div(height, fc::kVecTileY);
+        if (tiles > fc::kNoAllocMaxTiles)
+            fail(FC_ERR_INVALID_ARGUMENT,
+                "a %dx%d grid needs %lld tiles of 32x32 cells; the no-allocation path holds at most %d "
+                "(4,194,304 cells)", width, height, tiles, fc::kNoAllocMaxTiles);
+        unsigned char* scratch = static_cast<unsigned char*>(fc::noalloc_address());
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        // The arrival counter must start at zero; the partial slots are overwritten.
+        check(cudaMemsetAsync(scratch + fc::kNoAllocCounterOffset, 0, sizeof(unsigned int), s), "scratch clear");
+        if (precision == FC_PRECISION_FP64)
+            FC_LAUNCH(fc::k_divergence_noalloc<double>, int(tiles), fc::kVecThreads, 0, s,
+                static_cast<const double*>(u), static_cast<const double*>(v), width, height, cell_size, scratch, stats);
+        else
+            FC_LAUNCH(fc::k_divergence_noalloc<float>, int(tiles), fc::kVecThreads, 0, s,
+                static_cast<const float*>(u), static_cast<const float*>(v), width, height, cell_size, scratch, stats);
     });
 }
 

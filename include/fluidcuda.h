@@ -187,6 +187,27 @@ int fc_apply_preconditioner(fc_grid* grid, const double* residual, double residu
  * levels, z, d, q), so the physical state is unchanged. Profiling aid. */
 int fc_time_kernel(fc_grid* grid, int kernel, int repeats, double* mean_ms);
 
+/* Divergence statistics of caller-owned face velocities, for callers that cannot allocate
+ * device memory: a host whose own allocator owns all of the device's memory (a game engine or
+ * a framework with its own pool), a process held to a fixed device-memory budget, or a
+ * real-time loop that must not stall in the driver, where cudaMalloc can synchronise the
+ * device. No counterpart in the reference.
+ *
+ * u and v are device arrays in the reference layout ((width+1)*height and width*(height+1)),
+ * float for FC_PRECISION_FP32 or double for FC_PRECISION_FP64. stats is a device array of 3
+ * doubles receiving max |div u| (1/s; +inf if any cell is non-finite), the largest excess of
+ * |div u| over the cell's float rounding allowance, and the sum of div u squared. The work is
+ * queued on `stream` (a cudaStream_t, 0 for the legacy stream); the call does not wait.
+ *
+ * This entry point allocates nothing: its scratch is a fixed 128 KiB device array that every
+ * GPU loading this library keeps until process exit. Grids are limited to 4096 tiles of 32x32
+ * cells (4,194,304 cells, e.g. 2048x2048); larger ones are rejected with
+ * FC_ERR_INVALID_ARGUMENT. The first call on a device looks up the array's device address;
+ * make that first call before any stream capture. All calls share the one array, so calls
+ * whose work overlaps on the GPU race: order them on one stream or synchronise between them. */
+int fc_divergence_noalloc(const void* u, const void* v, int width, int height, double cell_size, int precision,
+    double* stats, void* stream);
+
 /* Device pointers of the face velocities (working precision), for zero-copy producers. */
 int fc_velocity_pointers(fc_grid* grid, void** u, void** v);
 /* The grid's stream (cudaStream_t) and a wait for all of its work. */

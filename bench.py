@@ -48,6 +48,8 @@ def parse():
     p.add_argument("--no-batched", action="store_true", help="skip the batched uneven-grid measurement")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--launch", choices=["graph", "stream"], default="graph",
+                   help="stream: host-driven launches of the same kernels (for per-kernel profilers)")
     return p.parse_args()
 
 
@@ -200,8 +202,10 @@ def run_cuda(args, world, rank, local_rank):
     import torch
 
     from fluidsim_b200 import FluidGrid, FluidGridState, ProjectionBatch, kernel_launches, scenes
+    from fluidsim_b200 import _native
 
     torch.cuda.set_device(local_rank)
+    _native.set_launch_mode(args.launch)
     size = args.size
     scene = scene_for(size, rank)
     pristine = FluidGrid(size, size, scene.cell_size, "fp32")
@@ -270,6 +274,7 @@ def run_cuda(args, world, rank, local_rank):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "launch": args.launch,
         "config": {"workload": f"dam_break_{size}x{size} projection (gravity + PCG-MG to 1e-6 relative)",
                    "cells": scene.cells, "tolerance": args.tolerance, "density_ratio": "1000:1",
                    "l2": "flushed (256 MiB write) before every timed step", "parallelism": f"replicas x{world}"},

@@ -64,6 +64,7 @@ SIGNATURES = {
     "fc_last_error": (C.c_char_p, []),
     "fc_status_string": (C.c_char_p, [_int]),
     "fc_kernel_launches": (C.c_longlong, []),
+    "fc_set_launch_mode": (_int, [_int]),
     "fc_create": (_int, [_int, _int, _dbl, _int, C.POINTER(_vp)]),
     "fc_destroy": (_int, [_vp]),
     "fc_get_geometry": (_int, [_vp, C.POINTER(_int), C.POINTER(_int), _dp]),
@@ -141,3 +142,8 @@ def check(status: int):
 
 def kernel_launches() -> int:
     return int(lib().fc_kernel_launches())
+
+
+def set_launch_mode(mode: str):
+    """'graph' (default: one CUDA graph per projection) or 'stream' (host-driven launches)."""
+    check(lib().fc_set_launch_mode({"graph": 0, "stream": 1}[mode]))

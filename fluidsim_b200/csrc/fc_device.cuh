@@ -21,9 +21,13 @@ namespace fc
 
 constexpr int kMaxLevels = 16;
 constexpr int kPadX = 2;   // column of x = 0 inside a padded row
-constexpr int kVecTileX = 32;
-constexpr int kVecTileY = 32;
+// Tiles of the fine-level vector kernels: 64 x 64 cells, 256 threads. Thread (lane, warp) covers
+// columns lane and lane + 32 of rows warp + 8m (kVecCells cells), or, in the strip kernels,
+// columns 2 lane and 2 lane + 1 of rows 8 warp .. 8 warp + 7.
+constexpr int kVecTileX = 64;
+constexpr int kVecTileY = 64;
 constexpr int kVecThreads = 256;
+constexpr int kVecCells = 16;
 
 __host__ __device__ inline int padded_stride(int w) { return ((w + 3) + 7) / 8 * 8; }
 __host__ __device__ inline long long padded_index(int S, int x, int y) { return (long long)(y + 1) * S + x + kPadX; }

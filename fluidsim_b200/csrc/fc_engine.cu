@@ -9,6 +9,7 @@
 #include "fc_device.cuh"
 #include "fc_multigrid.cuh"
 #include "fc_pcg.cuh"
+#include "fc_smooth.cuh"
 
 #include "../../include/fluidcuda.h"
 
@@ -221,14 +222,18 @@ struct Grid
     ~Grid();
 };
 
+// Strip heights of the smoothing kernels: tall strips (less halo overhead) on levels with
+// enough tiles to fill the GPU twice, short ones (half the per-CTA latency) below that.
 template <typename T> struct Tiling;
 template <> struct Tiling<float>
 {
-    static constexpr int K = 8;
+    static constexpr int big = 8;
+    static constexpr int small = 4;
 };
 template <> struct Tiling<double>
 {
-    static constexpr int K = 6;
+    static constexpr int big = 6;
+    static constexpr int small = 4;
 };
 
 struct TileSizes
@@ -236,13 +241,17 @@ struct TileSizes
     int pre_x, pre_y, post_x, post_y;
 };
 
-TileSizes tile_sizes(int precision)
+template <typename T, int K> TileSizes tile_sizes_of()
+{
+    return {TileShape<T, K, true>::OX, TileShape<T, K, true>::OY, TileShape<T, K, false>::OX,
+        TileShape<T, K, false>::OY};
+}
+
+TileSizes tile_sizes(int precision, bool big)
 {
     if (precision == FC_PRECISION_FP64)
-        return {TileShape<double, 6, true>::OX, TileShape<double, 6, true>::OY, TileShape<double, 6, false>::OX,
-            TileShape<double, 6, false>::OY};
-    return {TileShape<float, 8, true>::OX, TileShape<float, 8, true>::OY, TileShape<float, 8, false>::OX,
-        TileShape<float, 8, false>::OY};
+        return big ? tile_sizes_of<double, Tiling<double>::big>() : tile_sizes_of<double, Tiling<double>::small>();
+    return big ? tile_sizes_of<float, Tiling<float>::big>() : tile_sizes_of<float, Tiling<float>::small>();
 }
 
 // The coarse tail starts at the first level whose cells and shared-memory footprint fit one CTA.
@@ -298,7 +307,8 @@ void allocate_grid(Grid& g)
     const HostLevel& last = g.levels.back();
     d.ncoarse = last.w * last.h - 1;
     d.vec_tiles = ceil_div(W, kVecTileX) * ceil_div(H, kVecTileY);
-    const TileSizes ts = tile_sizes(g.precision);
+    // Partial slots for the most level-0 post tiles any plan can use (the short strips).
+    const TileSizes ts = tile_sizes(g.precision, false);
     d.post_tiles = g.tail > 0 ? ceil_div(W, ts.post_x) * ceil_div(H, ts.post_y) : 0;
 
     const size_t padded0 = size_t(g.S) * (H + 2);
@@ -467,9 +477,9 @@ __global__ void __launch_bounds__(kVecThreads) k_count_open(const GridDesc* grid
         return;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     double open = 0.0;
-    for (int k = 0; k < 4; ++k)
+    for (int k = 0; k < kVecCells; ++k)
     {
-        const int x = t.x0 + tx, y = t.y0 + ty + 8 * k;
+        const int x = t.x0 + tx + 32 * (k & 1), y = t.y0 + ty + 8 * (k >> 1);
         if (x >= g.W || y >= g.H)
             continue;
         open += g.solid[(long long)y * g.W + x] ? 0.0 : 1.0;
@@ -510,9 +520,9 @@ template <typename T> __global__ void k_gravity(const GridDesc* grids, const Til
     const GridDesc& g = grids[t.grid];
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     T* v = static_cast<T*>(g.v);
-    for (int k = 0; k < 4; ++k)
+    for (int k = 0; k < kVecCells; ++k)
     {
-        const int x = t.x0 + tx, y = t.y0 + ty + 8 * k;
+        const int x = t.x0 + tx + 32 * (k & 1), y = t.y0 + ty + 8 * (k >> 1);
         if (x >= g.W || y >= g.H || y == 0)
             continue;
         const long long f = (long long)y * g.W + x;
@@ -525,9 +535,9 @@ __global__ void k_classify(const GridDesc* grids, const Tile* tiles, const doubl
     const Tile t = tiles[blockIdx.x];
     const GridDesc& g = grids[t.grid];
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-    for (int k = 0; k < 4; ++k)
+    for (int k = 0; k < kVecCells; ++k)
     {
-        const int x = t.x0 + tx, y = t.y0 + ty + 8 * k;
+        const int x = t.x0 + tx + 32 * (k & 1), y = t.y0 + ty + 8 * (k >> 1);
         if (x >= g.W || y >= g.H)
             continue;
         const long long i = (long long)y * g.W + x;
@@ -563,6 +573,7 @@ struct Plan
     Range coarsen[kMaxLevels];
     Range pre[kMaxLevels];
     Range post[kMaxLevels];
+    bool tall[kMaxLevels] = {}; // strip height per level (true: Tiling::big)
     int max_levels = 0;
     int max_tail = 0;
     size_t tail_smem = 0;
@@ -617,8 +628,14 @@ void append_tiles(std::vector<Tile>& tiles, int grid, int w, int h, int tx, int 
 void upload_descriptors(Plan& plan)
 {
     std::vector<GridDesc> descs(plan.n());
+    const TileSizes ts = tile_sizes(plan.precision, plan.tall[0]);
     for (int i = 0; i < plan.n(); ++i)
+    {
         descs[i] = plan.grids[i]->desc;
+        // Level-0 post tiles of this grid in this plan: the count its z reduction waits for.
+        const Grid& g = *plan.grids[i];
+        descs[i].post_tiles = g.tail > 0 ? ceil_div(g.W, ts.post_x) * ceil_div(g.H, ts.post_y) : 0;
+    }
     check(cudaMemcpyAsync(plan.d_desc, descs.data(), descs.size() * sizeof(GridDesc), cudaMemcpyHostToDevice, plan.stream),
         "plan descriptors");
     check(cudaStreamSynchronize(plan.stream), "plan descriptors");
@@ -637,7 +654,6 @@ std::unique_ptr<Plan> make_plan(const std::vector<Grid*>& grids, cudaStream_t st
         plan->own_stream = true;
     }
     const int n = plan->n();
-    const TileSizes ts = tile_sizes(plan->precision);
     std::vector<Tile> tiles;
     auto add = [&](Range& r, auto&& body)
     {
@@ -668,8 +684,17 @@ std::unique_ptr<Plan> make_plan(const std::vector<Grid*>& grids, cudaStream_t st
             }
         });
     }
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, grids.front()->device);
     for (int l = 0; l < plan->max_tail; ++l)
     {
+        const TileSizes tall = tile_sizes(plan->precision, true);
+        long long tall_tiles = 0;
+        for (int i = 0; i < n; ++i)
+            if (l < grids[i]->tail)
+                tall_tiles += (long long)ceil_div(grids[i]->levels[l].w, tall.pre_x) * ceil_div(grids[i]->levels[l].h, tall.pre_y);
+        plan->tall[l] = tall_tiles >= 2LL * sms;
+        const TileSizes ts = tile_sizes(plan->precision, plan->tall[l]);
         add(plan->pre[l], [&]
         {
             for (int i = 0; i < n; ++i)
@@ -719,12 +744,22 @@ template <typename T> void launch_precondition(Plan& p, bool use_mg)
         FC_LAUNCH(k_precondition_diagonal<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
         return;
     }
-    constexpr int K = Tiling<T>::K;
+    constexpr int KB = Tiling<T>::big, KS = Tiling<T>::small;
     for (int l = 0; l < p.max_tail; ++l)
-        FC_LAUNCH((k_mg_pre<T, K>), p.pre[l].count, 256, 0, s, p.d_desc, p.at(p.pre[l]), l);
+    {
+        if (p.tall[l])
+            FC_LAUNCH((k_mg_pre<T, KB>), p.pre[l].count, 256, 0, s, p.d_desc, p.at(p.pre[l]), l);
+        else
+            FC_LAUNCH((k_mg_pre<T, KS>), p.pre[l].count, 256, 0, s, p.d_desc, p.at(p.pre[l]), l);
+    }
     FC_LAUNCH(k_mg_tail<T>, p.n(), kTailThreads, p.tail_smem, s, p.d_desc);
     for (int l = p.max_tail - 1; l >= 0; --l)
-        FC_LAUNCH((k_mg_post<T, K>), p.post[l].count, 256, 0, s, p.d_desc, p.at(p.post[l]), l);
+    {
+        if (p.tall[l])
+            FC_LAUNCH((k_mg_post<T, KB>), p.post[l].count, 256, 0, s, p.d_desc, p.at(p.post[l]), l);
+        else
+            FC_LAUNCH((k_mg_post<T, KS>), p.post[l].count, 256, 0, s, p.d_desc, p.at(p.post[l]), l);
+    }
 }
 
 template <typename T> void launch_iteration(Plan& p, bool use_mg, int parity)
@@ -742,6 +777,36 @@ template <typename T> void set_kernel_attributes(Plan& p)
         check(cudaFuncSetAttribute(k_mg_tail<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(p.tail_smem)),
             "tail shared memory");
 }
+
+// Projection set-up: states, right-hand side, warm start, first residual, first z.
+template <typename T> void launch_setup(Plan& p, bool use_mg)
+{
+    cudaStream_t s = p.stream;
+    FC_LAUNCH(k_init_states, ceil_div(p.n(), 128), 128, 0, s, p.d_desc, p.n(), p.d_params, p.d_body_count);
+    FC_LAUNCH(k_count_open, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
+    FC_LAUNCH(k_rhs<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
+    FC_LAUNCH(k_rhs_stats<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
+    FC_LAUNCH(k_warm_start, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
+    FC_LAUNCH(k_remove_pressure_mean, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
+    FC_LAUNCH(k_true_residual<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec), 1);
+    launch_precondition<T>(p, use_mg);
+}
+
+// After the solve: final mean removal, velocity update, divergence, results gathered.
+template <typename T> void launch_finish(Plan& p)
+{
+    cudaStream_t s = p.stream;
+    FC_LAUNCH(k_pressure_sum, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
+    FC_LAUNCH(k_velocity_update<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
+    FC_LAUNCH(k_remove_pressure_mean, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
+    FC_LAUNCH(k_divergence<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
+    FC_LAUNCH(k_gather_states, ceil_div(p.n(), 128), 128, 0, s, p.d_desc, p.n(), p.d_states);
+}
+
+// Launch mechanism of the PCG loop: one CUDA graph with a device-side WHILE node (default), or
+// host-driven launches that poll the per-grid done flags (for per-kernel profilers, and where
+// conditional graph nodes are unavailable). Both run the same kernels in the same order.
+std::atomic<int> launch_mode{FC_LAUNCH_GRAPH};
 
 // Captures the projection: set-up, WHILE { 2 iterations, condition }, velocity, divergence.
 template <typename T> void capture_projection(Plan& p, bool use_mg, int cap)
@@ -765,14 +830,7 @@ template <typename T> void capture_projection(Plan& p, bool use_mg, int cap)
     // Set-up, captured into the outer graph.
     const long long before_setup = launch_count.load();
     check(cudaStreamBeginCaptureToGraph(s, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal), "capture");
-    FC_LAUNCH(k_init_states, ceil_div(p.n(), 128), 128, 0, s, p.d_desc, p.n(), p.d_params, p.d_body_count);
-    FC_LAUNCH(k_count_open, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
-    FC_LAUNCH(k_rhs<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
-    FC_LAUNCH(k_rhs_stats<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
-    FC_LAUNCH(k_warm_start, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
-    FC_LAUNCH(k_remove_pressure_mean, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
-    FC_LAUNCH(k_true_residual<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec), 1);
-    launch_precondition<T>(p, use_mg);
+    launch_setup<T>(p, use_mg);
 
     // The conditional node depends on everything captured so far.
     cudaStreamCaptureStatus status;
@@ -793,11 +851,7 @@ template <typename T> void capture_projection(Plan& p, bool use_mg, int cap)
     check(cudaStreamUpdateCaptureDependencies(s, &loop, 1, cudaStreamSetCaptureDependencies), "capture deps");
 
     // Finishing kernels after the loop, in the outer graph.
-    FC_LAUNCH(k_pressure_sum, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
-    FC_LAUNCH(k_velocity_update<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
-    FC_LAUNCH(k_remove_pressure_mean, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
-    FC_LAUNCH(k_divergence<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
-    FC_LAUNCH(k_gather_states, ceil_div(p.n(), 128), 128, 0, s, p.d_desc, p.n(), p.d_states);
+    launch_finish<T>(p);
     cudaGraph_t captured;
     check(cudaStreamEndCapture(s, &captured), "end capture");
     p.setup_kernels = int(launch_count.load() - before_setup);
@@ -829,9 +883,40 @@ template <typename T> void capture_projection(Plan& p, bool use_mg, int cap)
     p.graph_use_mg = use_mg ? 1 : 0;
 }
 
-template <typename T> void run_projection(Plan& p, bool use_mg, int max_iterations)
+// Runs one projection of every grid of the plan; returns the kernels executed on the device.
+template <typename T> long long run_projection(Plan& p, bool use_mg, int max_iterations)
 {
     const int cap = (std::max(max_iterations, 0) + 1) / 2 + 8;
+    if (launch_mode.load() == FC_LAUNCH_STREAM)
+    {
+        set_kernel_attributes<T>(p);
+        const long long before = launch_count.load();
+        check(cudaMemcpyAsync(p.d_params, p.h_params, p.n() * sizeof(ProjectParams), cudaMemcpyHostToDevice, p.stream),
+            "params");
+        launch_setup<T>(p, use_mg);
+        int bodies = 0;
+        for (;;)
+        {
+            launch_iteration<T>(p, use_mg, 0);
+            launch_iteration<T>(p, use_mg, 1);
+            ++bodies;
+            FC_LAUNCH(k_gather_states, ceil_div(p.n(), 128), 128, 0, p.stream, p.d_desc, p.n(), p.d_states);
+            check(cudaMemcpyAsync(p.h_states, p.d_states, p.n() * sizeof(SolveState), cudaMemcpyDeviceToHost, p.stream),
+                "poll");
+            check(cudaStreamSynchronize(p.stream), "poll");
+            bool all_done = true;
+            for (int i = 0; i < p.n(); ++i)
+                all_done &= p.h_states[i].done != 0;
+            if (all_done || bodies >= cap)
+                break;
+        }
+        launch_finish<T>(p);
+        check(cudaMemcpyAsync(p.h_states, p.d_states, p.n() * sizeof(SolveState), cudaMemcpyDeviceToHost, p.stream),
+            "results");
+        check(cudaStreamSynchronize(p.stream), "projection");
+        p.h_bodies = bodies;
+        return launch_count.load() - before;
+    }
     if (!p.exec || p.graph_cap != cap || p.graph_use_mg != (use_mg ? 1 : 0))
         capture_projection<T>(p, use_mg, cap);
     check(cudaMemcpyAsync(p.d_params, p.h_params, p.n() * sizeof(ProjectParams), cudaMemcpyHostToDevice, p.stream),
@@ -841,6 +926,9 @@ template <typename T> void run_projection(Plan& p, bool use_mg, int max_iteratio
         "results");
     check(cudaMemcpyAsync(&p.h_bodies, p.d_body_count, sizeof(int), cudaMemcpyDeviceToHost, p.stream), "results");
     check(cudaStreamSynchronize(p.stream), "projection");
+    const long long executed = p.setup_kernels + (long long)p.h_bodies * p.body_kernels;
+    launch_count.fetch_add(executed);
+    return executed;
 }
 
 void fill_result(const Grid& g, const SolveState& s, double divergence_tolerance, fc_result* out)
@@ -959,20 +1047,19 @@ void project_plan(Plan& p, const double* dts, int max_iterations, double diverge
         q.max_iterations = max_iterations;
         q.use_mg = use_mg ? 1 : 0;
     }
+    long long executed = p.rebuild_kernels;
     dispatch(p.precision, [&](auto zero)
     {
         using T = decltype(zero);
-        run_projection<T>(p, use_mg, max_iterations);
+        executed += run_projection<T>(p, use_mg, max_iterations);
     });
-    const int executed = p.rebuild_kernels + p.setup_kernels + p.h_bodies * p.body_kernels;
-    launch_count.fetch_add(p.setup_kernels + p.h_bodies * p.body_kernels);
     for (int i = 0; i < p.n(); ++i)
     {
         const SolveState& s = p.h_states[i];
         if (!s.done)
             fail(FC_ERR_TIMEOUT, "pressure loop stopped at its iteration cap before grid %d finished", i);
         fill_result(*p.grids[i], s, divergence_tolerance, &results[i]);
-        results[i].kernels = executed;
+        results[i].kernels = int(executed);
     }
 }
 
@@ -1149,14 +1236,24 @@ double time_kernel(Grid& g, int kernel, int repeats)
     dispatch(g.precision, [&](auto zero)
     {
         using T = decltype(zero);
-        constexpr int K = Tiling<T>::K;
+        constexpr int KB = Tiling<T>::big, KS = Tiling<T>::small;
         set_kernel_attributes<T>(p);
         auto launch = [&]
         {
             switch (kernel)
             {
-            case 0: FC_LAUNCH((k_mg_pre<T, K>), p.pre[0].count, 256, 0, p.stream, p.d_desc, p.at(p.pre[0]), 0); break;
-            case 1: FC_LAUNCH((k_mg_post<T, K>), p.post[0].count, 256, 0, p.stream, p.d_desc, p.at(p.post[0]), 0); break;
+            case 0:
+                if (p.tall[0])
+                    FC_LAUNCH((k_mg_pre<T, KB>), p.pre[0].count, 256, 0, p.stream, p.d_desc, p.at(p.pre[0]), 0);
+                else
+                    FC_LAUNCH((k_mg_pre<T, KS>), p.pre[0].count, 256, 0, p.stream, p.d_desc, p.at(p.pre[0]), 0);
+                break;
+            case 1:
+                if (p.tall[0])
+                    FC_LAUNCH((k_mg_post<T, KB>), p.post[0].count, 256, 0, p.stream, p.d_desc, p.at(p.post[0]), 0);
+                else
+                    FC_LAUNCH((k_mg_post<T, KS>), p.post[0].count, 256, 0, p.stream, p.d_desc, p.at(p.post[0]), 0);
+                break;
             case 2: FC_LAUNCH(k_direction_operator<T>, p.vec.count, kVecThreads, 0, p.stream, p.d_desc, p.at(p.vec), 0); break;
             default: FC_LAUNCH(k_mg_tail<T>, p.n(), kTailThreads, p.tail_smem, p.stream, p.d_desc); break;
             }
@@ -1192,7 +1289,8 @@ double time_kernel(Grid& g, int kernel, int repeats)
 // fixed array below instead of a per-grid allocation. Every GPU that loads this library holds
 // the array until the process exits.
 
-constexpr int kNoAllocMaxTiles = 4096; // 32 x 32 cells per tile: at most 4,194,304 cells
+constexpr int kNoAllocTile = 32;       // tiles of 32 x 32 cells
+constexpr int kNoAllocMaxTiles = 4096; // at most 4,194,304 cells
 constexpr size_t kNoAllocCounterOffset = size_t(kNoAllocMaxTiles) * sizeof(double4);
 static __device__ __align__(256) unsigned char noalloc_scratch[kNoAllocCounterOffset + 256];
 
@@ -1205,8 +1303,8 @@ __global__ void __launch_bounds__(kVecThreads) k_divergence_noalloc(const T* u, 
 {
     double4* partial = reinterpret_cast<double4*>(scratch);
     unsigned int* counter = reinterpret_cast<unsigned int*>(scratch + kNoAllocCounterOffset);
-    const int tiles_x = (W + kVecTileX - 1) / kVecTileX;
-    const int x0 = (blockIdx.x % tiles_x) * kVecTileX, y0 = (blockIdx.x / tiles_x) * kVecTileY;
+    const int tiles_x = (W + kNoAllocTile - 1) / kNoAllocTile;
+    const int x0 = (blockIdx.x % tiles_x) * kNoAllocTile, y0 = (blockIdx.x / tiles_x) * kNoAllocTile;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     double mx = 0.0, excess = 0.0, sq = 0.0;
     int nonfinite = 0;
@@ -1327,6 +1425,16 @@ const char* fc_status_string(int status)
 }
 
 long long fc_kernel_launches(void) { return fc::launch_count.load(); }
+
+int fc_set_launch_mode(int mode)
+{
+    return guarded([&]
+    {
+        if (mode != FC_LAUNCH_GRAPH && mode != FC_LAUNCH_STREAM)
+            fail(FC_ERR_INVALID_ARGUMENT, "unknown launch mode %d", mode);
+        fc::launch_mode.store(mode);
+    });
+}
 
 int fc_create(int width, int height, double cell_size, int precision, fc_grid** out)
 {
@@ -1684,7 +1792,7 @@ int fc_divergence_noalloc(const void* u, const void* v, int width, int height, d
             fail(FC_ERR_INVALID_ARGUMENT, "grid geometry must be positive and finite");
         if (precision != FC_PRECISION_FP32 && precision != FC_PRECISION_FP64)
             fail(FC_ERR_INVALID_ARGUMENT, "precision must be FP32 or FP64");
-        const long long tiles = (long long)fc::ceil_div(width, fc::kVecTileX) * fc::ceil_div(height, fc::kVecTileY);
+        const long long tiles = (long long)fc::ceil_div(width, fc::kNoAllocTile) * fc::ceil_div(height, fc::kNoAllocTile);
         if (tiles > fc::kNoAllocMaxTiles)
             fail(FC_ERR_INVALID_ARGUMENT,
                 "a %dx%d grid needs %lld tiles of 32x32 cells; the no-allocation path holds at most %d "

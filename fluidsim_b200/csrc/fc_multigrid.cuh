@@ -7,13 +7,9 @@
 // level is solved directly with one cell pinned, then given a mean-zero gauge.
 //
 // B200 mapping:
-//  * k_mg_pre / k_mg_post: temporally blocked smoothing. A 256-thread CTA stages a 64 x 8K
-//    region of one level, keeps each cell's coefficients in registers (thread = two adjacent
-//    columns of K rows) and the solution in shared memory split by colour, so a half-sweep is
-//    four conflict-free shared loads per cell. All eight half-sweeps of a smoothing run on-chip;
-//    the region's halo (10 cells for pre, 8 for post) absorbs the dependency cone. The pre kernel
-//    fuses the residual and the restriction (writes the coarse rhs directly); the post kernel
-//    fuses the prolongation, and on the fine level the mean and r.z reductions of z.
+//  * k_mg_pre / k_mg_post (fc_smooth.cuh): temporally blocked smoothing of one level per launch,
+//    with the residual and restriction fused into the pre kernel and the prolongation and the
+//    fine-level z reductions fused into the post kernel.
 //  * k_mg_tail: the coarse levels that fit in shared memory are cycled by one CTA per grid,
 //    including the coarsest direct solve (explicit FP64 inverse of the pinned Cholesky system).
 #pragma once
@@ -57,9 +53,9 @@ __global__ void __launch_bounds__(kVecThreads) k_precondition_diagonal(const Gri
     T* z = static_cast<T*>(g.z);
     const double mean_r = s.mean_r;
     double sz = 0.0, srz = 0.0;
-    for (int k = 0; k < 4; ++k)
+    for (int k = 0; k < kVecCells; ++k)
     {
-        const int x = t.x0 + tx, y = t.y0 + ty + 8 * k;
+        const int x = t.x0 + tx + 32 * (k & 1), y = t.y0 + ty + 8 * (k >> 1);
         if (x >= g.W || y >= g.H)
             continue;
         const long long i = padded_index(g.S, x, y);
@@ -97,9 +93,9 @@ template <typename T> __global__ void k_coarsen(const GridDesc* grids, const Til
     T* cr = static_cast<T*>(c.right);
     T* cd = static_cast<T*>(c.down);
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-    for (int k = 0; k < 4; ++k)
+    for (int k = 0; k < kVecCells; ++k)
     {
-        const int x = t.x0 + tx, y = t.y0 + ty + 8 * k;
+        const int x = t.x0 + tx + 32 * (k & 1), y = t.y0 + ty + 8 * (k >> 1);
         if (x >= c.w || y >= c.h)
             continue;
         double right = 0.0, down = 0.0;
@@ -250,379 +246,131 @@ template <typename T> __global__ void __launch_bounds__(256) k_coarse_inverse(co
 }
 
 // ------------------------------------------------------------------------------------------
-// Temporally blocked red-black smoothing tiles
-// ------------------------------------------------------------------------------------------
-
-template <bool PRE> struct TileHalo
-{
-    // Pre: 8 half-sweeps (the first needs no neighbours) leave cells >= 7 from the region edge
-    // exact; the residual needs 8 and the restriction stencil (fine cells 2C-1 .. 2C+2) 9;
-    // rounded up to 10 to keep the region origin even. Post: 8 half-sweeps need 8.
-    static constexpr int value = PRE ? 10 : 8;
-};
-
-template <typename T, int K, bool PRE> struct TileShape
-{
-    static constexpr int RX = 64;
-    static constexpr int RY = 8 * K;
-    static constexpr int HALO = TileHalo<PRE>::value;
-    static constexpr int OX = RX - 2 * HALO;
-    static constexpr int OY = RY - 2 * HALO;
-};
-
-// Per-thread cell coefficients: cell (row warp + 8k, colour c) of the region.
-template <typename T, int K> struct TileCells
-{
-    T rhs[K][2];
-    T wl[K][2], wr[K][2], wu[K][2], wd[K][2];
-    T inv[K][2];
-};
-
-template <typename T, int K>
-__device__ __forceinline__ void tile_half_sweep(T (&sol)[2][8 * K + 2][34], const TileCells<T, K>& cells, int colour,
-    bool from_zero, int lane, int warp)
-{
-    const int other = colour ^ 1;
-#pragma unroll
-    for (int k = 0; k < K; ++k)
-    {
-        const int y = warp + 8 * k;
-        const int s = (colour + y) & 1;
-        T acc = cells.rhs[k][colour];
-        if (!from_zero)
-        {
-            const T sl = sol[other][y + 1][lane + s];
-            const T sr = sol[other][y + 1][lane + 1 + s];
-            const T su = sol[other][y][lane + 1];
-            const T sd = sol[other][y + 2][lane + 1];
-            acc = acc + ((cells.wl[k][colour] * sl + cells.wr[k][colour] * sr) +
-                            (cells.wu[k][colour] * su + cells.wd[k][colour] * sd));
-        }
-        sol[colour][y + 1][lane + 1] = acc * cells.inv[k][colour];
-    }
-    __syncthreads();
-}
-
-// Loads the region's coefficients (zero outside the level) into registers.
-template <typename T, int K>
-__device__ __forceinline__ void tile_load_cells(TileCells<T, K>& cells, const GridDesc& g, const LevelDesc& L,
-    int level, int X0, int Y0, int lane, int warp, double mean_r)
-{
-    const T* right = static_cast<const T*>(L.right);
-    const T* down = static_cast<const T*>(L.down);
-    const T* rhs = level == 0 ? static_cast<const T*>(g.r) : static_cast<const T*>(L.rhs);
-#pragma unroll
-    for (int k = 0; k < K; ++k)
-    {
-#pragma unroll
-        for (int c = 0; c < 2; ++c)
-        {
-            const int y = warp + 8 * k;
-            const int x = 2 * lane + ((c + y) & 1);
-            const int gx = X0 + x, gy = Y0 + y;
-            T b = T(0), wl = T(0), wr = T(0), wu = T(0), wd = T(0), inv = T(0);
-            if (gx >= 0 && gx < L.w && gy >= 0 && gy < L.h)
-            {
-                const long long i = padded_index(L.S, gx, gy);
-                wl = right[i - 1];
-                wr = right[i];
-                wu = down[i - L.S];
-                wd = down[i];
-                const T diag = ((wl + wr) + wu) + wd;
-                inv = diag > T(0) ? T(1) / diag : T(0);
-                // A cell without an open face takes no part (rhs 0): inside obstacles, or a 1x1 grid.
-                b = diag > T(0) ? (level == 0 ? T(double(rhs[i]) - mean_r) : rhs[i]) : T(0);
-            }
-            cells.rhs[k][c] = b;
-            cells.wl[k][c] = wl;
-            cells.wr[k][c] = wr;
-            cells.wu[k][c] = wu;
-            cells.wd[k][c] = wd;
-            cells.inv[k][c] = inv;
-        }
-    }
-}
-
-// Pre-smoothing (4 sweeps, the first from zero), residual and restriction of one tile.
-// PressureMultigrid.cpp:398-402 (cycle), :204-231 (smooth), :233-276 (restrictResidual).
-template <typename T, int K>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_mg_pre(const GridDesc* grids, const Tile* tiles, int level)
-{
-    using Shape = TileShape<T, K, true>;
-    const Tile t = tiles[blockIdx.x];
-    const GridDesc& g = grids[t.grid];
-    if (g.state->done)
-        return;
-    const LevelDesc& L = g.lev[level];
-    const LevelDesc& C = g.lev[level + 1];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int X0 = t.x0 - Shape::HALO, Y0 = t.y0 - Shape::HALO;
-
-    __shared__ T sol[2][Shape::RY + 2][34];
-    for (int i = threadIdx.x; i < 2 * (Shape::RY + 2) * 34; i += 256)
-        (&sol[0][0][0])[i] = T(0);
-
-    TileCells<T, K> cells;
-    tile_load_cells<T, K>(cells, g, L, level, X0, Y0, lane, warp, level == 0 ? g.state->mean_r : 0.0);
-    __syncthreads();
-
-    tile_half_sweep<T, K>(sol, cells, 0, true, lane, warp);
-    tile_half_sweep<T, K>(sol, cells, 1, false, lane, warp);
-#pragma unroll 1
-    for (int sweep = 1; sweep < 4; ++sweep)
-    {
-        tile_half_sweep<T, K>(sol, cells, 0, false, lane, warp);
-        tile_half_sweep<T, K>(sol, cells, 1, false, lane, warp);
-    }
-
-    // Residual of every owned cell, and the pre-smoothed solution of the tile's output cells.
-    T* pre = static_cast<T*>(L.pre);
-    T res[K][2];
-#pragma unroll
-    for (int k = 0; k < K; ++k)
-    {
-#pragma unroll
-        for (int c = 0; c < 2; ++c)
-        {
-            const int y = warp + 8 * k;
-            const int s = (c + y) & 1;
-            const int other = c ^ 1;
-            const T center = sol[c][y + 1][lane + 1];
-            const T sl = sol[other][y + 1][lane + s];
-            const T sr = sol[other][y + 1][lane + 1 + s];
-            const T su = sol[other][y][lane + 1];
-            const T sd = sol[other][y + 2][lane + 1];
-            const T product = (cells.wl[k][c] * (center - sl) + cells.wr[k][c] * (center - sr)) +
-                              (cells.wu[k][c] * (center - su) + cells.wd[k][c] * (center - sd));
-            res[k][c] = cells.rhs[k][c] - product;
-            const int x = 2 * lane + s;
-            const int gx = X0 + x, gy = Y0 + y;
-            if (x >= Shape::HALO && x < Shape::HALO + Shape::OX && y >= Shape::HALO && y < Shape::HALO + Shape::OY &&
-                gx < L.w && gy < L.h)
-                pre[padded_index(L.S, gx, gy)] = center;
-        }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < K; ++k)
-    {
-#pragma unroll
-        for (int c = 0; c < 2; ++c)
-            sol[c][warp + 8 * k + 1][lane + 1] = res[k][c];
-    }
-    __syncthreads();
-
-    // Transpose-bilinear restriction onto the tile's coarse cells.
-    T* crhs = static_cast<T*>(C.rhs);
-    constexpr int OCX = Shape::OX / 2, OCY = Shape::OY / 2;
-    const int cx0 = t.x0 / 2, cy0 = t.y0 / 2;
-    for (int q = threadIdx.x; q < OCX * OCY; q += 256)
-    {
-        const int cx = cx0 + q % OCX, cy = cy0 + q / OCX;
-        if (cx >= C.w || cy >= C.h)
-            continue;
-        const Gather gx = L.rx[cx];
-        const Gather gy = L.ry[cy];
-        double value = 0.0;
-        for (int iy = 0; iy < gy.count; ++iy)
-        {
-            const int y = gy.index[iy] - Y0;
-            double line = 0.0;
-            for (int ix = 0; ix < gx.count; ++ix)
-            {
-                const int x = gx.index[ix] - X0;
-                line += gx.weight[ix] * double(sol[(x + y) & 1][y + 1][(x >> 1) + 1]);
-            }
-            value += gy.weight[iy] * line;
-        }
-        crhs[padded_index(C.S, cx, cy)] = T(value);
-    }
-}
-
-// Prolongation of the coarse correction, then 4 sweeps in reversed colour order; on the fine
-// level also sum(z) and sum(r z). PressureMultigrid.cpp:403-407 (cycle), :278-298
-// (prolongCorrection); FluidGridCPU.cpp:1712-1726 (z mean and r.z).
-template <typename T, int K>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_mg_post(const GridDesc* grids, const Tile* tiles, int level)
-{
-    using Shape = TileShape<T, K, false>;
-    const Tile t = tiles[blockIdx.x];
-    const GridDesc& g = grids[t.grid];
-    SolveState& state = *g.state;
-    if (state.done)
-        return;
-    const LevelDesc& L = g.lev[level];
-    const LevelDesc& C = g.lev[level + 1];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int X0 = t.x0 - Shape::HALO, Y0 = t.y0 - Shape::HALO;
-
-    __shared__ T sol[2][Shape::RY + 2][34];
-    for (int i = threadIdx.x; i < 2 * (Shape::RY + 2) * 34; i += 256)
-        (&sol[0][0][0])[i] = T(0);
-
-    TileCells<T, K> cells;
-    tile_load_cells<T, K>(cells, g, L, level, X0, Y0, lane, warp, level == 0 ? state.mean_r : 0.0);
-    __syncthreads();
-
-    const T* pre = static_cast<const T*>(L.pre);
-    const T* coarse = static_cast<const T*>(C.sol);
-#pragma unroll
-    for (int k = 0; k < K; ++k)
-    {
-#pragma unroll
-        for (int c = 0; c < 2; ++c)
-        {
-            const int y = warp + 8 * k;
-            const int x = 2 * lane + ((c + y) & 1);
-            const int gx = X0 + x, gy = Y0 + y;
-            if (gx < 0 || gx >= L.w || gy < 0 || gy >= L.h)
-                continue;
-            const Interp px = L.px[gx];
-            const Interp py = L.py[gy];
-            const long long top = padded_index(C.S, 0, py.first);
-            const long long bottom = padded_index(C.S, 0, py.second);
-            const double a = (1.0 - px.weight) * double(coarse[top + px.first]) + px.weight * double(coarse[top + px.second]);
-            const double b =
-                (1.0 - px.weight) * double(coarse[bottom + px.first]) + px.weight * double(coarse[bottom + px.second]);
-            const double value = double(pre[padded_index(L.S, gx, gy)]) + ((1.0 - py.weight) * a + py.weight * b);
-            sol[c][y + 1][lane + 1] = T(value);
-        }
-    }
-    __syncthreads();
-
-#pragma unroll 1
-    for (int sweep = 0; sweep < 4; ++sweep)
-    {
-        tile_half_sweep<T, K>(sol, cells, 1, false, lane, warp);
-        tile_half_sweep<T, K>(sol, cells, 0, false, lane, warp);
-    }
-
-    T* out = static_cast<T*>(L.sol);
-    const T* r = static_cast<const T*>(g.r);
-    double sz = 0.0, srz = 0.0;
-#pragma unroll
-    for (int k = 0; k < K; ++k)
-    {
-#pragma unroll
-        for (int c = 0; c < 2; ++c)
-        {
-            const int y = warp + 8 * k;
-            const int x = 2 * lane + ((c + y) & 1);
-            const int gx = X0 + x, gy = Y0 + y;
-            if (x < Shape::HALO || x >= Shape::HALO + Shape::OX || y < Shape::HALO || y >= Shape::HALO + Shape::OY ||
-                gx >= L.w || gy >= L.h)
-                continue;
-            const long long i = padded_index(L.S, gx, gy);
-            const T value = sol[c][y + 1][lane + 1];
-            out[i] = value;
-            if (level == 0 && !(g.solid && g.solid[(long long)gy * g.W + gx]))
-            {
-                sz += double(value);
-                srz += double(r[i]) * double(value);
-            }
-        }
-    }
-    if (level != 0)
-        return;
-    __shared__ double4 total;
-    if (arrive_last<256>(g, t.index, g.post_tiles, block_reduce4<256>(make_double4(sz, srz, 0, 0), 0), &total, 0))
-    {
-        if (threadIdx.x == 0)
-            finish_preconditioner(state, total.x, total.y);
-    }
-}
-
-// ------------------------------------------------------------------------------------------
 // Coarse tail: the remaining levels cycled by one CTA in shared memory
 // ------------------------------------------------------------------------------------------
 
 constexpr int kTailThreads = 512;
+constexpr int kTailWarps = kTailThreads / 32;
+
+// Dynamic shared memory of the tail kernel. Levels address it through element offsets so that
+// every access is a shared-memory access.
+extern __shared__ __align__(16) unsigned char tail_smem[];
 
 template <typename T> struct TailLevel
 {
-    int w, h, s; // s = w + 2, one zero halo cell
-    T *right, *down, *inv, *rhs, *sol, *res;
+    int w, h, s;                      // s = w + 2, one zero halo cell
+    int right, down, inv, rhs, sol, res; // element offsets of the level's arrays
+    int px, py, rx, ry;               // byte offsets of the transfer tables
     __device__ int at(int x, int y) const { return (y + 1) * s + x + 1; }
 };
 
-// Shared-memory bytes of the tail of a grid starting at `first` (host and device agree).
-__host__ __device__ inline size_t tail_bytes(const int* w, const int* h, int first, int levels, size_t elem)
+template <typename T> __device__ __forceinline__ T* tail_array() { return reinterpret_cast<T*>(tail_smem); }
+template <typename E> __device__ __forceinline__ E* tail_table(int offset)
 {
-    size_t cells = 0;
-    for (int l = first; l < levels; ++l)
-        cells += size_t(w[l] + 2) * (h[l] + 2);
-    return cells * 6 * elem + 2 * kMaxCoarse * sizeof(double) + 64;
+    return reinterpret_cast<E*>(tail_smem + offset);
 }
 
-template <typename T> __device__ void tail_smooth(const TailLevel<T>& L, bool reverse, bool from_zero)
+__host__ __device__ inline size_t align16(size_t n) { return (n + 15) / 16 * 16; }
+__host__ __device__ inline int padded_index32_tail(int S, int x, int y) { return (y + 1) * S + x + kPadX; }
+
+// Shared-memory layout of the tail of a grid starting at level `first` (host and device
+// agree): per level six padded arrays, then the transfer tables, then the coarsest inverse and
+// two vectors of the coarsest solve.
+__host__ __device__ inline size_t tail_bytes(const int* w, const int* h, int first, int levels, size_t elem)
 {
-    const int half = (L.w + 1) / 2;
+    size_t bytes = 0;
+    for (int l = first; l < levels; ++l)
+        bytes += align16(size_t(w[l] + 2) * (h[l] + 2) * 6 * elem);
+    for (int l = first; l + 1 < levels; ++l)
+        bytes += align16((w[l] + h[l]) * sizeof(Interp)) + align16((w[l + 1] + h[l + 1]) * sizeof(Gather));
+    bytes += align16(size_t(kMaxCoarse) * kMaxCoarse * sizeof(double)) + 2 * kMaxCoarse * sizeof(double);
+    return bytes;
+}
+
+// One half-sweep pair (a full red-black sweep) over a tail level; warp = row, lane = column pair.
+template <typename T> __device__ void tail_smooth(const TailLevel<T> L, bool reverse, bool from_zero)
+{
+    T* const m = tail_array<T>();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int pass = 0; pass < 2; ++pass)
     {
         const int colour = reverse ? 1 - pass : pass;
-        for (int q = threadIdx.x; q < half * L.h; q += blockDim.x)
+        const bool skip = from_zero && pass == 0;
+        for (int y = warp; y < L.h; y += kTailWarps)
         {
-            const int y = q / half;
-            const int x = 2 * (q % half) + ((colour + y) & 1);
-            if (x >= L.w)
-                continue;
-            const int i = L.at(x, y);
-            T value = L.rhs[i];
-            if (!(from_zero && pass == 0))
-                value = value + ((L.right[i - 1] * L.sol[i - 1] + L.right[i] * L.sol[i + 1]) +
-                                    (L.down[i - L.s] * L.sol[i - L.s] + L.down[i] * L.sol[i + L.s]));
-            L.sol[i] = value * L.inv[i];
+            for (int x = 2 * lane + ((colour + y) & 1); x < L.w; x += 64)
+            {
+                const int i = L.at(x, y);
+                T value = m[L.rhs + i];
+                if (!skip)
+                    value = value + ((m[L.right + i - 1] * m[L.sol + i - 1] + m[L.right + i] * m[L.sol + i + 1]) +
+                                        (m[L.down + i - L.s] * m[L.sol + i - L.s] + m[L.down + i] * m[L.sol + i + L.s]));
+                m[L.sol + i] = value * m[L.inv + i];
+            }
         }
         __syncthreads();
     }
 }
 
-template <typename T>
-__device__ void tail_restrict(const TailLevel<T>& F, const TailLevel<T>& Cl, const LevelDesc& fine_desc)
+template <typename T> __device__ void tail_restrict(const TailLevel<T> F, const TailLevel<T> Cl)
 {
-    for (int q = threadIdx.x; q < F.w * F.h; q += blockDim.x)
+    T* const m = tail_array<T>();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int y = warp; y < F.h; y += kTailWarps)
     {
-        const int x = q % F.w, y = q / F.w;
-        const int i = F.at(x, y);
-        const T center = F.sol[i];
-        const T product = (F.right[i - 1] * (center - F.sol[i - 1]) + F.right[i] * (center - F.sol[i + 1])) +
-                          (F.down[i - F.s] * (center - F.sol[i - F.s]) + F.down[i] * (center - F.sol[i + F.s]));
-        // Cells without an open face pass no residual down (keeps the cycle symmetric).
-        F.res[i] = F.inv[i] > T(0) ? F.rhs[i] - product : T(0);
+        for (int x = lane; x < F.w; x += 32)
+        {
+            const int i = F.at(x, y);
+            const T center = m[F.sol + i];
+            const T product =
+                (m[F.right + i - 1] * (center - m[F.sol + i - 1]) + m[F.right + i] * (center - m[F.sol + i + 1])) +
+                (m[F.down + i - F.s] * (center - m[F.sol + i - F.s]) + m[F.down + i] * (center - m[F.sol + i + F.s]));
+            // Cells without an open face pass no residual down (keeps the cycle symmetric).
+            m[F.res + i] = m[F.inv + i] > T(0) ? m[F.rhs + i] - product : T(0);
+        }
     }
     __syncthreads();
-    for (int q = threadIdx.x; q < Cl.w * Cl.h; q += blockDim.x)
+    const Gather* rx = tail_table<const Gather>(F.rx);
+    const Gather* ry = tail_table<const Gather>(F.ry);
+    for (int cy = warp; cy < Cl.h; cy += kTailWarps)
     {
-        const int cx = q % Cl.w, cy = q / Cl.w;
-        const Gather gx = fine_desc.rx[cx];
-        const Gather gy = fine_desc.ry[cy];
-        double value = 0.0;
-        for (int iy = 0; iy < gy.count; ++iy)
+        const Gather gy = ry[cy];
+        for (int cx = lane; cx < Cl.w; cx += 32)
         {
-            double line = 0.0;
-            for (int ix = 0; ix < gx.count; ++ix)
-                line += gx.weight[ix] * double(F.res[F.at(gx.index[ix], gy.index[iy])]);
-            value += gy.weight[iy] * line;
+            const Gather& gx = rx[cx];
+            double value = 0.0;
+            for (int iy = 0; iy < gy.count; ++iy)
+            {
+                double line = 0.0;
+                for (int ix = 0; ix < gx.count; ++ix)
+                    line += gx.weight[ix] * double(m[F.res + F.at(gx.index[ix], gy.index[iy])]);
+                value += gy.weight[iy] * line;
+            }
+            m[Cl.rhs + Cl.at(cx, cy)] = T(value);
         }
-        Cl.rhs[Cl.at(cx, cy)] = T(value);
     }
     __syncthreads();
 }
 
-template <typename T>
-__device__ void tail_prolong(const TailLevel<T>& Cl, const TailLevel<T>& F, const LevelDesc& fine_desc)
+template <typename T> __device__ void tail_prolong(const TailLevel<T> Cl, const TailLevel<T> F)
 {
-    for (int q = threadIdx.x; q < F.w * F.h; q += blockDim.x)
+    T* const m = tail_array<T>();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const Interp* px = tail_table<const Interp>(F.px);
+    const Interp* pys = tail_table<const Interp>(F.py);
+    for (int y = warp; y < F.h; y += kTailWarps)
     {
-        const int x = q % F.w, y = q / F.w;
-        const Interp px = fine_desc.px[x];
-        const Interp py = fine_desc.py[y];
-        const double a = (1.0 - px.weight) * double(Cl.sol[Cl.at(px.first, py.first)]) +
-                         px.weight * double(Cl.sol[Cl.at(px.second, py.first)]);
-        const double b = (1.0 - px.weight) * double(Cl.sol[Cl.at(px.first, py.second)]) +
-                         px.weight * double(Cl.sol[Cl.at(px.second, py.second)]);
-        const int i = F.at(x, y);
-        F.sol[i] = T(double(F.sol[i]) + ((1.0 - py.weight) * a + py.weight * b));
+        const Interp py = pys[y];
+        for (int x = lane; x < F.w; x += 32)
+        {
+            const Interp& p = px[x];
+            const double a = (1.0 - p.weight) * double(m[Cl.sol + Cl.at(p.first, py.first)]) +
+                             p.weight * double(m[Cl.sol + Cl.at(p.second, py.first)]);
+            const double b = (1.0 - p.weight) * double(m[Cl.sol + Cl.at(p.first, py.second)]) +
+                             p.weight * double(m[Cl.sol + Cl.at(p.second, py.second)]);
+            const int i = F.at(x, y);
+            m[F.sol + i] = T(double(m[F.sol + i]) + ((1.0 - py.weight) * a + py.weight * b));
+        }
     }
     __syncthreads();
 }
@@ -630,41 +378,58 @@ __device__ void tail_prolong(const TailLevel<T>& Cl, const TailLevel<T>& F, cons
 // Mean-free rhs, explicit inverse, mean-zero gauge over the open cells.
 // PressureMultigrid.cpp:347-384 (solveCoarsest).
 template <typename T>
-__device__ void tail_solve_coarsest(const TailLevel<T>& L, const double* inverse, const CoarseInfo& info, double* b,
-    double* z)
+__device__ void tail_solve_coarsest(const TailLevel<T> L, int inverse_offset, int vectors_offset, const CoarseInfo& info)
 {
+    T* const m = tail_array<T>();
+    const double* inverse = tail_table<const double>(inverse_offset);
+    double* b = tail_table<double>(vectors_offset);
+    double* z = b + kMaxCoarse;
     __shared__ double mean_shared;
     const int cells = L.w * L.h, n = info.n;
-    double part = 0.0;
-    for (int q = threadIdx.x; q < cells; q += blockDim.x)
-        if (q == info.pinned || info.map[q] >= 0)
-            part += double(L.rhs[L.at(q % L.w, q / L.w)]);
-    const double4 total = block_reduce4<kTailThreads>(make_double4(part, 0, 0, 0), 0);
-    if (threadIdx.x == 0)
-        mean_shared = info.open > 0 ? total.x / info.open : 0.0;
+    // Single-warp reductions: the coarsest level has at most 64 cells.
+    if (threadIdx.x < 32)
+    {
+        double part = 0.0;
+        for (int q = threadIdx.x; q < cells; q += 32)
+            if (q == info.pinned || info.map[q] >= 0)
+                part += double(m[L.rhs + L.at(q % L.w, q / L.w)]);
+        part = warp_sum(part);
+        if (threadIdx.x == 0)
+            mean_shared = info.open > 0 ? part / info.open : 0.0;
+    }
     __syncthreads();
     const double mean = mean_shared;
     for (int q = threadIdx.x; q < cells; q += blockDim.x)
     {
         const int k = info.map[q];
         if (k >= 0)
-            b[k] = double(L.rhs[L.at(q % L.w, q / L.w)]) - mean;
+            b[k] = double(m[L.rhs + L.at(q % L.w, q / L.w)]) - mean;
     }
     __syncthreads();
-    for (int row = threadIdx.x; row < n; row += blockDim.x)
+    // z = inverse b: eight threads per row, then a shuffle fold within each group of eight.
+    for (int base = 0; base < n; base += kTailThreads / 8)
     {
+        const int row = base + int(threadIdx.x >> 3), part = threadIdx.x & 7;
         double value = 0.0;
-        for (int col = 0; col < n; ++col)
-            value += inverse[row * n + col] * b[col];
-        z[row] = value;
+        if (row < n)
+            for (int col = part; col < n; col += 8)
+                value += inverse[row * n + col] * b[col];
+        value += __shfl_xor_sync(0xffffffffu, value, 1);
+        value += __shfl_xor_sync(0xffffffffu, value, 2);
+        value += __shfl_xor_sync(0xffffffffu, value, 4);
+        if (row < n && part == 0)
+            z[row] = value;
     }
     __syncthreads();
-    double zpart = 0.0;
-    for (int k = threadIdx.x; k < n; k += blockDim.x)
-        zpart += z[k];
-    const double4 ztotal = block_reduce4<kTailThreads>(make_double4(zpart, 0, 0, 0), 0);
-    if (threadIdx.x == 0)
-        mean_shared = info.open > 0 ? ztotal.x / info.open : 0.0;
+    if (threadIdx.x < 32)
+    {
+        double part = 0.0;
+        for (int k = threadIdx.x; k < n; k += 32)
+            part += z[k];
+        part = warp_sum(part);
+        if (threadIdx.x == 0)
+            mean_shared = info.open > 0 ? part / info.open : 0.0;
+    }
     __syncthreads();
     const double zmean = mean_shared;
     for (int q = threadIdx.x; q < cells; q += blockDim.x)
@@ -675,7 +440,7 @@ __device__ void tail_solve_coarsest(const TailLevel<T>& L, const double* inverse
             value = z[k] - zmean;
         else if (q == info.pinned)
             value = -zmean;
-        L.sol[L.at(q % L.w, q / L.w)] = T(value);
+        m[L.sol + L.at(q % L.w, q / L.w)] = T(value);
     }
     __syncthreads();
 }
@@ -686,62 +451,109 @@ template <typename T> __global__ void __launch_bounds__(kTailThreads) k_mg_tail(
     SolveState& state = *g.state;
     if (state.done)
         return;
-    extern __shared__ __align__(16) unsigned char tail_smem[];
     const int first = g.tail, last = g.levels - 1;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    T* const m = tail_array<T>();
     TailLevel<T> lv[kMaxLevels];
-    size_t offset = 0;
-    T* base = reinterpret_cast<T*>(tail_smem);
+    int cursor = 0; // bytes
     for (int l = first; l <= last; ++l)
     {
         TailLevel<T>& L = lv[l];
         L.w = g.lev[l].w;
         L.h = g.lev[l].h;
         L.s = L.w + 2;
-        const size_t cells = size_t(L.s) * (L.h + 2);
-        T** arrays[6] = {&L.right, &L.down, &L.inv, &L.rhs, &L.sol, &L.res};
-        for (int a = 0; a < 6; ++a)
-        {
-            *arrays[a] = base + offset;
-            offset += cells;
-        }
+        const int cells = L.s * (L.h + 2);
+        const int base = cursor / int(sizeof(T));
+        L.right = base;
+        L.down = base + cells;
+        L.inv = base + 2 * cells;
+        L.rhs = base + 3 * cells;
+        L.sol = base + 4 * cells;
+        L.res = base + 5 * cells;
+        cursor += int(align16(size_t(cells) * 6 * sizeof(T)));
     }
-    double* b = reinterpret_cast<double*>(tail_smem + ((offset * sizeof(T) + 15) / 16) * 16);
-    double* z = b + kMaxCoarse;
-    for (size_t i = threadIdx.x; i < offset; i += blockDim.x)
-        base[i] = T(0);
-    __syncthreads();
+    for (int l = first; l < last; ++l)
+    {
+        TailLevel<T>& L = lv[l];
+        L.px = cursor;
+        L.py = cursor + L.w * int(sizeof(Interp));
+        cursor += int(align16((L.w + L.h) * sizeof(Interp)));
+        L.rx = cursor;
+        L.ry = cursor + lv[l + 1].w * int(sizeof(Gather));
+        cursor += int(align16((lv[l + 1].w + lv[l + 1].h) * sizeof(Gather)));
+    }
+    const int inverse_offset = cursor;
+    cursor += int(align16(size_t(kMaxCoarse) * kMaxCoarse * sizeof(double)));
+    const int vectors_offset = cursor;
+    const int array_elements = lv[last].res + (lv[last].s * (lv[last].h + 2)) - lv[first].right;
 
-    // Coefficients of every tail level and the first level's right-hand side.
+    // Everything the cycle touches is copied in once: coefficients, tables, the inverse, and
+    // the first level's right-hand side; halos and the other arrays start at zero.
+    for (int i = threadIdx.x; i < array_elements; i += blockDim.x)
+        m[i] = T(0);
+    __shared__ CoarseInfo info;
+    if (threadIdx.x < int(sizeof(CoarseInfo) / sizeof(int)))
+        reinterpret_cast<int*>(&info)[threadIdx.x] = reinterpret_cast<const int*>(g.coarse)[threadIdx.x];
+    __syncthreads();
     const double mean_r = first == 0 ? state.mean_r : 0.0;
     for (int l = first; l <= last; ++l)
     {
-        const TailLevel<T>& L = lv[l];
+        const TailLevel<T> L = lv[l];
         const LevelDesc& D = g.lev[l];
         const T* right = static_cast<const T*>(D.right);
         const T* down = static_cast<const T*>(D.down);
         const T* rhs = first == 0 ? static_cast<const T*>(g.r) : static_cast<const T*>(D.rhs);
-        for (int q = threadIdx.x; q < L.w * L.h; q += blockDim.x)
+        const bool with_rhs = l == first;
+        for (int y = warp; y < L.h; y += kTailWarps)
         {
-            const int x = q % L.w, y = q / L.w;
-            const long long i = padded_index(D.S, x, y);
-            const int j = L.at(x, y);
-            L.right[j] = right[i];
-            L.down[j] = down[i];
-            if (l == first)
-                L.rhs[j] = first == 0 ? T(double(rhs[i]) - mean_r) : rhs[i];
+            for (int x = lane; x < L.w; x += 32)
+            {
+                const int i = padded_index32_tail(D.S, x, y);
+                const int j = L.at(x, y);
+                const T wr = right[i], wd = down[i];
+                const T b = with_rhs ? rhs[i] : T(0);
+                m[L.right + j] = wr;
+                m[L.down + j] = wd;
+                if (with_rhs)
+                    m[L.rhs + j] = first == 0 ? T(double(b) - mean_r) : b;
+            }
         }
+        if (l < last)
+        {
+            Interp* px = tail_table<Interp>(L.px);
+            Interp* py = tail_table<Interp>(L.py);
+            Gather* rx = tail_table<Gather>(L.rx);
+            Gather* ry = tail_table<Gather>(L.ry);
+            for (int i = threadIdx.x; i < L.w; i += blockDim.x)
+                px[i] = D.px[i];
+            for (int i = threadIdx.x; i < L.h; i += blockDim.x)
+                py[i] = D.py[i];
+            for (int i = threadIdx.x; i < lv[l + 1].w; i += blockDim.x)
+                rx[i] = D.rx[i];
+            for (int i = threadIdx.x; i < lv[l + 1].h; i += blockDim.x)
+                ry[i] = D.ry[i];
+        }
+    }
+    {
+        double* inverse = tail_table<double>(inverse_offset);
+        const int n = info.n;
+        for (int i = threadIdx.x; i < n * n; i += blockDim.x)
+            inverse[i] = g.coarse_inverse[i];
     }
     __syncthreads();
     for (int l = first; l <= last; ++l)
     {
-        const TailLevel<T>& L = lv[l];
-        for (int q = threadIdx.x; q < L.w * L.h; q += blockDim.x)
+        const TailLevel<T> L = lv[l];
+        for (int y = warp; y < L.h; y += kTailWarps)
         {
-            const int j = L.at(q % L.w, q / L.w);
-            const T diag = ((L.right[j - 1] + L.right[j]) + L.down[j - L.s]) + L.down[j];
-            L.inv[j] = diag > T(0) ? T(1) / diag : T(0);
-            if (l == first && !(diag > T(0)))
-                L.rhs[j] = T(0);
+            for (int x = lane; x < L.w; x += 32)
+            {
+                const int j = L.at(x, y);
+                const T diag = ((m[L.right + j - 1] + m[L.right + j]) + m[L.down + j - L.s]) + m[L.down + j];
+                m[L.inv + j] = diag > T(0) ? T(1) / diag : T(0);
+                if (l == first && !(diag > T(0)))
+                    m[L.rhs + j] = T(0);
+            }
         }
     }
     __syncthreads();
@@ -751,32 +563,35 @@ template <typename T> __global__ void __launch_bounds__(kTailThreads) k_mg_tail(
         tail_smooth(lv[l], false, true);
         for (int sweep = 1; sweep < 4; ++sweep)
             tail_smooth(lv[l], false, false);
-        tail_restrict(lv[l], lv[l + 1], g.lev[l]);
+        tail_restrict(lv[l], lv[l + 1]);
     }
-    tail_solve_coarsest(lv[last], g.coarse_inverse, *g.coarse, b, z);
+    tail_solve_coarsest(lv[last], inverse_offset, vectors_offset, info);
     for (int l = last - 1; l >= first; --l)
     {
-        tail_prolong(lv[l + 1], lv[l], g.lev[l]);
+        tail_prolong(lv[l + 1], lv[l]);
         for (int sweep = 0; sweep < 4; ++sweep)
             tail_smooth(lv[l], true, false);
     }
 
     // Hand the first tail level's solution to the finer post-smoothing (or to z).
-    const TailLevel<T>& F = lv[first];
+    const TailLevel<T> F = lv[first];
     const LevelDesc& D = g.lev[first];
     T* out = static_cast<T*>(D.sol);
     const T* r = static_cast<const T*>(g.r);
     double sz = 0.0, srz = 0.0;
-    for (int q = threadIdx.x; q < F.w * F.h; q += blockDim.x)
+    for (int y = warp; y < F.h; y += kTailWarps)
     {
-        const int x = q % F.w, y = q / F.w;
-        const long long i = padded_index(D.S, x, y);
-        const T value = F.sol[F.at(x, y)];
-        out[i] = value;
-        if (first == 0 && !(g.solid && g.solid[(long long)y * g.W + x]))
+        for (int x = lane; x < F.w; x += 32)
         {
-            sz += double(value);
-            srz += double(r[i]) * double(value);
+            const int i = padded_index32_tail(D.S, x, y);
+            const T value = m[F.sol + F.at(x, y)];
+            out[i] = value;
+            if (first == 0)
+            {
+                // Cells without an open face hold z = 0; the rest add to both sums.
+                sz += double(value);
+                srz += double(r[i]) * double(value);
+            }
         }
     }
     if (first != 0)

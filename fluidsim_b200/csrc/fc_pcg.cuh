@@ -42,9 +42,9 @@ __global__ void k_density(const GridDesc* grids, const Tile* tiles)
 {
     FC_VEC_TILE_PROLOGUE
     const double inv_area = 1.0 / (g.dx * g.dx);
-    for (int k = 0; k < 4; ++k)
+    for (int k = 0; k < kVecCells; ++k)
     {
-        const int x = t.x0 + tx, y = t.y0 + ty + 8 * k;
+        const int x = t.x0 + tx + 32 * (k & 1), y = t.y0 + ty + 8 * (k >> 1);
         if (x >= g.W || y >= g.H)
             continue;
         const long long i = (long long)y * g.W + x;
@@ -63,9 +63,9 @@ template <typename T> __global__ void k_coefficients(const GridDesc* grids, cons
     const double* density = g.density;
     T* right = static_cast<T*>(g.lev[0].right);
     T* down = static_cast<T*>(g.lev[0].down);
-    for (int k = 0; k < 4; ++k)
+    for (int k = 0; k < kVecCells; ++k)
     {
-        const int x = t.x0 + tx, y = t.y0 + ty + 8 * k;
+        const int x = t.x0 + tx + 32 * (k & 1), y = t.y0 + ty + 8 * (k >> 1);
         if (x >= g.W || y >= g.H)
             continue;
         const long long c = (long long)y * g.W + x;
@@ -123,9 +123,9 @@ template <typename T> __global__ void __launch_bounds__(kVecThreads) k_rhs(const
     const double dt = g.state->dt;
     const double scale = g.dx * g.dx / dt;
     double sum = 0.0;
-    for (int k = 0; k < 4; ++k)
+    for (int k = 0; k < kVecCells; ++k)
     {
-        const int x = t.x0 + tx, y = t.y0 + ty + 8 * k;
+        const int x = t.x0 + tx + 32 * (k & 1), y = t.y0 + ty + 8 * (k >> 1);
         if (x >= g.W || y >= g.H)
             continue;
         double ul, ur, vu, vd;
@@ -152,9 +152,9 @@ template <typename T> __global__ void __launch_bounds__(kVecThreads) k_rhs_stats
     FC_VEC_TILE_PROLOGUE
     const double mean = g.state->mean_b;
     double mx = 0.0, sq = 0.0;
-    for (int k = 0; k < 4; ++k)
+    for (int k = 0; k < kVecCells; ++k)
     {
-        const int x = t.x0 + tx, y = t.y0 + ty + 8 * k;
+        const int x = t.x0 + tx + 32 * (k & 1), y = t.y0 + ty + 8 * (k >> 1);
         if (x >= g.W || y >= g.H || cell_solid(g, x, y))
             continue;
         const double b = g.b[padded_index(g.S, x, y)] - mean;
@@ -187,9 +187,9 @@ __global__ void __launch_bounds__(kVecThreads) k_warm_start(const GridDesc* grid
     FC_VEC_TILE_PROLOGUE
     const bool clear = g.state->status == kNoWork;
     double sum = 0.0;
-    for (int k = 0; k < 4; ++k)
+    for (int k = 0; k < kVecCells; ++k)
     {
-        const int x = t.x0 + tx, y = t.y0 + ty + 8 * k;
+        const int x = t.x0 + tx + 32 * (k & 1), y = t.y0 + ty + 8 * (k >> 1);
         if (x >= g.W || y >= g.H)
             continue;
         const long long i = padded_index(g.S, x, y);
@@ -220,9 +220,9 @@ __global__ void __launch_bounds__(kVecThreads) k_pressure_sum(const GridDesc* gr
     if (g.state->status == kBreakdown)
         return;
     double sum = 0.0;
-    for (int k = 0; k < 4; ++k)
+    for (int k = 0; k < kVecCells; ++k)
     {
-        const int x = t.x0 + tx, y = t.y0 + ty + 8 * k;
+        const int x = t.x0 + tx + 32 * (k & 1), y = t.y0 + ty + 8 * (k >> 1);
         if (x >= g.W || y >= g.H || cell_solid(g, x, y))
             continue;
         sum += g.p[padded_index(g.S, x, y)];
@@ -242,9 +242,9 @@ __global__ void k_remove_pressure_mean(const GridDesc* grids, const Tile* tiles)
     if (g.state->status == kBreakdown)
         return;
     const double mean = g.state->mean_p;
-    for (int k = 0; k < 4; ++k)
+    for (int k = 0; k < kVecCells; ++k)
     {
-        const int x = t.x0 + tx, y = t.y0 + ty + 8 * k;
+        const int x = t.x0 + tx + 32 * (k & 1), y = t.y0 + ty + 8 * (k >> 1);
         if (x >= g.W || y >= g.H)
             continue;
         const long long i = padded_index(g.S, x, y);
@@ -276,9 +276,9 @@ __global__ void __launch_bounds__(kVecThreads) k_true_residual(const GridDesc* g
     T* r = static_cast<T*>(g.r);
     const double mean_b = s.mean_b;
     double sum = 0.0, mx = 0.0, sq = 0.0;
-    for (int k = 0; k < 4; ++k)
+    for (int k = 0; k < kVecCells; ++k)
     {
-        const int x = t.x0 + tx, y = t.y0 + ty + 8 * k;
+        const int x = t.x0 + tx + 32 * (k & 1), y = t.y0 + ty + 8 * (k >> 1);
         if (x >= g.W || y >= g.H)
             continue;
         const long long i = padded_index(g.S, x, y);
@@ -329,22 +329,65 @@ __global__ void __launch_bounds__(kVecThreads) k_true_residual(const GridDesc* g
     }
 }
 
-// d_new = (z - mean z) + beta d_old at one cell (the reference's direction update, :1812-1816,
-// after the correction's mean removal at :1712-1722).
-template <typename T>
-__device__ __forceinline__ double direction_at(const T* z, const T* d_old, long long i, double mean_z, double beta)
+template <typename T> struct VecPair;
+template <> struct VecPair<float>
 {
-    return (dd(z[i]) - mean_z) + beta * dd(d_old[i]);
+    using type = float2;
+};
+template <> struct VecPair<double>
+{
+    using type = double2;
+};
+
+// Direction d = (z - mean z) + beta d_old at the column pair (gx, gx + 1) of padded row gy,
+// rounded to the working type (the operator and the p update read exactly the stored d); the
+// padded halo rows -1 and H read as zero fields. The reference forms z - mean at
+// FluidGridCPU.cpp:1712-1722 and d at :1812-1816.
+template <typename T>
+__device__ __forceinline__ typename VecPair<T>::type direction_pair(const GridDesc& g, const T* z, const T* d_old,
+    int gx, int gy, bool cols, double mean_z, double beta)
+{
+    using P = typename VecPair<T>::type;
+    P zz = P{}, dd2 = P{};
+    if (cols && gy >= -1 && gy <= g.H)
+    {
+        const long long i = padded_index(g.S, gx, gy);
+        zz = *reinterpret_cast<const P*>(z + i);
+        dd2 = *reinterpret_cast<const P*>(d_old + i);
+    }
+    P out;
+    out.x = T((double(zz.x) - mean_z) + beta * double(dd2.x));
+    out.y = T((double(zz.y) - mean_z) + beta * double(dd2.y));
+    return out;
 }
 
-// d = (z - mean z) + beta d_old; q = A d; returns d.q through the grid's reduction.
+template <typename T>
+__device__ __forceinline__ T direction_one(const GridDesc& g, const T* z, const T* d_old, int x, int y, double mean_z,
+    double beta)
+{
+    if (x + kPadX < 0 || x + kPadX >= g.S || y < -1 || y > g.H)
+        return T(0);
+    const long long i = padded_index(g.S, x, y);
+    return T((double(z[i]) - mean_z) + beta * double(d_old[i]));
+}
+
+// d = (z - mean z) + beta d_old; q = A d; d.q through the grid's reduction. Warp w handles rows
+// 8w .. 8w + 7 of the tile's 64 columns (lane = column pair) in two passes of four rows: all
+// loads of a pass (six rows of z and d, four rows of weights) are issued first, then the
+// directions and the operator are formed in registers; horizontal neighbours across pairs are
+// warp shuffles, and lanes 0 and 31 fetch the columns just outside the warp.
+// Operator: FluidGridCPU.cpp:1507-1598.
 template <typename T>
 __global__ void __launch_bounds__(kVecThreads) k_direction_operator(const GridDesc* grids, const Tile* tiles, int parity)
 {
-    FC_VEC_TILE_PROLOGUE
+    using P = typename VecPair<T>::type;
+    constexpr int R = 4;
+    const Tile t = tiles[blockIdx.x];
+    const GridDesc& g = grids[t.grid];
     SolveState& s = *g.state;
     if (s.done)
         return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const T* right = static_cast<const T*>(g.lev[0].right);
     const T* down = static_cast<const T*>(g.lev[0].down);
     const T* z = static_cast<const T*>(g.z);
@@ -353,24 +396,110 @@ __global__ void __launch_bounds__(kVecThreads) k_direction_operator(const GridDe
     T* q = static_cast<T*>(g.q);
     const double mean_z = s.mean_z, beta = s.beta;
     const int S = g.S;
+    const int gx = t.x0 + 2 * lane;
+    const bool cols = gx < g.W; // the pair's first column lies in the grid
+    const bool in_b = gx + 1 < g.W;
+    // Column just outside the warp: left of the first pair for lane 0, right of the last for 31.
+    const int edge_x = lane == 0 ? gx - 1 : gx + 2;
+    const bool edge = (lane == 0 && cols) || (lane == 31 && gx + 2 + kPadX < S);
+    P up_w = P{};
+    if (cols)
+        up_w = *reinterpret_cast<const P*>(down + padded_index(S, gx, t.y0 + 8 * warp - 1));
     double dot = 0.0;
-    for (int k = 0; k < 4; ++k)
+#pragma unroll 1
+    for (int pass = 0; pass < 2; ++pass)
     {
-        const int x = t.x0 + tx, y = t.y0 + ty + 8 * k;
-        if (x >= g.W || y >= g.H)
-            continue;
-        const long long i = padded_index(S, x, y);
-        // Direction values are rounded to the working type before the operator reads them, so
-        // that q = A d uses exactly the stored d (the p update reads the same stored d).
-        const T c = T(direction_at(z, d_old, i, mean_z, beta));
-        const T l = T(direction_at(z, d_old, i - 1, mean_z, beta));
-        const T rr = T(direction_at(z, d_old, i + 1, mean_z, beta));
-        const T u = T(direction_at(z, d_old, i - S, mean_z, beta));
-        const T dn = T(direction_at(z, d_old, i + S, mean_z, beta));
-        const T value = (right[i - 1] * (c - l) + right[i] * (c - rr)) + (down[i - S] * (c - u) + down[i] * (c - dn));
-        d_new[i] = c;
-        q[i] = value;
-        dot += dd(c) * dd(value);
+        const int y0 = t.y0 + 8 * warp + R * pass;
+        P zz[R + 2], dd0[R + 2], w[R], dn[R];
+        T ez[R], ed[R], ew[R];
+#pragma unroll
+        for (int k = 0; k < R + 2; ++k)
+        {
+            const int y = y0 - 1 + k;
+            zz[k] = P{};
+            dd0[k] = P{};
+            if (cols && y >= -1 && y <= g.H)
+            {
+                const long long i = padded_index(S, gx, y);
+                zz[k] = *reinterpret_cast<const P*>(z + i);
+                dd0[k] = *reinterpret_cast<const P*>(d_old + i);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < R; ++k)
+        {
+            const int y = y0 + k;
+            w[k] = P{};
+            dn[k] = P{};
+            ez[k] = ed[k] = ew[k] = T(0);
+            if (y < g.H)
+            {
+                const long long i = padded_index(S, gx, y);
+                if (cols)
+                {
+                    w[k] = *reinterpret_cast<const P*>(right + i);
+                    dn[k] = *reinterpret_cast<const P*>(down + i);
+                }
+                if (edge)
+                {
+                    const long long e = padded_index(S, edge_x, y);
+                    ez[k] = z[e];
+                    ed[k] = d_old[e];
+                    ew[k] = right[e]; // lane 0: the face between gx - 1 and gx
+                }
+            }
+        }
+        // Directions, rounded to the working type (the operator and the p update read the
+        // stored d); halo rows and padding columns read zero fields.
+        P dir[R + 2];
+#pragma unroll
+        for (int k = 0; k < R + 2; ++k)
+        {
+            dir[k].x = T((double(zz[k].x) - mean_z) + beta * double(dd0[k].x));
+            dir[k].y = T((double(zz[k].y) - mean_z) + beta * double(dd0[k].y));
+        }
+#pragma unroll
+        for (int k = 0; k < R; ++k)
+        {
+            const int y = y0 + k;
+            const P prev = dir[k], cur = dir[k + 1], next = dir[k + 2];
+            T left = __shfl_up_sync(0xffffffffu, cur.y, 1);
+            T right_d = __shfl_down_sync(0xffffffffu, cur.x, 1);
+            T wl = __shfl_up_sync(0xffffffffu, w[k].y, 1);
+            const T edge_dir = T((double(ez[k]) - mean_z) + beta * double(ed[k]));
+            if (lane == 0)
+            {
+                left = edge_dir;
+                wl = ew[k];
+            }
+            if (lane == 31)
+                right_d = edge_dir;
+            const P uw = k == 0 ? up_w : dn[k - 1];
+            if (cols && y < g.H)
+            {
+                const long long i = padded_index(S, gx, y);
+                const T ca = cur.x, cb = cur.y;
+                const T qa = (wl * (ca - left) + w[k].x * (ca - cb)) + (uw.x * (ca - prev.x) + dn[k].x * (ca - next.x));
+                const T qb =
+                    (w[k].x * (cb - ca) + w[k].y * (cb - right_d)) + (uw.y * (cb - prev.y) + dn[k].y * (cb - next.y));
+                if (in_b)
+                {
+                    *reinterpret_cast<P*>(d_new + i) = cur;
+                    P qq;
+                    qq.x = qa;
+                    qq.y = qb;
+                    *reinterpret_cast<P*>(q + i) = qq;
+                    dot += double(ca) * double(qa) + double(cb) * double(qb);
+                }
+                else
+                {
+                    d_new[i] = ca;
+                    q[i] = qa;
+                    dot += double(ca) * double(qa);
+                }
+            }
+        }
+        up_w = dn[R - 1];
     }
     __shared__ double4 total;
     if (arrive_last<kVecThreads>(g, t.index, g.vec_tiles, block_reduce4<kVecThreads>(make_double4(dot, 0, 0, 0), 0), &total, 0))
@@ -389,10 +518,26 @@ __global__ void __launch_bounds__(kVecThreads) k_direction_operator(const GridDe
 }
 
 // p += alpha d ; r -= alpha q ; residual stats. FluidGridCPU.cpp:1600-1641.
+// The padded halo and row padding of d, q, r and p are zero, so the update runs over the whole
+// padded array as one flat stream: tile t of the grid takes the t-th equal slice, four cells per
+// thread and load, every load of the slice issued before the arithmetic.
+template <typename T> struct Quad;
+template <> struct Quad<float>
+{
+    using type = float4;
+};
+template <> struct Quad<double>
+{
+    using type = double4;
+};
+
 template <typename T>
 __global__ void __launch_bounds__(kVecThreads) k_update(const GridDesc* grids, const Tile* tiles, int parity)
 {
-    FC_VEC_TILE_PROLOGUE
+    using Q = typename Quad<T>::type;
+    constexpr int U = 4; // quads per thread
+    const Tile t = tiles[blockIdx.x];
+    const GridDesc& g = grids[t.grid];
     SolveState& s = *g.state;
     if (s.done)
         return;
@@ -400,20 +545,55 @@ __global__ void __launch_bounds__(kVecThreads) k_update(const GridDesc* grids, c
     const T* q = static_cast<const T*>(g.q);
     T* r = static_cast<T*>(g.r);
     const double alpha = s.rz / s.dq;
+    // The padded length S * (H + 2) is a multiple of 8; slices are whole quads.
+    const long long quads = (long long)g.S * (g.H + 2) / 4;
+    const long long per = (quads + g.vec_tiles - 1) / g.vec_tiles;
+    const long long first = per * t.index;
+    const long long last = min(quads, first + per);
     double sum = 0.0, mx = 0.0, sq = 0.0;
-    for (int k = 0; k < 4; ++k)
+    for (long long base = first + threadIdx.x; base < last; base += (long long)kVecThreads * U)
     {
-        const int x = t.x0 + tx, y = t.y0 + ty + 8 * k;
-        if (x >= g.W || y >= g.H)
-            continue;
-        const long long i = padded_index(g.S, x, y);
-        g.p[i] += alpha * dd(d[i]);
-        const T value = T(dd(r[i]) - alpha * dd(q[i]));
-        r[i] = value;
-        const double rv = dd(value);
-        sum += rv;
-        mx = fmax(mx, fabs(rv));
-        sq += rv * rv;
+        Q dv[U], qv[U], rv[U];
+        double4 pv[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+        {
+            const long long j = base + (long long)u * kVecThreads;
+            if (j < last)
+            {
+                dv[u] = reinterpret_cast<const Q*>(d)[j];
+                qv[u] = reinterpret_cast<const Q*>(q)[j];
+                rv[u] = reinterpret_cast<const Q*>(r)[j];
+                pv[u] = reinterpret_cast<const double4*>(g.p)[j];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+        {
+            const long long j = base + (long long)u * kVecThreads;
+            if (j >= last)
+                continue;
+            double4 pp = pv[u];
+            pp.x += alpha * double(dv[u].x);
+            pp.y += alpha * double(dv[u].y);
+            pp.z += alpha * double(dv[u].z);
+            pp.w += alpha * double(dv[u].w);
+            Q rr;
+            rr.x = T(double(rv[u].x) - alpha * double(qv[u].x));
+            rr.y = T(double(rv[u].y) - alpha * double(qv[u].y));
+            rr.z = T(double(rv[u].z) - alpha * double(qv[u].z));
+            rr.w = T(double(rv[u].w) - alpha * double(qv[u].w));
+            reinterpret_cast<double4*>(g.p)[j] = pp;
+            reinterpret_cast<Q*>(r)[j] = rr;
+            const double e[4] = {double(rr.x), double(rr.y), double(rr.z), double(rr.w)};
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+            {
+                sum += e[c];
+                mx = fmax(mx, fabs(e[c]));
+                sq += e[c] * e[c];
+            }
+        }
     }
     __shared__ double4 total;
     if (arrive_last<kVecThreads>(g, t.index, g.vec_tiles, block_reduce4<kVecThreads>(make_double4(sum, mx, sq, 0), 2), &total, 2))
@@ -449,9 +629,9 @@ template <typename T> __global__ void k_velocity_update(const GridDesc* grids, c
     T* v = static_cast<T*>(g.v);
     const T* right = static_cast<const T*>(g.lev[0].right);
     const T* down = static_cast<const T*>(g.lev[0].down);
-    for (int k = 0; k < 4; ++k)
+    for (int k = 0; k < kVecCells; ++k)
     {
-        const int x = t.x0 + tx, y = t.y0 + ty + 8 * k;
+        const int x = t.x0 + tx + 32 * (k & 1), y = t.y0 + ty + 8 * (k >> 1);
         if (x >= g.W || y >= g.H)
             continue;
         const long long i = padded_index(g.S, x, y);
@@ -500,9 +680,9 @@ template <typename T> __global__ void __launch_bounds__(kVecThreads) k_divergenc
     const T* v = static_cast<const T*>(g.v);
     double mx = 0.0, excess = 0.0, sq = 0.0;
     int nonfinite = 0;
-    for (int k = 0; k < 4; ++k)
+    for (int k = 0; k < kVecCells; ++k)
     {
-        const int x = t.x0 + tx, y = t.y0 + ty + 8 * k;
+        const int x = t.x0 + tx + 32 * (k & 1), y = t.y0 + ty + 8 * (k >> 1);
         if (x >= g.W || y >= g.H)
             continue;
         const long long iu = (long long)y * (g.W + 1) + x;

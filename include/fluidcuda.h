@@ -48,6 +48,14 @@ typedef enum fc_precision
     FC_PRECISION_MIXED = 2  /* FP32 fine level, FP16-stored coarse multigrid levels */
 } fc_precision;
 
+/* How a projection's PCG loop is launched (process-wide). */
+typedef enum fc_launch_mode
+{
+    FC_LAUNCH_GRAPH = 0, /* one CUDA graph per projection with a device-side loop (default) */
+    FC_LAUNCH_STREAM = 1 /* host-driven launches polling the done flags: same kernels, for
+                            per-kernel profilers and drivers without conditional graph nodes */
+} fc_launch_mode;
+
 typedef enum fc_preconditioner
 {
     FC_PRECONDITIONER_DIAGONAL = 0, /* FluidGridCPU::PressurePreconditioner::Diagonal */
@@ -109,6 +117,8 @@ const char* fc_last_error(void);
 const char* fc_status_string(int status);
 /* Number of kernels this library has launched in the calling process (a launch counter). */
 long long fc_kernel_launches(void);
+/* Selects the launch mechanism of subsequent projections (fc_launch_mode). */
+int fc_set_launch_mode(int mode);
 
 /* FluidGridCPU::FluidGridCPU(w, h, cell_size) (UniformCPU/FluidGridCPU.h:63); the device is
  * the calling thread's current CUDA device. */

@@ -289,6 +289,25 @@ def test_edge_cases():
         fresh.configureMaterials([1.0], [0.001], liquid_viscosities=[1.0])
 
 
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_stream_launch_mode_matches_graph(precision):
+    from fluidsim_b200 import _native as N
+
+    s = scenes.random_pool(300, 220, seed=21, fill=0.6, obstacles=3, cell_size=1.0 / 300)
+    outs = []
+    try:
+        for mode in ("graph", "stream"):
+            N.set_launch_mode(mode)
+            g = gpu_grid(s, precision)
+            r = g.project(s.dt, 300, 1e-6, relative_tolerance=1e-6)
+            outs.append((r, g.download()))
+    finally:
+        N.set_launch_mode("graph")
+    (ra, a), (rb, b) = outs
+    assert ra.iterations == rb.iterations and ra.solve_status == rb.solve_status == "converged"
+    assert np.array_equal(a.u, b.u) and np.array_equal(a.v, b.v) and np.array_equal(a.pressure, b.pressure)
+
+
 def test_large_grid_converges_relative():
     s = scenes.dam_break(1024, 1024, seed=0, obstacles=16, velocity=1.0)
     g = gpu_grid(s, "fp32")

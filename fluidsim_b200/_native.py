@@ -82,6 +82,8 @@ SIGNATURES = {
     "fc_project": (_int, [_vp, _dbl, _int, _dbl, C.POINTER(FcResult)]),
     "fc_project_relative": (_int, [_vp, _dbl, _int, _dbl, _dbl, C.POINTER(FcResult)]),
     "fc_step": (_int, [_vp, _dbl, _int, _dbl, C.POINTER(FcResult), C.POINTER(FcTimings)]),
+    "fc_advect": (_int, [_vp, _dbl]),
+    "fc_sample_velocity": (_int, [_vp, _int, _vp, _vp]),
     "fc_apply_gravity": (_int, [_vp, _dbl]),
     "fc_max_divergence": (_int, [_vp, _dp]),
     "fc_classify": (_int, [_vp, C.POINTER(C.c_uint8)]),
@@ -91,6 +93,9 @@ SIGNATURES = {
     "fc_velocity_pointers": (_int, [_vp, C.POINTER(_vp), C.POINTER(_vp)]),
     "fc_get_stream": (_int, [_vp, C.POINTER(_vp)]),
     "fc_synchronize": (_int, [_vp]),
+    "fc_save_checkpoint": (_int, [_vp, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t), _vp, C.c_size_t,
+                                  C.POINTER(C.c_size_t)]),
+    "fc_load_checkpoint": (_int, [_vp, C.c_char_p, _vp, C.c_size_t]),
     "fc_batch_create": (_int, [C.POINTER(_vp), _int, C.POINTER(_vp)]),
     "fc_batch_destroy": (_int, [_vp]),
     "fc_batch_project": (_int, [_vp, _dp, _int, _dbl, _dbl, C.POINTER(FcResult)]),

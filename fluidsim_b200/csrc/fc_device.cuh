@@ -256,4 +256,12 @@ __device__ bool arrive_last(const GridDesc& g, int tile_index, int tiles, double
 
 __device__ __forceinline__ bool finite_d(double v) { return isfinite(v); }
 
+// Programmatic dependent launch. The kernels of the PCG loop are launched so that each may
+// start while its predecessor finishes: allow_dependents() lets the next kernel's CTAs be
+// scheduled once every CTA of this one has started, and dependency_wait() blocks until every
+// earlier kernel has completed and its writes are visible. Before the wait a kernel reads only
+// data no kernel of the projection writes (tiles, descriptors, face weights, transfer tables).
+__device__ __forceinline__ void dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void allow_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 } // namespace fc

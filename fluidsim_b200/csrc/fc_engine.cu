@@ -10,6 +10,8 @@
 #include "fc_multigrid.cuh"
 #include "fc_pcg.cuh"
 #include "fc_smooth.cuh"
+#include "fc_json.h"
+#include "fc_advect.cuh"
 
 #include "../../include/fluidcuda.h"
 
@@ -95,6 +97,31 @@ template <typename F> int guarded(F&& body)
             ::fc::launch_count.fetch_add(1, std::memory_order_relaxed);                            \
         }                                                                                          \
     } while (0)
+
+// Launch with programmatic stream serialization: the kernel may be scheduled before its
+// predecessor completes and orders itself with dependency_wait() (fc_device.cuh).
+template <typename... Params, typename... Args>
+void launch_dependent(const char* name, void (*kernel)(Params...), int blocks, int threads, size_t smem,
+    cudaStream_t stream, Args... args)
+{
+    if (blocks <= 0)
+        return;
+    cudaLaunchConfig_t config = {};
+    config.gridDim = dim3(blocks);
+    config.blockDim = dim3(threads);
+    config.dynamicSmemBytes = smem;
+    config.stream = stream;
+    cudaLaunchAttribute attribute[1];
+    attribute[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attribute[0].val.programmaticStreamSerializationAllowed = 1;
+    config.attrs = attribute;
+    config.numAttrs = 1;
+    check(cudaLaunchKernelEx(&config, kernel, static_cast<Params>(args)...), name);
+    launch_count.fetch_add(1, std::memory_order_relaxed);
+}
+
+#define FC_LAUNCH_DEP(kernel, blocks, threads, smem, stream, ...) \
+    launch_dependent(#kernel, kernel, (blocks), (threads), (smem), (stream), __VA_ARGS__)
 
 int ceil_div(int a, int b) { return (a + b - 1) / b; }
 
@@ -210,6 +237,8 @@ struct Grid
     double* masses = nullptr;     // components x W*H
     double** mass_ptrs = nullptr; // device array of component pointers
     double* staging = nullptr;    // FP64 staging for upload/download conversions
+    void* u_next = nullptr;       // advection outputs (working precision)
+    void* v_next = nullptr;
     size_t staging_count = 0;
     unsigned char* solid = nullptr;
     unsigned char* mask = nullptr;
@@ -331,6 +360,8 @@ void allocate_grid(Grid& g)
     add((void**)&d.density, g.cells * sizeof(double));
     add((void**)&g.fraction, g.cells * sizeof(double));
     add((void**)&g.staging, g.staging_count * sizeof(double));
+    add(&g.u_next, g.faces_u * elem);
+    add(&g.v_next, g.faces_v * elem);
     add((void**)&g.solid, g.cells);
     add((void**)&g.mask, g.cells);
     add((void**)&d.lev[0].pre, padded0 * elem);
@@ -494,6 +525,8 @@ __global__ void __launch_bounds__(kVecThreads) k_count_open(const GridDesc* grid
 
 __global__ void k_loop_condition(const GridDesc* grids, int n, int* body_count, int cap, cudaGraphConditionalHandle handle)
 {
+    allow_dependents();
+    dependency_wait();
     int running = 0;
     for (int i = threadIdx.x; i < n; i += blockDim.x)
         running |= grids[i].state->done == 0;
@@ -570,6 +603,7 @@ struct Plan
     SolveState* h_states = nullptr;    // pinned
     int* d_body_count = nullptr;
     Range vec;
+    Range faces; // tiles over the (W+1) x (H+1) face index space
     Range coarsen[kMaxLevels];
     Range pre[kMaxLevels];
     Range post[kMaxLevels];
@@ -666,6 +700,11 @@ std::unique_ptr<Plan> make_plan(const std::vector<Grid*>& grids, cudaStream_t st
         for (int i = 0; i < n; ++i)
             append_tiles(tiles, i, grids[i]->W, grids[i]->H, kVecTileX, kVecTileY);
     });
+    add(plan->faces, [&]
+    {
+        for (int i = 0; i < n; ++i)
+            append_tiles(tiles, i, grids[i]->W + 1, grids[i]->H + 1, kVecTileX, kVecTileY);
+    });
     for (Grid* g : grids)
     {
         plan->max_levels = std::max(plan->max_levels, int(g->levels.size()));
@@ -741,33 +780,33 @@ template <typename T> void launch_precondition(Plan& p, bool use_mg)
     cudaStream_t s = p.stream;
     if (!use_mg)
     {
-        FC_LAUNCH(k_precondition_diagonal<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
+        FC_LAUNCH_DEP(k_precondition_diagonal<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
         return;
     }
     constexpr int KB = Tiling<T>::big, KS = Tiling<T>::small;
     for (int l = 0; l < p.max_tail; ++l)
     {
         if (p.tall[l])
-            FC_LAUNCH((k_mg_pre<T, KB>), p.pre[l].count, 256, 0, s, p.d_desc, p.at(p.pre[l]), l);
+            FC_LAUNCH_DEP((k_mg_pre<T, KB>), p.pre[l].count, 256, 0, s, p.d_desc, p.at(p.pre[l]), l);
         else
-            FC_LAUNCH((k_mg_pre<T, KS>), p.pre[l].count, 256, 0, s, p.d_desc, p.at(p.pre[l]), l);
+            FC_LAUNCH_DEP((k_mg_pre<T, KS>), p.pre[l].count, 256, 0, s, p.d_desc, p.at(p.pre[l]), l);
     }
-    FC_LAUNCH(k_mg_tail<T>, p.n(), kTailThreads, p.tail_smem, s, p.d_desc);
+    FC_LAUNCH_DEP(k_mg_tail<T>, p.n(), kTailThreads, p.tail_smem, s, p.d_desc);
     for (int l = p.max_tail - 1; l >= 0; --l)
     {
         if (p.tall[l])
-            FC_LAUNCH((k_mg_post<T, KB>), p.post[l].count, 256, 0, s, p.d_desc, p.at(p.post[l]), l);
+            FC_LAUNCH_DEP((k_mg_post<T, KB>), p.post[l].count, 256, 0, s, p.d_desc, p.at(p.post[l]), l);
         else
-            FC_LAUNCH((k_mg_post<T, KS>), p.post[l].count, 256, 0, s, p.d_desc, p.at(p.post[l]), l);
+            FC_LAUNCH_DEP((k_mg_post<T, KS>), p.post[l].count, 256, 0, s, p.d_desc, p.at(p.post[l]), l);
     }
 }
 
 template <typename T> void launch_iteration(Plan& p, bool use_mg, int parity)
 {
     cudaStream_t s = p.stream;
-    FC_LAUNCH(k_direction_operator<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec), parity);
-    FC_LAUNCH(k_update<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec), parity);
-    FC_LAUNCH(k_true_residual<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec), 0);
+    FC_LAUNCH_DEP(k_direction_operator<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec), parity);
+    FC_LAUNCH_DEP(k_update<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec), parity);
+    FC_LAUNCH_DEP(k_true_residual<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec), 0);
     launch_precondition<T>(p, use_mg);
 }
 
@@ -867,7 +906,7 @@ template <typename T> void capture_projection(Plan& p, bool use_mg, int cap)
         q.stream = side;
         launch_iteration<T>(q, use_mg, 0);
         launch_iteration<T>(q, use_mg, 1);
-        FC_LAUNCH(k_loop_condition, 1, 256, 0, side, q.d_desc, q.n(), q.d_body_count, cap, handle);
+        FC_LAUNCH_DEP(k_loop_condition, 1, 256, 0, side, q.d_desc, q.n(), q.d_body_count, cap, handle);
         q.stream = saved;
     }
     cudaGraph_t body_captured;
@@ -1177,6 +1216,63 @@ void download(Grid& g, double* fraction, double* u, double* v, double* pressure,
     check(cudaStreamSynchronize(g.stream), "download");
 }
 
+// Semi-Lagrangian transport of the velocities, the liquid fraction and every component mass
+// through the velocity at the start of the step (fc_advect.cuh). Masses change, so the
+// pressure coefficients are rebuilt at the next projection.
+void advect(Grid& g, double dt)
+{
+    require_uploaded(g);
+    Plan& p = single_plan(g);
+    const double scale = dt / g.dx, half = 0.5 * scale;
+    cudaStream_t s = p.stream;
+    dispatch(g.precision, [&](auto zero)
+    {
+        using T = decltype(zero);
+        const int fields = 1 + g.components();
+        for (int k = 0; k < fields; ++k)
+        {
+            double* field = k == 0 ? g.fraction : g.masses + size_t(k - 1) * g.cells;
+            FC_LAUNCH(k_advect_cells<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec), scale, half, field,
+                g.staging);
+            check(cudaMemcpyAsync(field, g.staging, g.cells * sizeof(double), cudaMemcpyDeviceToDevice, s), "advect");
+        }
+        FC_LAUNCH(k_advect_velocity<T>, p.faces.count, kVecThreads, 0, s, p.d_desc, p.at(p.faces), scale, half,
+            static_cast<T*>(g.u_next), static_cast<T*>(g.v_next));
+        check(cudaMemcpyAsync(g.desc.u, g.u_next, g.faces_u * sizeof(T), cudaMemcpyDeviceToDevice, s), "advect");
+        check(cudaMemcpyAsync(g.desc.v, g.v_next, g.faces_v * sizeof(T), cudaMemcpyDeviceToDevice, s), "advect");
+    });
+    check(cudaStreamSynchronize(s), "advect");
+    g.coefficients_dirty = true;
+}
+
+// FluidGridCPU::sampleVelocity at `count` world positions (host arrays of (x, y) pairs).
+void sample_velocity(Grid& g, int count, const double* positions, double* velocities)
+{
+    require_uploaded(g);
+    Plan& p = single_plan(g);
+    const size_t bytes = size_t(count) * 2 * sizeof(double);
+    double* d = nullptr;
+    check(cudaMalloc(&d, 2 * bytes), "sample allocation");
+    try
+    {
+        check(cudaMemcpyAsync(d, positions, bytes, cudaMemcpyHostToDevice, p.stream), "sample upload");
+        dispatch(g.precision, [&](auto zero)
+        {
+            using T = decltype(zero);
+            FC_LAUNCH(k_sample_velocity<T>, (count + 255) / 256, 256, 0, p.stream, static_cast<const T*>(g.desc.u),
+                static_cast<const T*>(g.desc.v), g.W, g.H, g.origin_x, g.origin_y, g.dx, count, d, d + 2 * count);
+        });
+        check(cudaMemcpyAsync(velocities, d + 2 * count, bytes, cudaMemcpyDeviceToHost, p.stream), "sample download");
+        check(cudaStreamSynchronize(p.stream), "sample");
+    }
+    catch (...)
+    {
+        cudaFree(d);
+        throw;
+    }
+    check(cudaFree(d), "sample free");
+}
+
 // One preconditioner application to a given residual (PressureMultigrid::apply,
 // PressureMultigrid.cpp:410-434, or the diagonal at FluidGridCPU.cpp:1691-1698); the
 // correction is returned without its mean removed, as the reference's apply returns it.
@@ -1275,6 +1371,226 @@ double time_kernel(Grid& g, int kernel, int repeats)
     check(cudaMemcpyAsync(g.desc.state, &saved, sizeof(saved), cudaMemcpyHostToDevice, p.stream), "state");
     check(cudaStreamSynchronize(p.stream), "state");
     return double(ms) / repeats;
+}
+
+// ------------------------------------------------------------------------------------------
+// Checkpoints: the "cuda-uniform" native format
+// ------------------------------------------------------------------------------------------
+//
+// Modelled on the reference's "webgpu-uniform" checkpoint (UniformWebGPU/FluidGridGPU.cpp:
+// 567-892): JSON metadata (backend, version, scalar types, byte order, geometry, materials,
+// solver settings) and a payload of the physical state and solver history in a fixed order:
+// liquid fraction, u, v, pressure, previous pressure, component masses (liquid then gas), then
+// the obstacle mask when there is one. Each field keeps its device precision, so a loaded grid
+// continues bit for bit. Loading validates everything before it changes any state.
+
+constexpr int kCheckpointVersion = 1;
+
+struct PayloadLayout
+{
+    size_t fraction, u, v, pressure, previous, masses, solid, total;
+};
+
+PayloadLayout payload_layout(const Grid& g, int components, bool solid)
+{
+    PayloadLayout l{};
+    size_t at = 0;
+    l.fraction = at;
+    at += g.cells * sizeof(double);
+    l.u = at;
+    at += g.faces_u * g.elem;
+    l.v = at;
+    at += g.faces_v * g.elem;
+    l.pressure = at;
+    at += g.cells * sizeof(double);
+    l.previous = at;
+    at += g.cells * sizeof(double);
+    l.masses = at;
+    at += size_t(components) * g.cells * sizeof(double);
+    l.solid = at;
+    if (solid)
+        at += g.cells;
+    l.total = at;
+    return l;
+}
+
+std::string checkpoint_metadata(const Grid& g)
+{
+    using json::number;
+    using json::quoted;
+    auto mixture = [](const std::vector<double>& density, const std::vector<double>& viscosity)
+    {
+        std::string out = "[";
+        for (size_t i = 0; i < density.size(); ++i)
+        {
+            if (i)
+                out += ", ";
+            out += "{\"density\": " + number(density[i]) + ", \"dynamic_viscosity\": " + number(viscosity[i]) + "}";
+        }
+        return out + "]";
+    };
+    const bool little = [] { const unsigned one = 1; return *reinterpret_cast<const unsigned char*>(&one) == 1; }();
+    const PayloadLayout layout = payload_layout(g, g.components(), g.has_solid);
+    std::string m = "{";
+    m += "\"backend\": " + quoted("cuda-uniform");
+    m += ", \"version\": " + std::to_string(kCheckpointVersion);
+    m += ", \"scalar\": " + quoted(g.elem == 8 ? "float64" : "float32");
+    m += ", \"state_scalar\": " + quoted("float64");
+    m += ", \"byte_order\": " + quoted(little ? "little" : "big");
+    m += ", \"precision\": " + std::to_string(g.precision);
+    m += ", \"width\": " + std::to_string(g.W) + ", \"height\": " + std::to_string(g.H);
+    m += ", \"cell_size\": " + number(g.dx);
+    m += ", \"origin\": [" + number(g.origin_x) + ", " + number(g.origin_y) + "]";
+    m += ", \"gravity_y\": " + number(g.gravity_y);
+    m += ", \"preconditioner\": " + std::to_string(g.preconditioner);
+    m += ", \"liquid_mixture\": " + mixture(g.liquid_density, g.liquid_viscosity);
+    m += ", \"gas_mixture\": " + mixture(g.gas_density, g.gas_viscosity);
+    m += ", \"obstacles\": " + std::string(g.has_solid ? "true" : "false");
+    m += ", \"payload_bytes\": " + std::to_string(layout.total);
+    m += ", \"fields\": [\"liquid_fraction\", \"u\", \"v\", \"pressure\", \"previous_pressure\", \"component_masses\"" +
+         std::string(g.has_solid ? ", \"solid\"" : "") + "]";
+    return m + "}";
+}
+
+void save_checkpoint(Grid& g, char* metadata, size_t metadata_capacity, size_t* metadata_bytes, void* payload,
+    size_t payload_capacity, size_t* payload_bytes)
+{
+    require_uploaded(g);
+    const std::string text = checkpoint_metadata(g);
+    const PayloadLayout layout = payload_layout(g, g.components(), g.has_solid);
+    if (metadata_bytes)
+        *metadata_bytes = text.size() + 1;
+    if (payload_bytes)
+        *payload_bytes = layout.total;
+    if (!metadata && !payload)
+        return; // size query
+    if (!metadata || metadata_capacity < text.size() + 1 || !payload || payload_capacity < layout.total)
+        fail(FC_ERR_INVALID_ARGUMENT, "checkpoint buffers too small (%zu and %zu bytes needed)", text.size() + 1,
+            layout.total);
+    std::memcpy(metadata, text.c_str(), text.size() + 1);
+    char* out = static_cast<char*>(payload);
+    cudaStream_t s = g.stream;
+    check(cudaStreamSynchronize(s), "checkpoint");
+    check(cudaMemcpyAsync(out + layout.fraction, g.fraction, g.cells * sizeof(double), cudaMemcpyDeviceToHost, s), "checkpoint");
+    check(cudaMemcpyAsync(out + layout.u, g.desc.u, g.faces_u * g.elem, cudaMemcpyDeviceToHost, s), "checkpoint");
+    check(cudaMemcpyAsync(out + layout.v, g.desc.v, g.faces_v * g.elem, cudaMemcpyDeviceToHost, s), "checkpoint");
+    if (g.components() > 0)
+        check(cudaMemcpyAsync(out + layout.masses, g.masses, size_t(g.components()) * g.cells * sizeof(double),
+                  cudaMemcpyDeviceToHost, s), "checkpoint");
+    if (g.has_solid)
+        check(cudaMemcpyAsync(out + layout.solid, g.solid, g.cells, cudaMemcpyDeviceToHost, s), "checkpoint");
+    const double* fields[2] = {g.desc.p, g.desc.p_prev};
+    const size_t offsets[2] = {layout.pressure, layout.previous};
+    for (int k = 0; k < 2; ++k)
+    {
+        FC_LAUNCH(k_unpad_f64, blocks_for(g.cells), 256, 0, s, fields[k], g.staging, g.W, g.H, g.S);
+        check(cudaMemcpyAsync(out + offsets[k], g.staging, g.cells * sizeof(double), cudaMemcpyDeviceToHost, s), "checkpoint");
+        check(cudaStreamSynchronize(s), "checkpoint");
+    }
+}
+
+void load_checkpoint(Grid& g, const char* metadata, const void* payload, size_t payload_bytes)
+{
+    if (!metadata || !payload)
+        fail(FC_ERR_INVALID_ARGUMENT, "null checkpoint");
+    json::Value m;
+    try
+    {
+        m = json::Parser(metadata).parse();
+    }
+    catch (const std::exception& e)
+    {
+        fail(FC_ERR_INVALID_ARGUMENT, "checkpoint metadata is not valid JSON: %s", e.what());
+    }
+    auto need = [&](const char* key, json::Value::Kind kind) -> const json::Value&
+    {
+        const json::Value* v = m.kind == json::Value::Object ? m.find(key) : nullptr;
+        if (!v || v->kind != kind)
+            fail(FC_ERR_INVALID_ARGUMENT, "checkpoint metadata lacks a valid \"%s\"", key);
+        return *v;
+    };
+    if (need("backend", json::Value::String).text != "cuda-uniform")
+        fail(FC_ERR_INVALID_ARGUMENT, "checkpoint was written by another backend");
+    if (int(need("version", json::Value::Number).number) != kCheckpointVersion)
+        fail(FC_ERR_INVALID_ARGUMENT, "unsupported checkpoint version");
+    const bool little = [] { const unsigned one = 1; return *reinterpret_cast<const unsigned char*>(&one) == 1; }();
+    if (need("byte_order", json::Value::String).text != (little ? "little" : "big"))
+        fail(FC_ERR_INVALID_ARGUMENT, "checkpoint byte order differs from this host");
+    if (need("scalar", json::Value::String).text != (g.elem == 8 ? "float64" : "float32") ||
+        int(need("precision", json::Value::Number).number) != g.precision)
+        fail(FC_ERR_INVALID_ARGUMENT, "checkpoint precision differs from the grid's");
+    if (int(need("width", json::Value::Number).number) != g.W || int(need("height", json::Value::Number).number) != g.H ||
+        need("cell_size", json::Value::Number).number != g.dx)
+        fail(FC_ERR_INVALID_ARGUMENT, "checkpoint geometry differs from the grid's");
+    const json::Value& origin = need("origin", json::Value::Array);
+    if (origin.items.size() != 2 || origin.items[0].kind != json::Value::Number || origin.items[1].kind != json::Value::Number)
+        fail(FC_ERR_INVALID_ARGUMENT, "checkpoint origin is malformed");
+    auto mixture = [&](const char* key, std::vector<double>& density, std::vector<double>& viscosity)
+    {
+        density.clear();
+        viscosity.clear();
+        for (const json::Value& c : need(key, json::Value::Array).items)
+        {
+            const json::Value* d = c.find("density");
+            const json::Value* mu = c.find("dynamic_viscosity");
+            if (!d || d->kind != json::Value::Number || !(d->number > 0.0))
+                fail(FC_ERR_INVALID_ARGUMENT, "checkpoint mixture component is malformed");
+            density.push_back(d->number);
+            viscosity.push_back(mu && mu->kind == json::Value::Number ? mu->number : 0.0);
+        }
+    };
+    std::vector<double> ld, lv, gd, gv;
+    mixture("liquid_mixture", ld, lv);
+    mixture("gas_mixture", gd, gv);
+    for (double mu : lv)
+        if (mu != 0.0)
+            fail(FC_ERR_UNSUPPORTED, "checkpoint needs viscosity, which this build does not support");
+    for (double mu : gv)
+        if (mu != 0.0)
+            fail(FC_ERR_UNSUPPORTED, "checkpoint needs viscosity, which this build does not support");
+    const int preconditioner = int(need("preconditioner", json::Value::Number).number);
+    if (preconditioner != FC_PRECONDITIONER_DIAGONAL && preconditioner != FC_PRECONDITIONER_MULTIGRID)
+        fail(FC_ERR_INVALID_ARGUMENT, "checkpoint preconditioner is unknown");
+    const bool solid = need("obstacles", json::Value::Bool).boolean;
+    const double gravity = need("gravity_y", json::Value::Number).number;
+    const PayloadLayout layout = payload_layout(g, int(ld.size() + gd.size()), solid);
+    if (size_t(need("payload_bytes", json::Value::Number).number) != layout.total || payload_bytes != layout.total)
+        fail(FC_ERR_INVALID_ARGUMENT, "checkpoint payload has %zu bytes, %zu expected", payload_bytes, layout.total);
+
+    // Validated: apply.
+    g.liquid_density = ld;
+    g.liquid_viscosity = lv;
+    g.gas_density = gd;
+    g.gas_viscosity = gv;
+    g.configured = true;
+    g.preconditioner = preconditioner;
+    g.gravity_y = gravity;
+    g.origin_x = origin.items[0].number;
+    g.origin_y = origin.items[1].number;
+    allocate_masses(g);
+    g.has_solid = solid;
+    const char* in = static_cast<const char*>(payload);
+    cudaStream_t s = g.stream;
+    check(cudaStreamSynchronize(s), "checkpoint");
+    check(cudaMemcpyAsync(g.fraction, in + layout.fraction, g.cells * sizeof(double), cudaMemcpyHostToDevice, s), "checkpoint");
+    check(cudaMemcpyAsync(g.desc.u, in + layout.u, g.faces_u * g.elem, cudaMemcpyHostToDevice, s), "checkpoint");
+    check(cudaMemcpyAsync(g.desc.v, in + layout.v, g.faces_v * g.elem, cudaMemcpyHostToDevice, s), "checkpoint");
+    if (g.components() > 0)
+        check(cudaMemcpyAsync(g.masses, in + layout.masses, size_t(g.components()) * g.cells * sizeof(double),
+                  cudaMemcpyHostToDevice, s), "checkpoint");
+    if (solid)
+        check(cudaMemcpyAsync(g.solid, in + layout.solid, g.cells, cudaMemcpyHostToDevice, s), "checkpoint");
+    double* fields[2] = {g.desc.p, g.desc.p_prev};
+    const size_t offsets[2] = {layout.pressure, layout.previous};
+    for (int k = 0; k < 2; ++k)
+    {
+        check(cudaMemcpyAsync(g.staging, in + offsets[k], g.cells * sizeof(double), cudaMemcpyHostToDevice, s), "checkpoint");
+        FC_LAUNCH(k_pad_f64, blocks_for(g.cells), 256, 0, s, g.staging, fields[k], g.W, g.H, g.S);
+        check(cudaStreamSynchronize(s), "checkpoint");
+    }
+    refresh_descriptor(g);
+    g.uploaded = true;
+    g.coefficients_dirty = true;
 }
 
 // ------------------------------------------------------------------------------------------
@@ -1682,6 +1998,29 @@ int fc_project_relative(fc_grid* grid, double dt, int max_iterations, double rel
     return fc::project_one(grid->impl, dt, max_iterations, divergence_tolerance, relative_tolerance, result);
 }
 
+int fc_advect(fc_grid* grid, double dt)
+{
+    return guarded([&]
+    {
+        if (!grid)
+            fail(FC_ERR_INVALID_ARGUMENT, "null grid");
+        if (!(dt > 0.0) || !std::isfinite(dt))
+            fail(FC_ERR_INVALID_ARGUMENT, "time step must be positive and finite");
+        fc::advect(grid->impl, dt);
+    });
+}
+
+int fc_sample_velocity(fc_grid* grid, int count, const double* positions, double* velocities)
+{
+    return guarded([&]
+    {
+        if (!grid || count < 0 || (count > 0 && (!positions || !velocities)))
+            fail(FC_ERR_INVALID_ARGUMENT, "invalid sample arguments");
+        if (count > 0)
+            fc::sample_velocity(grid->impl, count, positions, velocities);
+    });
+}
+
 int fc_apply_gravity(fc_grid* grid, double dt)
 {
     return guarded([&]
@@ -1719,16 +2058,21 @@ int fc_step(fc_grid* grid, double dt, int max_iterations, double divergence_tole
         return FC_OK;
     }
     const auto t0 = Clock::now();
-    int status = fc_apply_gravity(grid, dt);
+    int status = fc_advect(grid, dt);
     if (status != FC_OK)
         return status;
     const auto t1 = Clock::now();
-    status = fc_project(grid, dt, max_iterations, divergence_tolerance, result);
+    status = fc_apply_gravity(grid, dt);
+    if (status != FC_OK)
+        return status;
     const auto t2 = Clock::now();
+    status = fc_project(grid, dt, max_iterations, divergence_tolerance, result);
+    const auto t3 = Clock::now();
     if (timings)
     {
-        timings->forces_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
-        timings->pressure_ms = std::chrono::duration<double, std::milli>(t2 - t1).count();
+        timings->transport_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+        timings->forces_ms = std::chrono::duration<double, std::milli>(t2 - t1).count();
+        timings->pressure_ms = std::chrono::duration<double, std::milli>(t3 - t2).count();
     }
     if (result)
         result->physical_steps = 1;
@@ -1850,6 +2194,28 @@ int fc_apply_preconditioner(fc_grid* grid, const double* residual, double residu
         if (!grid || !residual || !correction)
             fail(FC_ERR_INVALID_ARGUMENT, "null argument");
         fc::apply_preconditioner(grid->impl, residual, residual_mean, correction);
+    });
+}
+
+int fc_save_checkpoint(fc_grid* grid, char* metadata, size_t metadata_capacity, size_t* metadata_bytes, void* payload,
+    size_t payload_capacity, size_t* payload_bytes)
+{
+    return guarded([&]
+    {
+        if (!grid)
+            fail(FC_ERR_INVALID_ARGUMENT, "null grid");
+        fc::save_checkpoint(grid->impl, metadata, metadata_capacity, metadata_bytes, payload, payload_capacity,
+            payload_bytes);
+    });
+}
+
+int fc_load_checkpoint(fc_grid* grid, const char* metadata, const void* payload, size_t payload_bytes)
+{
+    return guarded([&]
+    {
+        if (!grid)
+            fail(FC_ERR_INVALID_ARGUMENT, "null grid");
+        fc::load_checkpoint(grid->impl, metadata, payload, payload_bytes);
     });
 }
 

@@ -41,9 +41,11 @@ __device__ __forceinline__ void finish_preconditioner(SolveState& s, double sum_
 template <typename T>
 __global__ void __launch_bounds__(kVecThreads) k_precondition_diagonal(const GridDesc* grids, const Tile* tiles)
 {
+    allow_dependents();
     const Tile t = tiles[blockIdx.x];
     const GridDesc& g = grids[t.grid];
     SolveState& s = *g.state;
+    dependency_wait();
     if (s.done)
         return;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
@@ -249,7 +251,7 @@ template <typename T> __global__ void __launch_bounds__(256) k_coarse_inverse(co
 // Coarse tail: the remaining levels cycled by one CTA in shared memory
 // ------------------------------------------------------------------------------------------
 
-constexpr int kTailThreads = 512;
+constexpr int kTailThreads = 1024;
 constexpr int kTailWarps = kTailThreads / 32;
 
 // Dynamic shared memory of the tail kernel. Levels address it through element offsets so that
@@ -447,8 +449,10 @@ __device__ void tail_solve_coarsest(const TailLevel<T> L, int inverse_offset, in
 
 template <typename T> __global__ void __launch_bounds__(kTailThreads) k_mg_tail(const GridDesc* grids)
 {
+    allow_dependents();
     const GridDesc& g = grids[blockIdx.x];
     SolveState& state = *g.state;
+    dependency_wait();
     if (state.done)
         return;
     const int first = g.tail, last = g.levels - 1;

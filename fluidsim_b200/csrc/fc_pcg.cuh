@@ -267,8 +267,10 @@ __device__ __forceinline__ double apply_cell_fp64(const T* right, const T* down,
 template <typename T>
 __global__ void __launch_bounds__(kVecThreads) k_true_residual(const GridDesc* grids, const Tile* tiles, int initial)
 {
+    allow_dependents();
     FC_VEC_TILE_PROLOGUE
     SolveState& s = *g.state;
+    dependency_wait();
     if (s.done || (!initial && !s.verify))
         return;
     const T* right = static_cast<const T*>(g.lev[0].right);
@@ -339,38 +341,6 @@ template <> struct VecPair<double>
     using type = double2;
 };
 
-// Direction d = (z - mean z) + beta d_old at the column pair (gx, gx + 1) of padded row gy,
-// rounded to the working type (the operator and the p update read exactly the stored d); the
-// padded halo rows -1 and H read as zero fields. The reference forms z - mean at
-// FluidGridCPU.cpp:1712-1722 and d at :1812-1816.
-template <typename T>
-__device__ __forceinline__ typename VecPair<T>::type direction_pair(const GridDesc& g, const T* z, const T* d_old,
-    int gx, int gy, bool cols, double mean_z, double beta)
-{
-    using P = typename VecPair<T>::type;
-    P zz = P{}, dd2 = P{};
-    if (cols && gy >= -1 && gy <= g.H)
-    {
-        const long long i = padded_index(g.S, gx, gy);
-        zz = *reinterpret_cast<const P*>(z + i);
-        dd2 = *reinterpret_cast<const P*>(d_old + i);
-    }
-    P out;
-    out.x = T((double(zz.x) - mean_z) + beta * double(dd2.x));
-    out.y = T((double(zz.y) - mean_z) + beta * double(dd2.y));
-    return out;
-}
-
-template <typename T>
-__device__ __forceinline__ T direction_one(const GridDesc& g, const T* z, const T* d_old, int x, int y, double mean_z,
-    double beta)
-{
-    if (x + kPadX < 0 || x + kPadX >= g.S || y < -1 || y > g.H)
-        return T(0);
-    const long long i = padded_index(g.S, x, y);
-    return T((double(z[i]) - mean_z) + beta * double(d_old[i]));
-}
-
 // d = (z - mean z) + beta d_old; q = A d; d.q through the grid's reduction. Warp w handles rows
 // 8w .. 8w + 7 of the tile's 64 columns (lane = column pair) in two passes of four rows: all
 // loads of a pass (six rows of z and d, four rows of weights) are issued first, then the
@@ -382,9 +352,11 @@ __global__ void __launch_bounds__(kVecThreads) k_direction_operator(const GridDe
 {
     using P = typename VecPair<T>::type;
     constexpr int R = 4;
+    allow_dependents();
     const Tile t = tiles[blockIdx.x];
     const GridDesc& g = grids[t.grid];
     SolveState& s = *g.state;
+    dependency_wait();
     if (s.done)
         return;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -394,7 +366,7 @@ __global__ void __launch_bounds__(kVecThreads) k_direction_operator(const GridDe
     const T* d_old = static_cast<const T*>(g.d[parity]);
     T* d_new = static_cast<T*>(g.d[parity ^ 1]);
     T* q = static_cast<T*>(g.q);
-    const double mean_z = s.mean_z, beta = s.beta;
+    const T mz = T(s.mean_z), b = T(s.beta);
     const int S = g.S;
     const int gx = t.x0 + 2 * lane;
     const bool cols = gx < g.W; // the pair's first column lies in the grid
@@ -449,14 +421,14 @@ __global__ void __launch_bounds__(kVecThreads) k_direction_operator(const GridDe
                 }
             }
         }
-        // Directions, rounded to the working type (the operator and the p update read the
+        // Directions in the working precision (the operator and the p update read exactly the
         // stored d); halo rows and padding columns read zero fields.
         P dir[R + 2];
 #pragma unroll
         for (int k = 0; k < R + 2; ++k)
         {
-            dir[k].x = T((double(zz[k].x) - mean_z) + beta * double(dd0[k].x));
-            dir[k].y = T((double(zz[k].y) - mean_z) + beta * double(dd0[k].y));
+            dir[k].x = (zz[k].x - mz) + b * dd0[k].x;
+            dir[k].y = (zz[k].y - mz) + b * dd0[k].y;
         }
 #pragma unroll
         for (int k = 0; k < R; ++k)
@@ -466,7 +438,7 @@ __global__ void __launch_bounds__(kVecThreads) k_direction_operator(const GridDe
             T left = __shfl_up_sync(0xffffffffu, cur.y, 1);
             T right_d = __shfl_down_sync(0xffffffffu, cur.x, 1);
             T wl = __shfl_up_sync(0xffffffffu, w[k].y, 1);
-            const T edge_dir = T((double(ez[k]) - mean_z) + beta * double(ed[k]));
+            const T edge_dir = (ez[k] - mz) + b * ed[k];
             if (lane == 0)
             {
                 left = edge_dir;
@@ -536,9 +508,11 @@ __global__ void __launch_bounds__(kVecThreads) k_update(const GridDesc* grids, c
 {
     using Q = typename Quad<T>::type;
     constexpr int U = 4; // quads per thread
+    allow_dependents();
     const Tile t = tiles[blockIdx.x];
     const GridDesc& g = grids[t.grid];
     SolveState& s = *g.state;
+    dependency_wait();
     if (s.done)
         return;
     const T* d = static_cast<const T*>(g.d[parity ^ 1]);

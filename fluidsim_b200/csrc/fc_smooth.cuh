@@ -81,54 +81,82 @@ template <typename T> struct Edges
     T bottom[2][10][32];
 };
 
+// Strip loading in three steps: strip_weights issues the face-weight loads (no kernel of the
+// projection writes them, so before the wait on the previous kernel), strip_rhs issues the
+// right-hand side loads (after the wait), strip_finish forms the left weights, inverse
+// diagonals and the right-hand side once the loads have landed. Callers issue their other
+// loads between strip_rhs and strip_finish so that all of them are in flight together.
+template <typename T, int K> struct StripRaw
+{
+    T wl0[K];
+};
+
 template <typename T, int K>
-__device__ __forceinline__ void strip_load(Strip<T, K>& s, const GridDesc& g, const LevelDesc& L, int level, int X0,
-    int Y0, int lane, int warp, double mean_r)
+__device__ __forceinline__ void strip_weights(Strip<T, K>& s, StripRaw<T, K>& raw, const LevelDesc& L, int X0, int Y0,
+    int lane, int warp)
 {
     using P = typename Pair<T>::type;
     const T* right = static_cast<const T*>(L.right);
     const T* down = static_cast<const T*>(L.down);
-    const T* rhs = level == 0 ? static_cast<const T*>(g.r) : static_cast<const T*>(L.rhs);
     const int gx = X0 + 2 * lane;
     // The pair (gx, gx + 1) is either wholly inside the padded row [0, S) or wholly outside.
     const bool cols = gx + kPadX >= 0 && gx + kPadX + 1 < L.S;
     const bool left_col = gx + kPadX - 1 >= 0 && gx + kPadX - 1 < L.S;
     const int y0 = Y0 + warp * K;
-    // Issue every load of the strip before using any of them.
-    T wl0[K];
 #pragma unroll
     for (int k = 0; k < K; ++k)
     {
         const int gy = y0 + k;
         const bool in = cols && gy >= -1 && gy <= L.h;
         const int i = padded_index32(L.S, gx, gy);
-        P r2 = P{}, w2 = P{}, d2 = P{};
+        P w2 = P{}, d2 = P{};
         if (in)
         {
-            r2 = *reinterpret_cast<const P*>(rhs + i);
             w2 = *reinterpret_cast<const P*>(right + i);
             d2 = *reinterpret_cast<const P*>(down + i);
         }
-        s.ra[k] = r2.x;
-        s.rb[k] = r2.y;
         s.wm[k] = w2.x;
         s.wr[k] = w2.y;
         s.da[k] = d2.x;
         s.db[k] = d2.y;
-        wl0[k] = (lane == 0 && left_col && gy >= -1 && gy <= L.h) ? right[i - 1] : T(0);
+        raw.wl0[k] = (lane == 0 && left_col && gy >= -1 && gy <= L.h) ? right[i - 1] : T(0);
     }
+    P u2 = P{};
+    if (cols && y0 - 1 >= -1 && y0 - 1 <= L.h)
+        u2 = *reinterpret_cast<const P*>(down + padded_index32(L.S, gx, y0 - 1));
+    s.ua = u2.x;
+    s.ub = u2.y;
+}
+
+template <typename T, int K>
+__device__ __forceinline__ void strip_rhs(Strip<T, K>& s, const GridDesc& g, const LevelDesc& L, int level, int X0,
+    int Y0, int lane, int warp)
+{
+    using P = typename Pair<T>::type;
+    const T* rhs = level == 0 ? static_cast<const T*>(g.r) : static_cast<const T*>(L.rhs);
+    const int gx = X0 + 2 * lane;
+    const bool cols = gx + kPadX >= 0 && gx + kPadX + 1 < L.S;
+    const int y0 = Y0 + warp * K;
+#pragma unroll
+    for (int k = 0; k < K; ++k)
     {
-        P u2 = P{};
-        if (cols && y0 - 1 >= -1 && y0 - 1 <= L.h)
-            u2 = *reinterpret_cast<const P*>(down + padded_index32(L.S, gx, y0 - 1));
-        s.ua = u2.x;
-        s.ub = u2.y;
+        const int gy = y0 + k;
+        P r2 = P{};
+        if (cols && gy >= -1 && gy <= L.h)
+            r2 = *reinterpret_cast<const P*>(rhs + padded_index32(L.S, gx, gy));
+        s.ra[k] = r2.x;
+        s.rb[k] = r2.y;
     }
+}
+
+template <typename T, int K>
+__device__ __forceinline__ void strip_finish(Strip<T, K>& s, const StripRaw<T, K>& raw, int level, int lane, double mean_r)
+{
 #pragma unroll
     for (int k = 0; k < K; ++k)
     {
         const T shifted = __shfl_up_sync(0xffffffffu, s.wr[k], 1);
-        s.wl[k] = lane == 0 ? wl0[k] : shifted;
+        s.wl[k] = lane == 0 ? raw.wl0[k] : shifted;
         const T up_a = k == 0 ? s.ua : s.da[k - 1];
         const T up_b = k == 0 ? s.ub : s.db[k - 1];
         const T diag_a = ((s.wl[k] + s.wm[k]) + up_a) + s.da[k];
@@ -207,10 +235,9 @@ template <typename T, int K>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_mg_pre(const GridDesc* grids, const Tile* tiles, int level)
 {
     using Shape = TileShape<T, K, true>;
+    allow_dependents();
     const Tile t = tiles[blockIdx.x];
     const GridDesc& g = grids[t.grid];
-    if (g.state->done)
-        return;
     const LevelDesc& L = g.lev[level];
     const LevelDesc& C = g.lev[level + 1];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -236,7 +263,13 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_mg_pre(const Gr
     }
     edges_clear<T, K>(edges);
     Strip<T, K> s;
-    strip_load<T, K>(s, g, L, level, X0, Y0, lane, warp, level == 0 ? g.state->mean_r : 0.0);
+    StripRaw<T, K> raw;
+    strip_weights<T, K>(s, raw, L, X0, Y0, lane, warp);
+    dependency_wait();
+    if (g.state->done)
+        return;
+    strip_rhs<T, K>(s, g, L, level, X0, Y0, lane, warp);
+    strip_finish<T, K>(s, raw, level, lane, level == 0 ? g.state->mean_r : 0.0);
 #pragma unroll
     for (int k = 0; k < K; ++k)
         s.a[k] = s.b[k] = T(0);
@@ -325,11 +358,10 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_mg_post(const G
 {
     using Shape = TileShape<T, K, false>;
     constexpr int CW = 36, CH = Shape::RY / 2 + 4;
+    allow_dependents();
     const Tile t = tiles[blockIdx.x];
     const GridDesc& g = grids[t.grid];
     SolveState& state = *g.state;
-    if (state.done)
-        return;
     const LevelDesc& L = g.lev[level];
     const LevelDesc& C = g.lev[level + 1];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -339,8 +371,24 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_mg_post(const G
     __shared__ Edges<T> edges;
     __shared__ T coarse[CH][CW];
     __shared__ Interp interp_y[Shape::RY];
-    // Stage the coarse solution under the region (cells outside the coarse level read 0) and
-    // the row interpolation table; every thread's loads are issued before its stores.
+    // Tables and weights first (written by no kernel of the projection); after the wait the
+    // right-hand side, the coarse solution under the region (cells outside the coarse level
+    // read 0) and the pre-smoothed values are all requested before any of them is used.
+    Interp iy{0, 0, 0.0};
+    if (threadIdx.x < Shape::RY)
+    {
+        const int gy = Y0 + int(threadIdx.x);
+        if (gy >= 0 && gy < L.h)
+            iy = L.py[gy];
+    }
+    Strip<T, K> s;
+    StripRaw<T, K> raw;
+    strip_weights<T, K>(s, raw, L, X0, Y0, lane, warp);
+    dependency_wait();
+    if (state.done)
+        return;
+    strip_rhs<T, K>(s, g, L, level, X0, Y0, lane, warp);
+    const double mean_r = level == 0 ? state.mean_r : 0.0;
     const T* csol = static_cast<const T*>(C.sol);
     constexpr int STAGE = (CH * CW + 255) / 256;
     T staged[STAGE];
@@ -351,15 +399,6 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_mg_post(const G
         const int cx = CX0 + q % CW, cy = CY0 + q / CW;
         staged[u] = (q < CH * CW && cx >= 0 && cx < C.w && cy >= 0 && cy < C.h) ? csol[padded_index32(C.S, cx, cy)] : T(0);
     }
-    Interp iy{0, 0, 0.0};
-    if (threadIdx.x < Shape::RY)
-    {
-        const int gy = Y0 + int(threadIdx.x);
-        if (gy >= 0 && gy < L.h)
-            iy = L.py[gy];
-    }
-    Strip<T, K> s;
-    strip_load<T, K>(s, g, L, level, X0, Y0, lane, warp, level == 0 ? state.mean_r : 0.0);
     // The pre-smoothed values of the strip.
     const T* pre = static_cast<const T*>(L.pre);
     const int gx = X0 + 2 * lane;
@@ -382,6 +421,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_mg_post(const G
         if (in_b)
             s.b[k] = pre[i + 1];
     }
+    strip_finish<T, K>(s, raw, level, lane, mean_r);
 #pragma unroll
     for (int u = 0; u < STAGE; ++u)
     {

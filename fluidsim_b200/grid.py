@@ -197,6 +197,27 @@ class FluidGrid:
         N.check(N.lib().fc_download(self.handle, _ptr(f), _ptr(u), _ptr(v), _ptr(p), lp, gp))
         return FluidGridState(f, u, v, p, lm, gm)
 
+    def saveCheckpoint(self):
+        """Returns (metadata dict, payload bytes) of the native "cuda-uniform" checkpoint."""
+        import json
+
+        mb, pb = C.c_size_t(), C.c_size_t()
+        N.check(N.lib().fc_save_checkpoint(self.handle, None, 0, C.byref(mb), None, 0, C.byref(pb)))
+        meta = C.create_string_buffer(mb.value)
+        payload = C.create_string_buffer(max(1, pb.value))
+        N.check(N.lib().fc_save_checkpoint(self.handle, meta, mb.value, C.byref(mb), payload, pb.value, C.byref(pb)))
+        return json.loads(meta.value.decode()), payload.raw[: pb.value]
+
+    def loadCheckpoint(self, metadata, payload: bytes):
+        import json
+
+        text = metadata if isinstance(metadata, str) else json.dumps(metadata)
+        buf = C.create_string_buffer(payload, len(payload))
+        N.check(N.lib().fc_load_checkpoint(self.handle, text.encode(), buf, len(payload)))
+        m = json.loads(text)
+        self._liquid = [c["density"] for c in m["liquid_mixture"]]
+        self._gas = [c["density"] for c in m["gas_mixture"]]
+
     def copyStateFrom(self, other: "FluidGrid"):
         N.check(N.lib().fc_copy_state(self.handle, other.handle))
 
@@ -220,6 +241,17 @@ class FluidGrid:
             N.check(N.lib().fc_project_relative(self.handle, float(dt), int(max_iterations),
                                                 float(relative_tolerance), float(divergence_tolerance), C.byref(r)))
         return ProjectionResult.from_c(r)
+
+    def advect(self, dt: float):
+        """Semi-Lagrangian transport of velocities, liquid fraction and component masses."""
+        N.check(N.lib().fc_advect(self.handle, float(dt)))
+
+    def sampleVelocity(self, positions) -> np.ndarray:
+        """FluidGridCPU::sampleVelocity at world positions, shape (n, 2) -> (n, 2)."""
+        pos = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1, 2)
+        out = np.empty_like(pos)
+        N.check(N.lib().fc_sample_velocity(self.handle, pos.shape[0], pos.ctypes.data, out.ctypes.data))
+        return out
 
     def applyGravity(self, dt: float):
         N.check(N.lib().fc_apply_gravity(self.handle, float(dt)))

@@ -199,6 +199,61 @@ public:
         }
     }
 
+    // saveCheckpoint (FluidGridBase.h:123): the engine's "cuda-uniform" metadata and payload,
+    // plus the host-side substance catalogue and mixture membership under "host".
+    bool saveCheckpoint(FluidCheckpoint& checkpoint) const override
+    {
+        size_t meta_bytes = 0, payload_bytes = 0;
+        check(fc_save_checkpoint(grid, nullptr, 0, &meta_bytes, nullptr, 0, &payload_bytes));
+        std::string meta(meta_bytes, '\0');
+        checkpoint.data.resize(payload_bytes);
+        check(fc_save_checkpoint(grid, meta.data(), meta_bytes, &meta_bytes, checkpoint.data.data(), payload_bytes,
+            &payload_bytes));
+        auto metadata = bl::JSON::json::parse(meta.c_str());
+        auto& host = metadata["host"];
+        host["substances"] = bl::JSON::json::array();
+        for (SubstanceId id = 0; id < substances.size(); ++id)
+            host["substances"].push_back({{"name", substances[id].name}, {"color", substances[id].color}});
+        for (const char* phase : {"liquid", "gas"})
+        {
+            auto& ids = host[std::string(phase) + "_substances"] = bl::JSON::json::array();
+            for (const auto& c : (phase[0] == 'l' ? liquid_mixture : gas_mixture).components)
+                ids.push_back(c.substance);
+        }
+        checkpoint.metadata = std::move(metadata);
+        return true;
+    }
+
+    // loadCheckpoint (FluidGridBase.h:125): validated by the engine before anything changes.
+    bool loadCheckpoint(const FluidCheckpoint& checkpoint) override
+    {
+        const auto& metadata = checkpoint.metadata;
+        check(fc_load_checkpoint(live(), metadata.dump().c_str(), checkpoint.data.data(), checkpoint.data.size()));
+        if (metadata.contains("host"))
+        {
+            const auto& host = metadata["host"];
+            SubstanceCatalogue catalogue;
+            for (const auto& entry : host["substances"])
+                catalogue.add({entry["name"].template get<std::string>(), entry["color"].template get<std::array<float, 3>>()});
+            auto mixture = [&](const char* key, const char* phase)
+            {
+                FluidMixture out;
+                const auto& ids = host[std::string(phase) + "_substances"];
+                size_t k = 0;
+                for (const auto& c : metadata[key])
+                {
+                    out.components.push_back({ids.at(k++).template get<SubstanceId>(), c["density"].template get<double>(),
+                        c["dynamic_viscosity"].template get<double>()});
+                }
+                return out;
+            };
+            liquid_mixture = mixture("liquid_mixture", "liquid");
+            gas_mixture = mixture("gas_mixture", "gas");
+            substances = std::move(catalogue);
+        }
+        return true;
+    }
+
     fc_grid* native() const { return grid; }
 
 protected:

@@ -169,10 +169,20 @@ int fc_project(fc_grid* grid, double dt, int max_iterations, double divergence_t
 int fc_project_relative(fc_grid* grid, double dt, int max_iterations, double relative_tolerance, double divergence_tolerance,
     fc_result* result);
 
-/* step (FluidGridBase.h:133-134): forces (gravity on interior v faces,
- * FluidGridCPU.cpp:987-996), then the projection. */
+/* step (FluidGridBase.h:133-134; FluidGridCPU.cpp:300-360): transport (fc_advect), forces
+ * (gravity on interior v faces, FluidGridCPU.cpp:987-996), then the projection. */
 int fc_step(fc_grid* grid, double dt, int max_iterations, double divergence_tolerance, fc_result* result,
     fc_timings* timings);
+/* FluidGridCPU::advect (UniformCPU/FluidGridCPU.h:121): this backend transports by second-order
+ * semi-Lagrangian back-tracing instead of the reference's PLIC (FluidGridCPU.cpp:362-463),
+ * sampling with the reference's staggered bilinear sampler (FluidGridCPU.cpp:67-90, 465-471).
+ * Face velocities, the liquid fraction and every component mass are traced through the
+ * velocity at the start of the step. */
+int fc_advect(fc_grid* grid, double dt);
+/* FluidGridCPU::sampleVelocity (UniformCPU/FluidGridCPU.h:132, FluidGridCPU.cpp:465-471): the
+ * staggered bilinear velocity at `count` world positions. positions and velocities are host
+ * arrays of interleaved (x, y) pairs. */
+int fc_sample_velocity(fc_grid* grid, int count, const double* positions, double* velocities);
 /* FluidGridCPU::applyGravity (FluidGridCPU.cpp:987-996). */
 int fc_apply_gravity(fc_grid* grid, double dt);
 
@@ -223,6 +233,18 @@ int fc_velocity_pointers(fc_grid* grid, void** u, void** v);
 /* The grid's stream (cudaStream_t) and a wait for all of its work. */
 int fc_get_stream(const fc_grid* grid, void** stream);
 int fc_synchronize(fc_grid* grid);
+
+/* saveCheckpoint (FluidGridBase.h:123): the "cuda-uniform" native checkpoint, modelled on the
+ * reference's "webgpu-uniform" one (UniformWebGPU/FluidGridGPU.cpp:567-695). JSON metadata
+ * (NUL-terminated) and a binary payload: liquid fraction, u, v, pressure, previous pressure,
+ * component masses, then the obstacle mask, each in the grid's device precision. With both
+ * buffers null the call only reports the sizes needed. */
+int fc_save_checkpoint(fc_grid* grid, char* metadata, size_t metadata_capacity, size_t* metadata_bytes, void* payload,
+    size_t payload_capacity, size_t* payload_bytes);
+/* loadCheckpoint (FluidGridBase.h:125; FluidGridGPU.cpp:697-892): restores materials, settings
+ * and state. Every field is validated before any state changes; a checkpoint of another
+ * backend, version, precision or geometry is rejected with FC_ERR_INVALID_ARGUMENT. */
+int fc_load_checkpoint(fc_grid* grid, const char* metadata, const void* payload, size_t payload_bytes);
 
 /* Batched projection: many independent grids of one precision, uneven sizes allowed, solved
  * together (one launch per kernel for all grids; per-grid convergence). No reference

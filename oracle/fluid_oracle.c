@@ -199,6 +199,7 @@ typedef struct
 
 struct or_mg
 {
+    int pre_sweeps, post_sweeps; /* 4 and 4 in the reference (PressureMultigrid.cpp:396) */
     int count;
     or_level* lev;
     int n;          /* coarsest unknowns: open cells - 1 (one pinned) */
@@ -273,6 +274,8 @@ static void build_axis(int nf, const double* fc, int nc, const double* cc, or_in
 or_mg* or_mg_create(int width, int height)
 {
     or_mg* mg = (or_mg*)calloc(1, sizeof(or_mg));
+    mg->pre_sweeps = 4;
+    mg->post_sweeps = 4;
     int w = width, h = height, spacing = 1, count = 0, cap = 4;
     mg->lev = (or_level*)calloc(cap, sizeof(or_level));
     for (;;)
@@ -328,6 +331,13 @@ void or_mg_destroy(or_mg* mg)
 }
 
 int or_mg_levels(const or_mg* mg) { return mg->count; }
+
+/* Sweep counts of the V-cycle (the reference's 4 and 4 by default); at least one pre-sweep. */
+void or_mg_set_sweeps(or_mg* mg, int pre, int post)
+{
+    mg->pre_sweeps = pre < 1 ? 1 : pre;
+    mg->post_sweeps = post < 0 ? 0 : post;
+}
 
 /* PressureMultigrid.cpp:104-117 (rebuildDiagonal). */
 static void level_diagonal(or_level* l)
@@ -615,12 +625,12 @@ static void mg_cycle(or_mg* mg, int index)
     or_level* f = &mg->lev[index];
     or_level* c = &mg->lev[index + 1];
     level_smooth(f, 0, 1);
-    for (int sweep = 1; sweep < 4; ++sweep)
+    for (int sweep = 1; sweep < mg->pre_sweeps; ++sweep)
         level_smooth(f, 0, 0);
     level_restrict(f, c);
     mg_cycle(mg, index + 1);
     level_prolong(c, f);
-    for (int sweep = 0; sweep < 4; ++sweep)
+    for (int sweep = 0; sweep < mg->post_sweeps; ++sweep)
         level_smooth(f, 1, 0);
 }
 
@@ -718,6 +728,8 @@ void or_grid_destroy(or_grid* g)
 }
 
 void or_grid_set_preconditioner(or_grid* g, int which) { g->preconditioner = which; }
+
+void or_grid_set_sweeps(or_grid* g, int pre, int post) { or_mg_set_sweeps(g->mg, pre, post); }
 
 /* FluidGridCPU.cpp:198-254 (upload): fields replaced, history reset, caches invalidated. */
 void or_grid_upload(or_grid* g, const double* density, const double* u, const double* v, const double* p)
@@ -995,4 +1007,111 @@ or_result or_grid_project(
     result.max_divergence = or_grid_max_divergence(g);
     result.converged = result.max_divergence <= divergence_tolerance;
     return result;
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* Semi-Lagrangian transport. The reference has no semi-Lagrangian step (its UniformCPU step   */
+/* transports with PLIC, FluidGridCPU.cpp:362-463); this restates the UniformCUDA transport   */
+/* on the reference's sampler, FluidGridCPU.cpp:67-90 (sampleScalar) and :465-471            */
+/* (sampleVelocity). Compiled without multiply-add contraction, like the device code.         */
+/* ------------------------------------------------------------------------------------------ */
+
+/* std::lerp (P0811R3, as libstdc++ implements it): the blend FluidGridCPU.cpp:86-89 uses. */
+static double or_lerp(double a, double b, double t)
+{
+    if ((a <= 0.0 && b >= 0.0) || (a >= 0.0 && b <= 0.0))
+        return t * b + (1.0 - t) * a;
+    if (t == 1.0)
+        return b;
+    const double x = a + t * (b - a);
+    return ((t > 1.0) == (b > a)) ? (b < x ? x : b) : (b > x ? x : b);
+}
+
+/* std::clamp(x, lo, hi), lo <= hi. */
+static double or_clamp(double x, double lo, double hi)
+{
+    const double m = x < lo ? lo : x;
+    return hi < m ? hi : m;
+}
+
+/* FluidGridCPU.cpp:67-90. */
+double or_sample_scalar(const double* data, int w, int h, double x, double y)
+{
+    x = or_clamp(x, 0.0, (double)(w - 1));
+    y = or_clamp(y, 0.0, (double)(h - 1));
+    const int x0 = (int)x, y0 = (int)y;
+    const int x1 = x0 + 1 < w - 1 ? x0 + 1 : w - 1;
+    const int y1 = y0 + 1 < h - 1 ? y0 + 1 : h - 1;
+    const double tx = x - x0, ty = y - y0;
+    const double a = or_lerp(data[(size_t)y0 * w + x0], data[(size_t)y0 * w + x1], tx);
+    const double b = or_lerp(data[(size_t)y1 * w + x0], data[(size_t)y1 * w + x1], tx);
+    return or_lerp(a, b, ty);
+}
+
+/* FluidGridCPU.cpp:465-471 in cell units. */
+static void or_velocity_at(int W, int H, const double* u, const double* v, double x, double y, double* vx, double* vy)
+{
+    *vx = or_sample_scalar(u, W + 1, H, x, y - 0.5);
+    *vy = or_sample_scalar(v, W, H + 1, x - 0.5, y);
+}
+
+void or_sample_velocity(int W, int H, double cell_size, double origin_x, double origin_y, const double* u,
+    const double* v, int count, const double* positions, double* velocities)
+{
+    for (int n = 0; n < count; ++n)
+    {
+        const double x = (positions[2 * n] - origin_x) / cell_size;
+        const double y = (positions[2 * n + 1] - origin_y) / cell_size;
+        or_velocity_at(W, H, u, v, x, y, velocities + 2 * n, velocities + 2 * n + 1);
+    }
+}
+
+/* Midpoint back-trace: mid = p - (s/2) V(p), back = p - s V(mid). */
+static void or_trace(int W, int H, const double* u, const double* v, double s, double x, double y, double* bx,
+    double* by)
+{
+    const double half = 0.5 * s;
+    double vx, vy;
+    or_velocity_at(W, H, u, v, x, y, &vx, &vy);
+    const double mx = x - half * vx, my = y - half * vy;
+    or_velocity_at(W, H, u, v, mx, my, &vx, &vy);
+    *bx = x - s * vx;
+    *by = y - s * vy;
+}
+
+void or_advect(int W, int H, double s, const double* u, const double* v, int fields, const double* const* in,
+    double* const* out, double* u_out, double* v_out)
+{
+    for (int j = 0; j < H; ++j)
+        for (int i = 0; i <= W; ++i)
+        {
+            double value = 0.0;
+            if (i > 0 && i < W)
+            {
+                double bx, by;
+                or_trace(W, H, u, v, s, (double)i, j + 0.5, &bx, &by);
+                value = or_sample_scalar(u, W + 1, H, bx, by - 0.5);
+            }
+            u_out[(size_t)j * (W + 1) + i] = value;
+        }
+    for (int j = 0; j <= H; ++j)
+        for (int i = 0; i < W; ++i)
+        {
+            double value = 0.0;
+            if (j > 0 && j < H)
+            {
+                double bx, by;
+                or_trace(W, H, u, v, s, i + 0.5, (double)j, &bx, &by);
+                value = or_sample_scalar(v, W, H + 1, bx - 0.5, by);
+            }
+            v_out[(size_t)j * W + i] = value;
+        }
+    for (int j = 0; j < H; ++j)
+        for (int i = 0; i < W; ++i)
+        {
+            double bx, by;
+            or_trace(W, H, u, v, s, i + 0.5, j + 0.5, &bx, &by);
+            for (int k = 0; k < fields; ++k)
+                out[k][(size_t)j * W + i] = or_sample_scalar(in[k], W, H, bx - 0.5, by - 0.5);
+        }
 }

@@ -68,8 +68,19 @@ void or_classify(int cells, const double* fraction, const unsigned char* solid, 
 or_mg* or_mg_create(int width, int height);
 void or_mg_destroy(or_mg* mg);
 int or_mg_levels(const or_mg* mg);
+void or_mg_set_sweeps(or_mg* mg, int pre, int post);
+void or_grid_set_sweeps(or_grid* grid, int pre, int post);
 int or_mg_rebuild(or_mg* mg, const double* inv_u, const double* inv_v); /* 1 ok, 0 breakdown */
 void or_mg_apply(or_mg* mg, const double* residual, double* correction, double residual_mean);
+
+/* Semi-Lagrangian transport on the reference's staggered bilinear sampler
+ * (FluidGridCPU.cpp:67-90, 465-471). s = dt / cell_size. u_out, v_out and out[k] must not alias
+ * the inputs. Wall-normal boundary faces are written as zero. */
+double or_sample_scalar(const double* data, int width, int height, double x, double y);
+void or_sample_velocity(int width, int height, double cell_size, double origin_x, double origin_y, const double* u,
+    const double* v, int count, const double* positions, double* velocities);
+void or_advect(int width, int height, double s, const double* u, const double* v, int fields,
+    const double* const* in, double* const* out, double* u_out, double* v_out);
 
 #ifdef __cplusplus
 }

@@ -99,6 +99,14 @@ def lib():
         L.or_mg_rebuild.restype = C.c_int
         L.or_mg_rebuild.argtypes = [C.c_void_p, _dp, _dp]
         L.or_mg_apply.argtypes = [C.c_void_p, _dp, _dp, C.c_double]
+        L.or_mg_set_sweeps.argtypes = [C.c_void_p, C.c_int, C.c_int]
+        L.or_grid_set_sweeps.argtypes = [C.c_void_p, C.c_int, C.c_int]
+        L.or_sample_scalar.restype = C.c_double
+        L.or_sample_scalar.argtypes = [_dp, C.c_int, C.c_int, C.c_double, C.c_double]
+        L.or_sample_velocity.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, _dp, _dp, C.c_int,
+                                         _dp, _dp]
+        L.or_advect.argtypes = [C.c_int, C.c_int, C.c_double, _dp, _dp, C.c_int, C.POINTER(_dp), C.POINTER(_dp),
+                                _dp, _dp]
         _lib = L
     return _lib
 
@@ -125,6 +133,8 @@ def ref():
         L.ref_download.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp]
         L.ref_project.restype = _RefResult
         L.ref_project.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_double]
+        L.ref_set_origin.argtypes = [C.c_void_p, C.c_double, C.c_double]
+        L.ref_sample_velocity.argtypes = [C.c_void_p, C.c_int, _dp, _dp]
         L.ref_step.restype = _RefResult
         L.ref_step.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_double]
         L.ref_apply_gravity.argtypes = [C.c_void_p, C.c_double]
@@ -217,6 +227,9 @@ class OracleGrid:
     def set_preconditioner(self, multigrid: bool):
         lib().or_grid_set_preconditioner(self.handle, 1 if multigrid else 0)
 
+    def set_sweeps(self, pre: int, post: int):
+        lib().or_grid_set_sweeps(self.handle, pre, post)
+
     def upload(self, density, u, v, pressure=None, solid=None):
         lib().or_grid_upload(self.handle, _ptr(_f64(density)), _ptr(_f64(u)), _ptr(_f64(v)), _ptr(_f64(pressure)))
         if solid is not None:
@@ -298,6 +311,52 @@ class ReferenceGrid:
 
     def max_divergence(self):
         return ref().ref_max_divergence(self.handle)
+
+    def set_origin(self, x, y):
+        ref().ref_set_origin(self.handle, x, y)
+
+    def sample_velocity(self, positions):
+        pos = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1, 2)
+        out = np.empty_like(pos)
+        ref().ref_sample_velocity(self.handle, pos.shape[0], _ptr(pos), _ptr(out))
+        return out
+
+
+def sample_scalar(data, x, y):
+    """FluidGridCPU.cpp:67-90 on a row-major (h, w) array at fractional index (x, y)."""
+    d = _f64(data)
+    h, w = d.shape
+    return lib().or_sample_scalar(_ptr(d), w, h, float(x), float(y))
+
+
+def sample_velocity(u, v, cell_size, positions, origin=(0.0, 0.0)):
+    """FluidGridCPU::sampleVelocity (FluidGridCPU.cpp:465-471) at (n, 2) world positions."""
+    u, v = _f64(u), _f64(v)
+    h, w1 = u.shape
+    pos = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1, 2)
+    out = np.empty_like(pos)
+    lib().or_sample_velocity(w1 - 1, h, float(cell_size), float(origin[0]), float(origin[1]), _ptr(u), _ptr(v),
+                             pos.shape[0], _ptr(pos), _ptr(out))
+    return out
+
+
+def advect(u, v, fields, dt, cell_size, storage=np.float64):
+    """Semi-Lagrangian transport of face velocities and cell fields (restatement of the
+    UniformCUDA transport). ``storage`` is the device's velocity storage type: velocities are
+    rounded to it before tracing and after, as the FP32 engine holds them."""
+    u = np.asarray(u, dtype=np.float64).astype(storage).astype(np.float64)
+    v = np.asarray(v, dtype=np.float64).astype(storage).astype(np.float64)
+    u, v = np.ascontiguousarray(u), np.ascontiguousarray(v)
+    h, w1 = u.shape
+    w = w1 - 1
+    ins = [_f64(f) for f in fields]
+    outs = [np.zeros((h, w)) for _ in ins]
+    u_out, v_out = np.zeros_like(u), np.zeros_like(v)
+    in_ptrs = (_dp * max(1, len(ins)))(*[_ptr(a) for a in ins])
+    out_ptrs = (_dp * max(1, len(outs)))(*[_ptr(a) for a in outs])
+    lib().or_advect(w, h, float(dt) / float(cell_size), _ptr(u), _ptr(v), len(ins), in_ptrs, out_ptrs, _ptr(u_out),
+                    _ptr(v_out))
+    return u_out.astype(storage).astype(np.float64), v_out.astype(storage).astype(np.float64), outs
 
 
 def reference_mg_apply(inv_u, inv_v, residual, residual_mean=0.0):

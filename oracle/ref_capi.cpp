@@ -138,6 +138,20 @@ ref_result ref_step(void* handle, double dt, int max_iterations, double toleranc
     return timed([&] { return grid.step(dt, max_iterations, tolerance); });
 }
 
+void ref_set_origin(void* handle, double x, double y) { static_cast<FluidGridCPU*>(handle)->setOrigin({x, y}); }
+
+// FluidGridCPU::sampleVelocity at interleaved (x, y) world positions.
+void ref_sample_velocity(void* handle, int count, const double* positions, double* velocities)
+{
+    const auto& grid = *static_cast<FluidGridCPU*>(handle);
+    for (int n = 0; n < count; ++n)
+    {
+        const bl::DVec2 v = grid.sampleVelocity({positions[2 * n], positions[2 * n + 1]});
+        velocities[2 * n] = v.x;
+        velocities[2 * n + 1] = v.y;
+    }
+}
+
 double ref_max_divergence(void* handle) { return static_cast<FluidGridCPU*>(handle)->maxDivergence(); }
 
 // Face weights as the engine caches them (valid after a projection).

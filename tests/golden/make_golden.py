@@ -71,6 +71,24 @@ def hydrostatic_case():
     print("hydrostatic", r.iterations, "rise", p[h - 1, 0] - p[0, 0])
 
 
+def sampler_case():
+    """FluidGridCPU::sampleVelocity on a 9 x 7 grid with origin (-7, 11) and cell size 2.5 (the
+    geometry of tests/FluidGridTests.cpp:53-93), seeded velocities, positions inside and outside
+    the sample domain."""
+    w, h, dx, origin = 9, 7, 2.5, (-7.0, 11.0)
+    rng = np.random.default_rng(53)
+    u = rng.standard_normal((h, w + 1))
+    v = rng.standard_normal((h + 1, w))
+    g = O.ReferenceGrid(w, h, dx)
+    g.set_origin(*origin)
+    g.upload(np.zeros((h, w)), u, v)
+    positions = np.column_stack([rng.uniform(-12.0, 20.0, 512), rng.uniform(5.0, 35.0, 512)])
+    velocities = g.sample_velocity(positions)
+    np.savez_compressed(os.path.join(HERE, "sampler_9x7.npz"), width=w, height=h, cell_size=dx,
+                        origin=np.array(origin), u=u, v=v, positions=positions, velocities=velocities)
+    print("sampler", positions.shape[0], "positions")
+
+
 def main():
     O.build(reference=True)
     O.set_reference_threads(1)
@@ -82,6 +100,7 @@ def main():
     for (w, h) in [(1, 1), (13, 9), (65, 37)]:
         multigrid_case(f"{w}x{h}", w, h)
     hydrostatic_case()
+    sampler_case()
 
 
 if __name__ == "__main__":

@@ -76,5 +76,8 @@ def test_cpp_adapter_compiles_against_reference_contract(tmp_path):
     src.write_text('#include "FluidGridCUDA.h"\nint main() { return fluid::FluidGridCUDA::kind() == 0; }\n')
     cmd = ["g++", "-std=c++23", "-fsyntax-only", f"-I{HEADER_DIR}", f"-I{reference}",
            f"-I{os.path.join(ROOT, 'oracle', 'ref_shim')}", str(src)]
+    nlohmann = "/opt/prime-rl/.venv/lib/python3.12/site-packages/include/cudnn_frontend/thirdparty"
+    if os.path.isdir(nlohmann):
+        cmd.insert(2, f"-I{nlohmann}")
     out = subprocess.run(cmd, capture_output=True, text=True)
     assert out.returncode == 0, out.stderr[-2000:]

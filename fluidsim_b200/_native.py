@@ -83,6 +83,11 @@ SIGNATURES = {
     "fc_project_relative": (_int, [_vp, _dbl, _int, _dbl, _dbl, C.POINTER(FcResult)]),
     "fc_step": (_int, [_vp, _dbl, _int, _dbl, C.POINTER(FcResult), C.POINTER(FcTimings)]),
     "fc_advect": (_int, [_vp, _dbl]),
+    "fc_get_surface_tension": (_int, [_vp, _dp]),
+    "fc_set_surface_tension": (_int, [_vp, _dbl]),
+    "fc_capillary_step_limit": (_int, [_vp, _dp]),
+    "fc_apply_surface_tension": (_int, [_vp, _dbl]),
+    "fc_surface_curvature": (_int, [_vp, _vp, _vp]),
     "fc_sample_velocity": (_int, [_vp, _int, _vp, _vp]),
     "fc_apply_gravity": (_int, [_vp, _dbl]),
     "fc_max_divergence": (_int, [_vp, _dp]),

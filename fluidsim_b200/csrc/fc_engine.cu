@@ -12,6 +12,7 @@
 #include "fc_smooth.cuh"
 #include "fc_json.h"
 #include "fc_advect.cuh"
+#include "fc_tension.cuh"
 
 #include "../../include/fluidcuda.h"
 
@@ -22,6 +23,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <memory>
 #include <mutex>
 #include <new>
@@ -87,10 +89,13 @@ template <typename F> int guarded(F&& body)
     }
 }
 
+inline long long launch_size(long long blocks) { return blocks; }
+inline long long launch_size(dim3 blocks) { return (long long)blocks.x * blocks.y * blocks.z; }
+
 #define FC_LAUNCH(kernel, blocks, threads, smem, stream, ...)                                      \
     do                                                                                             \
     {                                                                                              \
-        if ((blocks) > 0)                                                                          \
+        if (::fc::launch_size(blocks) > 0)                                                         \
         {                                                                                          \
             kernel<<<(blocks), (threads), (smem), (stream)>>>(__VA_ARGS__);                        \
             check(cudaGetLastError(), #kernel);                                                    \
@@ -219,6 +224,7 @@ struct Grid
     int device = 0;
     int preconditioner = FC_PRECONDITIONER_MULTIGRID;
     double gravity_y = 100.0; // FluidGridCPU.h:37
+    double surface_tension = 0.0;
     std::vector<double> liquid_density, gas_density, liquid_viscosity, gas_viscosity;
     bool configured = false;
     bool uploaded = false;
@@ -244,6 +250,8 @@ struct Grid
     unsigned char* mask = nullptr;
     size_t cells = 0, faces_u = 0, faces_v = 0;
     int mass_capacity = 0;
+    char* tension_arena = nullptr; // curvature sweeps, allocated on first use
+    TensionArrays tension{};
 
     std::unique_ptr<Plan> plan; // single-grid plan, built lazily
 
@@ -646,6 +654,7 @@ Grid::~Grid()
     plan.reset();
     cudaFree(masses);
     cudaFree(mass_ptrs);
+    cudaFree(tension_arena);
     cudaFree(arena);
     if (stream)
         cudaStreamDestroy(stream);
@@ -1273,6 +1282,85 @@ void sample_velocity(Grid& g, int count, const double* positions, double* veloci
     check(cudaFree(d), "sample free");
 }
 
+// FluidGridCPU::capillaryStepLimit (FluidGridCPU.cpp:843-860): half the period of the
+// shortest resolved capillary wave, from the lightest liquid and gas components.
+double capillary_step_limit(const Grid& g)
+{
+    if (g.surface_tension == 0.0 || g.liquid_density.empty() || g.gas_density.empty())
+        return INFINITY;
+    const double liquid = *std::min_element(g.liquid_density.begin(), g.liquid_density.end());
+    const double gas = *std::min_element(g.gas_density.begin(), g.gas_density.end());
+    constexpr double pi = 3.14159265358979323846;
+    return 0.5 * std::sqrt((liquid + gas) * g.dx * g.dx * g.dx / (2.0 * pi * g.surface_tension));
+}
+
+void ensure_tension(Grid& g)
+{
+    if (g.tension_arena)
+        return;
+    const size_t n = g.cells;
+    auto round = [](size_t b) { return (b + 255) / 256 * 256; };
+    const size_t sizes[6] = {round(n * sizeof(double2)), round(2 * n), round(n * sizeof(double)), round(n),
+        round(n * sizeof(double)), round(n)};
+    size_t total = 0;
+    for (size_t b : sizes)
+        total += b;
+    check(cudaMalloc(&g.tension_arena, total), "surface tension allocation");
+    char* at = g.tension_arena;
+    void* ptrs[6];
+    for (int i = 0; i < 6; ++i)
+    {
+        ptrs[i] = at;
+        at += sizes[i];
+    }
+    g.tension = {static_cast<double2*>(ptrs[0]), static_cast<signed char*>(ptrs[1]), static_cast<double*>(ptrs[2]),
+        static_cast<unsigned char*>(ptrs[3]), static_cast<double*>(ptrs[4]), static_cast<unsigned char*>(ptrs[5])};
+}
+
+// The three curvature sweeps of FluidSurfaceTensionCPU on the current liquid fraction.
+void launch_curvature(Grid& g, cudaStream_t s)
+{
+    ensure_tension(g);
+    const dim3 block(32, 8), grid_dim((g.W + 31) / 32, (g.H + 7) / 8);
+    FC_LAUNCH(k_tension_heights, grid_dim, block, 0, s, g.fraction, g.W, g.H, g.tension);
+    FC_LAUNCH(k_tension_curvature, grid_dim, block, 0, s, g.fraction, g.W, g.H, g.dx, g.tension);
+    FC_LAUNCH(k_tension_complete, grid_dim, block, 0, s, g.fraction, g.W, g.H, g.dx, g.tension);
+}
+
+// FluidGridCPU::applySurfaceTension (FluidGridCPU.cpp:862-926): curvature, then the capillary
+// force on every interior face with the pressure face weights of the current densities.
+void apply_surface_tension(Grid& g, double dt)
+{
+    require_uploaded(g);
+    if (g.surface_tension == 0.0)
+        return;
+    Plan& p = single_plan(g);
+    rebuild_if_dirty(p);
+    launch_curvature(g, p.stream);
+    const dim3 block(32, 8), grid_dim((g.W + 31) / 32, (g.H + 7) / 8);
+    dispatch(g.precision, [&](auto zero)
+    {
+        using T = decltype(zero);
+        FC_LAUNCH(k_tension_force<T>, grid_dim, block, 0, p.stream, p.d_desc, 0, g.fraction, g.tension, g.surface_tension,
+            dt);
+    });
+    check(cudaStreamSynchronize(p.stream), "surface tension");
+}
+
+// Completed curvature per cell and its validity, for inspection.
+void surface_curvature(Grid& g, double* values, unsigned char* valid)
+{
+    require_uploaded(g);
+    Plan& p = single_plan(g);
+    launch_curvature(g, p.stream);
+    if (values)
+        check(cudaMemcpyAsync(values, g.tension.kappa, g.cells * sizeof(double), cudaMemcpyDeviceToHost, p.stream),
+            "curvature download");
+    if (valid)
+        check(cudaMemcpyAsync(valid, g.tension.kappa_ok, g.cells, cudaMemcpyDeviceToHost, p.stream), "curvature download");
+    check(cudaStreamSynchronize(p.stream), "curvature");
+}
+
 // One preconditioner application to a given residual (PressureMultigrid::apply,
 // PressureMultigrid.cpp:410-434, or the diagonal at FluidGridCPU.cpp:1691-1698); the
 // correction is returned without its mean removed, as the reference's apply returns it.
@@ -1442,6 +1530,7 @@ std::string checkpoint_metadata(const Grid& g)
     m += ", \"cell_size\": " + number(g.dx);
     m += ", \"origin\": [" + number(g.origin_x) + ", " + number(g.origin_y) + "]";
     m += ", \"gravity_y\": " + number(g.gravity_y);
+    m += ", \"surface_tension\": " + number(g.surface_tension);
     m += ", \"preconditioner\": " + std::to_string(g.preconditioner);
     m += ", \"liquid_mixture\": " + mixture(g.liquid_density, g.liquid_viscosity);
     m += ", \"gas_mixture\": " + mixture(g.gas_density, g.gas_viscosity);
@@ -1553,6 +1642,14 @@ void load_checkpoint(Grid& g, const char* metadata, const void* payload, size_t 
         fail(FC_ERR_INVALID_ARGUMENT, "checkpoint preconditioner is unknown");
     const bool solid = need("obstacles", json::Value::Bool).boolean;
     const double gravity = need("gravity_y", json::Value::Number).number;
+    // Older checkpoints carry no surface tension: zero, the engine default.
+    double tension = 0.0;
+    if (const json::Value* st = m.find("surface_tension"))
+    {
+        if (st->kind != json::Value::Number || !std::isfinite(st->number) || st->number < 0.0)
+            fail(FC_ERR_INVALID_ARGUMENT, "checkpoint surface tension is malformed");
+        tension = st->number;
+    }
     const PayloadLayout layout = payload_layout(g, int(ld.size() + gd.size()), solid);
     if (size_t(need("payload_bytes", json::Value::Number).number) != layout.total || payload_bytes != layout.total)
         fail(FC_ERR_INVALID_ARGUMENT, "checkpoint payload has %zu bytes, %zu expected", payload_bytes, layout.total);
@@ -1565,6 +1662,7 @@ void load_checkpoint(Grid& g, const char* metadata, const void* payload, size_t 
     g.configured = true;
     g.preconditioner = preconditioner;
     g.gravity_y = gravity;
+    g.surface_tension = tension;
     g.origin_x = origin.items[0].number;
     g.origin_y = origin.items[1].number;
     allocate_masses(g);
@@ -1896,6 +1994,60 @@ int fc_set_gravity(fc_grid* grid, double gravity_y)
     });
 }
 
+int fc_get_surface_tension(const fc_grid* grid, double* coefficient)
+{
+    return guarded([&]
+    {
+        if (!grid || !coefficient)
+            fail(FC_ERR_INVALID_ARGUMENT, "null argument");
+        *coefficient = grid->impl.surface_tension;
+    });
+}
+
+int fc_set_surface_tension(fc_grid* grid, double coefficient)
+{
+    return guarded([&]
+    {
+        if (!grid)
+            fail(FC_ERR_INVALID_ARGUMENT, "null grid");
+        if (!std::isfinite(coefficient) || coefficient < 0.0)
+            fail(FC_ERR_INVALID_ARGUMENT, "Surface tension must be finite and nonnegative");
+        grid->impl.surface_tension = coefficient;
+    });
+}
+
+int fc_capillary_step_limit(const fc_grid* grid, double* limit)
+{
+    return guarded([&]
+    {
+        if (!grid || !limit)
+            fail(FC_ERR_INVALID_ARGUMENT, "null argument");
+        *limit = fc::capillary_step_limit(grid->impl);
+    });
+}
+
+int fc_apply_surface_tension(fc_grid* grid, double dt)
+{
+    return guarded([&]
+    {
+        if (!grid)
+            fail(FC_ERR_INVALID_ARGUMENT, "null grid");
+        if (!std::isfinite(dt))
+            fail(FC_ERR_INVALID_ARGUMENT, "time step must be finite");
+        fc::apply_surface_tension(grid->impl, dt);
+    });
+}
+
+int fc_surface_curvature(fc_grid* grid, double* curvature, unsigned char* valid)
+{
+    return guarded([&]
+    {
+        if (!grid)
+            fail(FC_ERR_INVALID_ARGUMENT, "null grid");
+        fc::surface_curvature(grid->impl, curvature, valid);
+    });
+}
+
 int fc_set_preconditioner(fc_grid* grid, int preconditioner)
 {
     return guarded([&]
@@ -2057,26 +2209,57 @@ int fc_step(fc_grid* grid, double dt, int max_iterations, double divergence_tole
         }
         return FC_OK;
     }
-    const auto t0 = Clock::now();
-    int status = fc_advect(grid, dt);
-    if (status != FC_OK)
-        return status;
-    const auto t1 = Clock::now();
-    status = fc_apply_gravity(grid, dt);
-    if (status != FC_OK)
-        return status;
-    const auto t2 = Clock::now();
-    status = fc_project(grid, dt, max_iterations, divergence_tolerance, result);
-    const auto t3 = Clock::now();
-    if (timings)
+    // Capillary subdivisions (FluidGridCPU.cpp:309-320): each advances transport, forces and
+    // the projection together.
+    const bool tension = grid->impl.surface_tension > 0.0;
+    const double subdivisions = tension ? std::max(1.0, std::ceil(dt / fc::capillary_step_limit(grid->impl))) : 1.0;
+    // The reference throws std::runtime_error here.
+    if (subdivisions > double(std::numeric_limits<int>::max()))
+        return guarded([] { fail(FC_ERR_UNSUPPORTED, "Surface tension requires too many physical substeps for this timestep"); });
+    const int count = int(subdivisions);
+    const double step = dt / count;
+    fc_result total{};
+    fc_result one{};
+    int status = FC_OK;
+    auto previous = Clock::now();
+    auto elapsed = [&]
     {
-        timings->transport_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
-        timings->forces_ms = std::chrono::duration<double, std::milli>(t2 - t1).count();
-        timings->pressure_ms = std::chrono::duration<double, std::milli>(t3 - t2).count();
+        const auto now = Clock::now();
+        const double ms = std::chrono::duration<double, std::milli>(now - previous).count();
+        previous = now;
+        return ms;
+    };
+    for (int i = 0; i < count; ++i)
+    {
+        if ((status = fc_advect(grid, step)) != FC_OK)
+            return status;
+        if (timings)
+            timings->transport_ms += elapsed();
+        if ((status = fc_apply_gravity(grid, step)) != FC_OK)
+            return status;
+        if (tension && (status = fc_apply_surface_tension(grid, step)) != FC_OK)
+            return status;
+        if (timings)
+            timings->forces_ms += elapsed();
+        if ((status = fc_project(grid, step, max_iterations, divergence_tolerance, &one)) != FC_OK)
+            return status;
+        if (timings)
+            timings->pressure_ms += elapsed();
+        const int iterations = total.iterations + one.iterations;
+        const int restarts = total.restarts + one.restarts;
+        const int kernels = total.kernels + one.kernels;
+        const int steps = total.physical_steps + 1;
+        total = one;
+        total.iterations = iterations;
+        total.restarts = restarts;
+        total.kernels = kernels;
+        total.physical_steps = steps;
+        if (!one.converged)
+            break;
     }
     if (result)
-        result->physical_steps = 1;
-    return status;
+        *result = total;
+    return FC_OK;
 }
 
 int fc_max_divergence(fc_grid* grid, double* out)

@@ -246,6 +246,29 @@ class FluidGrid:
         """Semi-Lagrangian transport of velocities, liquid fraction and component masses."""
         N.check(N.lib().fc_advect(self.handle, float(dt)))
 
+    def getSurfaceTension(self) -> float:
+        out = C.c_double()
+        N.check(N.lib().fc_get_surface_tension(self.handle, C.byref(out)))
+        return out.value
+
+    def setSurfaceTension(self, coefficient: float):
+        N.check(N.lib().fc_set_surface_tension(self.handle, float(coefficient)))
+
+    def capillaryStepLimit(self) -> float:
+        out = C.c_double()
+        N.check(N.lib().fc_capillary_step_limit(self.handle, C.byref(out)))
+        return out.value
+
+    def applySurfaceTension(self, dt: float):
+        N.check(N.lib().fc_apply_surface_tension(self.handle, float(dt)))
+
+    def surfaceCurvature(self):
+        """Completed height-function curvature per cell (1/length) and its validity mask."""
+        k = np.empty((self.height, self.width))
+        ok = np.empty((self.height, self.width), dtype=np.uint8)
+        N.check(N.lib().fc_surface_curvature(self.handle, k.ctypes.data, ok.ctypes.data))
+        return k, ok.astype(bool)
+
     def sampleVelocity(self, positions) -> np.ndarray:
         """FluidGridCPU::sampleVelocity at world positions, shape (n, 2) -> (n, 2)."""
         pos = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1, 2)

@@ -183,6 +183,21 @@ int fc_advect(fc_grid* grid, double dt);
  * staggered bilinear velocity at `count` world positions. positions and velocities are host
  * arrays of interleaved (x, y) pairs. */
 int fc_sample_velocity(fc_grid* grid, int count, const double* positions, double* velocities);
+/* Surface tension coefficient (FluidGridBase.h get/setSurfaceTension; FluidGridCPU.cpp:835-841:
+ * negative or non-finite values are rejected). fc_step subdivides dt by the capillary limit
+ * (FluidGridCPU.cpp:309-320) and applies the capillary force after gravity. */
+int fc_get_surface_tension(const fc_grid* grid, double* coefficient);
+int fc_set_surface_tension(fc_grid* grid, double coefficient);
+/* FluidGridCPU::capillaryStepLimit (FluidGridCPU.cpp:843-860); +inf without tension. */
+int fc_capillary_step_limit(const fc_grid* grid, double* limit);
+/* FluidGridCPU::applySurfaceTension (FluidGridCPU.cpp:862-926): height-function curvature
+ * (UniformCPU/FluidSurfaceTensionCPU.h) and the capillary face force. No-op when the
+ * coefficient is zero. */
+int fc_apply_surface_tension(fc_grid* grid, double dt);
+/* The completed curvature of every cell (1/length) and its validity flag (1 = valid), computed
+ * from the current liquid fraction; either output may be NULL. No reference counterpart: it
+ * exposes FluidSurfaceTensionCPU::curvature for inspection. */
+int fc_surface_curvature(fc_grid* grid, double* curvature, unsigned char* valid);
 /* FluidGridCPU::applyGravity (FluidGridCPU.cpp:987-996). */
 int fc_apply_gravity(fc_grid* grid, double dt);
 

@@ -134,6 +134,11 @@ def ref():
         L.ref_project.restype = _RefResult
         L.ref_project.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_double]
         L.ref_set_origin.argtypes = [C.c_void_p, C.c_double, C.c_double]
+        L.ref_set_surface_tension.argtypes = [C.c_void_p, C.c_double]
+        L.ref_capillary_step_limit.restype = C.c_double
+        L.ref_capillary_step_limit.argtypes = [C.c_void_p]
+        L.ref_apply_surface_tension.argtypes = [C.c_void_p, C.c_double]
+        L.ref_surface_curvature.argtypes = [C.c_int, C.c_int, C.c_double, _dp, _dp, _u8p]
         L.ref_sample_velocity.argtypes = [C.c_void_p, C.c_int, _dp, _dp]
         L.ref_step.restype = _RefResult
         L.ref_step.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_double]
@@ -312,6 +317,16 @@ class ReferenceGrid:
     def max_divergence(self):
         return ref().ref_max_divergence(self.handle)
 
+    def set_surface_tension(self, sigma):
+        ref().ref_set_surface_tension(self.handle, float(sigma))
+
+    def capillary_step_limit(self):
+        return ref().ref_capillary_step_limit(self.handle)
+
+    def apply_surface_tension(self, dt):
+        """FluidGridCPU::applySurfaceTension (the reference's own code)."""
+        ref().ref_apply_surface_tension(self.handle, float(dt))
+
     def set_origin(self, x, y):
         ref().ref_set_origin(self.handle, x, y)
 
@@ -320,6 +335,17 @@ class ReferenceGrid:
         out = np.empty_like(pos)
         ref().ref_sample_velocity(self.handle, pos.shape[0], _ptr(pos), _ptr(out))
         return out
+
+
+def reference_surface_curvature(fraction, cell_size):
+    """FluidSurfaceTensionCPU (the reference's own header) on a fraction field: completed
+    curvature per cell and its validity."""
+    f = _f64(fraction)
+    h, w = f.shape
+    k = np.zeros((h, w))
+    ok = np.zeros((h, w), dtype=np.uint8)
+    ref().ref_surface_curvature(w, h, float(cell_size), _ptr(f), _ptr(k), ok.ctypes.data_as(_u8p))
+    return k, ok.astype(bool)
 
 
 def sample_scalar(data, x, y):

@@ -5,6 +5,7 @@
 // golden fixtures under tests/golden/, and as the timed CPU baseline of bench.py.
 #include "UniformCPU/FluidGridCPU.h"
 #include "UniformCPU/PressureMultigrid.h"
+#include "UniformCPU/FluidSurfaceTensionCPU.h"
 #include <bitloop/core/threads.h>
 #include <chrono>
 #include <cstring>
@@ -20,6 +21,23 @@ const FluidField::Layout& FluidField::layout() const { std::terminate(); }
 bool FluidField::isWebGPU() const { std::terminate(); }
 std::span<const float> FluidField::values() const { std::terminate(); }
 std::span<float> FluidField::values() { std::terminate(); }
+}
+
+// FluidGridCPU::applySurfaceTension is private. An explicit template instantiation may name a
+// private member ([temp.explicit]), which hands its address to a friend function here, so the
+// oracle can run the reference's own force code on a given state.
+namespace
+{
+struct TensionMember
+{
+    using type = void (FluidGridCPU::*)(double);
+};
+template <typename Tag, typename Tag::type Member> struct Expose
+{
+    friend typename Tag::type member_of(Tag) { return Member; }
+};
+TensionMember::type member_of(TensionMember);
+template struct Expose<TensionMember, &FluidGridCPU::applySurfaceTension>;
 }
 
 extern "C" {
@@ -136,6 +154,40 @@ ref_result ref_step(void* handle, double dt, int max_iterations, double toleranc
 {
     auto& grid = *static_cast<FluidGridCPU*>(handle);
     return timed([&] { return grid.step(dt, max_iterations, tolerance); });
+}
+
+void ref_set_surface_tension(void* handle, double sigma) { static_cast<FluidGridCPU*>(handle)->setSurfaceTension(sigma); }
+
+double ref_capillary_step_limit(void* handle) { return static_cast<FluidGridCPU*>(handle)->capillaryStepLimit(); }
+
+// FluidGridCPU::applySurfaceTension(dt) on the uploaded state.
+void ref_apply_surface_tension(void* handle, double dt)
+{
+    auto& grid = *static_cast<FluidGridCPU*>(handle);
+    (grid.*member_of(TensionMember{}))(dt);
+}
+
+// FluidSurfaceTensionCPU's three sweeps on a fraction field: completed curvature and validity.
+void ref_surface_curvature(int width, int height, double cell_size, const double* fraction, double* curvature,
+    unsigned char* valid)
+{
+    fluid::FluidSurfaceTensionCPU geometry(width, height);
+    geometry.liquid = std::span<const double>(fraction, size_t(width) * height);
+    geometry.cell_size = cell_size;
+    for (int y = 0; y < height; ++y)
+        for (int x = 0; x < width; ++x)
+            geometry.buildHeight(x, y);
+    for (int y = 0; y < height; ++y)
+        for (int x = 0; x < width; ++x)
+            geometry.buildCurvature(x, y);
+    for (int y = 0; y < height; ++y)
+        for (int x = 0; x < width; ++x)
+            geometry.completeCurvature(x, y);
+    for (size_t i = 0; i < size_t(width) * height; ++i)
+    {
+        curvature[i] = geometry.curvature[i].valid ? geometry.curvature[i].value : 0.0;
+        valid[i] = geometry.curvature[i].valid ? 1 : 0;
+    }
 }
 
 void ref_set_origin(void* handle, double x, double y) { static_cast<FluidGridCPU*>(handle)->setOrigin({x, y}); }

@@ -89,6 +89,54 @@ def sampler_case():
     print("sampler", positions.shape[0], "positions")
 
 
+def antialiased(w, h, inside, sub=8):
+    """Liquid fraction of each cell from sub x sub point samples of an inside(x, y) test."""
+    y, x = np.mgrid[0:h, 0:w].astype(float)
+    f = np.zeros((h, w))
+    for sy in range(sub):
+        for sx in range(sub):
+            f += inside(x + (sx + 0.5) / sub, y + (sy + 0.5) / sub)
+    return f / (sub * sub)
+
+
+def tension_case(name, fraction, cell_size, sigma=0.07, dt=1.0 / 120.0, seed=0):
+    """FluidGridCPU::applySurfaceTension and FluidSurfaceTensionCPU's curvature, run by the
+    reference itself on one liquid (1000) and one gas (1) component."""
+    h, w = fraction.shape
+    rng = np.random.default_rng(seed)
+    u = rng.uniform(-1.0, 1.0, (h, w + 1))
+    v = rng.uniform(-1.0, 1.0, (h + 1, w))
+    area = cell_size * cell_size
+    g = O.ReferenceGrid(w, h, cell_size, 1000.0, 1.0)
+    g.set_surface_tension(sigma)
+    g.upload(fraction, u, v, None, 1000.0 * fraction * area, 1.0 * (1.0 - fraction) * area)
+    limit = g.capillary_step_limit()
+    g.apply_surface_tension(dt)
+    _, u_out, v_out, _ = g.download()
+    kappa, valid = O.reference_surface_curvature(fraction, cell_size)
+    np.savez_compressed(os.path.join(HERE, f"tension_{name}.npz"), width=w, height=h, cell_size=cell_size,
+                        sigma=sigma, dt=dt, fraction=fraction, u_in=u, v_in=v, u=u_out, v=v_out,
+                        curvature=kappa, valid=valid, capillary_step_limit=limit)
+    print("tension", name, "valid", int(valid.sum()), "max |du|", np.abs(u_out - u).max())
+
+
+def tension_cases():
+    drop = antialiased(48, 40, lambda x, y: (x - 24.0) ** 2 + (y - 20.0) ** 2 < 12.0 ** 2)
+    tension_case("drop48x40", drop, 1.0 / 48.0)
+    wave = antialiased(64, 48, lambda x, y: y > 24.0 + 4.0 * np.sin(2.0 * np.pi * x / 32.0))
+    tension_case("wave64x48", wave, 1.0 / 64.0, seed=1)
+    # Seeded blobs, thin filaments and near-pure cells a few ulps from 0 and 1.
+    rng = np.random.default_rng(17)
+    blobs = np.zeros((37, 53))
+    for _ in range(9):
+        cx, cy, r = rng.uniform(0, 53), rng.uniform(0, 37), rng.uniform(1.0, 7.0)
+        blobs = np.maximum(blobs, antialiased(53, 37, lambda x, y: (x - cx) ** 2 + (y - cy) ** 2 < r * r))
+    blobs[5, 3:40] = np.maximum(blobs[5, 3:40], 0.3)
+    blobs[blobs == 1.0] -= 4e-16 * (rng.uniform(size=(blobs == 1.0).sum()) < 0.2)
+    blobs[blobs == 0.0] += 3e-17 * (rng.uniform(size=(blobs == 0.0).sum()) < 0.2)
+    tension_case("blobs53x37", blobs, 0.02, sigma=0.5, seed=2)
+
+
 def main():
     O.build(reference=True)
     O.set_reference_threads(1)
@@ -101,6 +149,7 @@ def main():
         multigrid_case(f"{w}x{h}", w, h)
     hydrostatic_case()
     sampler_case()
+    tension_cases()
 
 
 if __name__ == "__main__":

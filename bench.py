@@ -48,6 +48,9 @@ def parse():
     p.add_argument("--no-batched", action="store_true", help="skip the batched uneven-grid measurement")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-serve", action="store_true", help="skip the serving (continuous batching) measurement")
+    p.add_argument("--serve-requests", type=int, default=16)
+    p.add_argument("--serve-steps", type=int, default=300)
     p.add_argument("--launch", choices=["graph", "stream"], default="graph",
                    help="stream: host-driven launches of the same kernels (for per-kernel profilers)")
     return p.parse_args()
@@ -297,6 +300,8 @@ def run_cuda(args, world, rank, local_rank):
                                 "sample": f"1 projection of the {size}x{size} workload"}
     if rank == 0 and not args.no_batched:
         line["batched"] = batched_measure(args, torch)
+    if rank == 0 and not args.no_serve:
+        line["serve"] = serve_measure(args)
     return line
 
 
@@ -400,6 +405,60 @@ def batched_measure(args, torch, count=256):
             "ms_per_batch": batched_ms, "plain_one_at_a_time_cells_per_s": cells / (plain_ms / 1e3),
             "speedup_vs_plain": plain_ms / batched_ms, "all_converged": ok,
             "max_iterations": max(r.iterations for r in res)}
+
+
+def serve_measure(args, rate=200.0, budget=150 * 10**9):
+    """Serving: Poisson arrivals (mean `rate` per second) of dam breaks with surface tension
+    (sigma 0.07, liquid 1000, air 1), square sides log-uniform 64..2048, each run for
+    serve_steps steps of dt 1/120 to the max-norm rule at the bench tolerance, admitted by a
+    device-memory budget and batched as they arrive. The same simulations are then run one at a
+    time through fc_step (the plain path). A bounded sample: serve_requests requests."""
+    import time
+
+    from fluidsim_b200 import FluidGrid, scenes
+    from fluidsim_b200.serving import Server, poisson_arrivals, serve
+
+    reqs = scenes.serving_requests(args.serve_requests, seed=5)
+    arrivals = poisson_arrivals(rate, len(reqs), seed=6)
+    steps = args.serve_steps
+    cell_steps = steps * sum(s.cells for s in reqs)
+    server = Server(budget, max_active=256)
+    out = serve(server, reqs, arrivals, steps, 200, args.tolerance)
+    stats = server.stats()
+    served_ok = all(st.state == "done" for st in out["statuses"])
+    for sim in out["ids"]:
+        server.release(sim)
+    server.close()
+
+    plain_lat = []
+    t0 = time.perf_counter()
+    for s in reqs:
+        g = FluidGrid(s.width, s.height, s.cell_size, "fp32")
+        scenes.upload_scene(g, s)
+        for _ in range(steps):
+            a = time.perf_counter()
+            g.step(s.dt, 200, args.tolerance)
+            plain_lat.append((time.perf_counter() - a) * 1e3)
+        g.destroy()
+    plain_s = time.perf_counter() - t0
+    plain_lat = np.sort(np.array(plain_lat))
+
+    def pct(a, q):
+        return float(a[max(0, int(np.ceil(q * len(a))) - 1)])
+
+    served = cell_steps / out["wall_s"]
+    plain = cell_steps / plain_s
+    return {"value": served, "unit": UNIT, "requests": len(reqs), "steps_per_request": steps,
+            "arrival_rate_per_s": rate, "sizes": sorted(s.width for s in reqs),
+            "sample": f"{len(reqs)} requests (bounded sample of the Poisson stream), sides log-uniform 64..2048, "
+                      f"dx 1/128, sigma 0.07, dt 1/120",
+            "wall_s": out["wall_s"], "step_p50_ms": stats["step_p50_ms"], "step_p99_ms": stats["step_p99_ms"],
+            "step_max_ms": stats["step_max_ms"], "peak_active": stats["peak_active"],
+            "peak_device_bytes": stats["peak_bytes"], "budget_bytes": budget, "batch_plans_built": stats["batch_rebuilds"],
+            "all_done": served_ok,
+            "plain": {"value": plain, "unit": UNIT, "wall_s": plain_s, "step_p50_ms": pct(plain_lat, 0.5),
+                      "step_p99_ms": pct(plain_lat, 0.99)},
+            "speedup_vs_plain": served / plain}
 
 
 def main():

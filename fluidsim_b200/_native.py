@@ -52,6 +52,37 @@ class FcTimings(C.Structure):
                 ("transport_ms", "viscosity_ms", "forces_ms", "pressure_ms", "selection_ms", "regrid_ms")]
 
 
+class FcSimDesc(C.Structure):
+    """Mirror of fc_sim_desc: one simulation submitted to the serving loop."""
+    _fields_ = [
+        ("width", C.c_int), ("height", C.c_int), ("cell_size", C.c_double), ("precision", C.c_int),
+        ("liquid_count", C.c_int), ("liquid_densities", C.c_void_p),
+        ("gas_count", C.c_int), ("gas_densities", C.c_void_p),
+        ("gravity_y", C.c_double), ("surface_tension", C.c_double),
+        ("solid", C.c_void_p),
+        ("liquid_fraction", C.c_void_p), ("u", C.c_void_p), ("v", C.c_void_p), ("pressure", C.c_void_p),
+        ("liquid_mass", C.c_void_p), ("gas_mass", C.c_void_p),
+        ("steps", C.c_int), ("dt", C.c_double), ("max_iterations", C.c_int), ("divergence_tolerance", C.c_double),
+    ]
+
+
+class FcSimStatus(C.Structure):
+    _fields_ = [
+        ("state", C.c_int), ("error", C.c_int), ("steps_done", C.c_int), ("physical_steps", C.c_int),
+        ("iterations", C.c_longlong), ("converged", C.c_int), ("max_divergence", C.c_double),
+        ("queued_ms", C.c_double), ("run_ms", C.c_double), ("device_bytes", C.c_size_t),
+    ]
+
+
+class FcServerStats(C.Structure):
+    _fields_ = [
+        ("ticks", C.c_longlong), ("steps", C.c_longlong), ("physical_steps", C.c_longlong),
+        ("cell_steps", C.c_double), ("busy_ms", C.c_double),
+        ("step_p50_ms", C.c_double), ("step_p99_ms", C.c_double), ("step_max_ms", C.c_double),
+        ("peak_active", C.c_int), ("peak_bytes", C.c_size_t), ("batch_rebuilds", C.c_longlong),
+    ]
+
+
 _dp = C.POINTER(C.c_double)
 _dpp = C.POINTER(_dp)
 _vp = C.c_void_p
@@ -83,6 +114,17 @@ SIGNATURES = {
     "fc_project_relative": (_int, [_vp, _dbl, _int, _dbl, _dbl, C.POINTER(FcResult)]),
     "fc_step": (_int, [_vp, _dbl, _int, _dbl, C.POINTER(FcResult), C.POINTER(FcTimings)]),
     "fc_advect": (_int, [_vp, _dbl]),
+    "fc_grid_device_bytes": (_int, [_int, _int, _int, _int, _int, C.POINTER(C.c_size_t)]),
+    "fc_get_device_bytes": (_int, [_vp, C.POINTER(C.c_size_t)]),
+    "fc_server_create": (_int, [C.c_size_t, _int, C.POINTER(_vp)]),
+    "fc_server_destroy": (_int, [_vp]),
+    "fc_server_submit": (_int, [_vp, C.POINTER(FcSimDesc), C.POINTER(C.c_longlong)]),
+    "fc_server_status": (_int, [_vp, C.c_longlong, C.POINTER(FcSimStatus)]),
+    "fc_server_wait": (_int, [_vp, C.c_longlong, _dbl, C.POINTER(FcSimStatus)]),
+    "fc_server_download": (_int, [_vp, C.c_longlong, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "fc_server_release": (_int, [_vp, C.c_longlong]),
+    "fc_server_get_stats": (_int, [_vp, C.POINTER(FcServerStats)]),
+    "fc_server_step_latencies": (_int, [_vp, _vp, C.c_size_t, C.POINTER(C.c_size_t)]),
     "fc_get_surface_tension": (_int, [_vp, _dp]),
     "fc_set_surface_tension": (_int, [_vp, _dbl]),
     "fc_capillary_step_limit": (_int, [_vp, _dp]),

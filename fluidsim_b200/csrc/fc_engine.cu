@@ -13,6 +13,7 @@
 #include "fc_json.h"
 #include "fc_advect.cuh"
 #include "fc_tension.cuh"
+#include "fc_errors.h"
 
 #include "../../include/fluidcuda.h"
 
@@ -40,11 +41,6 @@ namespace fc
 thread_local std::string last_error;
 std::atomic<long long> launch_count{0};
 
-struct Failure
-{
-    int status;
-};
-
 [[noreturn]] void fail(int status, const char* format, ...)
 {
     char buffer[512];
@@ -63,29 +59,6 @@ void check(cudaError_t err, const char* what)
         cudaGetLastError();
         fail(err == cudaErrorMemoryAllocation ? FC_ERR_OUT_OF_MEMORY : FC_ERR_CUDA, "%s: %s", what,
             cudaGetErrorString(err));
-    }
-}
-
-template <typename F> int guarded(F&& body)
-{
-    try
-    {
-        body();
-        return FC_OK;
-    }
-    catch (const Failure& f)
-    {
-        return f.status;
-    }
-    catch (const std::bad_alloc&)
-    {
-        last_error = "host allocation failed";
-        return FC_ERR_OUT_OF_MEMORY;
-    }
-    catch (...)
-    {
-        last_error = "unexpected exception";
-        return FC_ERR_CUDA;
     }
 }
 
@@ -314,8 +287,9 @@ void choose_tail(Grid& g)
     g.tail_smem = tail_bytes(w.data(), h.data(), n - 1, n, g.elem);
 }
 
-// Lays out every device field of a grid in one allocation and fills the descriptor.
-void allocate_grid(Grid& g)
+// Lays out every device field of a grid in one allocation and fills the descriptor. With
+// allocate false it only returns the arena size (no CUDA calls).
+size_t allocate_grid(Grid& g, bool allocate = true)
 {
     const int W = g.W, H = g.H;
     g.levels = build_levels(W, H);
@@ -408,6 +382,8 @@ void allocate_grid(Grid& g)
         offsets.push_back(total);
         total += (s.bytes + 255) / 256 * 256;
     }
+    if (!allocate)
+        return total;
     check(cudaMalloc(&g.arena, total), "grid allocation");
     g.arena_bytes = total;
     check(cudaMemsetAsync(g.arena, 0, total, g.stream), "grid clear");
@@ -436,6 +412,35 @@ void allocate_grid(Grid& g)
     }
     d.solid = nullptr;
     check(cudaStreamSynchronize(g.stream), "grid set-up");
+    return total;
+}
+
+// Bytes of the surface-tension sweeps of a grid (ensure_tension lays them out this way).
+void tension_layout(size_t cells, size_t sizes[6])
+{
+    auto round = [](size_t b) { return (b + 255) / 256 * 256; };
+    sizes[0] = round(cells * sizeof(double2));
+    sizes[1] = round(2 * cells);
+    sizes[2] = round(cells * sizeof(double));
+    sizes[3] = round(cells);
+    sizes[4] = round(cells * sizeof(double));
+    sizes[5] = round(cells);
+}
+
+size_t tension_bytes(size_t cells)
+{
+    size_t sizes[6], total = 0;
+    tension_layout(cells, sizes);
+    for (size_t b : sizes)
+        total += b;
+    return total;
+}
+
+// Device bytes of a single-grid plan: descriptors, tile tables, solve states and parameters.
+size_t plan_bytes(int W, int H)
+{
+    const size_t tiles = size_t(ceil_div(W, 16) + 1) * (ceil_div(H, 4) + 1) * 6;
+    return (1u << 20) + tiles * 16;
 }
 
 // Component masses live in their own allocation (their count follows configureMaterials).
@@ -652,10 +657,9 @@ struct Plan
 Grid::~Grid()
 {
     plan.reset();
-    cudaFree(masses);
-    cudaFree(mass_ptrs);
-    cudaFree(tension_arena);
-    cudaFree(arena);
+    for (void* ptr : {(void*)masses, (void*)mass_ptrs, (void*)tension_arena, (void*)arena})
+        if (ptr)
+            cudaFree(ptr);
     if (stream)
         cudaStreamDestroy(stream);
 }
@@ -1298,11 +1302,8 @@ void ensure_tension(Grid& g)
 {
     if (g.tension_arena)
         return;
-    const size_t n = g.cells;
-    auto round = [](size_t b) { return (b + 255) / 256 * 256; };
-    const size_t sizes[6] = {round(n * sizeof(double2)), round(2 * n), round(n * sizeof(double)), round(n),
-        round(n * sizeof(double)), round(n)};
-    size_t total = 0;
+    size_t sizes[6], total = 0;
+    tension_layout(g.cells, sizes);
     for (size_t b : sizes)
         total += b;
     check(cudaMalloc(&g.tension_arena, total), "surface tension allocation");
@@ -1876,6 +1877,43 @@ int fc_create(int width, int height, double cell_size, int precision, fc_grid** 
         check(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking), "stream");
         fc::allocate_grid(g);
         *out = handle.release();
+    });
+}
+
+int fc_grid_device_bytes(int width, int height, int precision, int components, int surface_tension, size_t* bytes)
+{
+    return guarded([&]
+    {
+        if (!bytes || width <= 0 || height <= 0 || components < 0 || (long long)width * height > (1ll << 30))
+            fail(FC_ERR_INVALID_ARGUMENT, "invalid grid description");
+        if (precision != FC_PRECISION_FP32 && precision != FC_PRECISION_FP64)
+            fail(FC_ERR_INVALID_ARGUMENT, "unknown precision %d", precision);
+        fc::Grid g;
+        g.W = width;
+        g.H = height;
+        g.precision = precision;
+        g.elem = precision == FC_PRECISION_FP64 ? 8 : 4;
+        size_t total = fc::allocate_grid(g, false);
+        total += size_t(components) * g.cells * sizeof(double) + 256 + size_t(std::max(components, 1)) * sizeof(double*);
+        if (surface_tension)
+            total += fc::tension_bytes(g.cells);
+        total += fc::plan_bytes(width, height);
+        *bytes = total;
+    });
+}
+
+int fc_get_device_bytes(const fc_grid* grid, size_t* bytes)
+{
+    return guarded([&]
+    {
+        if (!grid || !bytes)
+            fail(FC_ERR_INVALID_ARGUMENT, "null argument");
+        const Grid& g = grid->impl;
+        size_t total = g.arena_bytes + size_t(g.mass_capacity) * g.cells * sizeof(double);
+        if (g.tension_arena)
+            total += fc::tension_bytes(g.cells);
+        total += fc::plan_bytes(g.W, g.H);
+        *bytes = total;
     });
 }
 

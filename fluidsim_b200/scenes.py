@@ -29,6 +29,7 @@ class Scene:
     v: np.ndarray                 # (h+1) x w
     gravity: float = 0.0
     solid: Optional[np.ndarray] = None  # h x w uint8, or None
+    surface_tension: float = 0.0
     name: str = ""
     liquid_mass: List[np.ndarray] = field(default_factory=list)
     gas_mass: List[np.ndarray] = field(default_factory=list)
@@ -92,11 +93,13 @@ def liquid_box(width=128, height=128, seed=0, dt=1.0 / 60.0) -> Scene:
 
 
 def dam_break(width=1024, height=1024, seed=0, dt=1.0 / 120.0, obstacles=16, block=(200, 300),
-              liquid_density=1000.0, gas_density=1.0, gravity=-9.8, velocity=0.0) -> Scene:
+              liquid_density=1000.0, gas_density=1.0, gravity=-9.8, velocity=0.0, cell_size=None,
+              surface_tension=0.0) -> Scene:
     """Dam break: liquid below half height plus a seeded block, optional circular obstacles.
 
     Rows are y; gravity acts along y, so the liquid sits in the low rows. Block sizes are in
-    cells and shrink with the grid when it is smaller than 1024.
+    cells and shrink with the grid when it is smaller than 1024. The cell size defaults to
+    1/width (a unit-wide domain).
     """
     rng = np.random.default_rng(seed)
     f = np.zeros((height, width))
@@ -115,8 +118,23 @@ def dam_break(width=1024, height=1024, seed=0, dt=1.0 / 120.0, obstacles=16, blo
         scale = width / 1024.0
         solid = _circles(rng, width, height, obstacles, max(1.0, 8 * scale), max(2.0, 40 * scale))
         f[solid != 0] = 0.0
-    return Scene(width, height, 1.0 / width, dt, liquid_density, gas_density, f, u, v, gravity=gravity,
-                 solid=solid, name=f"dam_break_{width}x{height}")
+    dx = cell_size if cell_size is not None else 1.0 / width
+    return Scene(width, height, dx, dt, liquid_density, gas_density, f, u, v, gravity=gravity,
+                 solid=solid, name=f"dam_break_{width}x{height}", surface_tension=surface_tension)
+
+
+def serving_requests(count, seed=0, min_side=64, max_side=2048, sigma=0.07, cell_size=1.0 / 128.0) -> List[Scene]:
+    """Simulation requests of the serving workload: square dam breaks with sides log-uniform in
+    [min_side, max_side], surface tension sigma, liquid 1000 and air 1, gravity -9.8, dt 1/120.
+    The resolution is fixed (cell_size, default 1/128 m) so the domain grows with the grid; at
+    this resolution one capillary substep covers dt = 1/120."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        side = int(round(np.exp(rng.uniform(np.log(min_side), np.log(max_side)))))
+        out.append(dam_break(side, side, seed=int(rng.integers(0, 2**31 - 1)), obstacles=0, cell_size=cell_size,
+                             surface_tension=sigma))
+    return out
 
 
 def sloped_pool(width, height, cell_size=4.0, dt=1.0 / 120.0, liquid_density=100.0, gas_density=0.1) -> Scene:
@@ -177,5 +195,7 @@ def upload_scene(grid, scene: Scene, pressure=None):
 
     grid.configureMaterials([scene.liquid_density], [scene.gas_density])
     grid.setGravityY(scene.gravity)
+    if scene.surface_tension:
+        grid.setSurfaceTension(scene.surface_tension)
     grid.setObstacles(scene.solid)
     grid.upload(FluidGridState(scene.fraction, scene.u, scene.v, pressure, scene.liquid_mass, scene.gas_mass))

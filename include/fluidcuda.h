@@ -264,12 +264,111 @@ int fc_load_checkpoint(fc_grid* grid, const char* metadata, const void* payload,
 /* Batched projection: many independent grids of one precision, uneven sizes allowed, solved
  * together (one launch per kernel for all grids; per-grid convergence). No reference
  * counterpart: the reference steps scenes one after another (FluidSim.cpp:90-93, 120-131). */
+/* Device bytes a grid of this description holds once created, configured with `components`
+ * material components and (surface_tension != 0) the curvature sweeps, including its
+ * single-grid solve plan. Host arithmetic only: no device call. No reference counterpart (the
+ * serving loop admits simulations by this figure). */
+int fc_grid_device_bytes(int width, int height, int precision, int components, int surface_tension, size_t* bytes);
+/* Device bytes a live grid holds, counted the same way. */
+int fc_get_device_bytes(const fc_grid* grid, size_t* bytes);
+
 int fc_batch_create(fc_grid* const* grids, int count, fc_batch** out);
 int fc_batch_destroy(fc_batch* batch);
 /* dts: one time step per grid. relative_tolerance > 0 selects the relative rule. */
 int fc_batch_project(fc_batch* batch, const double* dts, int max_iterations, double divergence_tolerance,
     double relative_tolerance, fc_result* results);
 int fc_batch_get_stream(const fc_batch* batch, void** stream);
+
+/* ---- Serving: continuous batching of many simulations on one GPU ----------------------------
+ * A request loop in the spirit of FluidScene::sceneProcess (FluidScene.inl:328-420) for many
+ * independent simulations. A worker thread owns every grid. Each tick it admits queued
+ * simulations in arrival order while their device bytes (fc_grid_device_bytes) fit the budget
+ * and a slot is free, runs one physical (sub)step of transport and forces per active grid, then
+ * projects all active grids in one batched solve, and retires the simulations that finished
+ * (their final state is copied to host memory and their device memory freed). State stays
+ * device-resident between steps. Every simulation computes exactly what fc_step would compute
+ * on it alone. */
+typedef struct fc_server fc_server;
+
+typedef struct fc_sim_desc
+{
+    int width, height;
+    double cell_size;
+    int precision;
+    int liquid_count;
+    const double* liquid_densities;
+    int gas_count;
+    const double* gas_densities;
+    double gravity_y;
+    double surface_tension;
+    const unsigned char* solid;      /* width*height obstacle cells, or NULL */
+    const double* liquid_fraction;   /* initial state as for fc_upload; NULL arrays mean zero */
+    const double* u;
+    const double* v;
+    const double* pressure;
+    const double* const* liquid_mass;
+    const double* const* gas_mass;
+    int steps;                       /* time steps to run */
+    double dt;
+    int max_iterations;
+    double divergence_tolerance;     /* the max-norm rule of fc_project */
+} fc_sim_desc;
+
+typedef enum fc_sim_state
+{
+    FC_SIM_QUEUED = 0,
+    FC_SIM_RUNNING = 1,
+    FC_SIM_DONE = 2,
+    FC_SIM_FAILED = 3
+} fc_sim_state;
+
+typedef struct fc_sim_status
+{
+    int state;               /* fc_sim_state */
+    int error;               /* fc_status of a failure, else FC_OK */
+    int steps_done;
+    int physical_steps;      /* capillary subdivisions included */
+    long long iterations;    /* PCG iterations over all steps */
+    int converged;           /* every projection converged */
+    double max_divergence;   /* after the last projection */
+    double queued_ms;        /* submission to admission */
+    double run_ms;           /* admission to completion */
+    size_t device_bytes;     /* charged against the budget while running */
+} fc_sim_status;
+
+typedef struct fc_server_stats
+{
+    long long ticks;
+    long long steps;            /* completed time steps over all simulations */
+    long long physical_steps;
+    double cell_steps;          /* sum over completed steps of the grid's cells */
+    double busy_ms;             /* wall time with at least one simulation running */
+    double step_p50_ms;         /* latency of a time step: its first tick's start to its last tick's end */
+    double step_p99_ms;
+    double step_max_ms;
+    int peak_active;
+    size_t peak_bytes;
+    long long batch_rebuilds;   /* batched solve plans built (one per change of membership) */
+} fc_server_stats;
+
+/* device_budget_bytes: device memory the simulations may hold together; max_active: slots. */
+int fc_server_create(size_t device_budget_bytes, int max_active, fc_server** out);
+/* Stops the worker; simulations still queued or running are dropped. */
+int fc_server_destroy(fc_server* server);
+/* Copies the description and initial state; never blocks on the GPU. A simulation that could
+ * never fit the budget is rejected with FC_ERR_INVALID_ARGUMENT. */
+int fc_server_submit(fc_server* server, const fc_sim_desc* desc, long long* id);
+int fc_server_status(fc_server* server, long long id, fc_sim_status* status);
+/* Waits until the simulation is done or failed; FC_ERR_TIMEOUT after timeout_seconds. */
+int fc_server_wait(fc_server* server, long long id, double timeout_seconds, fc_sim_status* status);
+/* Final state of a finished simulation (as fc_download; NULL outputs are skipped). */
+int fc_server_download(fc_server* server, long long id, double* liquid_fraction, double* u, double* v,
+    double* pressure, double* const* liquid_mass, double* const* gas_mass);
+/* Forgets a finished simulation and its host copy of the final state. */
+int fc_server_release(fc_server* server, long long id);
+int fc_server_get_stats(fc_server* server, fc_server_stats* stats);
+/* Latency of every completed time step in completion order; count receives the total. */
+int fc_server_step_latencies(fc_server* server, double* ms, size_t capacity, size_t* count);
 
 #ifdef __cplusplus
 }

@@ -15,6 +15,8 @@
 #include <stdlib.h>
 #include <string.h>
 
+#define OR_MAX_LEVELS 16
+
 /* ------------------------------------------------------------------------------------------ */
 /* Materials and coefficients                                                                  */
 /* ------------------------------------------------------------------------------------------ */
@@ -1114,4 +1116,502 @@ void or_advect(int W, int H, double s, const double* u, const double* v, int fie
             for (int k = 0; k < fields; ++k)
                 out[k][(size_t)j * W + i] = or_sample_scalar(in[k], W, H, bx - 0.5, by - 0.5);
         }
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* Implicit viscosity. The reference solves it only on the GPU (WGSL, FP32); this restates     */
+/* its algorithm in FP64:                                                                      */
+/*   operator, diagonal, smoother, transfers  UniformWebGPU/ViscosityKernels.h:8-400           */
+/*   levels and V-cycle                       UniformWebGPU/ViscositySolverGPU.cpp:61-167      */
+/*   CG with the true-residual check          UniformWebGPU/ViscositySolverGPU.cpp:170-294     */
+/*   cell viscosity blend                     UniformWebGPU/FluidGridGPU.cpp:172-217, 987-1037 */
+/* Fields live on the (w+1) x (h+1) node lattice: node p carries u face p (x component) and   */
+/* v face p (y component). Reads outside a field clamp to its edge, as the reference's field   */
+/* accessor does.                                                                              */
+/* ------------------------------------------------------------------------------------------ */
+
+typedef struct
+{
+    int w, h;
+    double dx;
+    double* material; /* 2 per cell: density, viscosity */
+    double* coeff;    /* 4 per node: cell mu, vertex mu, u-face mass, v-face mass */
+    double *x, *next, *rhs, *res;
+} or_vlevel;
+
+struct or_visc
+{
+    int w, h, levels;
+    or_vlevel lev[OR_MAX_LEVELS];
+    double *solution, *rhs, *residual, *direction, *product, *truth;
+    double dt;
+};
+
+static int vclampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+static const double* vmat(const or_vlevel* L, int x, int y)
+{
+    return L->material + 2 * ((size_t)vclampi(y, 0, L->h - 1) * L->w + vclampi(x, 0, L->w - 1));
+}
+
+static const double* vco(const or_vlevel* L, int x, int y)
+{
+    return L->coeff + 4 * ((size_t)vclampi(y, 0, L->h) * (L->w + 1) + vclampi(x, 0, L->w));
+}
+
+static const double* vsrc(const or_vlevel* L, const double* f, int x, int y)
+{
+    return f + 2 * ((size_t)vclampi(y, 0, L->h) * (L->w + 1) + vclampi(x, 0, L->w));
+}
+
+static int valid_u(const or_vlevel* L, int x, int y) { return x > 0 && x < L->w && y < L->h; }
+static int valid_v(const or_vlevel* L, int x, int y) { return y > 0 && y < L->h && x < L->w; }
+
+or_visc* or_visc_create(int width, int height)
+{
+    or_visc* s = (or_visc*)calloc(1, sizeof(or_visc));
+    s->w = width;
+    s->h = height;
+    int w = width, h = height;
+    for (;;)
+    {
+        or_vlevel* L = &s->lev[s->levels++];
+        const size_t nodes = (size_t)(w + 1) * (h + 1);
+        L->w = w;
+        L->h = h;
+        L->material = (double*)calloc(2 * (size_t)w * h, sizeof(double));
+        L->coeff = (double*)calloc(4 * nodes, sizeof(double));
+        L->x = (double*)calloc(2 * nodes, sizeof(double));
+        L->next = (double*)calloc(2 * nodes, sizeof(double));
+        L->rhs = (double*)calloc(2 * nodes, sizeof(double));
+        L->res = (double*)calloc(2 * nodes, sizeof(double));
+        if (w * h <= 64 || s->levels == OR_MAX_LEVELS)
+            break;
+        w = (w + 1) / 2;
+        h = (h + 1) / 2;
+    }
+    const size_t nodes = (size_t)(width + 1) * (height + 1);
+    double** v[] = {&s->solution, &s->rhs, &s->residual, &s->direction, &s->product, &s->truth};
+    for (int k = 0; k < 6; ++k)
+        *v[k] = (double*)calloc(2 * nodes, sizeof(double));
+    return s;
+}
+
+void or_visc_destroy(or_visc* s)
+{
+    if (!s)
+        return;
+    for (int l = 0; l < s->levels; ++l)
+    {
+        or_vlevel* L = &s->lev[l];
+        free(L->material);
+        free(L->coeff);
+        free(L->x);
+        free(L->next);
+        free(L->rhs);
+        free(L->res);
+    }
+    double* v[] = {s->solution, s->rhs, s->residual, s->direction, s->product, s->truth};
+    for (int k = 0; k < 6; ++k)
+        free(v[k]);
+    free(s);
+}
+
+int or_visc_levels(const or_visc* s) { return s->levels; }
+
+/* Coefficients of one level (ViscosityKernels.h "viscosity coefficients"). */
+static void visc_coefficients(or_vlevel* L)
+{
+    for (int y = 0; y <= L->h; ++y)
+        for (int x = 0; x <= L->w; ++x)
+        {
+            const double* m = vmat(L, x, y);
+            double mu = 0.0;
+            if (x > 0 && y > 0 && x < L->w && y < L->h)
+                mu = 0.25 * (m[1] + vmat(L, x - 1, y)[1] + vmat(L, x, y - 1)[1] + vmat(L, x - 1, y - 1)[1]);
+            double* c = L->coeff + 4 * ((size_t)y * (L->w + 1) + x);
+            c[0] = m[1];
+            c[1] = mu;
+            c[2] = 0.5 * L->dx * L->dx * (m[0] + vmat(L, x - 1, y)[0]);
+            c[3] = 0.5 * L->dx * L->dx * (m[0] + vmat(L, x, y - 1)[0]);
+        }
+}
+
+/* 2x2 mean of the existing fine cells (ViscosityKernels.h "viscosity coarse material"). */
+static void visc_coarsen(const or_vlevel* F, or_vlevel* C)
+{
+    for (int y = 0; y < C->h; ++y)
+        for (int x = 0; x < C->w; ++x)
+        {
+            double a = 0.0, b = 0.0, n = 0.0;
+            for (int j = 0; j < 2; ++j)
+                for (int i = 0; i < 2; ++i)
+                {
+                    const int qx = 2 * x + i, qy = 2 * y + j;
+                    if (qx < F->w && qy < F->h)
+                    {
+                        a += F->material[2 * ((size_t)qy * F->w + qx)];
+                        b += F->material[2 * ((size_t)qy * F->w + qx) + 1];
+                        n += 1.0;
+                    }
+                }
+            C->material[2 * ((size_t)y * C->w + x)] = a / n;
+            C->material[2 * ((size_t)y * C->w + x) + 1] = b / n;
+        }
+}
+
+static double shear_at(const or_vlevel* L, const double* f, int x, int y)
+{
+    return vco(L, x, y)[1] * ((vsrc(L, f, x, y)[0] - vsrc(L, f, x, y - 1)[0]) + (vsrc(L, f, x, y)[1] - vsrc(L, f, x - 1, y)[1]));
+}
+
+/* (A f)(p) = mass f(p) + dt * stress(f)(p) on valid faces, zero elsewhere
+ * (ViscosityKernels.h "stressProduct" and "product"). */
+static void visc_product(const or_vlevel* L, double dt, const double* f, int x, int y, double out[2])
+{
+    const double* c = vsrc(L, f, x, y);
+    const double* a = vco(L, x, y);
+    const double t = shear_at(L, f, x, y);
+    const double nx = 2.0 * (vco(L, x - 1, y)[0] * (c[0] - vsrc(L, f, x - 1, y)[0]) + a[0] * (c[0] - vsrc(L, f, x + 1, y)[0]));
+    const double ny = 2.0 * (vco(L, x, y - 1)[0] * (c[1] - vsrc(L, f, x, y - 1)[1]) + a[0] * (c[1] - vsrc(L, f, x, y + 1)[1]));
+    const double sx = nx + (t - shear_at(L, f, x, y + 1));
+    const double sy = ny + (t - shear_at(L, f, x + 1, y));
+    out[0] = valid_u(L, x, y) ? a[2] * c[0] + dt * sx : 0.0;
+    out[1] = valid_v(L, x, y) ? a[3] * c[1] + dt * sy : 0.0;
+}
+
+static void visc_diagonal(const or_vlevel* L, double dt, int x, int y, double d[2])
+{
+    const double* c = vco(L, x, y);
+    d[0] = c[2] + dt * (2.0 * (c[0] + vco(L, x - 1, y)[0]) + c[1] + vco(L, x, y + 1)[1]);
+    d[1] = c[3] + dt * (2.0 * (c[0] + vco(L, x, y - 1)[0]) + c[1] + vco(L, x + 1, y)[1]);
+}
+
+void or_visc_apply(or_visc* s, int level, double dt, const double* f, double* out)
+{
+    const or_vlevel* L = &s->lev[level];
+    for (int y = 0; y <= L->h; ++y)
+        for (int x = 0; x <= L->w; ++x)
+            visc_product(L, dt, f, x, y, out + 2 * ((size_t)y * (L->w + 1) + x));
+}
+
+/* Residual b - A f on valid faces. */
+static void visc_residual(const or_vlevel* L, double dt, const double* f, const double* b, double* out)
+{
+    for (int y = 0; y <= L->h; ++y)
+        for (int x = 0; x <= L->w; ++x)
+        {
+            const size_t i = 2 * ((size_t)y * (L->w + 1) + x);
+            double a[2];
+            visc_product(L, dt, f, x, y, a);
+            out[i] = valid_u(L, x, y) ? b[i] - a[0] : 0.0;
+            out[i + 1] = valid_v(L, x, y) ? b[i + 1] - a[1] : 0.0;
+        }
+}
+
+/* Damped Jacobi x <- x + (b - A x) / (2 D), or b / (2 D) from zero. */
+static void visc_smooth(or_vlevel* L, double dt, const double* b, int zero)
+{
+    for (int y = 0; y <= L->h; ++y)
+        for (int x = 0; x <= L->w; ++x)
+        {
+            const size_t i = 2 * ((size_t)y * (L->w + 1) + x);
+            double d[2], a[2] = {0.0, 0.0}, v[2];
+            visc_diagonal(L, dt, x, y, d);
+            if (zero)
+            {
+                v[0] = 0.5 * b[i] / d[0];
+                v[1] = 0.5 * b[i + 1] / d[1];
+            }
+            else
+            {
+                visc_product(L, dt, L->x, x, y, a);
+                v[0] = L->x[i] + 0.5 * (b[i] - a[0]) / d[0];
+                v[1] = L->x[i + 1] + 0.5 * (b[i + 1] - a[1]) / d[1];
+            }
+            L->next[i] = valid_u(L, x, y) ? v[0] : 0.0;
+            L->next[i + 1] = valid_v(L, x, y) ? v[1] : 0.0;
+        }
+    double* t = L->x;
+    L->x = L->next;
+    L->next = t;
+}
+
+/* Bilinear transfer between levels on face locations (ViscosityKernels.h transfer). */
+static double voffset_x(int component) { return component == 1 ? 0.5 : 0.0; }
+static double voffset_y(int component) { return component == 1 ? 0.0 : 0.5; }
+
+static void coarse_point(int bx, int by, int component, int sw, int sh, int* cx, int* cy)
+{
+    *cx = vclampi(bx, 0, sw - (component == 1 ? 1 : 0));
+    *cy = vclampi(by, 0, sh - (component == 1 ? 0 : 1));
+}
+
+static double transfer_weight(int fx, int fy, int px, int py, int component, int sw, int sh)
+{
+    const double lx = (fx + voffset_x(component)) * 0.5 - voffset_x(component);
+    const double ly = (fy + voffset_y(component)) * 0.5 - voffset_y(component);
+    const int bx = (int)floor(lx), by = (int)floor(ly);
+    const double tx = lx - bx, ty = ly - by;
+    double result = 0.0;
+    for (int y = 0; y < 2; ++y)
+        for (int x = 0; x < 2; ++x)
+        {
+            int cx, cy;
+            coarse_point(bx + x, by + y, component, sw, sh, &cx, &cy);
+            if (cx == px && cy == py)
+                result += (x == 1 ? tx : 1.0 - tx) * (y == 1 ? ty : 1.0 - ty);
+        }
+    return result;
+}
+
+static void visc_restrict(const or_vlevel* F, or_vlevel* C)
+{
+    for (int py = 0; py <= C->h; ++py)
+        for (int px = 0; px <= C->w; ++px)
+        {
+            double value[2] = {0.0, 0.0};
+            for (int component = 0; component < 2; ++component)
+            {
+                if ((component == 0 && (px == 0 || px == C->w || py == C->h)) ||
+                    (component == 1 && (py == 0 || py == C->h || px == C->w)))
+                    continue;
+                const int ex = component == 1 ? 2 : 1, ey = component == 1 ? 1 : 2;
+                for (int y = -1; y <= ey; ++y)
+                    for (int x = -1; x <= ex; ++x)
+                    {
+                        const int qx = 2 * px + x, qy = 2 * py + y;
+                        if (qx < 0 || qy < 0 || qx > F->w || qy > F->h)
+                            continue;
+                        value[component] += transfer_weight(qx, qy, px, py, component, C->w, C->h) *
+                                            F->res[2 * ((size_t)qy * (F->w + 1) + qx) + component];
+                    }
+            }
+            C->rhs[2 * ((size_t)py * (C->w + 1) + px)] = value[0];
+            C->rhs[2 * ((size_t)py * (C->w + 1) + px) + 1] = value[1];
+        }
+}
+
+static void visc_prolong(or_vlevel* F, const or_vlevel* C)
+{
+    for (int py = 0; py <= F->h; ++py)
+        for (int px = 0; px <= F->w; ++px)
+        {
+            const size_t i = 2 * ((size_t)py * (F->w + 1) + px);
+            double value[2] = {F->x[i], F->x[i + 1]};
+            for (int component = 0; component < 2; ++component)
+            {
+                const double lx = (px + voffset_x(component)) * 0.5 - voffset_x(component);
+                const double ly = (py + voffset_y(component)) * 0.5 - voffset_y(component);
+                const int bx = (int)floor(lx), by = (int)floor(ly);
+                const double tx = lx - bx, ty = ly - by;
+                for (int y = 0; y < 2; ++y)
+                    for (int x = 0; x < 2; ++x)
+                    {
+                        int cx, cy;
+                        coarse_point(bx + x, by + y, component, C->w, C->h, &cx, &cy);
+                        value[component] += (x == 1 ? tx : 1.0 - tx) * (y == 1 ? ty : 1.0 - ty) *
+                                            C->x[2 * ((size_t)cy * (C->w + 1) + cx) + component];
+                    }
+            }
+            F->next[i] = valid_u(F, px, py) ? value[0] : 0.0;
+            F->next[i + 1] = valid_v(F, px, py) ? value[1] : 0.0;
+        }
+    double* t = F->x;
+    F->x = F->next;
+    F->next = t;
+}
+
+/* V-cycle (ViscositySolverGPU.cpp:137-167): two Jacobi sweeps down (the first from zero),
+ * residual, restriction, recursion, prolongation, two sweeps up; the coarsest level takes 16
+ * Jacobi sweeps from zero. */
+static void visc_cycle(or_visc* s, int level, const double* b)
+{
+    or_vlevel* L = &s->lev[level];
+    const double dt = s->dt;
+    if (level + 1 == s->levels)
+    {
+        memset(L->x, 0, 2 * (size_t)(L->w + 1) * (L->h + 1) * sizeof(double));
+        for (int sweep = 0; sweep < 16; ++sweep)
+            visc_smooth(L, dt, b, 0);
+        return;
+    }
+    visc_smooth(L, dt, b, 1);
+    visc_smooth(L, dt, b, 0);
+    visc_residual(L, dt, L->x, b, L->res);
+    or_vlevel* C = &s->lev[level + 1];
+    visc_restrict(L, C);
+    visc_cycle(s, level + 1, C->rhs);
+    visc_prolong(L, C);
+    visc_smooth(L, dt, b, 0);
+    visc_smooth(L, dt, b, 0);
+}
+
+void or_visc_precondition(or_visc* s, const double* r, double* z)
+{
+    visc_cycle(s, 0, r);
+    memcpy(z, s->lev[0].x, 2 * (size_t)(s->w + 1) * (s->h + 1) * sizeof(double));
+}
+
+/* Level materials and coefficients from cell density and viscosity (2 per cell). */
+void or_visc_setup(or_visc* s, const double* material, double dt, double cell_size)
+{
+    s->dt = dt;
+    memcpy(s->lev[0].material, material, 2 * (size_t)s->w * s->h * sizeof(double));
+    for (int l = 0; l < s->levels; ++l)
+    {
+        s->lev[l].dx = ldexp(cell_size, l);
+        if (l > 0)
+            visc_coarsen(&s->lev[l - 1], &s->lev[l]);
+        visc_coefficients(&s->lev[l]);
+    }
+}
+
+/* Sum over nodes of a.a / mass and the other statistics of ViscosityKernels.h "first_reduce". */
+static double visc_mass_norm(const or_visc* s, const double* a)
+{
+    const or_vlevel* L = &s->lev[0];
+    double sum = 0.0;
+    for (size_t n = 0; n < (size_t)(s->w + 1) * (s->h + 1); ++n)
+        sum += a[2 * n] / L->coeff[4 * n + 2] * a[2 * n] + a[2 * n + 1] / L->coeff[4 * n + 3] * a[2 * n + 1];
+    return sum;
+}
+
+static double visc_dot(const or_visc* s, const double* a, const double* b)
+{
+    double sum = 0.0;
+    for (size_t n = 0; n < 2 * (size_t)(s->w + 1) * (s->h + 1); ++n)
+        sum += a[n] * b[n];
+    return sum;
+}
+
+/* Backward-Euler viscosity solve (ViscositySolverGPU.cpp:170-294). u, v: face velocities (in,
+ * out); material: density and viscosity per cell. Returns the iteration count (a multiple of
+ * the 4-iteration check interval), -1 on breakdown or non-finite state, -2 when max_iterations
+ * (>= 0) is reached without convergence. relative_residual receives sqrt(|r|^2_M / |x0|^2_M). */
+int or_visc_solve(or_visc* s, double* u, double* v, const double* material, double dt, double cell_size,
+    double tolerance, int max_iterations, double* relative_residual)
+{
+    const int w = s->w, h = s->h;
+    const size_t nodes = (size_t)(w + 1) * (h + 1);
+    if (relative_residual)
+        *relative_residual = 0.0;
+    if (dt <= 0.0)
+        return 0;
+    or_visc_setup(s, material, dt, cell_size);
+    const or_vlevel* L = &s->lev[0];
+    /* Pack: solution = velocities on valid faces, rhs = mass * solution. */
+    for (int y = 0; y <= h; ++y)
+        for (int x = 0; x <= w; ++x)
+        {
+            const size_t n = (size_t)y * (w + 1) + x;
+            s->solution[2 * n] = valid_u(L, x, y) ? u[(size_t)y * (w + 1) + x] : 0.0;
+            s->solution[2 * n + 1] = valid_v(L, x, y) ? v[(size_t)y * w + x] : 0.0;
+            s->rhs[2 * n] = L->coeff[4 * n + 2] * s->solution[2 * n];
+            s->rhs[2 * n + 1] = L->coeff[4 * n + 3] * s->solution[2 * n + 1];
+        }
+    visc_residual(L, dt, s->solution, s->rhs, s->residual);
+    double energy = 0.0, total_mass = 0.0;
+    for (size_t n = 0; n < nodes; ++n)
+    {
+        energy += L->coeff[4 * n + 2] * s->solution[2 * n] * s->solution[2 * n] +
+                  L->coeff[4 * n + 3] * s->solution[2 * n + 1] * s->solution[2 * n + 1];
+        total_mass += L->coeff[4 * n + 2] + L->coeff[4 * n + 3];
+    }
+    double rnorm = visc_mass_norm(s, s->residual);
+    if (!isfinite(rnorm) || !isfinite(energy) || !isfinite(total_mass))
+        return -1;
+    const double target = tolerance * tolerance * energy + 1e-12 * total_mass;
+    if (relative_residual)
+        *relative_residual = sqrt(rnorm / fmax(energy, 1e-30));
+    if (rnorm <= target)
+        return 0;
+
+    double rz = 0.0, alpha = 0.0, beta = 0.0;
+    int count = 0, iterations = 0, stopped = 0;
+    double* z = s->lev[0].x;
+    for (;;)
+    {
+        if (max_iterations >= 0 && iterations >= max_iterations)
+            return -2;
+        const int batch = max_iterations < 0 ? 4 : (max_iterations - iterations < 4 ? max_iterations - iterations : 4);
+        for (int i = 0; i < batch; ++i)
+        {
+            if (stopped)
+                break;
+            visc_cycle(s, 0, s->residual);
+            z = s->lev[0].x;
+            const double rz_new = visc_dot(s, s->residual, z);
+            rnorm = visc_mass_norm(s, s->residual);
+            if (rnorm <= target)
+            {
+                stopped = 1;
+                break;
+            }
+            if (!(rz_new > 0.0) || !isfinite(rz_new))
+                return -1;
+            beta = count > 0 ? rz_new / rz : 0.0;
+            rz = rz_new;
+            for (size_t n = 0; n < 2 * nodes; ++n)
+                s->direction[n] = z[n] + (count > 0 ? beta * s->direction[n] : 0.0);
+            or_visc_apply(s, 0, dt, s->direction, s->product);
+            const double dq = visc_dot(s, s->direction, s->product);
+            if (!(dq > 0.0) || !isfinite(dq))
+                return -1;
+            alpha = rz / dq;
+            ++count;
+            for (size_t n = 0; n < 2 * nodes; ++n)
+            {
+                s->solution[n] += alpha * s->direction[n];
+                s->residual[n] -= alpha * s->product[n];
+            }
+        }
+        iterations += batch;
+        visc_residual(L, dt, s->solution, s->rhs, s->truth);
+        const double truth = visc_mass_norm(s, s->truth);
+        if (relative_residual)
+            *relative_residual = sqrt(truth / fmax(energy, 1e-30));
+        if (!isfinite(truth))
+            return -1;
+        if (truth <= target)
+            break;
+        if (stopped)
+        {
+            /* The recurrence claimed convergence: restart from the true residual. */
+            memcpy(s->residual, s->truth, 2 * nodes * sizeof(double));
+            rz = alpha = beta = 0.0;
+            count = 0;
+            stopped = 0;
+        }
+    }
+    /* Unpack (ViscosityKernels.h "unpack"): every face of the solution. */
+    for (int y = 0; y < h; ++y)
+        for (int x = 0; x <= w; ++x)
+            u[(size_t)y * (w + 1) + x] = s->solution[2 * ((size_t)y * (w + 1) + x)];
+    for (int y = 0; y <= h; ++y)
+        for (int x = 0; x < w; ++x)
+            v[(size_t)y * w + x] = s->solution[2 * ((size_t)y * (w + 1) + x) + 1];
+    return iterations;
+}
+
+/* Cell density and volume-weighted dynamic viscosity (FluidGridGPU.cpp:172-217, 987-1037):
+ * rho = sum m_k / dx^2, mu = sum (m_k mu_k / rho_k) / sum (m_k / rho_k); a cell without mass
+ * gets mu = 0. material receives 2 values per cell. */
+void or_visc_material(int cells, int components, const double* const* masses, const double* densities,
+    const double* viscosities, double cell_size, double* material)
+{
+    const double inv_area = 1.0 / (cell_size * cell_size);
+    for (int i = 0; i < cells; ++i)
+    {
+        double total = 0.0, weighted = 0.0, volume = 0.0;
+        for (int k = 0; k < components; ++k)
+        {
+            const double m = masses[k][i];
+            total += m;
+            weighted += m * (viscosities[k] / densities[k]);
+            volume += m * (1.0 / densities[k]);
+        }
+        material[2 * i] = total * inv_area;
+        material[2 * i + 1] = volume > 0.0 ? weighted / volume : 0.0;
+    }
 }

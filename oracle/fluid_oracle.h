@@ -82,6 +82,21 @@ void or_sample_velocity(int width, int height, double cell_size, double origin_x
 void or_advect(int width, int height, double s, const double* u, const double* v, int fields,
     const double* const* in, double* const* out, double* u_out, double* v_out);
 
+/* Implicit viscosity restated in FP64 (UniformWebGPU/ViscosityKernels.h,
+ * UniformWebGPU/ViscositySolverGPU.cpp). Node fields hold 2 values per node of the
+ * (w+1) x (h+1) lattice: u face p and v face p. */
+typedef struct or_visc or_visc;
+or_visc* or_visc_create(int width, int height);
+void or_visc_destroy(or_visc* solver);
+int or_visc_levels(const or_visc* solver);
+void or_visc_setup(or_visc* solver, const double* material, double dt, double cell_size);
+void or_visc_apply(or_visc* solver, int level, double dt, const double* field, double* out);
+void or_visc_precondition(or_visc* solver, const double* residual, double* correction);
+int or_visc_solve(or_visc* solver, double* u, double* v, const double* material, double dt, double cell_size,
+    double tolerance, int max_iterations, double* relative_residual);
+void or_visc_material(int cells, int components, const double* const* masses, const double* densities,
+    const double* viscosities, double cell_size, double* material);
+
 #ifdef __cplusplus
 }
 #endif

@@ -105,6 +105,17 @@ def lib():
         L.or_sample_scalar.argtypes = [_dp, C.c_int, C.c_int, C.c_double, C.c_double]
         L.or_sample_velocity.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, _dp, _dp, C.c_int,
                                          _dp, _dp]
+        L.or_visc_create.restype = C.c_void_p
+        L.or_visc_create.argtypes = [C.c_int, C.c_int]
+        L.or_visc_destroy.argtypes = [C.c_void_p]
+        L.or_visc_levels.restype = C.c_int
+        L.or_visc_levels.argtypes = [C.c_void_p]
+        L.or_visc_setup.argtypes = [C.c_void_p, _dp, C.c_double, C.c_double]
+        L.or_visc_apply.argtypes = [C.c_void_p, C.c_int, C.c_double, _dp, _dp]
+        L.or_visc_precondition.argtypes = [C.c_void_p, _dp, _dp]
+        L.or_visc_solve.restype = C.c_int
+        L.or_visc_solve.argtypes = [C.c_void_p, _dp, _dp, _dp, C.c_double, C.c_double, C.c_double, C.c_int, _dp]
+        L.or_visc_material.argtypes = [C.c_int, C.c_int, C.POINTER(_dp), _dp, _dp, C.c_double, _dp]
         L.or_advect.argtypes = [C.c_int, C.c_int, C.c_double, _dp, _dp, C.c_int, C.POINTER(_dp), C.POINTER(_dp),
                                 _dp, _dp]
         _lib = L
@@ -383,6 +394,61 @@ def advect(u, v, fields, dt, cell_size, storage=np.float64):
     lib().or_advect(w, h, float(dt) / float(cell_size), _ptr(u), _ptr(v), len(ins), in_ptrs, out_ptrs, _ptr(u_out),
                     _ptr(v_out))
     return u_out.astype(storage).astype(np.float64), v_out.astype(storage).astype(np.float64), outs
+
+
+class Viscosity:
+    """The FP64 restatement of the reference's implicit viscosity solve
+    (UniformWebGPU/ViscositySolverGPU.cpp). Node fields are (h+1, w+1, 2) arrays: [..., 0] is u
+    face (x, y), [..., 1] is v face (x, y)."""
+
+    def __init__(self, width, height):
+        self.w, self.h = width, height
+        self.handle = lib().or_visc_create(width, height)
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            lib().or_visc_destroy(self.handle)
+            self.handle = None
+
+    @property
+    def levels(self):
+        return lib().or_visc_levels(self.handle)
+
+    def setup(self, material, dt, cell_size):
+        m = _f64(material)
+        lib().or_visc_setup(self.handle, _ptr(m), float(dt), float(cell_size))
+
+    def apply(self, field, dt, level=0):
+        f = _f64(field)
+        out = np.zeros_like(f)
+        lib().or_visc_apply(self.handle, level, float(dt), _ptr(f), _ptr(out))
+        return out
+
+    def precondition(self, residual):
+        r = _f64(residual)
+        z = np.zeros_like(r)
+        lib().or_visc_precondition(self.handle, _ptr(r), _ptr(z))
+        return z
+
+    def solve(self, u, v, material, dt, cell_size, tolerance=1e-4, max_iterations=-1):
+        """Returns (iterations, u, v, relative_residual); iterations -1 = breakdown or
+        non-finite state, -2 = the iteration cap was reached."""
+        u, v, m = _f64(u).copy(), _f64(v).copy(), _f64(material)
+        rel = C.c_double()
+        it = lib().or_visc_solve(self.handle, _ptr(u), _ptr(v), _ptr(m), float(dt), float(cell_size),
+                                 float(tolerance), int(max_iterations), C.byref(rel))
+        return it, u, v, rel.value
+
+
+def viscosity_material(masses, densities, viscosities, cell_size):
+    """Cell density and volume-weighted viscosity (FluidGridGPU.cpp:172-217), (h, w, 2)."""
+    ms = [_f64(m) for m in masses]
+    h, w = ms[0].shape
+    out = np.zeros((h, w, 2))
+    table = (_dp * len(ms))(*[_ptr(m) for m in ms])
+    d, mu = _f64(np.asarray(densities, dtype=float)), _f64(np.asarray(viscosities, dtype=float))
+    lib().or_visc_material(w * h, len(ms), table, _ptr(d), _ptr(mu), float(cell_size), _ptr(out))
+    return out
 
 
 def reference_mg_apply(inv_u, inv_v, residual, residual_mean=0.0):

@@ -9,7 +9,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIBRARY = os.path.join(HERE, "libfluidcuda.so")
 SOURCES = ["fc_engine.cu", "fc_server.cpp"]
-HEADERS = ["fc_device.cuh", "fc_pcg.cuh", "fc_multigrid.cuh", "fc_smooth.cuh", "fc_advect.cuh", "fc_tension.cuh", "fc_json.h", "fc_errors.h"]
+HEADERS = ["fc_device.cuh", "fc_pcg.cuh", "fc_multigrid.cuh", "fc_smooth.cuh", "fc_advect.cuh", "fc_tension.cuh", "fc_viscosity.cuh", "fc_json.h", "fc_errors.h"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -13,6 +13,7 @@
 #include "fc_json.h"
 #include "fc_advect.cuh"
 #include "fc_tension.cuh"
+#include "fc_viscosity.cuh"
 #include "fc_errors.h"
 
 #include "../../include/fluidcuda.h"
@@ -225,6 +226,8 @@ struct Grid
     int mass_capacity = 0;
     char* tension_arena = nullptr; // curvature sweeps, allocated on first use
     TensionArrays tension{};
+    char* visc_arena = nullptr;    // viscosity solver workspace, allocated on first use
+    size_t visc_bytes = 0;
 
     std::unique_ptr<Plan> plan; // single-grid plan, built lazily
 
@@ -657,7 +660,7 @@ struct Plan
 Grid::~Grid()
 {
     plan.reset();
-    for (void* ptr : {(void*)masses, (void*)mass_ptrs, (void*)tension_arena, (void*)arena})
+    for (void* ptr : {(void*)masses, (void*)mass_ptrs, (void*)tension_arena, (void*)visc_arena, (void*)arena})
         if (ptr)
             cudaFree(ptr);
     if (stream)
@@ -1362,6 +1365,257 @@ void surface_curvature(Grid& g, double* values, unsigned char* valid)
     check(cudaStreamSynchronize(p.stream), "curvature");
 }
 
+// ------------------------------------------------------------------------------------------
+// Implicit viscosity (fc_viscosity.cuh)
+// ------------------------------------------------------------------------------------------
+
+bool has_viscosity(const Grid& g)
+{
+    for (double mu : g.liquid_viscosity)
+        if (mu != 0.0)
+            return true;
+    for (double mu : g.gas_viscosity)
+        if (mu != 0.0)
+            return true;
+    return false;
+}
+
+// Level sizes of the viscosity hierarchy (ViscositySolverGPU.cpp:74-86): halve, rounding up,
+// until a level has at most 64 cells.
+std::vector<std::pair<int, int>> viscosity_levels(int w, int h)
+{
+    std::vector<std::pair<int, int>> out;
+    for (;;)
+    {
+        out.push_back({w, h});
+        if ((long long)w * h <= 64 || out.size() == size_t(kMaxLevels))
+            break;
+        w = (w + 1) / 2;
+        h = (h + 1) / 2;
+    }
+    return out;
+}
+
+struct ViscWork
+{
+    std::vector<ViscLevel> lev;
+    void *solution, *rhs, *residual, *direction, *product, *truth;
+    ViscState* state;
+    double4* partial;
+    unsigned int* counter;
+    double2* comp;
+};
+
+// Lays out (and with allocate, allocates) the viscosity workspace of a grid.
+size_t viscosity_layout(const Grid& g, ViscWork* work, char* base)
+{
+    const size_t e = g.elem;
+    const auto sizes = viscosity_levels(g.W, g.H);
+    size_t total = 0;
+    auto take = [&](size_t bytes) -> void*
+    {
+        void* p = base ? base + total : nullptr;
+        total += (bytes + 255) / 256 * 256;
+        return p;
+    };
+    const size_t nodes0 = size_t(g.W + 1) * (g.H + 1);
+    if (work)
+        work->lev.assign(sizes.size(), ViscLevel{});
+    for (size_t l = 0; l < sizes.size(); ++l)
+    {
+        const int w = sizes[l].first, h = sizes[l].second;
+        const size_t nodes = size_t(w + 1) * (h + 1);
+        ViscLevel v{};
+        v.w = w;
+        v.h = h;
+        v.dx = std::ldexp(g.dx, int(l));
+        v.material = take(size_t(w) * h * 2 * e);
+        v.coeff = take(nodes * 4 * e);
+        v.x = take(nodes * 2 * e);
+        v.next = take(nodes * 2 * e);
+        v.rhs = take(nodes * 2 * e);
+        v.res = take(nodes * 2 * e);
+        if (work)
+            work->lev[l] = v;
+    }
+    void* vecs[6];
+    for (void*& p : vecs)
+        p = take(nodes0 * 2 * e);
+    void* state = take(sizeof(ViscState));
+    const int blocks = ceil_div(int(nodes0), kViscThreads);
+    void* partial = take(size_t(blocks) * sizeof(double4));
+    void* counter = take(sizeof(unsigned int) * 4);
+    void* comp = take(size_t(std::max(g.components(), 1)) * sizeof(double2));
+    if (work)
+    {
+        work->solution = vecs[0];
+        work->rhs = vecs[1];
+        work->residual = vecs[2];
+        work->direction = vecs[3];
+        work->product = vecs[4];
+        work->truth = vecs[5];
+        work->state = static_cast<ViscState*>(state);
+        work->partial = static_cast<double4*>(partial);
+        work->counter = static_cast<unsigned int*>(counter);
+        work->comp = static_cast<double2*>(comp);
+    }
+    return total;
+}
+
+ViscWork viscosity_workspace(Grid& g, cudaStream_t s)
+{
+    const size_t bytes = viscosity_layout(g, nullptr, nullptr);
+    if (!g.visc_arena || g.visc_bytes < bytes)
+    {
+        if (g.visc_arena)
+            cudaFree(g.visc_arena);
+        g.visc_arena = nullptr;
+        g.visc_bytes = 0;
+        check(cudaMalloc(&g.visc_arena, bytes), "viscosity allocation");
+        g.visc_bytes = bytes;
+        check(cudaMemsetAsync(g.visc_arena, 0, bytes, s), "viscosity clear");
+    }
+    ViscWork w;
+    viscosity_layout(g, &w, g.visc_arena);
+    return w;
+}
+
+template <typename T> void viscosity_cycle(ViscWork& w, size_t l, void* b, double dt, const unsigned char* solid,
+    cudaStream_t s)
+{
+    ViscLevel& L = w.lev[l];
+    const unsigned char* mask = l == 0 ? solid : nullptr;
+    const int blocks = ceil_div((L.w + 1) * (L.h + 1), kViscThreads);
+    if (l + 1 == w.lev.size())
+    {
+        ViscLevel c = L;
+        c.rhs = b;
+        FC_LAUNCH(k_visc_coarse<T>, 1, kViscCoarseNodes, 0, s, c, dt, mask, w.state);
+        return;
+    }
+    auto smooth = [&](int zero)
+    {
+        FC_LAUNCH(k_visc_smooth<T>, blocks, kViscThreads, 0, s, L, dt, mask, b, zero, w.state);
+        std::swap(L.x, L.next);
+    };
+    smooth(1);
+    smooth(0);
+    FC_LAUNCH((k_visc_residual<T, kResidualPlain>), blocks, kViscThreads, 0, s, L, dt, mask, L.x, b, L.res, w.state,
+        w.partial, w.counter, 0.0);
+    ViscLevel& C = w.lev[l + 1];
+    FC_LAUNCH(k_visc_restrict<T>, ceil_div((C.w + 1) * (C.h + 1), kViscThreads), kViscThreads, 0, s, L, C, w.state);
+    viscosity_cycle<T>(w, l + 1, C.rhs, dt, solid, s);
+    FC_LAUNCH(k_visc_prolong<T>, blocks, kViscThreads, 0, s, L, C, mask, w.state);
+    std::swap(L.x, L.next);
+    smooth(0);
+    smooth(0);
+}
+
+struct ViscResult
+{
+    int iterations;
+    double relative_residual;
+};
+
+// Backward-Euler viscosity solve of the grid's face velocities (ViscositySolverGPU.cpp:170-294):
+// CG preconditioned by the V-cycle, the true residual checked every 4 iterations, the
+// velocities written only on success. max_iterations < 0 means no cap.
+template <typename T> ViscResult viscosity_solve(Grid& g, double dt, double tolerance, int max_iterations)
+{
+    Plan& p = single_plan(g);
+    cudaStream_t s = p.stream;
+    ViscWork w = viscosity_workspace(g, s);
+    // Per-component (mu / rho, 1 / rho), liquid components first, as the masses are stored.
+    std::vector<double2> comp;
+    for (size_t k = 0; k < g.liquid_density.size(); ++k)
+        comp.push_back(make_double2(g.liquid_viscosity[k] / g.liquid_density[k], 1.0 / g.liquid_density[k]));
+    for (size_t k = 0; k < g.gas_density.size(); ++k)
+        comp.push_back(make_double2(g.gas_viscosity[k] / g.gas_density[k], 1.0 / g.gas_density[k]));
+    if (!comp.empty())
+        check(cudaMemcpyAsync(w.comp, comp.data(), comp.size() * sizeof(double2), cudaMemcpyHostToDevice, s), "viscosity");
+    const int cells = g.W * g.H;
+    FC_LAUNCH(k_visc_material<T>, ceil_div(cells, kViscThreads), kViscThreads, 0, s, g.desc.masses, g.components(),
+        w.comp, cells, 1.0 / (g.dx * g.dx), const_cast<void*>(w.lev[0].material));
+    for (size_t l = 0; l < w.lev.size(); ++l)
+    {
+        const ViscLevel& L = w.lev[l];
+        if (l > 0)
+        {
+            const ViscLevel& F = w.lev[l - 1];
+            FC_LAUNCH(k_visc_coarsen<T>, ceil_div(L.w * L.h, kViscThreads), kViscThreads, 0, s, F.material, F.w, F.h,
+                const_cast<void*>(L.material), L.w, L.h);
+        }
+        FC_LAUNCH(k_visc_coefficients<T>, ceil_div((L.w + 1) * (L.h + 1), kViscThreads), kViscThreads, 0, s,
+            L.material, L.w, L.h, L.dx, const_cast<void*>(L.coeff));
+    }
+    const unsigned char* solid = g.has_solid ? g.solid : nullptr;
+    const int nodes = (g.W + 1) * (g.H + 1);
+    const int blocks = ceil_div(nodes, kViscThreads);
+    ViscLevel& L0 = w.lev[0];
+    FC_LAUNCH(k_visc_pack<T>, blocks, kViscThreads, 0, s, g.W, g.H, g.desc.u, g.desc.v, L0.coeff, solid, w.solution, w.rhs);
+    FC_LAUNCH((k_visc_residual<T, kResidualInitial>), blocks, kViscThreads, 0, s, L0, dt, solid, w.solution, w.rhs,
+        w.residual, w.state, w.partial, w.counter, tolerance);
+    ViscState h{};
+    auto read_state = [&]
+    {
+        check(cudaMemcpyAsync(&h, w.state, sizeof(ViscState), cudaMemcpyDeviceToHost, s), "viscosity state");
+        check(cudaStreamSynchronize(s), "viscosity");
+    };
+    read_state();
+    if (h.breakdown)
+        fail(FC_ERR_NONFINITE, "Viscosity received nonfinite velocity/material state");
+    ViscResult result{0, std::sqrt(h.rnorm / std::max(h.energy, 1e-30))};
+    if (h.rnorm <= h.target)
+        return result;
+    for (;;)
+    {
+        if (max_iterations >= 0 && result.iterations >= max_iterations)
+            fail(FC_ERR_TIMEOUT, "Implicit viscosity did not converge; relative residual %g", result.relative_residual);
+        const int batch = max_iterations < 0 ? 4 : std::min(4, max_iterations - result.iterations);
+        for (int i = 0; i < batch; ++i)
+        {
+            viscosity_cycle<T>(w, 0, w.residual, dt, solid, s);
+            FC_LAUNCH(k_visc_dot_rz<T>, blocks, kViscThreads, 0, s, nodes, L0.coeff, w.residual, L0.x, w.state,
+                w.partial, w.counter);
+            FC_LAUNCH(k_visc_direction<T>, blocks, kViscThreads, 0, s, nodes, L0.x, w.direction, w.state);
+            FC_LAUNCH((k_visc_apply<T, true>), blocks, kViscThreads, 0, s, L0, dt, solid, w.direction, w.product,
+                w.state, w.partial, w.counter);
+            FC_LAUNCH(k_visc_update<T>, blocks, kViscThreads, 0, s, nodes, w.solution, w.residual, w.direction,
+                w.product, w.state);
+        }
+        result.iterations += batch;
+        FC_LAUNCH((k_visc_residual<T, kResidualTruth>), blocks, kViscThreads, 0, s, L0, dt, solid, w.solution, w.rhs,
+            w.truth, w.state, w.partial, w.counter, tolerance);
+        read_state();
+        result.relative_residual = std::sqrt(h.truth / std::max(h.energy, 1e-30));
+        if (h.breakdown)
+            fail(FC_ERR_BREAKDOWN, "Implicit viscosity solver breakdown");
+        if (h.truth <= h.target)
+            break;
+        if (h.stopped)
+            FC_LAUNCH(k_visc_refresh<T>, blocks, kViscThreads, 0, s, nodes, w.truth, w.residual, w.state);
+    }
+    FC_LAUNCH(k_visc_unpack<T>, blocks, kViscThreads, 0, s, g.W, g.H, w.solution, g.desc.u, g.desc.v);
+    check(cudaStreamSynchronize(s), "viscosity");
+    return result;
+}
+
+// FluidGridGPU::applyViscosity (FluidGridGPU.cpp:987-1045): tolerance 1e-4 relative, no cap in
+// the reference; max_iterations bounds it here when >= 0.
+ViscResult apply_viscosity(Grid& g, double dt, double tolerance, int max_iterations)
+{
+    require_uploaded(g);
+    if (!(dt > 0.0) || !has_viscosity(g))
+        return {0, 0.0};
+    ViscResult r{};
+    dispatch(g.precision, [&](auto zero)
+    {
+        using T = decltype(zero);
+        r = viscosity_solve<T>(g, dt, tolerance, max_iterations);
+    });
+    return r;
+}
+
 // One preconditioner application to a given residual (PressureMultigrid::apply,
 // PressureMultigrid.cpp:410-434, or the diagonal at FluidGridCPU.cpp:1691-1698); the
 // correction is returned without its mean removed, as the reference's apply returns it.
@@ -1633,11 +1887,11 @@ void load_checkpoint(Grid& g, const char* metadata, const void* payload, size_t 
     mixture("liquid_mixture", ld, lv);
     mixture("gas_mixture", gd, gv);
     for (double mu : lv)
-        if (mu != 0.0)
-            fail(FC_ERR_UNSUPPORTED, "checkpoint needs viscosity, which this build does not support");
+        if (!std::isfinite(mu) || mu < 0.0)
+            fail(FC_ERR_INVALID_ARGUMENT, "Invalid saved material viscosity");
     for (double mu : gv)
-        if (mu != 0.0)
-            fail(FC_ERR_UNSUPPORTED, "checkpoint needs viscosity, which this build does not support");
+        if (!std::isfinite(mu) || mu < 0.0)
+            fail(FC_ERR_INVALID_ARGUMENT, "Invalid saved material viscosity");
     const int preconditioner = int(need("preconditioner", json::Value::Number).number);
     if (preconditioner != FC_PRECONDITIONER_DIAGONAL && preconditioner != FC_PRECONDITIONER_MULTIGRID)
         fail(FC_ERR_INVALID_ARGUMENT, "checkpoint preconditioner is unknown");
@@ -1912,6 +2166,7 @@ int fc_get_device_bytes(const fc_grid* grid, size_t* bytes)
         size_t total = g.arena_bytes + size_t(g.mass_capacity) * g.cells * sizeof(double);
         if (g.tension_arena)
             total += fc::tension_bytes(g.cells);
+        total += g.visc_bytes;
         total += fc::plan_bytes(g.W, g.H);
         *bytes = total;
     });
@@ -1996,12 +2251,13 @@ int fc_configure_materials(fc_grid* grid, int liquid_count, const double* liquid
         for (int i = 0; i < gas_count; ++i)
             if (!(gas_densities[i] > 0.0) || !std::isfinite(gas_densities[i]))
                 fail(FC_ERR_INVALID_ARGUMENT, "component densities must be positive and finite");
+        // FluidGridGPU.cpp:381-382.
         for (int i = 0; i < liquid_count && liquid_viscosities; ++i)
-            if (liquid_viscosities[i] != 0.0)
-                fail(FC_ERR_UNSUPPORTED, "viscosity is not available in this build");
+            if (!std::isfinite(liquid_viscosities[i]) || liquid_viscosities[i] < 0.0)
+                fail(FC_ERR_INVALID_ARGUMENT, "Material viscosity must be finite and nonnegative");
         for (int i = 0; i < gas_count && gas_viscosities; ++i)
-            if (gas_viscosities[i] != 0.0)
-                fail(FC_ERR_UNSUPPORTED, "viscosity is not available in this build");
+            if (!std::isfinite(gas_viscosities[i]) || gas_viscosities[i] < 0.0)
+                fail(FC_ERR_INVALID_ARGUMENT, "Material viscosity must be finite and nonnegative");
         take(g.liquid_density, liquid_count, liquid_densities);
         take(g.gas_density, gas_count, gas_densities);
         take(g.liquid_viscosity, liquid_count, liquid_viscosities);
@@ -2061,6 +2317,39 @@ int fc_capillary_step_limit(const fc_grid* grid, double* limit)
         if (!grid || !limit)
             fail(FC_ERR_INVALID_ARGUMENT, "null argument");
         *limit = fc::capillary_step_limit(grid->impl);
+    });
+}
+
+int fc_apply_viscosity(fc_grid* grid, double dt, double tolerance, int max_iterations, int* iterations,
+    double* relative_residual)
+{
+    return guarded([&]
+    {
+        if (!grid)
+            fail(FC_ERR_INVALID_ARGUMENT, "null grid");
+        if (!std::isfinite(dt) || !(tolerance >= 0.0))
+            fail(FC_ERR_INVALID_ARGUMENT, "invalid viscosity time step or tolerance");
+        const fc::ViscResult r = fc::apply_viscosity(grid->impl, dt, tolerance, max_iterations);
+        if (iterations)
+            *iterations = r.iterations;
+        if (relative_residual)
+            *relative_residual = r.relative_residual;
+    });
+}
+
+int fc_set_component_viscosity(fc_grid* grid, int phase, int component, double coefficient)
+{
+    return guarded([&]
+    {
+        if (!grid)
+            fail(FC_ERR_INVALID_ARGUMENT, "null grid");
+        if (!std::isfinite(coefficient) || coefficient < 0.0)
+            fail(FC_ERR_INVALID_ARGUMENT, "Material viscosity must be finite and nonnegative");
+        Grid& g = grid->impl;
+        std::vector<double>& mu = phase == 0 ? g.liquid_viscosity : g.gas_viscosity;
+        if ((phase != 0 && phase != 1) || component < 0 || size_t(component) >= mu.size())
+            fail(FC_ERR_INVALID_ARGUMENT, "no such material component");
+        mu[component] = coefficient;
     });
 }
 
@@ -2229,6 +2518,10 @@ int fc_apply_gravity(fc_grid* grid, double dt)
     });
 }
 
+// The reference's step runs the viscosity solve without an iteration cap; this bound only turns
+// a solve that cannot converge into an error instead of an endless loop.
+constexpr int kViscosityCap = 20000;
+
 int fc_step(fc_grid* grid, double dt, int max_iterations, double divergence_tolerance, fc_result* result,
     fc_timings* timings)
 {
@@ -2273,6 +2566,16 @@ int fc_step(fc_grid* grid, double dt, int max_iterations, double divergence_tole
             return status;
         if (timings)
             timings->transport_ms += elapsed();
+        // Implicit viscosity after transport (FluidGridGPU.cpp:1139-1146), 1e-4 relative.
+        if (fc::has_viscosity(grid->impl))
+        {
+            int viscous = 0;
+            if ((status = fc_apply_viscosity(grid, step, 1e-4, kViscosityCap, &viscous, nullptr)) != FC_OK)
+                return status;
+            total.viscosity_iterations += viscous;
+            if (timings)
+                timings->viscosity_ms += elapsed();
+        }
         if ((status = fc_apply_gravity(grid, step)) != FC_OK)
             return status;
         if (tension && (status = fc_apply_surface_tension(grid, step)) != FC_OK)
@@ -2287,7 +2590,9 @@ int fc_step(fc_grid* grid, double dt, int max_iterations, double divergence_tole
         const int restarts = total.restarts + one.restarts;
         const int kernels = total.kernels + one.kernels;
         const int steps = total.physical_steps + 1;
+        const int viscous = total.viscosity_iterations;
         total = one;
+        total.viscosity_iterations = viscous;
         total.iterations = iterations;
         total.restarts = restarts;
         total.kernels = kernels;

@@ -246,6 +246,17 @@ class FluidGrid:
         """Semi-Lagrangian transport of velocities, liquid fraction and component masses."""
         N.check(N.lib().fc_advect(self.handle, float(dt)))
 
+    def applyViscosity(self, dt: float, tolerance: float = 1e-4, max_iterations: int = -1):
+        """Implicit viscosity step; returns (iterations, relative residual)."""
+        it, rel = C.c_int(), C.c_double()
+        N.check(N.lib().fc_apply_viscosity(self.handle, float(dt), float(tolerance), int(max_iterations),
+                                           C.byref(it), C.byref(rel)))
+        return it.value, rel.value
+
+    def setComponentViscosity(self, phase: str, component: int, coefficient: float):
+        N.check(N.lib().fc_set_component_viscosity(self.handle, {"liquid": 0, "gas": 1}[phase], int(component),
+                                                   float(coefficient)))
+
     def getSurfaceTension(self) -> float:
         out = C.c_double()
         N.check(N.lib().fc_get_surface_tension(self.handle, C.byref(out)))

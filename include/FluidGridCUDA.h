@@ -69,6 +69,14 @@ public:
         gas_mixture = std::move(gas);
     }
 
+    // setComponentViscosity (FluidGridBase.h:47-52): a coefficient edit; membership stays fixed.
+    void setComponentViscosity(Phase phase, size_t component, double coefficient) override
+    {
+        check(fc_set_component_viscosity(live(), phase == Phase::Liquid ? 0 : 1, int(component), coefficient));
+        auto& mixture = phase == Phase::Liquid ? liquid_mixture : gas_mixture;
+        mixture.components.at(component).dynamic_viscosity = coefficient;
+    }
+
     const SubstanceCatalogue& getSubstances() const override { return substances; }
 
     const FluidMixture& getLiquidMixture() const override { return liquid_mixture; }

@@ -198,6 +198,18 @@ int fc_apply_surface_tension(fc_grid* grid, double dt);
  * from the current liquid fraction; either output may be NULL. No reference counterpart: it
  * exposes FluidSurfaceTensionCPU::curvature for inspection. */
 int fc_surface_curvature(fc_grid* grid, double* curvature, unsigned char* valid);
+/* FluidGridGPU::applyViscosity (UniformWebGPU/FluidGridGPU.cpp:987-1045) and
+ * ViscositySolverGPU::solve (UniformWebGPU/ViscositySolverGPU.cpp:170-294): backward-Euler
+ * viscosity on the face velocities, with the cell viscosity the volume-weighted mean of the
+ * component viscosities. CG with a multigrid preconditioner stops when the true residual, checked
+ * every 4 iterations, satisfies |r|^2_M <= tolerance^2 |v0|^2_M + 1e-12 total mass. No-op for
+ * dt <= 0 or when no component is viscous. max_iterations < 0: no cap; reaching a cap returns
+ * FC_ERR_TIMEOUT with the velocities unchanged. Outputs may be NULL. fc_step calls this after
+ * transport with tolerance 1e-4. */
+int fc_apply_viscosity(fc_grid* grid, double dt, double tolerance, int max_iterations, int* iterations,
+    double* relative_residual);
+/* setComponentViscosity (FluidGridBase.h:48-52): phase 0 liquid, 1 gas. */
+int fc_set_component_viscosity(fc_grid* grid, int phase, int component, double coefficient);
 /* FluidGridCPU::applyGravity (FluidGridCPU.cpp:987-996). */
 int fc_apply_gravity(fc_grid* grid, double dt);
 

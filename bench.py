@@ -298,8 +298,11 @@ def run_cuda(args, world, rank, local_rank):
         line["cpu_baseline"] = {"value": scene.cells / seconds, "unit": UNIT, "cores": min(8, host_threads()),
                                 "kind": kind, "iterations": it,
                                 "sample": f"1 projection of the {size}x{size} workload"}
-    if rank == 0 and not args.no_batched:
-        line["batched"] = batched_measure(args, torch)
+    if not args.no_batched:
+        # Every rank projects its share of the batch (placement.py); rank 0 reports.
+        batched = batched_measure(args, torch, world, rank)
+        if rank == 0:
+            line["batched"] = batched
     if rank == 0 and not args.no_serve:
         line["serve"] = serve_measure(args)
     return line
@@ -351,12 +354,20 @@ def e2e_measure(args, scene, torch):
             "ms_per_step": ms}
 
 
-def batched_measure(args, torch, count=256):
+def batched_measure(args, torch, world=1, rank=0, count=256):
     """Uneven grids (sides log-uniform 64..1024, aspect <= 2:1, fill 0.3-0.9, 0-8 obstacles)
-    projected together, against the same grids projected one at a time."""
+    projected together, against the same grids projected one at a time. With several ranks the
+    grids are placed whole on the ranks (no exchange between them) and the slowest rank's time
+    is reported."""
     from fluidsim_b200 import FluidGrid, ProjectionBatch, scenes
+    from fluidsim_b200.placement import max_over_ranks, mine, place
+    from fluidsim_b200.serving import grid_device_bytes
 
-    batch_scenes = scenes.uneven_batch(count, seed=7)
+    all_scenes = scenes.uneven_batch(count, seed=7)
+    total_cells = sum(s.cells for s in all_scenes)
+    assignment = place([s.cells for s in all_scenes],
+                       [2 * grid_device_bytes(s.width, s.height) for s in all_scenes], world, 150 * 10**9)
+    batch_scenes = [all_scenes[i] for i in mine(assignment, rank)]
     grids, pristine = [], []
     for s in batch_scenes:
         p = FluidGrid(s.width, s.height, s.cell_size, "fp32")
@@ -401,8 +412,13 @@ def batched_measure(args, torch, count=256):
         stop.synchronize()
         plain_ms += start.elapsed_time(stop)
     batch.destroy()
-    return {"value": cells / (batched_ms / 1e3), "unit": UNIT, "grids": count, "cells": cells,
-            "ms_per_batch": batched_ms, "plain_one_at_a_time_cells_per_s": cells / (plain_ms / 1e3),
+    dev = torch.device("cuda", torch.cuda.current_device())
+    batched_ms = max_over_ranks(batched_ms, dev)
+    plain_ms = max_over_ranks(plain_ms, dev)
+    ok = max_over_ranks(0.0 if ok else 1.0, dev) == 0.0
+    return {"value": total_cells / (batched_ms / 1e3), "unit": UNIT, "grids": count, "cells": total_cells,
+            "ranks": world, "ms_per_batch": batched_ms,
+            "plain_one_at_a_time_cells_per_s": total_cells / (plain_ms / 1e3),
             "speedup_vs_plain": plain_ms / batched_ms, "all_converged": ok,
             "max_iterations": max(r.iterations for r in res)}
 

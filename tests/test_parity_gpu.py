@@ -285,8 +285,10 @@ def test_edge_cases():
     fresh.configureMaterials([1.0], [0.001])
     with pytest.raises(FluidLifecycleError):
         fresh.step(0.01)
-    with pytest.raises(FluidCudaError):
-        fresh.configureMaterials([1.0], [0.001], liquid_viscosities=[1.0])
+    # Viscosities must be finite and nonnegative (FluidGridGPU.cpp:381-382).
+    with pytest.raises(FluidInvalidArgument):
+        fresh.configureMaterials([1.0], [0.001], liquid_viscosities=[-1.0])
+    fresh.configureMaterials([1.0], [0.001], liquid_viscosities=[1.0])
 
 
 @pytest.mark.parametrize("precision", ["fp32", "fp64"])

@@ -49,6 +49,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-serve", action="store_true", help="skip the serving (continuous batching) measurement")
+    p.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision comparison")
     p.add_argument("--serve-requests", type=int, default=16)
     p.add_argument("--serve-steps", type=int, default=300)
     p.add_argument("--launch", choices=["graph", "stream"], default="graph",
@@ -291,6 +292,8 @@ def run_cuda(args, world, rank, local_rank):
         "gpu_launches": launches,
     }
 
+    if rank == 0 and not args.no_mixed:
+        line["mixed"] = mixed_measure(args, scene, torch, flush)
     if rank == 0 and not args.no_e2e:
         line["e2e"] = e2e_measure(args, scene, torch)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -306,6 +309,54 @@ def run_cuda(args, world, rank, local_rank):
     if rank == 0 and not args.no_serve:
         line["serve"] = serve_measure(args)
     return line
+
+
+def mixed_measure(args, scene, torch, flush, steps=5, warmup=2):
+    """The same projection in plain FP32 and in mixed precision (FP16 multigrid weights), timed
+    like the main line, with the error of each against an FP64 solve of the same scene to a
+    1e-12 relative residual (the device FP64 path, which matches the FP64 CPU restatement to
+    1e-8 in the parity tests)."""
+    from fluidsim_b200 import FluidGrid, scenes
+
+    ref = FluidGrid(scene.width, scene.height, scene.cell_size, "fp64")
+    scenes.upload_scene(ref, scene)
+    ref.applyGravity(scene.dt)
+    ref.project(scene.dt, 2000, 1e-12, relative_tolerance=1e-12)
+    exact = ref.download()
+    ref.destroy()
+    scale = max(np.abs(exact.u).max(), np.abs(exact.v).max())
+    out = {"fp64_reference": "device FP64 solve to 1e-12 relative"}
+    for precision in ("fp32", "mixed"):
+        pristine = FluidGrid(scene.width, scene.height, scene.cell_size, precision)
+        scenes.upload_scene(pristine, scene)
+        work = FluidGrid(scene.width, scene.height, scene.cell_size, precision)
+        work.configureMaterials([scene.liquid_density], [scene.gas_density])
+        work.setGravityY(scene.gravity)
+        stream = torch.cuda.ExternalStream(work.stream())
+        times, iters = [], []
+        for i in range(warmup + steps):
+            work.copyStateFrom(pristine)
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+                start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                start.record(stream)
+            work.applyGravity(scene.dt)
+            r = work.project(scene.dt, 200, args.tolerance, relative_tolerance=args.tolerance)
+            stop.record(stream)
+            stop.synchronize()
+            if i >= warmup:
+                times.append(start.elapsed_time(stop))
+                iters.append(r.iterations)
+        s = work.download()
+        err = max(np.abs(s.u - exact.u).max(), np.abs(s.v - exact.v).max()) / scale
+        ms = statistics.mean(times)
+        out[precision] = {"value": scene.cells / (ms / 1e3), "unit": UNIT, "ms_per_step": ms,
+                          "iterations": statistics.mean(iters), "velocity_error_vs_fp64": err,
+                          "converged": r.solve_status == "converged"}
+        work.destroy()
+        pristine.destroy()
+    out["speedup_vs_fp32"] = out["fp32"]["ms_per_step"] / out["mixed"]["ms_per_step"]
+    return out
 
 
 def e2e_measure(args, scene, torch):

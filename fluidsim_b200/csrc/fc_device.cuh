@@ -13,6 +13,8 @@
 // (PressureMultigrid.cpp:142-202).
 #pragma once
 
+#include <cuda_fp16.h>
+
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -108,6 +110,11 @@ struct LevelDesc
     int w, h, S;
     void* right;
     void* down;
+    // Mixed precision: FP16 copies of right/down read by the smoothing kernels, stored divided
+    // by wscale (a per-level scale that keeps every weight in FP16's normal range).
+    const void* right_h;
+    const void* down_h;
+    float wscale;
     void* rhs;           // levels >= 1 (level 0 reads the PCG residual minus its mean)
     void* pre;           // pre-smoothed solution, read by the post-smoothing of the same level
     void* sol;           // final solution of the level (level 0: the PCG vector z)

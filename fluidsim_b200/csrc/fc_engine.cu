@@ -362,6 +362,13 @@ size_t allocate_grid(Grid& g, bool allocate = true)
         const size_t padded = size_t(L.S) * (L.h + 2);
         add(&ld.right, padded * elem);
         add(&ld.down, padded * elem);
+        // Mixed precision: FP16 copies of the weights of the coarse levels the strip kernels
+        // smooth (the fine level keeps FP32 weights).
+        if (g.precision == FC_PRECISION_MIXED && l >= 1 && int(l) < g.tail)
+        {
+            add(const_cast<void**>(&ld.right_h), padded * sizeof(__half));
+            add(const_cast<void**>(&ld.down_h), padded * sizeof(__half));
+        }
         if (l > 0)
         {
             add(&ld.rhs, padded * elem);
@@ -626,6 +633,7 @@ struct Plan
     bool tall[kMaxLevels] = {}; // strip height per level (true: Tiling::big)
     int max_levels = 0;
     int max_tail = 0;
+    int padded_max[kMaxLevels] = {}; // largest padded level array of any grid, per level
     size_t tail_smem = 0;
     cudaGraphExec_t exec = nullptr;
     cudaGraph_t graph = nullptr;
@@ -726,6 +734,8 @@ std::unique_ptr<Plan> make_plan(const std::vector<Grid*>& grids, cudaStream_t st
         plan->max_levels = std::max(plan->max_levels, int(g->levels.size()));
         plan->max_tail = std::max(plan->max_tail, g->tail);
         plan->tail_smem = std::max(plan->tail_smem, g->tail_smem);
+        for (size_t l = 0; l < g->levels.size(); ++l)
+            plan->padded_max[l] = std::max(plan->padded_max[l], g->levels[l].S * (g->levels[l].h + 2));
     }
     for (int l = 0; l + 1 < plan->max_levels; ++l)
     {
@@ -788,6 +798,9 @@ template <typename T> void launch_rebuild(Plan& p)
     for (int l = 0; l + 1 < p.max_levels; ++l)
         FC_LAUNCH(k_coarsen<T>, p.coarsen[l].count, kVecThreads, 0, s, p.d_desc, p.at(p.coarsen[l]), l);
     FC_LAUNCH(k_coarse_inverse<T>, p.n(), 256, 0, s, p.d_desc);
+    if (p.precision == FC_PRECISION_MIXED)
+        for (int l = 1; l < p.max_tail; ++l)
+            FC_LAUNCH(k_weights_half, dim3(ceil_div(p.padded_max[l], 256), p.n()), 256, 0, s, p.d_desc, l);
 }
 
 // One application of the preconditioner to r: z, mean z, r.z and beta.
@@ -800,9 +813,20 @@ template <typename T> void launch_precondition(Plan& p, bool use_mg)
         return;
     }
     constexpr int KB = Tiling<T>::big, KS = Tiling<T>::small;
+    const bool mixed = p.precision == FC_PRECISION_MIXED;
     for (int l = 0; l < p.max_tail; ++l)
     {
-        if (p.tall[l])
+        if (mixed && l >= 1)
+        {
+            if constexpr (sizeof(T) == 4)
+            {
+                if (p.tall[l])
+                    FC_LAUNCH_DEP((k_mg_pre<T, KB, true>), p.pre[l].count, 256, 0, s, p.d_desc, p.at(p.pre[l]), l);
+                else
+                    FC_LAUNCH_DEP((k_mg_pre<T, KS, true>), p.pre[l].count, 256, 0, s, p.d_desc, p.at(p.pre[l]), l);
+            }
+        }
+        else if (p.tall[l])
             FC_LAUNCH_DEP((k_mg_pre<T, KB>), p.pre[l].count, 256, 0, s, p.d_desc, p.at(p.pre[l]), l);
         else
             FC_LAUNCH_DEP((k_mg_pre<T, KS>), p.pre[l].count, 256, 0, s, p.d_desc, p.at(p.pre[l]), l);
@@ -810,7 +834,17 @@ template <typename T> void launch_precondition(Plan& p, bool use_mg)
     FC_LAUNCH_DEP(k_mg_tail<T>, p.n(), kTailThreads, p.tail_smem, s, p.d_desc);
     for (int l = p.max_tail - 1; l >= 0; --l)
     {
-        if (p.tall[l])
+        if (mixed && l >= 1)
+        {
+            if constexpr (sizeof(T) == 4)
+            {
+                if (p.tall[l])
+                    FC_LAUNCH_DEP((k_mg_post<T, KB, true>), p.post[l].count, 256, 0, s, p.d_desc, p.at(p.post[l]), l);
+                else
+                    FC_LAUNCH_DEP((k_mg_post<T, KS, true>), p.post[l].count, 256, 0, s, p.d_desc, p.at(p.post[l]), l);
+            }
+        }
+        else if (p.tall[l])
             FC_LAUNCH_DEP((k_mg_post<T, KB>), p.post[l].count, 256, 0, s, p.d_desc, p.at(p.post[l]), l);
         else
             FC_LAUNCH_DEP((k_mg_post<T, KS>), p.post[l].count, 256, 0, s, p.d_desc, p.at(p.post[l]), l);
@@ -1039,8 +1073,22 @@ template <typename F> void dispatch(int precision, F&& body)
         body(float{});
 }
 
+// Per-level scale of the FP16 weights: a fine weight 2 / (rho_a + rho_b) is at most 1 / rho_min,
+// and each coarsening at most doubles the largest weight (two parallel rows of series faces),
+// so level l's weights divided by 2^l / rho_min lie in (0, 1].
+void set_weight_scales(Grid& g)
+{
+    double rho_min = 0.0;
+    for (const auto* set : {&g.liquid_density, &g.gas_density})
+        for (double rho : *set)
+            rho_min = rho_min == 0.0 ? rho : std::min(rho_min, rho);
+    for (size_t l = 0; l < g.levels.size(); ++l)
+        g.desc.lev[l].wscale = float(rho_min > 0.0 ? std::ldexp(1.0 / rho_min, int(l)) : 1.0);
+}
+
 void refresh_descriptor(Grid& g)
 {
+    set_weight_scales(g);
     g.desc.solid = g.has_solid ? g.solid : nullptr;
     g.desc.masses = g.mass_ptrs;
     g.desc.components = g.components();
@@ -2116,9 +2164,7 @@ int fc_create(int width, int height, double cell_size, int precision, fc_grid** 
             fail(FC_ERR_INVALID_ARGUMENT, "grid geometry must be positive and finite");
         if ((long long)width * height > (1ll << 30))
             fail(FC_ERR_INVALID_ARGUMENT, "grid too large");
-        if (precision == FC_PRECISION_MIXED)
-            fail(FC_ERR_UNSUPPORTED, "mixed precision is not available in this build");
-        if (precision != FC_PRECISION_FP32 && precision != FC_PRECISION_FP64)
+        if (precision != FC_PRECISION_FP32 && precision != FC_PRECISION_FP64 && precision != FC_PRECISION_MIXED)
             fail(FC_ERR_INVALID_ARGUMENT, "unknown precision %d", precision);
         auto handle = std::make_unique<fc_grid>();
         Grid& g = handle->impl;
@@ -2140,7 +2186,7 @@ int fc_grid_device_bytes(int width, int height, int precision, int components, i
     {
         if (!bytes || width <= 0 || height <= 0 || components < 0 || (long long)width * height > (1ll << 30))
             fail(FC_ERR_INVALID_ARGUMENT, "invalid grid description");
-        if (precision != FC_PRECISION_FP32 && precision != FC_PRECISION_FP64)
+        if (precision != FC_PRECISION_FP32 && precision != FC_PRECISION_FP64 && precision != FC_PRECISION_MIXED)
             fail(FC_ERR_INVALID_ARGUMENT, "unknown precision %d", precision);
         fc::Grid g;
         g.W = width;

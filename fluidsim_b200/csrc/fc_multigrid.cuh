@@ -82,6 +82,27 @@ __global__ void __launch_bounds__(kVecThreads) k_precondition_diagonal(const Gri
 // Rebuild: coarse conductances and the coarsest inverse
 // ------------------------------------------------------------------------------------------
 
+// Mixed precision: FP16 copies of a level's face weights for the strip kernels, divided by
+// the level's scale and saturated at the largest finite FP16 value (blockIdx.y = grid).
+__global__ void k_weights_half(const GridDesc* grids, int level)
+{
+    const GridDesc& g = grids[blockIdx.y];
+    if (level < 1 || level >= g.tail)
+        return;
+    const LevelDesc& L = g.lev[level];
+    const int n = L.S * (L.h + 2);
+    const float inv = 1.0f / L.wscale;
+    const float* right = static_cast<const float*>(L.right);
+    const float* down = static_cast<const float*>(L.down);
+    __half* rh = static_cast<__half*>(const_cast<void*>(L.right_h));
+    __half* dh = static_cast<__half*>(const_cast<void*>(L.down_h));
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        rh[i] = __float2half_rn(fminf(right[i] * inv, 65504.0f));
+        dh[i] = __float2half_rn(fminf(down[i] * inv, 65504.0f));
+    }
+}
+
 // Coarse level `level + 1` from `level`. PressureMultigrid.cpp:142-202 (coarsen) and
 // :104-117 (the diagonal is recomputed on the fly wherever it is needed).
 template <typename T> __global__ void k_coarsen(const GridDesc* grids, const Tile* tiles, int level)

@@ -91,41 +91,76 @@ template <typename T, int K> struct StripRaw
     T wl0[K];
 };
 
-template <typename T, int K>
+// Face weights of the strip. With kHalf (mixed precision, T = float) they come from the level's
+// FP16 copies and are scaled back by wscale; the arithmetic stays FP32.
+template <typename T, int K, bool kHalf = false>
 __device__ __forceinline__ void strip_weights(Strip<T, K>& s, StripRaw<T, K>& raw, const LevelDesc& L, int X0, int Y0,
     int lane, int warp)
 {
     using P = typename Pair<T>::type;
-    const T* right = static_cast<const T*>(L.right);
-    const T* down = static_cast<const T*>(L.down);
     const int gx = X0 + 2 * lane;
     // The pair (gx, gx + 1) is either wholly inside the padded row [0, S) or wholly outside.
     const bool cols = gx + kPadX >= 0 && gx + kPadX + 1 < L.S;
     const bool left_col = gx + kPadX - 1 >= 0 && gx + kPadX - 1 < L.S;
     const int y0 = Y0 + warp * K;
-#pragma unroll
-    for (int k = 0; k < K; ++k)
+    if constexpr (kHalf)
     {
-        const int gy = y0 + k;
-        const bool in = cols && gy >= -1 && gy <= L.h;
-        const int i = padded_index32(L.S, gx, gy);
-        P w2 = P{}, d2 = P{};
-        if (in)
+        static_assert(sizeof(T) == 4, "FP16 weights feed FP32 smoothing");
+        const __half* right = static_cast<const __half*>(L.right_h);
+        const __half* down = static_cast<const __half*>(L.down_h);
+        const float scale = L.wscale;
+#pragma unroll
+        for (int k = 0; k < K; ++k)
         {
-            w2 = *reinterpret_cast<const P*>(right + i);
-            d2 = *reinterpret_cast<const P*>(down + i);
+            const int gy = y0 + k;
+            const bool in = cols && gy >= -1 && gy <= L.h;
+            const int i = padded_index32(L.S, gx, gy);
+            float2 w2 = make_float2(0.f, 0.f), d2 = make_float2(0.f, 0.f);
+            if (in)
+            {
+                w2 = __half22float2(*reinterpret_cast<const __half2*>(right + i));
+                d2 = __half22float2(*reinterpret_cast<const __half2*>(down + i));
+            }
+            s.wm[k] = w2.x * scale;
+            s.wr[k] = w2.y * scale;
+            s.da[k] = d2.x * scale;
+            s.db[k] = d2.y * scale;
+            raw.wl0[k] = (lane == 0 && left_col && gy >= -1 && gy <= L.h) ? __half2float(right[i - 1]) * scale : T(0);
         }
-        s.wm[k] = w2.x;
-        s.wr[k] = w2.y;
-        s.da[k] = d2.x;
-        s.db[k] = d2.y;
-        raw.wl0[k] = (lane == 0 && left_col && gy >= -1 && gy <= L.h) ? right[i - 1] : T(0);
+        float2 u2 = make_float2(0.f, 0.f);
+        if (cols && y0 - 1 >= -1 && y0 - 1 <= L.h)
+            u2 = __half22float2(*reinterpret_cast<const __half2*>(down + padded_index32(L.S, gx, y0 - 1)));
+        s.ua = u2.x * scale;
+        s.ub = u2.y * scale;
     }
-    P u2 = P{};
-    if (cols && y0 - 1 >= -1 && y0 - 1 <= L.h)
-        u2 = *reinterpret_cast<const P*>(down + padded_index32(L.S, gx, y0 - 1));
-    s.ua = u2.x;
-    s.ub = u2.y;
+    else
+    {
+        const T* right = static_cast<const T*>(L.right);
+        const T* down = static_cast<const T*>(L.down);
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+        {
+            const int gy = y0 + k;
+            const bool in = cols && gy >= -1 && gy <= L.h;
+            const int i = padded_index32(L.S, gx, gy);
+            P w2 = P{}, d2 = P{};
+            if (in)
+            {
+                w2 = *reinterpret_cast<const P*>(right + i);
+                d2 = *reinterpret_cast<const P*>(down + i);
+            }
+            s.wm[k] = w2.x;
+            s.wr[k] = w2.y;
+            s.da[k] = d2.x;
+            s.db[k] = d2.y;
+            raw.wl0[k] = (lane == 0 && left_col && gy >= -1 && gy <= L.h) ? right[i - 1] : T(0);
+        }
+        P u2 = P{};
+        if (cols && y0 - 1 >= -1 && y0 - 1 <= L.h)
+            u2 = *reinterpret_cast<const P*>(down + padded_index32(L.S, gx, y0 - 1));
+        s.ua = u2.x;
+        s.ub = u2.y;
+    }
 }
 
 template <typename T, int K>
@@ -231,7 +266,7 @@ __device__ __forceinline__ void edges_clear(Edges<T>& e)
         flat[i] = T(0);
 }
 
-template <typename T, int K>
+template <typename T, int K, bool kHalf = false>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_mg_pre(const GridDesc* grids, const Tile* tiles, int level)
 {
     using Shape = TileShape<T, K, true>;
@@ -264,7 +299,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_mg_pre(const Gr
     edges_clear<T, K>(edges);
     Strip<T, K> s;
     StripRaw<T, K> raw;
-    strip_weights<T, K>(s, raw, L, X0, Y0, lane, warp);
+    strip_weights<T, K, kHalf>(s, raw, L, X0, Y0, lane, warp);
     dependency_wait();
     if (g.state->done)
         return;
@@ -353,7 +388,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_mg_pre(const Gr
     }
 }
 
-template <typename T, int K>
+template <typename T, int K, bool kHalf = false>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_mg_post(const GridDesc* grids, const Tile* tiles, int level)
 {
     using Shape = TileShape<T, K, false>;
@@ -383,7 +418,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) k_mg_post(const G
     }
     Strip<T, K> s;
     StripRaw<T, K> raw;
-    strip_weights<T, K>(s, raw, L, X0, Y0, lane, warp);
+    strip_weights<T, K, kHalf>(s, raw, L, X0, Y0, lane, warp);
     dependency_wait();
     if (state.done)
         return;

@@ -45,7 +45,7 @@ typedef enum fc_precision
 {
     FC_PRECISION_FP32 = 0,  /* plain FP32 working arrays; FP64 pressure, dots and coarse solve */
     FC_PRECISION_FP64 = 1,  /* everything FP64: the reference's arithmetic */
-    FC_PRECISION_MIXED = 2  /* FP32 fine level, FP16-stored coarse multigrid levels */
+    FC_PRECISION_MIXED = 2  /* FP32, with the coarse multigrid levels' face weights stored in FP16 */
 } fc_precision;
 
 /* How a projection's PCG loop is launched (process-wide). */

@@ -157,6 +157,7 @@ struct GridDesc
     double* density;         // W x H, unpadded
     double* const* masses;   // device array of `components` W x H mass fields
     int components;
+    const void* maps;        // TMA tensor maps of the smoothed levels (see fc_stage.cuh)
 };
 
 // One CTA of work: grid index, tile origin in cells, and the tile's index within its grid.

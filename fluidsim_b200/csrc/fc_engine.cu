@@ -10,6 +10,7 @@
 #include "fc_multigrid.cuh"
 #include "fc_pcg.cuh"
 #include "fc_smooth.cuh"
+#include "fc_stage.cuh"
 #include "fc_json.h"
 #include "fc_advect.cuh"
 #include "fc_tension.cuh"
@@ -17,6 +18,9 @@
 #include "fc_errors.h"
 
 #include "../../include/fluidcuda.h"
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <atomic>
@@ -290,6 +294,89 @@ void choose_tail(Grid& g)
     g.tail_smem = tail_bytes(w.data(), h.data(), n - 1, n, g.elem);
 }
 
+// ------------------------------------------------------------------------------------------
+// TMA tensor maps of the smoothed levels
+// ------------------------------------------------------------------------------------------
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link against libcuda).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, []
+    {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        else
+            cudaGetLastError();
+    });
+    if (!fn)
+        fail(FC_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+    return fn;
+}
+
+// A 2D map over a padded level array (S columns, rows rows) with a box_w x box_h box.
+void encode_box(CUtensorMap& map, const void* base, CUtensorMapDataType type, size_t elem, int S, int rows, int box_w,
+    int box_h)
+{
+    const cuuint64_t dims[2] = {cuuint64_t(S), cuuint64_t(rows)};
+    const cuuint64_t strides[1] = {cuuint64_t(S) * elem};
+    const cuuint32_t box[2] = {cuuint32_t(box_w), cuuint32_t(box_h)};
+    const cuuint32_t element_strides[2] = {1, 1};
+    const CUresult r = tensor_map_encoder()(&map, type, 2, const_cast<void*>(base), dims, strides, box, element_strides,
+        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+        fail(FC_ERR_CUDA, "tensor map encoding failed (%d)", int(r));
+}
+
+// Maps of every level the strip kernels smooth (levels below the tail), for both strip heights:
+// weights (FP16 copies on coarse levels in mixed precision), the level's input vector, its
+// pre-smoothed solution and the next level's solution.
+void encode_stage_maps(Grid& g)
+{
+    const bool fp64 = g.precision == FC_PRECISION_FP64;
+    const CUtensorMapDataType vt = fp64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    const int heights[2] = {fp64 ? Tiling<double>::big : Tiling<float>::big,
+        fp64 ? Tiling<double>::small : Tiling<float>::small};
+    std::vector<CUtensorMap> maps(g.levels.size() * 2 * kMapsPerSet);
+    std::memset(maps.data(), 0, maps.size() * sizeof(CUtensorMap));
+    const GridDesc& d = g.desc;
+    for (int l = 0; l < g.tail; ++l)
+    {
+        const LevelDesc& L = d.lev[l];
+        const LevelDesc& C = d.lev[l + 1];
+        const bool half = g.precision == FC_PRECISION_MIXED && l >= 1;
+        for (int set = 0; set < 2; ++set)
+        {
+            const int K = heights[set];
+            const int bh = 8 * K + 1;
+            CUtensorMap* m = &maps[(l * 2 + set) * kMapsPerSet];
+            if (half)
+            {
+                encode_box(m[kMapRight], L.right_h, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, L.S, L.h + 2, 72, bh);
+                encode_box(m[kMapDown], L.down_h, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, L.S, L.h + 2, 72, bh);
+            }
+            else
+            {
+                encode_box(m[kMapRight], L.right, vt, g.elem, L.S, L.h + 2, 72, bh);
+                encode_box(m[kMapDown], L.down, vt, g.elem, L.S, L.h + 2, 72, bh);
+            }
+            encode_box(m[kMapVector], l == 0 ? d.r : L.rhs, vt, g.elem, L.S, L.h + 2, 72, bh);
+            encode_box(m[kMapPre], L.pre, vt, g.elem, L.S, L.h + 2, 72, bh);
+            encode_box(m[kMapCoarse], C.sol, vt, g.elem, C.S, C.h + 2, 40, 4 * K + 4);
+        }
+    }
+    check(cudaMemcpyAsync(const_cast<void*>(d.maps), maps.data(), maps.size() * sizeof(CUtensorMap),
+              cudaMemcpyHostToDevice, g.stream),
+        "tensor maps");
+    // The host vector must outlive the copy.
+    check(cudaStreamSynchronize(g.stream), "tensor maps");
+}
+
 // Lays out every device field of a grid in one allocation and fills the descriptor. With
 // allocate false it only returns the arena size (no CUDA calls).
 size_t allocate_grid(Grid& g, bool allocate = true)
@@ -385,6 +472,8 @@ size_t allocate_grid(Grid& g, bool allocate = true)
             add(&ry[l], L.ry.size() * sizeof(Gather));
         }
     }
+    // TMA maps: per level, two strip heights, kMapsPerSet maps of 128 bytes.
+    add(const_cast<void**>(&d.maps), g.levels.size() * 2 * kMapsPerSet * sizeof(CUtensorMap));
     size_t total = 0;
     std::vector<size_t> offsets;
     for (auto& s : slots)
@@ -421,6 +510,7 @@ size_t allocate_grid(Grid& g, bool allocate = true)
         }
     }
     d.solid = nullptr;
+    encode_stage_maps(g);
     check(cudaStreamSynchronize(g.stream), "grid set-up");
     return total;
 }
@@ -803,6 +893,69 @@ template <typename T> void launch_rebuild(Plan& p)
             FC_LAUNCH(k_weights_half, dim3(ceil_div(p.padded_max[l], 256), p.n()), 256, 0, s, p.d_desc, l);
 }
 
+// Resident CTAs of the persistent smoothing kernels: two per SM in FP32, one in FP64 (their
+// launch bounds and shared-memory staging).
+int smoothing_ctas(bool fp64)
+{
+    static int sms = 0;
+    if (!sms)
+    {
+        int device = 0;
+        check(cudaGetDevice(&device), "device");
+        check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "SM count");
+    }
+    return sms * (fp64 ? 1 : 2);
+}
+
+template <typename T, int K, typename W, bool PRE>
+void launch_smooth_kernel(Plan& p, int level, int set, bool dependent, cudaStream_t s)
+{
+    using St = Stage<T, W, K, PRE>;
+    const Range& r = PRE ? p.pre[level] : p.post[level];
+    if (r.count <= 0)
+        return;
+    auto kernel = PRE ? k_smooth_pre<T, K, W> : k_smooth_post<T, K, W>;
+    static const bool configured = [&]
+    {
+        check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(St::bytes)),
+            "smoothing shared memory");
+        return true;
+    }();
+    (void)configured;
+    const int ctas = std::min(r.count, smoothing_ctas(sizeof(T) == 8));
+    if (dependent)
+        FC_LAUNCH_DEP(kernel, ctas, 256, St::bytes, s, p.d_desc, p.at(r), r.count, level, set);
+    else
+        FC_LAUNCH(kernel, ctas, 256, St::bytes, s, p.d_desc, p.at(r), r.count, level, set);
+}
+
+// The pre- or post-smoothing kernel of one level: tall or short strips, FP16 weights on the
+// coarse levels of a mixed-precision plan.
+template <typename T> void launch_smooth(Plan& p, int level, bool pre, bool dependent, cudaStream_t s)
+{
+    constexpr int KB = Tiling<T>::big, KS = Tiling<T>::small;
+    const int set = p.tall[level] ? 0 : 1;
+    if constexpr (sizeof(T) == 4)
+    {
+        if (p.precision == FC_PRECISION_MIXED && level >= 1)
+        {
+            if (pre)
+                set == 0 ? launch_smooth_kernel<T, KB, __half, true>(p, level, set, dependent, s)
+                         : launch_smooth_kernel<T, KS, __half, true>(p, level, set, dependent, s);
+            else
+                set == 0 ? launch_smooth_kernel<T, KB, __half, false>(p, level, set, dependent, s)
+                         : launch_smooth_kernel<T, KS, __half, false>(p, level, set, dependent, s);
+            return;
+        }
+    }
+    if (pre)
+        set == 0 ? launch_smooth_kernel<T, KB, T, true>(p, level, set, dependent, s)
+                 : launch_smooth_kernel<T, KS, T, true>(p, level, set, dependent, s);
+    else
+        set == 0 ? launch_smooth_kernel<T, KB, T, false>(p, level, set, dependent, s)
+                 : launch_smooth_kernel<T, KS, T, false>(p, level, set, dependent, s);
+}
+
 // One application of the preconditioner to r: z, mean z, r.z and beta.
 template <typename T> void launch_precondition(Plan& p, bool use_mg)
 {
@@ -812,43 +965,11 @@ template <typename T> void launch_precondition(Plan& p, bool use_mg)
         FC_LAUNCH_DEP(k_precondition_diagonal<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
         return;
     }
-    constexpr int KB = Tiling<T>::big, KS = Tiling<T>::small;
-    const bool mixed = p.precision == FC_PRECISION_MIXED;
     for (int l = 0; l < p.max_tail; ++l)
-    {
-        if (mixed && l >= 1)
-        {
-            if constexpr (sizeof(T) == 4)
-            {
-                if (p.tall[l])
-                    FC_LAUNCH_DEP((k_mg_pre<T, KB, true>), p.pre[l].count, 256, 0, s, p.d_desc, p.at(p.pre[l]), l);
-                else
-                    FC_LAUNCH_DEP((k_mg_pre<T, KS, true>), p.pre[l].count, 256, 0, s, p.d_desc, p.at(p.pre[l]), l);
-            }
-        }
-        else if (p.tall[l])
-            FC_LAUNCH_DEP((k_mg_pre<T, KB>), p.pre[l].count, 256, 0, s, p.d_desc, p.at(p.pre[l]), l);
-        else
-            FC_LAUNCH_DEP((k_mg_pre<T, KS>), p.pre[l].count, 256, 0, s, p.d_desc, p.at(p.pre[l]), l);
-    }
+        launch_smooth<T>(p, l, true, true, s);
     FC_LAUNCH_DEP(k_mg_tail<T>, p.n(), kTailThreads, p.tail_smem, s, p.d_desc);
     for (int l = p.max_tail - 1; l >= 0; --l)
-    {
-        if (mixed && l >= 1)
-        {
-            if constexpr (sizeof(T) == 4)
-            {
-                if (p.tall[l])
-                    FC_LAUNCH_DEP((k_mg_post<T, KB, true>), p.post[l].count, 256, 0, s, p.d_desc, p.at(p.post[l]), l);
-                else
-                    FC_LAUNCH_DEP((k_mg_post<T, KS, true>), p.post[l].count, 256, 0, s, p.d_desc, p.at(p.post[l]), l);
-            }
-        }
-        else if (p.tall[l])
-            FC_LAUNCH_DEP((k_mg_post<T, KB>), p.post[l].count, 256, 0, s, p.d_desc, p.at(p.post[l]), l);
-        else
-            FC_LAUNCH_DEP((k_mg_post<T, KS>), p.post[l].count, 256, 0, s, p.d_desc, p.at(p.post[l]), l);
-    }
+        launch_smooth<T>(p, l, false, true, s);
 }
 
 template <typename T> void launch_iteration(Plan& p, bool use_mg, int parity)
@@ -1723,24 +1844,13 @@ double time_kernel(Grid& g, int kernel, int repeats)
     dispatch(g.precision, [&](auto zero)
     {
         using T = decltype(zero);
-        constexpr int KB = Tiling<T>::big, KS = Tiling<T>::small;
         set_kernel_attributes<T>(p);
         auto launch = [&]
         {
             switch (kernel)
             {
-            case 0:
-                if (p.tall[0])
-                    FC_LAUNCH((k_mg_pre<T, KB>), p.pre[0].count, 256, 0, p.stream, p.d_desc, p.at(p.pre[0]), 0);
-                else
-                    FC_LAUNCH((k_mg_pre<T, KS>), p.pre[0].count, 256, 0, p.stream, p.d_desc, p.at(p.pre[0]), 0);
-                break;
-            case 1:
-                if (p.tall[0])
-                    FC_LAUNCH((k_mg_post<T, KB>), p.post[0].count, 256, 0, p.stream, p.d_desc, p.at(p.post[0]), 0);
-                else
-                    FC_LAUNCH((k_mg_post<T, KS>), p.post[0].count, 256, 0, p.stream, p.d_desc, p.at(p.post[0]), 0);
-                break;
+            case 0: launch_smooth<T>(p, 0, true, false, p.stream); break;
+            case 1: launch_smooth<T>(p, 0, false, false, p.stream); break;
             case 2: FC_LAUNCH(k_direction_operator<T>, p.vec.count, kVecThreads, 0, p.stream, p.d_desc, p.at(p.vec), 0); break;
             default: FC_LAUNCH(k_mg_tail<T>, p.n(), kTailThreads, p.tail_smem, p.stream, p.d_desc); break;
             }

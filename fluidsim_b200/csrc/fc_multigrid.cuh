@@ -7,7 +7,7 @@
 // level is solved directly with one cell pinned, then given a mean-zero gauge.
 //
 // B200 mapping:
-//  * k_mg_pre / k_mg_post (fc_smooth.cuh): temporally blocked smoothing of one level per launch,
+//  * k_smooth_pre / k_smooth_post (fc_stage.cuh): temporally blocked smoothing of one level per launch,
 //    with the residual and restriction fused into the pre kernel and the prolongation and the
 //    fine-level z reductions fused into the post kernel.
 //  * k_mg_tail: the coarse levels that fit in shared memory are cycled by one CTA per grid,

@@ -1,0 +1,534 @@
+// Persistent, TMA-staged red-black smoothing of the multigrid levels (the V-cycle's hot kernels).
+//
+// Same arithmetic as the register strips of fc_smooth.cuh (a warp owns K rows x 64 columns,
+// lane j columns 2j and 2j+1, every cell's values in registers, one shuffle per horizontal
+// neighbour, edge rows through shared memory), but each CTA now walks a list of tiles and the
+// inputs of its next tile stream into shared memory by TMA while the current tile computes:
+//
+//   wait for tile i's boxes -> load the strips from shared memory -> barrier ->
+//   issue tile i+1's boxes -> sweep tile i from registers -> write tile i's outputs
+//
+// so the HBM latency of one tile hides behind the arithmetic of the previous one. The boxes are
+// 2D tiles of the padded level arrays (72 columns x 8K+1 rows: the strip rows and the row above,
+// the column left of the region, rounded out to 16-byte alignment); coordinates outside an array
+// read as zero, which is what the direct loads of the first form read there.
+#pragma once
+
+#include "fc_smooth.cuh"
+#include "fc_tma.cuh"
+
+namespace fc
+{
+
+// One padded level array's box, and the per-tile layout of the staging buffer.
+template <typename T, typename W, int K, bool PRE> struct Stage
+{
+    static constexpr int BW = 72;        // box columns (elements)
+    static constexpr int BH = 8 * K + 1; // strip rows plus the row above
+    static constexpr int CBW = 40;       // coarse box (post): columns
+    static constexpr int CBH = 4 * K + 4; //   and rows
+    static constexpr size_t round(size_t b) { return (b + 127) / 128 * 128; }
+    static constexpr size_t WB = round(size_t(BW) * BH * sizeof(W));
+    static constexpr size_t VB = round(size_t(BW) * BH * sizeof(T));
+    static constexpr size_t CB = PRE ? 0 : round(size_t(CBW) * CBH * sizeof(T));
+    static constexpr size_t right = 0, down = WB, vec = 2 * WB, pre = 2 * WB + VB;
+    static constexpr size_t coarse = PRE ? pre : pre + VB;
+    static constexpr size_t bytes = coarse + CB;
+    // Bytes the boxes of one tile deliver (full boxes, zero-filled parts included).
+    static constexpr unsigned tx = unsigned(2 * BW * BH * sizeof(W) + (PRE ? 1 : 2) * BW * BH * sizeof(T) +
+                                            (PRE ? 0 : CBW * CBH * sizeof(T)));
+};
+
+// Tensor maps of a grid: per level, per strip height (0 tall, 1 short), five maps.
+enum StageMap
+{
+    kMapRight = 0,
+    kMapDown = 1,
+    kMapVector = 2, // level 0: the PCG residual r; coarser levels: the restricted rhs
+    kMapPre = 3,
+    kMapCoarse = 4, // the next level's solution (post)
+    kMapsPerSet = 5
+};
+constexpr int kTensorMapBytes = 128;
+
+__device__ __forceinline__ const void* stage_map(const GridDesc& g, int level, int set, int which)
+{
+    return static_cast<const char*>(g.maps) + size_t((level * 2 + set) * kMapsPerSet + which) * kTensorMapBytes;
+}
+
+// First box column of a region whose leftmost needed padded column is v: a TMA box must start
+// at a multiple of 16 bytes, i.e. of 16 / sizeof(E) elements (4 for FP32, 8 for FP16).
+template <typename E> __host__ __device__ __forceinline__ int box_start(int v)
+{
+    return sizeof(E) >= 4 ? (v & ~3) : (v & ~7);
+}
+
+// Issues the boxes of the tile whose region starts at (X0, Y0); one thread.
+template <typename T, typename W, int K, bool PRE>
+__device__ __forceinline__ void stage_issue(const GridDesc& g, int level, int set, int X0, int Y0, char* stage,
+    uint64_t* bar)
+{
+    using S = Stage<T, W, K, PRE>;
+    // Padded coordinates: column gx + 2, row gy + 1. The region needs columns X0-1 .. X0+63 and
+    // rows Y0-1 .. Y0+8K-1.
+    const int bx = box_start<T>(X0 + 1), bw = box_start<W>(X0 + 1), by = Y0;
+    mbarrier_expect_tx(bar, S::tx);
+    tma_load_2d(stage + S::right, stage_map(g, level, set, kMapRight), bw, by, bar);
+    tma_load_2d(stage + S::down, stage_map(g, level, set, kMapDown), bw, by, bar);
+    tma_load_2d(stage + S::vec, stage_map(g, level, set, kMapVector), bx, by, bar);
+    if (!PRE)
+    {
+        tma_load_2d(stage + S::pre, stage_map(g, level, set, kMapPre), bx, by, bar);
+        const int CX0 = X0 / 2 - 1, CY0 = Y0 / 2 - 1;
+        tma_load_2d(stage + S::coarse, stage_map(g, level, set, kMapCoarse), box_start<T>(CX0 + 2), CY0 + 1, bar);
+    }
+}
+
+template <typename W> __device__ __forceinline__ float2 weight_pair(const W* p, float scale);
+template <> __device__ __forceinline__ float2 weight_pair<float>(const float* p, float)
+{
+    return *reinterpret_cast<const float2*>(p);
+}
+template <> __device__ __forceinline__ float2 weight_pair<__half>(const __half* p, float scale)
+{
+    const float2 v = __half22float2(*reinterpret_cast<const __half2*>(p));
+    return make_float2(v.x * scale, v.y * scale);
+}
+template <typename W> __device__ __forceinline__ float weight_one(const W* p, float scale);
+template <> __device__ __forceinline__ float weight_one<float>(const float* p, float) { return *p; }
+template <> __device__ __forceinline__ float weight_one<__half>(const __half* p, float scale)
+{
+    return __half2float(*p) * scale;
+}
+
+// Strip registers from the staged boxes: weights, inverse-diagonal inputs and right-hand side
+// (the values strip_weights and strip_rhs read from global memory).
+template <typename T, typename W, int K, bool PRE>
+__device__ __forceinline__ void stage_strip(Strip<T, K>& s, StripRaw<T, K>& raw, const char* stage, int X0,
+    float wscale, int lane, int warp)
+{
+    using S = Stage<T, W, K, PRE>;
+    using P = typename Pair<T>::type;
+    // Box columns of cell X0 + 2 lane in the vector and the weight boxes.
+    const int c = (X0 + 2 - box_start<T>(X0 + 1)) + 2 * lane;
+    const int cw = (X0 + 2 - box_start<W>(X0 + 1)) + 2 * lane;
+    const W* right = reinterpret_cast<const W*>(stage + S::right);
+    const W* down = reinterpret_cast<const W*>(stage + S::down);
+    const T* vec = reinterpret_cast<const T*>(stage + S::vec);
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+    {
+        const int r = (warp * K + k + 1) * S::BW + c;
+        const int rw = (warp * K + k + 1) * S::BW + cw;
+        if constexpr (sizeof(T) == 8)
+        {
+            const P w2 = *reinterpret_cast<const P*>(right + rw);
+            const P d2 = *reinterpret_cast<const P*>(down + rw);
+            s.wm[k] = w2.x;
+            s.wr[k] = w2.y;
+            s.da[k] = d2.x;
+            s.db[k] = d2.y;
+            raw.wl0[k] = lane == 0 ? T(right[rw - 1]) : T(0);
+        }
+        else
+        {
+            const float2 w2 = weight_pair<W>(right + rw, wscale);
+            const float2 d2 = weight_pair<W>(down + rw, wscale);
+            s.wm[k] = w2.x;
+            s.wr[k] = w2.y;
+            s.da[k] = d2.x;
+            s.db[k] = d2.y;
+            raw.wl0[k] = lane == 0 ? weight_one<W>(right + rw - 1, wscale) : 0.0f;
+        }
+        const P r2 = *reinterpret_cast<const P*>(vec + r);
+        s.ra[k] = r2.x;
+        s.rb[k] = r2.y;
+    }
+    const int u = (warp * K) * S::BW + cw;
+    if constexpr (sizeof(T) == 8)
+    {
+        const P u2 = *reinterpret_cast<const P*>(down + u);
+        s.ua = u2.x;
+        s.ub = u2.y;
+    }
+    else
+    {
+        const float2 u2 = weight_pair<W>(down + u, wscale);
+        s.ua = u2.x;
+        s.ub = u2.y;
+    }
+}
+
+__device__ __forceinline__ void stage_failed_at(SolveState* state)
+{
+    state->status = kBreakdown;
+    state->done = 1;
+}
+
+// Records a failed wait (the staged data never arrived) on the tile's grid; returns true then.
+__device__ __forceinline__ bool stage_failed(bool ok, SolveState* state)
+{
+    if (__syncthreads_or(!ok))
+    {
+        if (threadIdx.x == 0)
+            stage_failed_at(state);
+        return true;
+    }
+    return false;
+}
+
+// Pre-smoothing of `count` tiles (tiles[0 .. count)): four sweeps from zero, the residual, the
+// pre-smoothed solution of the output cells and the transpose-bilinear restriction into the
+// coarse right-hand side (PressureMultigrid.cpp:398-402, 204-231, 233-276).
+template <typename T, int K, typename W>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
+    k_smooth_pre(const GridDesc* grids, const Tile* tiles, int count, int level, int set)
+{
+    using Shape = TileShape<T, K, true>;
+    using S = Stage<T, W, K, true>;
+    extern __shared__ __align__(128) char stage[];
+    __shared__ uint64_t bar;
+    __shared__ Edges<T> edges;
+    __shared__ __align__(16) T res[Shape::RY][Shape::RX]; // written as pairs
+    constexpr int OCX = Shape::OX / 2, OCY = Shape::OY / 2;
+    __shared__ Gather gather_x[OCX], gather_y[OCY];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    allow_dependents();
+    dependency_wait();
+    // TMA writes shared memory at 128-byte aligned addresses only; a misplaced staging buffer is
+    // reported on the first tile's grid instead of being written.
+    if (smem_address(stage) & 127u)
+    {
+        if (threadIdx.x == 0 && int(blockIdx.x) < count)
+            stage_failed_at(grids[tiles[blockIdx.x].grid].state);
+        return;
+    }
+    if (threadIdx.x == 0)
+    {
+        mbarrier_init(&bar, 1);
+        fence_async_shared();
+    }
+    edges_clear<T, K>(edges);
+    __syncthreads();
+    int i = blockIdx.x;
+    if (threadIdx.x == 0 && i < count)
+    {
+        const Tile t = tiles[i];
+        stage_issue<T, W, K, true>(grids[t.grid], level, set, t.x0 - Shape::HALO, t.y0 - Shape::HALO, stage, &bar);
+    }
+    unsigned parity = 0;
+    for (; i < count; i += gridDim.x)
+    {
+        const Tile t = tiles[i];
+        const GridDesc& g = grids[t.grid];
+        const LevelDesc& L = g.lev[level];
+        const LevelDesc& C = g.lev[level + 1];
+        const int X0 = t.x0 - Shape::HALO, Y0 = t.y0 - Shape::HALO;
+        const int cx0 = t.x0 / 2, cy0 = t.y0 / 2;
+        // The restriction tables of the tile's coarse cells, while its boxes land.
+        Gather gt{};
+        if (threadIdx.x < OCX)
+        {
+            if (cx0 + int(threadIdx.x) < C.w)
+                gt = L.rx[cx0 + threadIdx.x];
+        }
+        else if (threadIdx.x < OCX + OCY)
+        {
+            if (cy0 + int(threadIdx.x) - OCX < C.h)
+                gt = L.ry[cy0 + threadIdx.x - OCX];
+        }
+        const bool done = g.state->done != 0;
+        const double mean_r = level == 0 ? g.state->mean_r : 0.0;
+        const bool ok = mbarrier_wait(&bar, parity);
+        if (stage_failed(ok, g.state))
+            return;
+        parity ^= 1u;
+        Strip<T, K> s;
+        StripRaw<T, K> raw;
+        if (!done)
+        {
+            stage_strip<T, W, K, true>(s, raw, stage, X0, L.wscale, lane, warp);
+            strip_finish<T, K>(s, raw, level, lane, mean_r);
+        }
+        __syncthreads();
+        // The staging buffer is free: the next tile's boxes stream in while this one sweeps.
+        const int next = i + gridDim.x;
+        if (threadIdx.x == 0 && next < count)
+        {
+            fence_async_shared();
+            const Tile n = tiles[next];
+            stage_issue<T, W, K, true>(grids[n.grid], level, set, n.x0 - Shape::HALO, n.y0 - Shape::HALO, stage, &bar);
+        }
+        if (done)
+            continue;
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+            s.a[k] = s.b[k] = T(0);
+        strip_sweep<T, K>(s, edges, 0, true, 0, lane, warp);
+        strip_sweep<T, K>(s, edges, 1, false, 1, lane, warp);
+#pragma unroll 1
+        for (int sweep = 1; sweep < 4; ++sweep)
+        {
+            strip_sweep<T, K>(s, edges, 0, false, 0, lane, warp);
+            strip_sweep<T, K>(s, edges, 1, false, 1, lane, warp);
+        }
+        // Residual of every cell into shared memory; the edge buffers hold the final values:
+        // buffer 0 colour 0, buffer 1 colour 1.
+        const T above_a = edges.bottom[1][warp][lane], above_b = edges.bottom[0][warp][lane];
+        const T below_a = edges.top[0][warp + 2][lane], below_b = edges.top[1][warp + 2][lane];
+        T* pre = static_cast<T*>(L.pre);
+        const int gx = X0 + 2 * lane;
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+        {
+            T left = __shfl_up_sync(0xffffffffu, s.b[k], 1);
+            T right = __shfl_down_sync(0xffffffffu, s.a[k], 1);
+            left = lane == 0 ? T(0) : left;
+            right = lane == 31 ? T(0) : right;
+            const T ua = k == 0 ? above_a : s.a[k - 1];
+            const T ub = k == 0 ? above_b : s.b[k - 1];
+            const T na = k == K - 1 ? below_a : s.a[k + 1];
+            const T nb = k == K - 1 ? below_b : s.b[k + 1];
+            const T wua = k == 0 ? s.ua : s.da[k - 1];
+            const T wub = k == 0 ? s.ub : s.db[k - 1];
+            const T a = s.a[k], b = s.b[k];
+            const T pa = (s.wl[k] * (a - left) + s.wm[k] * (a - b)) + (wua * (a - ua) + s.da[k] * (a - na));
+            const T pb = (s.wm[k] * (b - a) + s.wr[k] * (b - right)) + (wub * (b - ub) + s.db[k] * (b - nb));
+            const int y = warp * K + k;
+            typename Pair<T>::type rr;
+            rr.x = s.ia[k] > T(0) ? s.ra[k] - pa : T(0);
+            rr.y = s.ib[k] > T(0) ? s.rb[k] - pb : T(0);
+            *reinterpret_cast<typename Pair<T>::type*>(&res[y][2 * lane]) = rr;
+            const int gy = Y0 + y;
+            if (y >= Shape::HALO && y < Shape::HALO + Shape::OY && 2 * lane >= Shape::HALO &&
+                2 * lane < Shape::HALO + Shape::OX && gy < L.h && gx < L.w)
+            {
+                const int idx = padded_index32(L.S, gx, gy);
+                if (gx + 1 < L.w)
+                {
+                    typename Pair<T>::type ab;
+                    ab.x = a;
+                    ab.y = b;
+                    *reinterpret_cast<typename Pair<T>::type*>(pre + idx) = ab;
+                }
+                else
+                    pre[idx] = a;
+            }
+        }
+        if (threadIdx.x < OCX)
+            gather_x[threadIdx.x] = gt;
+        else if (threadIdx.x < OCX + OCY)
+            gather_y[threadIdx.x - OCX] = gt;
+        __syncthreads();
+        // Transpose-bilinear restriction onto the tile's coarse cells.
+        T* crhs = static_cast<T*>(C.rhs);
+        for (int q = threadIdx.x; q < OCX * OCY; q += 256)
+        {
+            const int qx = q % OCX, qy = q / OCX;
+            const int cx = cx0 + qx, cy = cy0 + qy;
+            if (cx >= C.w || cy >= C.h)
+                continue;
+            const Gather& gxr = gather_x[qx];
+            const Gather& gyr = gather_y[qy];
+            T value = T(0);
+            for (int iy = 0; iy < gyr.count; ++iy)
+            {
+                const int y = gyr.index[iy] - Y0;
+                T line = T(0);
+                for (int ix = 0; ix < gxr.count; ++ix)
+                    line += T(gxr.weight[ix]) * res[y][gxr.index[ix] - X0];
+                value += T(gyr.weight[iy]) * line;
+            }
+            crhs[padded_index32(C.S, cx, cy)] = value;
+        }
+        __syncthreads(); // res and the gather tables are rewritten by the next tile
+    }
+}
+
+// Post-smoothing of `count` tiles: the bilinear prolongation of the coarse solution added to
+// the pre-smoothed one, four sweeps in reversed colour order, and on the fine level sum(z) and
+// r.z for the PCG scalars (PressureMultigrid.cpp:403-407, 278-298; FluidGridCPU.cpp:1712-1726).
+template <typename T, int K, typename W>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
+    k_smooth_post(const GridDesc* grids, const Tile* tiles, int count, int level, int set)
+{
+    using Shape = TileShape<T, K, false>;
+    using S = Stage<T, W, K, false>;
+    extern __shared__ __align__(128) char stage[];
+    __shared__ uint64_t bar;
+    __shared__ Edges<T> edges;
+    __shared__ Interp interp_y[Shape::RY];
+    __shared__ double4 total;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    allow_dependents();
+    dependency_wait();
+    // TMA writes shared memory at 128-byte aligned addresses only; a misplaced staging buffer is
+    // reported on the first tile's grid instead of being written.
+    if (smem_address(stage) & 127u)
+    {
+        if (threadIdx.x == 0 && int(blockIdx.x) < count)
+            stage_failed_at(grids[tiles[blockIdx.x].grid].state);
+        return;
+    }
+    if (threadIdx.x == 0)
+    {
+        mbarrier_init(&bar, 1);
+        fence_async_shared();
+    }
+    edges_clear<T, K>(edges);
+    __syncthreads();
+    int i = blockIdx.x;
+    if (threadIdx.x == 0 && i < count)
+    {
+        const Tile t = tiles[i];
+        stage_issue<T, W, K, false>(grids[t.grid], level, set, t.x0 - Shape::HALO, t.y0 - Shape::HALO, stage, &bar);
+    }
+    unsigned parity = 0;
+    for (; i < count; i += gridDim.x)
+    {
+        const Tile t = tiles[i];
+        const GridDesc& g = grids[t.grid];
+        SolveState& state = *g.state;
+        const LevelDesc& L = g.lev[level];
+        const int X0 = t.x0 - Shape::HALO, Y0 = t.y0 - Shape::HALO;
+        const int CX0 = X0 / 2 - 1, CY0 = Y0 / 2 - 1;
+        // Interpolation tables of the tile's rows and columns, while its boxes land.
+        Interp iy{0, 0, 0.0};
+        if (threadIdx.x < Shape::RY)
+        {
+            const int gy = Y0 + int(threadIdx.x);
+            if (gy >= 0 && gy < L.h)
+                iy = L.py[gy];
+        }
+        const int gx = X0 + 2 * lane;
+        const bool in_a = gx >= 0 && gx < L.w, in_b = gx + 1 >= 0 && gx + 1 < L.w;
+        Interp pa{0, 0, 0.0}, pb{0, 0, 0.0};
+        if (in_a)
+            pa = L.px[gx];
+        if (in_b)
+            pb = L.px[gx + 1];
+        const bool done = state.done != 0;
+        const double mean_r = level == 0 ? state.mean_r : 0.0;
+        const bool ok = mbarrier_wait(&bar, parity);
+        if (stage_failed(ok, g.state))
+            return;
+        parity ^= 1u;
+        Strip<T, K> s;
+        StripRaw<T, K> raw;
+        if (threadIdx.x < Shape::RY)
+            interp_y[threadIdx.x] = iy;
+        if (!done)
+        {
+            stage_strip<T, W, K, false>(s, raw, stage, X0, L.wscale, lane, warp);
+            // The pre-smoothed values of the strip.
+            const T* pre = reinterpret_cast<const T*>(stage + S::pre);
+            const int c = (X0 + 2 - box_start<T>(X0 + 1)) + 2 * lane;
+#pragma unroll
+            for (int k = 0; k < K; ++k)
+            {
+                const typename Pair<T>::type ab =
+                    *reinterpret_cast<const typename Pair<T>::type*>(pre + (warp * K + k + 1) * S::BW + c);
+                s.a[k] = ab.x;
+                s.b[k] = ab.y;
+            }
+            strip_finish<T, K>(s, raw, level, lane, mean_r);
+        }
+        __syncthreads();
+        if (!done)
+        {
+            // Add the prolonged coarse correction, in-level cells only.
+            const T* coarse = reinterpret_cast<const T*>(stage + S::coarse);
+            const int coff = CX0 + 2 - box_start<T>(CX0 + 2);
+            const T wxa = T(pa.weight), wxb = T(pb.weight);
+            const int fa = pa.first - CX0 + coff, sa = pa.second - CX0 + coff;
+            const int fb = pb.first - CX0 + coff, sb = pb.second - CX0 + coff;
+#pragma unroll
+            for (int k = 0; k < K; ++k)
+            {
+                const int gy = Y0 + warp * K + k;
+                if (gy < 0 || gy >= L.h)
+                    continue;
+                const Interp& py = interp_y[warp * K + k];
+                const T* top = coarse + (py.first - CY0) * S::CBW;
+                const T* bottom = coarse + (py.second - CY0) * S::CBW;
+                const T wy = T(py.weight);
+                if (in_a)
+                {
+                    const T u = (T(1) - wxa) * top[fa] + wxa * top[sa];
+                    const T d = (T(1) - wxa) * bottom[fa] + wxa * bottom[sa];
+                    s.a[k] = s.a[k] + ((T(1) - wy) * u + wy * d);
+                }
+                if (in_b)
+                {
+                    const T u = (T(1) - wxb) * top[fb] + wxb * top[sb];
+                    const T d = (T(1) - wxb) * bottom[fb] + wxb * bottom[sb];
+                    s.b[k] = s.b[k] + ((T(1) - wy) * u + wy * d);
+                }
+            }
+        }
+        __syncthreads();
+        // The staging buffer is free: the next tile's boxes stream in while this one sweeps.
+        const int next = i + gridDim.x;
+        if (threadIdx.x == 0 && next < count)
+        {
+            fence_async_shared();
+            const Tile n = tiles[next];
+            stage_issue<T, W, K, false>(grids[n.grid], level, set, n.x0 - Shape::HALO, n.y0 - Shape::HALO, stage, &bar);
+        }
+        if (done)
+            continue;
+        // The first half-sweep (colour 1) reads colour-0 edges from buffer 1.
+        edges.top[1][warp + 1][lane] = s.a[0];
+        edges.bottom[1][warp + 1][lane] = s.b[K - 1];
+        __syncthreads();
+#pragma unroll 1
+        for (int sweep = 0; sweep < 4; ++sweep)
+        {
+            strip_sweep<T, K>(s, edges, 1, false, 0, lane, warp);
+            strip_sweep<T, K>(s, edges, 0, false, 1, lane, warp);
+        }
+        T* out = static_cast<T*>(L.sol);
+        double sz = 0.0, srz = 0.0;
+        const bool cols_out = 2 * lane >= Shape::HALO && 2 * lane < Shape::HALO + Shape::OX;
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+        {
+            const int y = warp * K + k;
+            const int gy = Y0 + y;
+            if (!cols_out || y < Shape::HALO || y >= Shape::HALO + Shape::OY || gy >= L.h || !in_a)
+                continue;
+            const int idx = padded_index32(L.S, gx, gy);
+            if (in_b)
+            {
+                typename Pair<T>::type ab;
+                ab.x = s.a[k];
+                ab.y = s.b[k];
+                *reinterpret_cast<typename Pair<T>::type*>(out + idx) = ab;
+            }
+            else
+                out[idx] = s.a[k];
+            if (level == 0)
+            {
+                // Cells without an open face hold z = 0 and rhs = 0: they add nothing to either sum.
+                sz += double(s.a[k]);
+                srz += double(s.ra[k]) * double(s.a[k]);
+                if (in_b)
+                {
+                    sz += double(s.b[k]);
+                    srz += double(s.rb[k]) * double(s.b[k]);
+                }
+            }
+        }
+        if (level == 0)
+        {
+            if (arrive_last<256>(g, t.index, g.post_tiles, block_reduce4<256>(make_double4(sz, srz, 0, 0), 0), &total, 0))
+            {
+                // The strips hold r - mean r: sum r z = sum (r - mean r) z + mean r sum z.
+                if (threadIdx.x == 0)
+                    finish_preconditioner(state, total.x, total.y + state.mean_r * total.x);
+            }
+        }
+    }
+}
+
+} // namespace fc

@@ -114,6 +114,9 @@ SIGNATURES = {
     "fc_project_relative": (_int, [_vp, _dbl, _int, _dbl, _dbl, C.POINTER(FcResult)]),
     "fc_step": (_int, [_vp, _dbl, _int, _dbl, C.POINTER(FcResult), C.POINTER(FcTimings)]),
     "fc_advect": (_int, [_vp, _dbl]),
+    "fc_autotune": (_int, [_vp, _int, C.POINTER(_int), _dp]),
+    "fc_batch_autotune": (_int, [_vp, _int, C.POINTER(_int), _dp]),
+    "fc_set_tail_cells": (_int, [_vp, _int]),
     "fc_apply_viscosity": (_int, [_vp, _dbl, _dbl, _int, C.POINTER(_int), _dp]),
     "fc_set_component_viscosity": (_int, [_vp, _int, _int, _dbl]),
     "fc_grid_device_bytes": (_int, [_int, _int, _int, _int, _int, C.POINTER(C.c_size_t)]),

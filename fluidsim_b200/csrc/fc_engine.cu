@@ -212,6 +212,7 @@ struct Grid
     std::vector<HostLevel> levels;
     int tail = 0;
     size_t tail_smem = 0;
+    int tail_cells = 1024; // largest level the one-CTA tail takes (autotuned)
 
     cudaStream_t stream = nullptr;
     char* arena = nullptr;
@@ -271,10 +272,11 @@ TileSizes tile_sizes(int precision, bool big)
     return big ? tile_sizes_of<float, Tiling<float>::big>() : tile_sizes_of<float, Tiling<float>::small>();
 }
 
-// The coarse tail starts at the first level whose cells and shared-memory footprint fit one CTA.
+// The coarse tail starts at the first level of at most g.tail_cells cells (and 1024 in FP64)
+// whose shared-memory footprint fits one CTA.
 void choose_tail(Grid& g)
 {
-    const int limit_cells = g.elem == 4 ? 4096 : 1024;
+    const int limit_cells = g.elem == 4 ? g.tail_cells : std::min(g.tail_cells, 1024);
     const size_t limit_bytes = 200 * 1024;
     std::vector<int> w, h;
     for (auto& l : g.levels)
@@ -345,7 +347,8 @@ void encode_stage_maps(Grid& g)
     std::vector<CUtensorMap> maps(g.levels.size() * 2 * kMapsPerSet);
     std::memset(maps.data(), 0, maps.size() * sizeof(CUtensorMap));
     const GridDesc& d = g.desc;
-    for (int l = 0; l < g.tail; ++l)
+    // Every level that has a coarser one: the tail threshold may move after allocation.
+    for (int l = 0; l + 1 < int(g.levels.size()); ++l)
     {
         const LevelDesc& L = d.lev[l];
         const LevelDesc& C = d.lev[l + 1];
@@ -451,7 +454,7 @@ size_t allocate_grid(Grid& g, bool allocate = true)
         add(&ld.down, padded * elem);
         // Mixed precision: FP16 copies of the weights of the coarse levels the strip kernels
         // smooth (the fine level keeps FP32 weights).
-        if (g.precision == FC_PRECISION_MIXED && l >= 1 && int(l) < g.tail)
+        if (g.precision == FC_PRECISION_MIXED && l >= 1 && l + 1 < g.levels.size())
         {
             add(const_cast<void**>(&ld.right_h), padded * sizeof(__half));
             add(const_cast<void**>(&ld.down_h), padded * sizeof(__half));
@@ -1875,6 +1878,108 @@ double time_kernel(Grid& g, int kernel, int repeats)
 }
 
 // ------------------------------------------------------------------------------------------
+// Autotuning of the multigrid schedule
+// ------------------------------------------------------------------------------------------
+//
+// The tail threshold (the largest level the one-CTA tail cycles in shared memory; the levels
+// above it run the strip kernels) changes which kernels run, not the arithmetic: both apply
+// the same red-black sweeps, transfers and coarsest solve. The tuner times V-cycles of a plan
+// under each candidate and keeps the fastest.
+
+// Applies a tail threshold to a grid. The grid's single-grid plan is rebuilt on next use; the
+// caller rebuilds any batch plan holding it.
+void set_tail_cells(Grid& g, int cells)
+{
+    g.tail_cells = cells;
+    choose_tail(g);
+    g.desc.tail = g.tail;
+    g.plan.reset();
+    g.coefficients_dirty = true; // mixed precision: FP16 copies of the newly smoothed levels
+}
+
+// Mean time of one V-cycle of a plan, in ms, over `repeats` after two warm-up cycles. The
+// solve states are saved before and restored after, so timing leaves the grids as they were.
+double time_vcycles(Plan& p, int repeats)
+{
+    rebuild_if_dirty(p);
+    std::vector<SolveState> saved(p.n());
+    for (int i = 0; i < p.n(); ++i)
+        check(cudaMemcpyAsync(&saved[i], p.grids[i]->desc.state, sizeof(SolveState), cudaMemcpyDeviceToHost, p.stream),
+            "state");
+    check(cudaStreamSynchronize(p.stream), "state");
+    cudaEvent_t start = nullptr, stop = nullptr;
+    check(cudaEventCreate(&start), "event");
+    check(cudaEventCreate(&stop), "event");
+    float ms = 0.0f;
+    try
+    {
+        auto cycle = [&]
+        {
+            for (int i = 0; i < p.n(); ++i)
+            {
+                SolveState running = saved[i];
+                running.done = 0;
+                check(cudaMemcpyAsync(p.grids[i]->desc.state, &running, sizeof(running), cudaMemcpyHostToDevice, p.stream),
+                    "state");
+            }
+            dispatch(p.precision, [&](auto zero)
+            {
+                using T = decltype(zero);
+                set_kernel_attributes<T>(p);
+                launch_precondition<T>(p, true);
+            });
+        };
+        cycle();
+        cycle();
+        check(cudaEventRecord(start, p.stream), "event");
+        for (int r = 0; r < repeats; ++r)
+            cycle();
+        check(cudaEventRecord(stop, p.stream), "event");
+        check(cudaEventSynchronize(stop), "event");
+        check(cudaEventElapsedTime(&ms, start, stop), "event");
+    }
+    catch (...)
+    {
+        cudaEventDestroy(start);
+        cudaEventDestroy(stop);
+        throw;
+    }
+    cudaEventDestroy(start);
+    cudaEventDestroy(stop);
+    for (int i = 0; i < p.n(); ++i)
+        check(cudaMemcpyAsync(p.grids[i]->desc.state, &saved[i], sizeof(SolveState), cudaMemcpyHostToDevice, p.stream),
+            "state");
+    check(cudaStreamSynchronize(p.stream), "state");
+    return double(ms) / repeats;
+}
+
+constexpr int kTailCandidates[] = {256, 1024, 4096};
+
+struct TuneResult
+{
+    int tail_cells;
+    double ms;
+};
+
+// Tries every tail threshold on the grids of a plan; `remake` rebuilds the plan after a change.
+template <typename Remake> TuneResult autotune_plan(std::vector<Grid*> grids, Remake&& remake, int repeats)
+{
+    TuneResult best{grids.front()->tail_cells, INFINITY};
+    for (int cells : kTailCandidates)
+    {
+        for (Grid* g : grids)
+            set_tail_cells(*g, cells);
+        const double ms = time_vcycles(remake(), repeats);
+        if (ms < best.ms)
+            best = {cells, ms};
+    }
+    for (Grid* g : grids)
+        set_tail_cells(*g, best.tail_cells);
+    remake();
+    return best;
+}
+
+// ------------------------------------------------------------------------------------------
 // Checkpoints: the "cuda-uniform" native format
 // ------------------------------------------------------------------------------------------
 //
@@ -2797,6 +2902,34 @@ int fc_classify(fc_grid* grid, unsigned char* mask)
     });
 }
 
+int fc_autotune(fc_grid* grid, int repeats, int* tail_cells, double* vcycle_ms)
+{
+    return guarded([&]
+    {
+        if (!grid || repeats <= 0)
+            fail(FC_ERR_INVALID_ARGUMENT, "invalid autotune arguments");
+        Grid& g = grid->impl;
+        fc::require_uploaded(g);
+        if (g.preconditioner != FC_PRECONDITIONER_MULTIGRID)
+            fail(FC_ERR_INVALID_ARGUMENT, "autotuning needs the multigrid preconditioner");
+        const fc::TuneResult r = fc::autotune_plan({&g}, [&]() -> fc::Plan& { return fc::single_plan(g); }, repeats);
+        if (tail_cells)
+            *tail_cells = r.tail_cells;
+        if (vcycle_ms)
+            *vcycle_ms = r.ms;
+    });
+}
+
+int fc_set_tail_cells(fc_grid* grid, int cells)
+{
+    return guarded([&]
+    {
+        if (!grid || cells < 1)
+            fail(FC_ERR_INVALID_ARGUMENT, "tail threshold must be positive");
+        fc::set_tail_cells(grid->impl, cells);
+    });
+}
+
 int fc_time_kernel(fc_grid* grid, int kernel, int repeats, double* mean_ms)
 {
     return guarded([&]
@@ -2962,6 +3095,35 @@ int fc_batch_project(fc_batch* batch, const double* dts, int max_iterations, dou
         }
         fc::upload_descriptors(p);
         fc::project_plan(p, dts, max_iterations, divergence_tolerance, relative_tolerance, results);
+    });
+}
+
+int fc_batch_autotune(fc_batch* batch, int repeats, int* tail_cells, double* vcycle_ms)
+{
+    return guarded([&]
+    {
+        if (!batch || repeats <= 0)
+            fail(FC_ERR_INVALID_ARGUMENT, "invalid autotune arguments");
+        std::vector<Grid*> grids;
+        for (fc_grid* g : batch->grids)
+        {
+            fc::require_uploaded(g->impl);
+            if (g->impl.preconditioner != FC_PRECONDITIONER_MULTIGRID)
+                fail(FC_ERR_INVALID_ARGUMENT, "autotuning needs the multigrid preconditioner");
+            grids.push_back(&g->impl);
+        }
+        cudaStream_t stream = batch->plan->stream;
+        const fc::TuneResult r = fc::autotune_plan(grids, [&]() -> fc::Plan&
+        {
+            batch->plan.reset();
+            batch->plan = fc::make_plan(grids, nullptr);
+            (void)stream;
+            return *batch->plan;
+        }, repeats);
+        if (tail_cells)
+            *tail_cells = r.tail_cells;
+        if (vcycle_ms)
+            *vcycle_ms = r.ms;
     });
 }
 

@@ -257,6 +257,15 @@ class FluidGrid:
         N.check(N.lib().fc_set_component_viscosity(self.handle, {"liquid": 0, "gas": 1}[phase], int(component),
                                                    float(coefficient)))
 
+    def autotune(self, repeats: int = 10):
+        """Picks the fastest multigrid tail threshold for this grid; returns (cells, V-cycle ms)."""
+        cells, ms = C.c_int(), C.c_double()
+        N.check(N.lib().fc_autotune(self.handle, int(repeats), C.byref(cells), C.byref(ms)))
+        return cells.value, ms.value
+
+    def setTailCells(self, cells: int):
+        N.check(N.lib().fc_set_tail_cells(self.handle, int(cells)))
+
     def getSurfaceTension(self) -> float:
         out = C.c_double()
         N.check(N.lib().fc_get_surface_tension(self.handle, C.byref(out)))
@@ -360,3 +369,10 @@ class ProjectionBatch:
         s = C.c_void_p()
         N.check(N.lib().fc_batch_get_stream(self._h, C.byref(s)))
         return s.value or 0
+
+    def autotune(self, repeats: int = 10):
+        """Picks the fastest multigrid tail threshold for the batch; returns (cells, V-cycle ms).
+        The batch's stream changes (its plan is rebuilt)."""
+        cells, ms = C.c_int(), C.c_double()
+        N.check(N.lib().fc_batch_autotune(self._h, int(repeats), C.byref(cells), C.byref(ms)))
+        return cells.value, ms.value

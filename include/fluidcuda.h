@@ -291,6 +291,16 @@ int fc_batch_project(fc_batch* batch, const double* dts, int max_iterations, dou
     double relative_tolerance, fc_result* results);
 int fc_batch_get_stream(const fc_batch* batch, void** stream);
 
+/* Autotuning of the multigrid schedule (no reference counterpart). The tail threshold is the
+ * largest level the one-block tail cycles in shared memory; larger levels run the strip
+ * kernels. It changes which kernels run, not the arithmetic. fc_autotune and fc_batch_autotune
+ * time `repeats` V-cycles of the grid's (or the batch's) plan under each candidate threshold
+ * (256, 1024, 4096 cells) and keep the fastest; the grids' states are left as they were.
+ * Outputs may be NULL. fc_set_tail_cells sets the threshold directly (default 1024). */
+int fc_autotune(fc_grid* grid, int repeats, int* tail_cells, double* vcycle_ms);
+int fc_batch_autotune(fc_batch* batch, int repeats, int* tail_cells, double* vcycle_ms);
+int fc_set_tail_cells(fc_grid* grid, int cells);
+
 /* ---- Serving: continuous batching of many simulations on one GPU ----------------------------
  * A request loop in the spirit of FluidScene::sceneProcess (FluidScene.inl:328-420) for many
  * independent simulations. A worker thread owns every grid. Each tick it admits queued

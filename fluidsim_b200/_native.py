@@ -20,6 +20,7 @@ STATUS_NAMES = {
 
 PRECISION = {"fp32": 0, "fp64": 1, "mixed": 2}
 PRECONDITIONER = {"diagonal": 0, "multigrid": 1}
+TRANSPORT = {"semi_lagrangian": 0, "plic": 1}
 SOLVE_STATUS = {0: "running", 1: "converged", 2: "iteration_limit", 3: "stalled", 4: "no_work", 5: "breakdown"}
 
 
@@ -114,6 +115,8 @@ SIGNATURES = {
     "fc_project_relative": (_int, [_vp, _dbl, _int, _dbl, _dbl, C.POINTER(FcResult)]),
     "fc_step": (_int, [_vp, _dbl, _int, _dbl, C.POINTER(FcResult), C.POINTER(FcTimings)]),
     "fc_advect": (_int, [_vp, _dbl]),
+    "fc_set_transport": (_int, [_vp, _int]),
+    "fc_get_transport": (_int, [_vp, C.POINTER(_int)]),
     "fc_autotune": (_int, [_vp, _int, C.POINTER(_int), _dp]),
     "fc_batch_autotune": (_int, [_vp, _int, C.POINTER(_int), _dp]),
     "fc_set_tail_cells": (_int, [_vp, _int]),

@@ -15,6 +15,7 @@
 #include "fc_advect.cuh"
 #include "fc_tension.cuh"
 #include "fc_viscosity.cuh"
+#include "fc_plic.cuh"
 #include "fc_errors.h"
 
 #include "../../include/fluidcuda.h"
@@ -34,6 +35,7 @@
 #include <mutex>
 #include <new>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 namespace fc
@@ -233,6 +235,9 @@ struct Grid
     TensionArrays tension{};
     char* visc_arena = nullptr;    // viscosity solver workspace, allocated on first use
     size_t visc_bytes = 0;
+    int transport = FC_TRANSPORT_SEMI_LAGRANGIAN;
+    char* plic_arena = nullptr;    // PLIC transport workspace, allocated on first use
+    size_t plic_bytes = 0;
 
     std::unique_ptr<Plan> plan; // single-grid plan, built lazily
 
@@ -761,7 +766,8 @@ struct Plan
 Grid::~Grid()
 {
     plan.reset();
-    for (void* ptr : {(void*)masses, (void*)mass_ptrs, (void*)tension_arena, (void*)visc_arena, (void*)arena})
+    for (void* ptr : {(void*)masses, (void*)mass_ptrs, (void*)tension_arena, (void*)visc_arena, (void*)plic_arena,
+             (void*)arena})
         if (ptr)
             cudaFree(ptr);
     if (stream)
@@ -1407,7 +1413,7 @@ void download(Grid& g, double* fraction, double* u, double* v, double* pressure,
 // Semi-Lagrangian transport of the velocities, the liquid fraction and every component mass
 // through the velocity at the start of the step (fc_advect.cuh). Masses change, so the
 // pressure coefficients are rebuilt at the next projection.
-void advect(Grid& g, double dt)
+void advect_semi_lagrangian(Grid& g, double dt)
 {
     require_uploaded(g);
     Plan& p = single_plan(g);
@@ -1788,6 +1794,143 @@ ViscResult apply_viscosity(Grid& g, double dt, double tolerance, int max_iterati
     return r;
 }
 
+// ------------------------------------------------------------------------------------------
+// Conservative PLIC transport (fc_plic.cuh)
+// ------------------------------------------------------------------------------------------
+
+size_t plic_layout(const Grid& g, plic::PlicArrays* a, char* base)
+{
+    const size_t cells = g.cells, k = size_t(g.components());
+    size_t total = 0;
+    auto take = [&](size_t bytes) -> char*
+    {
+        char* p = base ? base + total : nullptr;
+        total += (bytes + 255) / 256 * 256;
+        return p;
+    };
+    plic::PlicArrays t{};
+    t.mom_u = reinterpret_cast<double*>(take(g.faces_u * 8));
+    t.mom_v = reinterpret_cast<double*>(take(g.faces_v * 8));
+    t.next_u = reinterpret_cast<double*>(take(g.faces_u * 8));
+    t.next_v = reinterpret_cast<double*>(take(g.faces_v * 8));
+    t.lt_u = reinterpret_cast<double*>(take(g.faces_u * 8));
+    t.lt_v = reinterpret_cast<double*>(take(g.faces_v * 8));
+    t.mt_u = reinterpret_cast<double*>(take(g.faces_u * 8));
+    t.mt_v = reinterpret_cast<double*>(take(g.faces_v * 8));
+    t.normal = reinterpret_cast<double2*>(take(cells * 16));
+    t.offset = reinterpret_cast<double*>(take(cells * 8));
+    t.split = reinterpret_cast<unsigned char*>(take(cells));
+    t.corr = reinterpret_cast<double*>(take(std::max<size_t>(k, 1) * cells * 8));
+    t.mcorr = reinterpret_cast<double*>(take(cells * 8));
+    t.fnext = reinterpret_cast<double*>(take(cells * 8));
+    t.mnext = reinterpret_cast<double*>(take(std::max<size_t>(k, 1) * cells * 8));
+    t.outflow = reinterpret_cast<unsigned long long*>(take(8));
+    if (a)
+        *a = t;
+    return total;
+}
+
+plic::PlicArrays plic_workspace(Grid& g, cudaStream_t s)
+{
+    const size_t bytes = plic_layout(g, nullptr, nullptr);
+    if (!g.plic_arena || g.plic_bytes < bytes)
+    {
+        if (g.plic_arena)
+            cudaFree(g.plic_arena);
+        g.plic_arena = nullptr;
+        g.plic_bytes = 0;
+        check(cudaMalloc(&g.plic_arena, bytes), "transport allocation");
+        g.plic_bytes = bytes;
+        check(cudaMemsetAsync(g.plic_arena, 0, bytes, s), "transport clear");
+    }
+    plic::PlicArrays a{};
+    plic_layout(g, &a, g.plic_arena);
+    return a;
+}
+
+// FluidGridCPU::advect (FluidGridCPU.cpp:362-463): CFL substeps of an X pass and a Y pass.
+template <typename T> void advect_plic_t(Grid& g, double dt)
+{
+    using namespace plic;
+    Plan& p = single_plan(g);
+    cudaStream_t s = p.stream;
+    PlicArrays a = plic_workspace(g, s);
+    const int W = g.W, H = g.H, cells = int(g.cells), K = g.components(), L = int(g.liquid_density.size());
+    const double inverse_volume = 1.0 / (g.dx * g.dx);
+    T* u = static_cast<T*>(g.desc.u);
+    T* v = static_cast<T*>(g.desc.v);
+    double* const* masses = g.desc.masses;
+    const int cell_blocks = ceil_div(cells, 256), face_blocks = ceil_div((W + 1) * (H + 1), 256);
+
+    FC_LAUNCH(k_plic_density, cell_blocks, 256, 0, s, cells, masses, K, inverse_volume, g.desc.density);
+    FC_LAUNCH(k_plic_begin<T>, face_blocks, 256, 0, s, W, H, u, v, g.desc.density, a);
+    check(cudaMemsetAsync(a.outflow, 0, 8, s), "transport");
+    FC_LAUNCH(k_plic_outflow<T>, cell_blocks, 256, 0, s, W, H, u, v, a);
+    unsigned long long bits = 0;
+    check(cudaMemcpyAsync(&bits, a.outflow, 8, cudaMemcpyDeviceToHost, s), "transport");
+    check(cudaStreamSynchronize(s), "transport");
+    double max_outflow;
+    std::memcpy(&max_outflow, &bits, 8);
+    if (!std::isfinite(max_outflow))
+        fail(FC_ERR_NONFINITE, "transport received a non-finite velocity");
+    // Limit transport so no cell exports more than half its volume per substep.
+    const double max_step = max_outflow > 0.0 ? 0.5 * g.dx / max_outflow : dt;
+    if (dt / max_step > 1e6)
+        fail(FC_ERR_UNSUPPORTED, "transport would need more than a million substeps");
+
+    auto pass = [&](auto axis, double step)
+    {
+        constexpr int AXIS = decltype(axis)::value;
+        const double scale = step / g.dx;
+        const T* flow = AXIS == 0 ? u : v;
+        double* lt = AXIS == 0 ? a.lt_u : a.lt_v;
+        double* mt = AXIS == 0 ? a.mt_u : a.mt_v;
+        FC_LAUNCH(k_plic_interfaces, cell_blocks, 256, 0, s, W, H, g.fraction, a);
+        FC_LAUNCH((k_plic_transfer<T, AXIS>), face_blocks, 256, 0, s, W, H, flow, g.fraction, scale, a, lt);
+        FC_LAUNCH((k_plic_mass_transfer<T, AXIS>), face_blocks, 256, 0, s, W, H, flow, g.fraction, lt, masses, L, K,
+            scale, inverse_volume, mt);
+        FC_LAUNCH((k_plic_components<T, AXIS>), cell_blocks, 256, 0, s, W, H, flow, g.fraction, lt, masses, L, K, scale, a);
+        FC_LAUNCH((k_plic_momentum<T, AXIS>), face_blocks, 256, 0, s, W, H, u, v, mt, scale, a);
+        FC_LAUNCH((k_plic_fraction<T, AXIS>), cell_blocks, 256, 0, s, W, H, flow, g.fraction, lt, scale, a);
+        check(cudaMemcpyAsync(g.fraction, a.fnext, size_t(cells) * 8, cudaMemcpyDeviceToDevice, s), "transport");
+        if (K > 0)
+            check(cudaMemcpyAsync(g.masses, a.mnext, size_t(K) * cells * 8, cudaMemcpyDeviceToDevice, s), "transport");
+        FC_LAUNCH(k_plic_density, cell_blocks, 256, 0, s, cells, masses, K, inverse_volume, g.desc.density);
+        FC_LAUNCH(k_plic_recover, face_blocks, 256, 0, s, W, H, g.desc.density, a);
+    };
+    double remaining = dt;
+    while (remaining > 0.0)
+    {
+        const double step = max_step < remaining ? max_step : remaining;
+        // Frozen for both passes of the substep.
+        FC_LAUNCH(k_plic_freeze, cell_blocks, 256, 0, s, W, H, g.fraction, masses, L, K, inverse_volume, a);
+        pass(std::integral_constant<int, 0>{}, step);
+        pass(std::integral_constant<int, 1>{}, step);
+        remaining -= step;
+    }
+    FC_LAUNCH(k_plic_finish<T>, face_blocks, 256, 0, s, W, H, a, u, v);
+    check(cudaStreamSynchronize(s), "transport");
+}
+
+void advect_plic(Grid& g, double dt)
+{
+    require_uploaded(g);
+    dispatch(g.precision, [&](auto zero)
+    {
+        using T = decltype(zero);
+        advect_plic_t<T>(g, dt);
+    });
+    g.coefficients_dirty = true;
+}
+
+void advect(Grid& g, double dt)
+{
+    if (g.transport == FC_TRANSPORT_PLIC)
+        advect_plic(g, dt);
+    else
+        advect_semi_lagrangian(g, dt);
+}
+
 // One preconditioner application to a given residual (PressureMultigrid::apply,
 // PressureMultigrid.cpp:410-434, or the diagonal at FluidGridCPU.cpp:1691-1698); the
 // correction is returned without its mean removed, as the reference's apply returns it.
@@ -2049,6 +2192,7 @@ std::string checkpoint_metadata(const Grid& g)
     m += ", \"origin\": [" + number(g.origin_x) + ", " + number(g.origin_y) + "]";
     m += ", \"gravity_y\": " + number(g.gravity_y);
     m += ", \"surface_tension\": " + number(g.surface_tension);
+    m += ", \"transport\": " + std::to_string(g.transport);
     m += ", \"preconditioner\": " + std::to_string(g.preconditioner);
     m += ", \"liquid_mixture\": " + mixture(g.liquid_density, g.liquid_viscosity);
     m += ", \"gas_mixture\": " + mixture(g.gas_density, g.gas_viscosity);
@@ -2168,6 +2312,14 @@ void load_checkpoint(Grid& g, const char* metadata, const void* payload, size_t 
             fail(FC_ERR_INVALID_ARGUMENT, "checkpoint surface tension is malformed");
         tension = st->number;
     }
+    // Older checkpoints carry no transport scheme: semi-Lagrangian, the engine default.
+    int transport = FC_TRANSPORT_SEMI_LAGRANGIAN;
+    if (const json::Value* tr = m.find("transport"))
+    {
+        if (tr->kind != json::Value::Number || (tr->number != FC_TRANSPORT_SEMI_LAGRANGIAN && tr->number != FC_TRANSPORT_PLIC))
+            fail(FC_ERR_INVALID_ARGUMENT, "checkpoint transport scheme is unknown");
+        transport = int(tr->number);
+    }
     const PayloadLayout layout = payload_layout(g, int(ld.size() + gd.size()), solid);
     if (size_t(need("payload_bytes", json::Value::Number).number) != layout.total || payload_bytes != layout.total)
         fail(FC_ERR_INVALID_ARGUMENT, "checkpoint payload has %zu bytes, %zu expected", payload_bytes, layout.total);
@@ -2181,6 +2333,7 @@ void load_checkpoint(Grid& g, const char* metadata, const void* payload, size_t 
     g.preconditioner = preconditioner;
     g.gravity_y = gravity;
     g.surface_tension = tension;
+    g.transport = transport;
     g.origin_x = origin.items[0].number;
     g.origin_y = origin.items[1].number;
     allocate_masses(g);
@@ -2747,6 +2900,28 @@ int fc_advect(fc_grid* grid, double dt)
         if (!(dt > 0.0) || !std::isfinite(dt))
             fail(FC_ERR_INVALID_ARGUMENT, "time step must be positive and finite");
         fc::advect(grid->impl, dt);
+    });
+}
+
+int fc_set_transport(fc_grid* grid, int transport)
+{
+    return guarded([&]
+    {
+        if (!grid)
+            fail(FC_ERR_INVALID_ARGUMENT, "null grid");
+        if (transport != FC_TRANSPORT_SEMI_LAGRANGIAN && transport != FC_TRANSPORT_PLIC)
+            fail(FC_ERR_INVALID_ARGUMENT, "unknown transport scheme %d", transport);
+        grid->impl.transport = transport;
+    });
+}
+
+int fc_get_transport(const fc_grid* grid, int* transport)
+{
+    return guarded([&]
+    {
+        if (!grid || !transport)
+            fail(FC_ERR_INVALID_ARGUMENT, "null argument");
+        *transport = grid->impl.transport;
     });
 }
 

@@ -473,9 +473,6 @@ template <typename T> __global__ void __launch_bounds__(kTailThreads) k_mg_tail(
     allow_dependents();
     const GridDesc& g = grids[blockIdx.x];
     SolveState& state = *g.state;
-    dependency_wait();
-    if (state.done)
-        return;
     const int first = g.tail, last = g.levels - 1;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     T* const m = tail_array<T>();
@@ -512,35 +509,30 @@ template <typename T> __global__ void __launch_bounds__(kTailThreads) k_mg_tail(
     const int vectors_offset = cursor;
     const int array_elements = lv[last].res + (lv[last].s * (lv[last].h + 2)) - lv[first].right;
 
-    // Everything the cycle touches is copied in once: coefficients, tables, the inverse, and
-    // the first level's right-hand side; halos and the other arrays start at zero.
+    // Everything the cycle touches except the right-hand side is written by no kernel of the
+    // projection (coefficients, transfer tables, the coarsest inverse and its unknown map), so it
+    // is copied in before waiting on the previous kernel; halos and the other arrays start at
+    // zero.
     for (int i = threadIdx.x; i < array_elements; i += blockDim.x)
         m[i] = T(0);
     __shared__ CoarseInfo info;
     if (threadIdx.x < int(sizeof(CoarseInfo) / sizeof(int)))
         reinterpret_cast<int*>(&info)[threadIdx.x] = reinterpret_cast<const int*>(g.coarse)[threadIdx.x];
     __syncthreads();
-    const double mean_r = first == 0 ? state.mean_r : 0.0;
     for (int l = first; l <= last; ++l)
     {
         const TailLevel<T> L = lv[l];
         const LevelDesc& D = g.lev[l];
         const T* right = static_cast<const T*>(D.right);
         const T* down = static_cast<const T*>(D.down);
-        const T* rhs = first == 0 ? static_cast<const T*>(g.r) : static_cast<const T*>(D.rhs);
-        const bool with_rhs = l == first;
         for (int y = warp; y < L.h; y += kTailWarps)
         {
             for (int x = lane; x < L.w; x += 32)
             {
                 const int i = padded_index32_tail(D.S, x, y);
                 const int j = L.at(x, y);
-                const T wr = right[i], wd = down[i];
-                const T b = with_rhs ? rhs[i] : T(0);
-                m[L.right + j] = wr;
-                m[L.down + j] = wd;
-                if (with_rhs)
-                    m[L.rhs + j] = first == 0 ? T(double(b) - mean_r) : b;
+                m[L.right + j] = right[i];
+                m[L.down + j] = down[i];
             }
         }
         if (l < last)
@@ -576,8 +568,27 @@ template <typename T> __global__ void __launch_bounds__(kTailThreads) k_mg_tail(
                 const int j = L.at(x, y);
                 const T diag = ((m[L.right + j - 1] + m[L.right + j]) + m[L.down + j - L.s]) + m[L.down + j];
                 m[L.inv + j] = diag > T(0) ? T(1) / diag : T(0);
-                if (l == first && !(diag > T(0)))
-                    m[L.rhs + j] = T(0);
+            }
+        }
+    }
+
+    // The right-hand side of the first tail level comes from the previous kernel.
+    dependency_wait();
+    if (state.done)
+        return;
+    {
+        const TailLevel<T> L = lv[first];
+        const LevelDesc& D = g.lev[first];
+        const T* rhs = first == 0 ? static_cast<const T*>(g.r) : static_cast<const T*>(D.rhs);
+        const double mean_r = first == 0 ? state.mean_r : 0.0;
+        for (int y = warp; y < L.h; y += kTailWarps)
+        {
+            for (int x = lane; x < L.w; x += 32)
+            {
+                const int j = L.at(x, y);
+                const T b = rhs[padded_index32_tail(D.S, x, y)];
+                // Cells with no open face take no part.
+                m[L.rhs + j] = m[L.inv + j] > T(0) ? (first == 0 ? T(double(b) - mean_r) : b) : T(0);
             }
         }
     }

@@ -63,18 +63,29 @@ template <typename E> __host__ __device__ __forceinline__ int box_start(int v)
     return sizeof(E) >= 4 ? (v & ~3) : (v & ~7);
 }
 
-// Issues the boxes of the tile whose region starts at (X0, Y0); one thread.
+// Issues the boxes of the tile whose region starts at (X0, Y0); one thread. The weights are
+// written by no kernel of the projection, so a kernel may issue them before waiting on its
+// predecessor (stage_issue_weights); the other boxes follow (stage_issue_data). The barrier
+// expects the bytes of all of them from the first call.
 template <typename T, typename W, int K, bool PRE>
-__device__ __forceinline__ void stage_issue(const GridDesc& g, int level, int set, int X0, int Y0, char* stage,
+__device__ __forceinline__ void stage_issue_weights(const GridDesc& g, int level, int set, int X0, int Y0, char* stage,
     uint64_t* bar)
 {
     using S = Stage<T, W, K, PRE>;
     // Padded coordinates: column gx + 2, row gy + 1. The region needs columns X0-1 .. X0+63 and
     // rows Y0-1 .. Y0+8K-1.
-    const int bx = box_start<T>(X0 + 1), bw = box_start<W>(X0 + 1), by = Y0;
+    const int bw = box_start<W>(X0 + 1), by = Y0;
     mbarrier_expect_tx(bar, S::tx);
     tma_load_2d(stage + S::right, stage_map(g, level, set, kMapRight), bw, by, bar);
     tma_load_2d(stage + S::down, stage_map(g, level, set, kMapDown), bw, by, bar);
+}
+
+template <typename T, typename W, int K, bool PRE>
+__device__ __forceinline__ void stage_issue_data(const GridDesc& g, int level, int set, int X0, int Y0, char* stage,
+    uint64_t* bar)
+{
+    using S = Stage<T, W, K, PRE>;
+    const int bx = box_start<T>(X0 + 1), by = Y0;
     tma_load_2d(stage + S::vec, stage_map(g, level, set, kMapVector), bx, by, bar);
     if (!PRE)
     {
@@ -82,6 +93,14 @@ __device__ __forceinline__ void stage_issue(const GridDesc& g, int level, int se
         const int CX0 = X0 / 2 - 1, CY0 = Y0 / 2 - 1;
         tma_load_2d(stage + S::coarse, stage_map(g, level, set, kMapCoarse), box_start<T>(CX0 + 2), CY0 + 1, bar);
     }
+}
+
+template <typename T, typename W, int K, bool PRE>
+__device__ __forceinline__ void stage_issue(const GridDesc& g, int level, int set, int X0, int Y0, char* stage,
+    uint64_t* bar)
+{
+    stage_issue_weights<T, W, K, PRE>(g, level, set, X0, Y0, stage, bar);
+    stage_issue_data<T, W, K, PRE>(g, level, set, X0, Y0, stage, bar);
 }
 
 template <typename W> __device__ __forceinline__ float2 weight_pair(const W* p, float scale);
@@ -194,15 +213,9 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
     __shared__ Gather gather_x[OCX], gather_y[OCY];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     allow_dependents();
-    dependency_wait();
     // TMA writes shared memory at 128-byte aligned addresses only; a misplaced staging buffer is
-    // reported on the first tile's grid instead of being written.
-    if (smem_address(stage) & 127u)
-    {
-        if (threadIdx.x == 0 && int(blockIdx.x) < count)
-            stage_failed_at(grids[tiles[blockIdx.x].grid].state);
-        return;
-    }
+    // reported on the first tile's grid (after the wait) instead of being written.
+    const bool misplaced = (smem_address(stage) & 127u) != 0;
     if (threadIdx.x == 0)
     {
         mbarrier_init(&bar, 1);
@@ -211,10 +224,24 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
     edges_clear<T, K>(edges);
     __syncthreads();
     int i = blockIdx.x;
+    // The first tile's weights stream in while the previous kernel finishes.
+    if (threadIdx.x == 0 && i < count && !misplaced)
+    {
+        const Tile t = tiles[i];
+        stage_issue_weights<T, W, K, true>(grids[t.grid], level, set, t.x0 - Shape::HALO, t.y0 - Shape::HALO, stage,
+            &bar);
+    }
+    dependency_wait();
+    if (misplaced)
+    {
+        if (threadIdx.x == 0 && i < count)
+            stage_failed_at(grids[tiles[i].grid].state);
+        return;
+    }
     if (threadIdx.x == 0 && i < count)
     {
         const Tile t = tiles[i];
-        stage_issue<T, W, K, true>(grids[t.grid], level, set, t.x0 - Shape::HALO, t.y0 - Shape::HALO, stage, &bar);
+        stage_issue_data<T, W, K, true>(grids[t.grid], level, set, t.x0 - Shape::HALO, t.y0 - Shape::HALO, stage, &bar);
     }
     unsigned parity = 0;
     for (; i < count; i += gridDim.x)
@@ -361,15 +388,9 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
     __shared__ double4 total;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     allow_dependents();
-    dependency_wait();
     // TMA writes shared memory at 128-byte aligned addresses only; a misplaced staging buffer is
-    // reported on the first tile's grid instead of being written.
-    if (smem_address(stage) & 127u)
-    {
-        if (threadIdx.x == 0 && int(blockIdx.x) < count)
-            stage_failed_at(grids[tiles[blockIdx.x].grid].state);
-        return;
-    }
+    // reported on the first tile's grid (after the wait) instead of being written.
+    const bool misplaced = (smem_address(stage) & 127u) != 0;
     if (threadIdx.x == 0)
     {
         mbarrier_init(&bar, 1);
@@ -378,10 +399,24 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
     edges_clear<T, K>(edges);
     __syncthreads();
     int i = blockIdx.x;
+    // The first tile's weights stream in while the previous kernel finishes.
+    if (threadIdx.x == 0 && i < count && !misplaced)
+    {
+        const Tile t = tiles[i];
+        stage_issue_weights<T, W, K, false>(grids[t.grid], level, set, t.x0 - Shape::HALO, t.y0 - Shape::HALO, stage,
+            &bar);
+    }
+    dependency_wait();
+    if (misplaced)
+    {
+        if (threadIdx.x == 0 && i < count)
+            stage_failed_at(grids[tiles[i].grid].state);
+        return;
+    }
     if (threadIdx.x == 0 && i < count)
     {
         const Tile t = tiles[i];
-        stage_issue<T, W, K, false>(grids[t.grid], level, set, t.x0 - Shape::HALO, t.y0 - Shape::HALO, stage, &bar);
+        stage_issue_data<T, W, K, false>(grids[t.grid], level, set, t.x0 - Shape::HALO, t.y0 - Shape::HALO, stage, &bar);
     }
     unsigned parity = 0;
     for (; i < count; i += gridDim.x)

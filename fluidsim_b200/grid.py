@@ -242,6 +242,15 @@ class FluidGrid:
                                                 float(relative_tolerance), float(divergence_tolerance), C.byref(r)))
         return ProjectionResult.from_c(r)
 
+    def setTransport(self, scheme: str):
+        """'semi_lagrangian' (default) or 'plic' (UniformCPU's conservative transport)."""
+        N.check(N.lib().fc_set_transport(self.handle, N.TRANSPORT[scheme]))
+
+    def getTransport(self) -> str:
+        out = C.c_int()
+        N.check(N.lib().fc_get_transport(self.handle, C.byref(out)))
+        return {v: k for k, v in N.TRANSPORT.items()}[out.value]
+
     def advect(self, dt: float):
         """Semi-Lagrangian transport of velocities, liquid fraction and component masses."""
         N.check(N.lib().fc_advect(self.handle, float(dt)))

@@ -49,6 +49,12 @@ typedef enum fc_precision
 } fc_precision;
 
 /* How a projection's PCG loop is launched (process-wide). */
+typedef enum fc_transport
+{
+    FC_TRANSPORT_SEMI_LAGRANGIAN = 0, /* midpoint back-tracing on the staggered sampler (default) */
+    FC_TRANSPORT_PLIC = 1             /* UniformCPU's conservative PLIC/MYC transport */
+} fc_transport;
+
 typedef enum fc_launch_mode
 {
     FC_LAUNCH_GRAPH = 0, /* one CUDA graph per projection with a device-side loop (default) */
@@ -179,6 +185,12 @@ int fc_step(fc_grid* grid, double dt, int max_iterations, double divergence_tole
  * Face velocities, the liquid fraction and every component mass are traced through the
  * velocity at the start of the step. */
 int fc_advect(fc_grid* grid, double dt);
+/* Transport scheme of fc_advect and fc_step. FC_TRANSPORT_PLIC is FluidGridCPU::advect
+ * (UniformCPU/FluidGridCPU.cpp:362-463): conservative, directionally split PLIC/MYC transport of
+ * the liquid fraction, every component mass and the face momenta in CFL substeps, evaluated in
+ * FP64 whatever the grid's precision. */
+int fc_set_transport(fc_grid* grid, int transport);
+int fc_get_transport(const fc_grid* grid, int* transport);
 /* FluidGridCPU::sampleVelocity (UniformCPU/FluidGridCPU.h:132, FluidGridCPU.cpp:465-471): the
  * staggered bilinear velocity at `count` world positions. positions and velocities are host
  * arrays of interleaved (x, y) pairs. */

@@ -145,6 +145,8 @@ def ref():
         L.ref_project.restype = _RefResult
         L.ref_project.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_double]
         L.ref_set_origin.argtypes = [C.c_void_p, C.c_double, C.c_double]
+        L.ref_advect.argtypes = [C.c_void_p, C.c_double]
+        L.ref_masses.argtypes = [C.c_void_p, _dp, _dp]
         L.ref_set_surface_tension.argtypes = [C.c_void_p, C.c_double]
         L.ref_capillary_step_limit.restype = C.c_double
         L.ref_capillary_step_limit.argtypes = [C.c_void_p]
@@ -327,6 +329,16 @@ class ReferenceGrid:
 
     def max_divergence(self):
         return ref().ref_max_divergence(self.handle)
+
+    def advect(self, dt):
+        """FluidGridCPU::advect (the reference's own PLIC transport)."""
+        ref().ref_advect(self.handle, float(dt))
+
+    def masses(self):
+        lm = np.zeros((self.h, self.w))
+        gm = np.zeros((self.h, self.w))
+        ref().ref_masses(self.handle, _ptr(lm), _ptr(gm))
+        return lm, gm
 
     def set_surface_tension(self, sigma):
         ref().ref_set_surface_tension(self.handle, float(sigma))

@@ -190,6 +190,17 @@ void ref_surface_curvature(int width, int height, double cell_size, const double
     }
 }
 
+// FluidGridCPU::advect(dt) (FluidGridCPU.cpp:362-463) on the uploaded state.
+void ref_advect(void* handle, double dt) { static_cast<FluidGridCPU*>(handle)->advect(dt); }
+
+// Component masses of the single liquid and gas components.
+void ref_masses(void* handle, double* liquid, double* gas)
+{
+    const auto& grid = *static_cast<FluidGridCPU*>(handle);
+    std::memcpy(liquid, grid.liquid_mass[0].data(), grid.liquid_mass[0].size() * sizeof(double));
+    std::memcpy(gas, grid.gas_mass[0].data(), grid.gas_mass[0].size() * sizeof(double));
+}
+
 void ref_set_origin(void* handle, double x, double y) { static_cast<FluidGridCPU*>(handle)->setOrigin({x, y}); }
 
 // FluidGridCPU::sampleVelocity at interleaved (x, y) world positions.

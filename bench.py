@@ -34,7 +34,7 @@ L2_FLUSH_BYTES = 256 << 20
 # rhs; post reads the pre-smoothed solution, a quarter cell of coarse solution, r, right, down
 # and writes z.
 ALGORITHMIC_BYTES = {0: 4 + 4 + 4 + 4 + 1, 1: 4 + 1 + 4 + 4 + 4 + 4}
-KERNEL_NAMES = {0: "k_smooth_pre<float,8> (fine level)", 1: "k_smooth_post<float,8> (fine level)"}
+KERNEL_NAMES = {0: "k_smooth_pre (fine level)", 1: "k_smooth_post (fine level)"}
 
 
 def parse():

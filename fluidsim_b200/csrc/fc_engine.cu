@@ -264,17 +264,23 @@ struct TileSizes
     int pre_x, pre_y, post_x, post_y;
 };
 
-template <typename T, int K> TileSizes tile_sizes_of()
+template <typename T, int K, int WARPS> TileSizes tile_sizes_of()
 {
-    return {TileShape<T, K, true>::OX, TileShape<T, K, true>::OY, TileShape<T, K, false>::OX,
-        TileShape<T, K, false>::OY};
+    return {TileShape<T, K, true, WARPS>::OX, TileShape<T, K, true, WARPS>::OY, TileShape<T, K, false, WARPS>::OX,
+        TileShape<T, K, false, WARPS>::OY};
 }
 
-TileSizes tile_sizes(int precision, bool big)
+// Output region of the smoothing kernels for a region shape (kShapeTall/Short/Wide).
+TileSizes tile_sizes(int precision, int shape)
 {
     if (precision == FC_PRECISION_FP64)
-        return big ? tile_sizes_of<double, Tiling<double>::big>() : tile_sizes_of<double, Tiling<double>::small>();
-    return big ? tile_sizes_of<float, Tiling<float>::big>() : tile_sizes_of<float, Tiling<float>::small>();
+        return shape == kShapeShort ? tile_sizes_of<double, Tiling<double>::small, 8>()
+                                    : tile_sizes_of<double, Tiling<double>::big, 8>();
+    if (shape == kShapeShort)
+        return tile_sizes_of<float, Tiling<float>::small, 8>();
+    if (shape == kShapeWide)
+        return tile_sizes_of<float, Tiling<float>::big, 16>();
+    return tile_sizes_of<float, Tiling<float>::big, 8>();
 }
 
 // The coarse tail starts at the first level of at most g.tail_cells cells (and 1024 in FP64)
@@ -347,9 +353,11 @@ void encode_stage_maps(Grid& g)
 {
     const bool fp64 = g.precision == FC_PRECISION_FP64;
     const CUtensorMapDataType vt = fp64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
-    const int heights[2] = {fp64 ? Tiling<double>::big : Tiling<float>::big,
-        fp64 ? Tiling<double>::small : Tiling<float>::small};
-    std::vector<CUtensorMap> maps(g.levels.size() * 2 * kMapsPerSet);
+    const int big = fp64 ? Tiling<double>::big : Tiling<float>::big;
+    const int small = fp64 ? Tiling<double>::small : Tiling<float>::small;
+    // Strip rows of a region per shape: warps x strip height.
+    const int rows[kShapes] = {8 * big, 8 * small, 16 * big};
+    std::vector<CUtensorMap> maps(g.levels.size() * kShapes * kMapsPerSet);
     std::memset(maps.data(), 0, maps.size() * sizeof(CUtensorMap));
     const GridDesc& d = g.desc;
     // Every level that has a coarser one: the tail threshold may move after allocation.
@@ -358,11 +366,10 @@ void encode_stage_maps(Grid& g)
         const LevelDesc& L = d.lev[l];
         const LevelDesc& C = d.lev[l + 1];
         const bool half = g.precision == FC_PRECISION_MIXED && l >= 1;
-        for (int set = 0; set < 2; ++set)
+        for (int set = 0; set < kShapes; ++set)
         {
-            const int K = heights[set];
-            const int bh = 8 * K + 1;
-            CUtensorMap* m = &maps[(l * 2 + set) * kMapsPerSet];
+            const int bh = rows[set] + 1;
+            CUtensorMap* m = &maps[(l * kShapes + set) * kMapsPerSet];
             if (half)
             {
                 encode_box(m[kMapRight], L.right_h, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, L.S, L.h + 2, 72, bh);
@@ -375,7 +382,7 @@ void encode_stage_maps(Grid& g)
             }
             encode_box(m[kMapVector], l == 0 ? d.r : L.rhs, vt, g.elem, L.S, L.h + 2, 72, bh);
             encode_box(m[kMapPre], L.pre, vt, g.elem, L.S, L.h + 2, 72, bh);
-            encode_box(m[kMapCoarse], C.sol, vt, g.elem, C.S, C.h + 2, 40, 4 * K + 4);
+            encode_box(m[kMapCoarse], C.sol, vt, g.elem, C.S, C.h + 2, 40, rows[set] / 2 + 4);
         }
     }
     check(cudaMemcpyAsync(const_cast<void*>(d.maps), maps.data(), maps.size() * sizeof(CUtensorMap),
@@ -417,7 +424,8 @@ size_t allocate_grid(Grid& g, bool allocate = true)
     d.ncoarse = last.w * last.h - 1;
     d.vec_tiles = ceil_div(W, kVecTileX) * ceil_div(H, kVecTileY);
     // Partial slots for the most level-0 post tiles any plan can use (the short strips).
-    const TileSizes ts = tile_sizes(g.precision, false);
+    // The short regions have the most output tiles.
+    const TileSizes ts = tile_sizes(g.precision, kShapeShort);
     d.post_tiles = g.tail > 0 ? ceil_div(W, ts.post_x) * ceil_div(H, ts.post_y) : 0;
 
     const size_t padded0 = size_t(g.S) * (H + 2);
@@ -480,8 +488,8 @@ size_t allocate_grid(Grid& g, bool allocate = true)
             add(&ry[l], L.ry.size() * sizeof(Gather));
         }
     }
-    // TMA maps: per level, two strip heights, kMapsPerSet maps of 128 bytes.
-    add(const_cast<void**>(&d.maps), g.levels.size() * 2 * kMapsPerSet * sizeof(CUtensorMap));
+    // TMA maps: per level, kShapes region shapes, kMapsPerSet maps of 128 bytes.
+    add(const_cast<void**>(&d.maps), g.levels.size() * kShapes * kMapsPerSet * sizeof(CUtensorMap));
     size_t total = 0;
     std::vector<size_t> offsets;
     for (auto& s : slots)
@@ -728,7 +736,9 @@ struct Plan
     Range coarsen[kMaxLevels];
     Range pre[kMaxLevels];
     Range post[kMaxLevels];
-    bool tall[kMaxLevels] = {}; // strip height per level (true: Tiling::big)
+    // Region shape (RegionShape) of each level's pre- and post-smoothing kernels.
+    int shape_pre[kMaxLevels] = {};
+    int shape_post[kMaxLevels] = {};
     int max_levels = 0;
     int max_tail = 0;
     int padded_max[kMaxLevels] = {}; // largest padded level array of any grid, per level
@@ -785,7 +795,7 @@ void append_tiles(std::vector<Tile>& tiles, int grid, int w, int h, int tx, int 
 void upload_descriptors(Plan& plan)
 {
     std::vector<GridDesc> descs(plan.n());
-    const TileSizes ts = tile_sizes(plan.precision, plan.tall[0]);
+    const TileSizes ts = tile_sizes(plan.precision, plan.shape_post[0]);
     for (int i = 0; i < plan.n(); ++i)
     {
         descs[i] = plan.grids[i]->desc;
@@ -852,24 +862,36 @@ std::unique_ptr<Plan> make_plan(const std::vector<Grid*>& grids, cudaStream_t st
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, grids.front()->device);
     for (int l = 0; l < plan->max_tail; ++l)
     {
-        const TileSizes tall = tile_sizes(plan->precision, true);
-        long long tall_tiles = 0;
-        for (int i = 0; i < n; ++i)
-            if (l < grids[i]->tail)
-                tall_tiles += (long long)ceil_div(grids[i]->levels[l].w, tall.pre_x) * ceil_div(grids[i]->levels[l].h, tall.pre_y);
-        plan->tall[l] = tall_tiles >= 2LL * sms;
-        const TileSizes ts = tile_sizes(plan->precision, plan->tall[l]);
+        auto tiles_of = [&](int shape)
+        {
+            const TileSizes t = tile_sizes(plan->precision, shape);
+            long long count = 0;
+            for (int i = 0; i < n; ++i)
+                if (l < grids[i]->tail)
+                    count += (long long)ceil_div(grids[i]->levels[l].w, t.pre_x) * ceil_div(grids[i]->levels[l].h, t.pre_y);
+            return count;
+        };
+        // Tall regions need two waves of their two CTAs per SM; short strips halve each CTA's
+        // latency on the small levels. The post-smoothing kernel also has a wide shape (FP32,
+        // one 16-warp CTA per SM, the least halo per output cell), used with four waves of
+        // regions; the pre-smoothing kernel, heavier in barriers, runs faster as two tall CTAs.
+        const int base = tiles_of(kShapeTall) >= 2LL * sms ? kShapeTall : kShapeShort;
+        plan->shape_pre[l] = base;
+        plan->shape_post[l] =
+            plan->precision != FC_PRECISION_FP64 && tiles_of(kShapeWide) >= 4LL * sms ? kShapeWide : base;
+        const TileSizes tp = tile_sizes(plan->precision, plan->shape_pre[l]);
+        const TileSizes tq = tile_sizes(plan->precision, plan->shape_post[l]);
         add(plan->pre[l], [&]
         {
             for (int i = 0; i < n; ++i)
                 if (l < grids[i]->tail)
-                    append_tiles(tiles, i, grids[i]->levels[l].w, grids[i]->levels[l].h, ts.pre_x, ts.pre_y);
+                    append_tiles(tiles, i, grids[i]->levels[l].w, grids[i]->levels[l].h, tp.pre_x, tp.pre_y);
         });
         add(plan->post[l], [&]
         {
             for (int i = 0; i < n; ++i)
                 if (l < grids[i]->tail)
-                    append_tiles(tiles, i, grids[i]->levels[l].w, grids[i]->levels[l].h, ts.post_x, ts.post_y);
+                    append_tiles(tiles, i, grids[i]->levels[l].w, grids[i]->levels[l].h, tq.post_x, tq.post_y);
         });
     }
     check(cudaMalloc(&plan->d_tiles, std::max<size_t>(1, tiles.size()) * sizeof(Tile)), "plan tiles");
@@ -916,14 +938,14 @@ int smoothing_ctas(bool fp64)
     return sms * (fp64 ? 1 : 2);
 }
 
-template <typename T, int K, typename W, bool PRE>
+template <typename T, int K, typename W, bool PRE, int WARPS>
 void launch_smooth_kernel(Plan& p, int level, int set, bool dependent, cudaStream_t s)
 {
-    using St = Stage<T, W, K, PRE>;
+    using St = Stage<T, W, K, PRE, WARPS>;
     const Range& r = PRE ? p.pre[level] : p.post[level];
     if (r.count <= 0)
         return;
-    auto kernel = PRE ? k_smooth_pre<T, K, W> : k_smooth_post<T, K, W>;
+    auto kernel = PRE ? k_smooth_pre<T, K, W, WARPS> : k_smooth_post<T, K, W, WARPS>;
     static const bool configured = [&]
     {
         check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(St::bytes)),
@@ -931,38 +953,43 @@ void launch_smooth_kernel(Plan& p, int level, int set, bool dependent, cudaStrea
         return true;
     }();
     (void)configured;
-    const int ctas = std::min(r.count, smoothing_ctas(sizeof(T) == 8));
+    // Resident CTAs: two per SM for 8-warp FP32 regions, one otherwise.
+    const int ctas = std::min(r.count, smoothing_ctas(sizeof(T) == 8 || WARPS > 8));
     if (dependent)
-        FC_LAUNCH_DEP(kernel, ctas, 256, St::bytes, s, p.d_desc, p.at(r), r.count, level, set);
+        FC_LAUNCH_DEP(kernel, ctas, 32 * WARPS, St::bytes, s, p.d_desc, p.at(r), r.count, level, set);
     else
-        FC_LAUNCH(kernel, ctas, 256, St::bytes, s, p.d_desc, p.at(r), r.count, level, set);
+        FC_LAUNCH(kernel, ctas, 32 * WARPS, St::bytes, s, p.d_desc, p.at(r), r.count, level, set);
 }
 
-// The pre- or post-smoothing kernel of one level: tall or short strips, FP16 weights on the
-// coarse levels of a mixed-precision plan.
-template <typename T> void launch_smooth(Plan& p, int level, bool pre, bool dependent, cudaStream_t s)
+template <typename T, typename W, bool PRE> void launch_smooth_shape(Plan& p, int level, bool dependent, cudaStream_t s)
 {
     constexpr int KB = Tiling<T>::big, KS = Tiling<T>::small;
-    const int set = p.tall[level] ? 0 : 1;
+    const int shape = PRE ? p.shape_pre[level] : p.shape_post[level];
+    if constexpr (sizeof(T) == 4)
+    {
+        if (shape == kShapeWide)
+            return launch_smooth_kernel<T, KB, W, PRE, 16>(p, level, shape, dependent, s);
+    }
+    if (shape == kShapeShort)
+        launch_smooth_kernel<T, KS, W, PRE, 8>(p, level, shape, dependent, s);
+    else
+        launch_smooth_kernel<T, KB, W, PRE, 8>(p, level, shape, dependent, s);
+}
+
+// The pre- or post-smoothing kernel of one level in the plan's region shape, with FP16 weights
+// on the coarse levels of a mixed-precision plan.
+template <typename T> void launch_smooth(Plan& p, int level, bool pre, bool dependent, cudaStream_t s)
+{
     if constexpr (sizeof(T) == 4)
     {
         if (p.precision == FC_PRECISION_MIXED && level >= 1)
         {
-            if (pre)
-                set == 0 ? launch_smooth_kernel<T, KB, __half, true>(p, level, set, dependent, s)
-                         : launch_smooth_kernel<T, KS, __half, true>(p, level, set, dependent, s);
-            else
-                set == 0 ? launch_smooth_kernel<T, KB, __half, false>(p, level, set, dependent, s)
-                         : launch_smooth_kernel<T, KS, __half, false>(p, level, set, dependent, s);
+            pre ? launch_smooth_shape<T, __half, true>(p, level, dependent, s)
+                : launch_smooth_shape<T, __half, false>(p, level, dependent, s);
             return;
         }
     }
-    if (pre)
-        set == 0 ? launch_smooth_kernel<T, KB, T, true>(p, level, set, dependent, s)
-                 : launch_smooth_kernel<T, KS, T, true>(p, level, set, dependent, s);
-    else
-        set == 0 ? launch_smooth_kernel<T, KB, T, false>(p, level, set, dependent, s)
-                 : launch_smooth_kernel<T, KS, T, false>(p, level, set, dependent, s);
+    pre ? launch_smooth_shape<T, T, true>(p, level, dependent, s) : launch_smooth_shape<T, T, false>(p, level, dependent, s);
 }
 
 // One application of the preconditioner to r: z, mean z, r.z and beta.

@@ -29,10 +29,10 @@ template <bool PRE> struct TileHalo
     static constexpr int value = PRE ? 10 : 8;
 };
 
-template <typename T, int K, bool PRE> struct TileShape
+template <typename T, int K, bool PRE, int WARPS = 8> struct TileShape
 {
     static constexpr int RX = 64;
-    static constexpr int RY = 8 * K;
+    static constexpr int RY = WARPS * K;
     static constexpr int HALO = TileHalo<PRE>::value;
     static constexpr int OX = RX - 2 * HALO;
     static constexpr int OY = RY - 2 * HALO;
@@ -72,10 +72,10 @@ template <typename T, int K> struct Strip
 };
 
 // Shared edge rows of the strips: [buffer][warp + 1][lane]; warps -1 and 8 stay zero.
-template <typename T> struct Edges
+template <typename T, int WARPS = 8> struct Edges
 {
-    T top[2][10][32];
-    T bottom[2][10][32];
+    T top[2][WARPS + 2][32];
+    T bottom[2][WARPS + 2][32];
 };
 
 // Strip assembly: the staged loads (fc_stage.cuh) fill the weights, right-hand side and the
@@ -116,8 +116,8 @@ __device__ __forceinline__ void strip_finish(Strip<T, K>& s, const StripRaw<T, K
 
 // One red-black half-sweep of colour c over the strip; publishes the strip's edge rows of that
 // colour into buffer `buf` and reads the neighbours' edges from buffer buf ^ 1.
-template <typename T, int K>
-__device__ __forceinline__ void strip_sweep(Strip<T, K>& s, Edges<T>& e, int c, bool from_zero, int buf, int lane,
+template <typename T, int K, int WARPS = 8>
+__device__ __forceinline__ void strip_sweep(Strip<T, K>& s, Edges<T, WARPS>& e, int c, bool from_zero, int buf, int lane,
     int warp)
 {
     const T above = from_zero ? T(0) : e.bottom[buf ^ 1][warp][lane];
@@ -160,11 +160,11 @@ __device__ __forceinline__ void strip_sweep(Strip<T, K>& s, Edges<T>& e, int c, 
     __syncthreads();
 }
 
-template <typename T, int K>
-__device__ __forceinline__ void edges_clear(Edges<T>& e)
+template <typename T, int K, int WARPS = 8>
+__device__ __forceinline__ void edges_clear(Edges<T, WARPS>& e)
 {
     T* flat = &e.top[0][0][0];
-    for (int i = threadIdx.x; i < int(sizeof(Edges<T>) / sizeof(T)); i += blockDim.x)
+    for (int i = threadIdx.x; i < int(sizeof(Edges<T, WARPS>) / sizeof(T)); i += blockDim.x)
         flat[i] = T(0);
 }
 

@@ -21,12 +21,12 @@ namespace fc
 {
 
 // One padded level array's box, and the per-tile layout of the staging buffer.
-template <typename T, typename W, int K, bool PRE> struct Stage
+template <typename T, typename W, int K, bool PRE, int WARPS = 8> struct Stage
 {
-    static constexpr int BW = 72;        // box columns (elements)
-    static constexpr int BH = 8 * K + 1; // strip rows plus the row above
-    static constexpr int CBW = 40;       // coarse box (post): columns
-    static constexpr int CBH = 4 * K + 4; //   and rows
+    static constexpr int BW = 72;            // box columns (elements)
+    static constexpr int BH = WARPS * K + 1; // strip rows plus the row above
+    static constexpr int CBW = 40;           // coarse box (post): columns
+    static constexpr int CBH = WARPS * K / 2 + 4; //   and rows
     static constexpr size_t round(size_t b) { return (b + 127) / 128 * 128; }
     static constexpr size_t WB = round(size_t(BW) * BH * sizeof(W));
     static constexpr size_t VB = round(size_t(BW) * BH * sizeof(T));
@@ -39,7 +39,16 @@ template <typename T, typename W, int K, bool PRE> struct Stage
                                             (PRE ? 0 : CBW * CBH * sizeof(T)));
 };
 
-// Tensor maps of a grid: per level, per strip height (0 tall, 1 short), five maps.
+// Tensor maps of a grid: per level, per region shape (kShapeTall, kShapeShort, kShapeWide),
+// five maps.
+enum RegionShape
+{
+    kShapeTall = 0,  // 8 warps of the larger strip height
+    kShapeShort = 1, // 8 warps of the smaller strip height
+    kShapeWide = 2,  // 16 warps of the larger strip height (FP32): twice the rows per region
+    kShapes = 3
+};
+
 enum StageMap
 {
     kMapRight = 0,
@@ -53,7 +62,7 @@ constexpr int kTensorMapBytes = 128;
 
 __device__ __forceinline__ const void* stage_map(const GridDesc& g, int level, int set, int which)
 {
-    return static_cast<const char*>(g.maps) + size_t((level * 2 + set) * kMapsPerSet + which) * kTensorMapBytes;
+    return static_cast<const char*>(g.maps) + size_t((level * kShapes + set) * kMapsPerSet + which) * kTensorMapBytes;
 }
 
 // First box column of a region whose leftmost needed padded column is v: a TMA box must start
@@ -67,24 +76,24 @@ template <typename E> __host__ __device__ __forceinline__ int box_start(int v)
 // written by no kernel of the projection, so a kernel may issue them before waiting on its
 // predecessor (stage_issue_weights); the other boxes follow (stage_issue_data). The barrier
 // expects the bytes of all of them from the first call.
-template <typename T, typename W, int K, bool PRE>
+template <typename T, typename W, int K, bool PRE, int WARPS>
 __device__ __forceinline__ void stage_issue_weights(const GridDesc& g, int level, int set, int X0, int Y0, char* stage,
     uint64_t* bar)
 {
-    using S = Stage<T, W, K, PRE>;
+    using S = Stage<T, W, K, PRE, WARPS>;
     // Padded coordinates: column gx + 2, row gy + 1. The region needs columns X0-1 .. X0+63 and
-    // rows Y0-1 .. Y0+8K-1.
+    // rows Y0-1 .. Y0+WARPS*K-1.
     const int bw = box_start<W>(X0 + 1), by = Y0;
     mbarrier_expect_tx(bar, S::tx);
     tma_load_2d(stage + S::right, stage_map(g, level, set, kMapRight), bw, by, bar);
     tma_load_2d(stage + S::down, stage_map(g, level, set, kMapDown), bw, by, bar);
 }
 
-template <typename T, typename W, int K, bool PRE>
+template <typename T, typename W, int K, bool PRE, int WARPS>
 __device__ __forceinline__ void stage_issue_data(const GridDesc& g, int level, int set, int X0, int Y0, char* stage,
     uint64_t* bar)
 {
-    using S = Stage<T, W, K, PRE>;
+    using S = Stage<T, W, K, PRE, WARPS>;
     const int bx = box_start<T>(X0 + 1), by = Y0;
     tma_load_2d(stage + S::vec, stage_map(g, level, set, kMapVector), bx, by, bar);
     if (!PRE)
@@ -95,12 +104,12 @@ __device__ __forceinline__ void stage_issue_data(const GridDesc& g, int level, i
     }
 }
 
-template <typename T, typename W, int K, bool PRE>
+template <typename T, typename W, int K, bool PRE, int WARPS>
 __device__ __forceinline__ void stage_issue(const GridDesc& g, int level, int set, int X0, int Y0, char* stage,
     uint64_t* bar)
 {
-    stage_issue_weights<T, W, K, PRE>(g, level, set, X0, Y0, stage, bar);
-    stage_issue_data<T, W, K, PRE>(g, level, set, X0, Y0, stage, bar);
+    stage_issue_weights<T, W, K, PRE, WARPS>(g, level, set, X0, Y0, stage, bar);
+    stage_issue_data<T, W, K, PRE, WARPS>(g, level, set, X0, Y0, stage, bar);
 }
 
 template <typename W> __device__ __forceinline__ float2 weight_pair(const W* p, float scale);
@@ -122,11 +131,11 @@ template <> __device__ __forceinline__ float weight_one<__half>(const __half* p,
 
 // Strip registers from the staged boxes: weights, inverse-diagonal inputs and right-hand side
 // (the values strip_weights and strip_rhs read from global memory).
-template <typename T, typename W, int K, bool PRE>
+template <typename T, typename W, int K, bool PRE, int WARPS>
 __device__ __forceinline__ void stage_strip(Strip<T, K>& s, StripRaw<T, K>& raw, const char* stage, int X0,
     float wscale, int lane, int warp)
 {
-    using S = Stage<T, W, K, PRE>;
+    using S = Stage<T, W, K, PRE, WARPS>;
     using P = typename Pair<T>::type;
     // Box columns of cell X0 + 2 lane in the vector and the weight boxes.
     const int c = (X0 + 2 - box_start<T>(X0 + 1)) + 2 * lane;
@@ -199,15 +208,16 @@ __device__ __forceinline__ bool stage_failed(bool ok, SolveState* state)
 // Pre-smoothing of `count` tiles (tiles[0 .. count)): four sweeps from zero, the residual, the
 // pre-smoothed solution of the output cells and the transpose-bilinear restriction into the
 // coarse right-hand side (PressureMultigrid.cpp:398-402, 204-231, 233-276).
-template <typename T, int K, typename W>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
+template <typename T, int K, typename W, int WARPS>
+__global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2 : 1)
     k_smooth_pre(const GridDesc* grids, const Tile* tiles, int count, int level, int set)
 {
-    using Shape = TileShape<T, K, true>;
-    using S = Stage<T, W, K, true>;
+    using Shape = TileShape<T, K, true, WARPS>;
+    using S = Stage<T, W, K, true, WARPS>;
+    constexpr int NT = 32 * WARPS;
     extern __shared__ __align__(128) char stage[];
     __shared__ uint64_t bar;
-    __shared__ Edges<T> edges;
+    __shared__ Edges<T, WARPS> edges;
     __shared__ __align__(16) T res[Shape::RY][Shape::RX]; // written as pairs
     constexpr int OCX = Shape::OX / 2, OCY = Shape::OY / 2;
     __shared__ Gather gather_x[OCX], gather_y[OCY];
@@ -221,14 +231,14 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
         mbarrier_init(&bar, 1);
         fence_async_shared();
     }
-    edges_clear<T, K>(edges);
+    edges_clear<T, K, WARPS>(edges);
     __syncthreads();
     int i = blockIdx.x;
     // The first tile's weights stream in while the previous kernel finishes.
     if (threadIdx.x == 0 && i < count && !misplaced)
     {
         const Tile t = tiles[i];
-        stage_issue_weights<T, W, K, true>(grids[t.grid], level, set, t.x0 - Shape::HALO, t.y0 - Shape::HALO, stage,
+        stage_issue_weights<T, W, K, true, WARPS>(grids[t.grid], level, set, t.x0 - Shape::HALO, t.y0 - Shape::HALO, stage,
             &bar);
     }
     dependency_wait();
@@ -241,7 +251,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
     if (threadIdx.x == 0 && i < count)
     {
         const Tile t = tiles[i];
-        stage_issue_data<T, W, K, true>(grids[t.grid], level, set, t.x0 - Shape::HALO, t.y0 - Shape::HALO, stage, &bar);
+        stage_issue_data<T, W, K, true, WARPS>(grids[t.grid], level, set, t.x0 - Shape::HALO, t.y0 - Shape::HALO, stage, &bar);
     }
     unsigned parity = 0;
     for (; i < count; i += gridDim.x)
@@ -274,7 +284,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
         StripRaw<T, K> raw;
         if (!done)
         {
-            stage_strip<T, W, K, true>(s, raw, stage, X0, L.wscale, lane, warp);
+            stage_strip<T, W, K, true, WARPS>(s, raw, stage, X0, L.wscale, lane, warp);
             strip_finish<T, K>(s, raw, level, lane, mean_r);
         }
         __syncthreads();
@@ -284,20 +294,20 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
         {
             fence_async_shared();
             const Tile n = tiles[next];
-            stage_issue<T, W, K, true>(grids[n.grid], level, set, n.x0 - Shape::HALO, n.y0 - Shape::HALO, stage, &bar);
+            stage_issue<T, W, K, true, WARPS>(grids[n.grid], level, set, n.x0 - Shape::HALO, n.y0 - Shape::HALO, stage, &bar);
         }
         if (done)
             continue;
 #pragma unroll
         for (int k = 0; k < K; ++k)
             s.a[k] = s.b[k] = T(0);
-        strip_sweep<T, K>(s, edges, 0, true, 0, lane, warp);
-        strip_sweep<T, K>(s, edges, 1, false, 1, lane, warp);
+        strip_sweep<T, K, WARPS>(s, edges, 0, true, 0, lane, warp);
+        strip_sweep<T, K, WARPS>(s, edges, 1, false, 1, lane, warp);
 #pragma unroll 1
         for (int sweep = 1; sweep < 4; ++sweep)
         {
-            strip_sweep<T, K>(s, edges, 0, false, 0, lane, warp);
-            strip_sweep<T, K>(s, edges, 1, false, 1, lane, warp);
+            strip_sweep<T, K, WARPS>(s, edges, 0, false, 0, lane, warp);
+            strip_sweep<T, K, WARPS>(s, edges, 1, false, 1, lane, warp);
         }
         // Residual of every cell into shared memory; the edge buffers hold the final values:
         // buffer 0 colour 0, buffer 1 colour 1.
@@ -349,7 +359,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
         __syncthreads();
         // Transpose-bilinear restriction onto the tile's coarse cells.
         T* crhs = static_cast<T*>(C.rhs);
-        for (int q = threadIdx.x; q < OCX * OCY; q += 256)
+        for (int q = threadIdx.x; q < OCX * OCY; q += NT)
         {
             const int qx = q % OCX, qy = q / OCX;
             const int cx = cx0 + qx, cy = cy0 + qy;
@@ -375,15 +385,16 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
 // Post-smoothing of `count` tiles: the bilinear prolongation of the coarse solution added to
 // the pre-smoothed one, four sweeps in reversed colour order, and on the fine level sum(z) and
 // r.z for the PCG scalars (PressureMultigrid.cpp:403-407, 278-298; FluidGridCPU.cpp:1712-1726).
-template <typename T, int K, typename W>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
+template <typename T, int K, typename W, int WARPS>
+__global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2 : 1)
     k_smooth_post(const GridDesc* grids, const Tile* tiles, int count, int level, int set)
 {
-    using Shape = TileShape<T, K, false>;
-    using S = Stage<T, W, K, false>;
+    using Shape = TileShape<T, K, false, WARPS>;
+    using S = Stage<T, W, K, false, WARPS>;
+    constexpr int NT = 32 * WARPS;
     extern __shared__ __align__(128) char stage[];
     __shared__ uint64_t bar;
-    __shared__ Edges<T> edges;
+    __shared__ Edges<T, WARPS> edges;
     __shared__ Interp interp_y[Shape::RY];
     __shared__ double4 total;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -396,14 +407,14 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
         mbarrier_init(&bar, 1);
         fence_async_shared();
     }
-    edges_clear<T, K>(edges);
+    edges_clear<T, K, WARPS>(edges);
     __syncthreads();
     int i = blockIdx.x;
     // The first tile's weights stream in while the previous kernel finishes.
     if (threadIdx.x == 0 && i < count && !misplaced)
     {
         const Tile t = tiles[i];
-        stage_issue_weights<T, W, K, false>(grids[t.grid], level, set, t.x0 - Shape::HALO, t.y0 - Shape::HALO, stage,
+        stage_issue_weights<T, W, K, false, WARPS>(grids[t.grid], level, set, t.x0 - Shape::HALO, t.y0 - Shape::HALO, stage,
             &bar);
     }
     dependency_wait();
@@ -416,7 +427,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
     if (threadIdx.x == 0 && i < count)
     {
         const Tile t = tiles[i];
-        stage_issue_data<T, W, K, false>(grids[t.grid], level, set, t.x0 - Shape::HALO, t.y0 - Shape::HALO, stage, &bar);
+        stage_issue_data<T, W, K, false, WARPS>(grids[t.grid], level, set, t.x0 - Shape::HALO, t.y0 - Shape::HALO, stage, &bar);
     }
     unsigned parity = 0;
     for (; i < count; i += gridDim.x)
@@ -454,7 +465,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
             interp_y[threadIdx.x] = iy;
         if (!done)
         {
-            stage_strip<T, W, K, false>(s, raw, stage, X0, L.wscale, lane, warp);
+            stage_strip<T, W, K, false, WARPS>(s, raw, stage, X0, L.wscale, lane, warp);
             // The pre-smoothed values of the strip.
             const T* pre = reinterpret_cast<const T*>(stage + S::pre);
             const int c = (X0 + 2 - box_start<T>(X0 + 1)) + 2 * lane;
@@ -508,7 +519,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
         {
             fence_async_shared();
             const Tile n = tiles[next];
-            stage_issue<T, W, K, false>(grids[n.grid], level, set, n.x0 - Shape::HALO, n.y0 - Shape::HALO, stage, &bar);
+            stage_issue<T, W, K, false, WARPS>(grids[n.grid], level, set, n.x0 - Shape::HALO, n.y0 - Shape::HALO, stage, &bar);
         }
         if (done)
             continue;
@@ -519,8 +530,8 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
 #pragma unroll 1
         for (int sweep = 0; sweep < 4; ++sweep)
         {
-            strip_sweep<T, K>(s, edges, 1, false, 0, lane, warp);
-            strip_sweep<T, K>(s, edges, 0, false, 1, lane, warp);
+            strip_sweep<T, K, WARPS>(s, edges, 1, false, 0, lane, warp);
+            strip_sweep<T, K, WARPS>(s, edges, 0, false, 1, lane, warp);
         }
         T* out = static_cast<T*>(L.sol);
         double sz = 0.0, srz = 0.0;
@@ -556,7 +567,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
         }
         if (level == 0)
         {
-            if (arrive_last<256>(g, t.index, g.post_tiles, block_reduce4<256>(make_double4(sz, srz, 0, 0), 0), &total, 0))
+            if (arrive_last<NT>(g, t.index, g.post_tiles, block_reduce4<NT>(make_double4(sz, srz, 0, 0), 0), &total, 0))
             {
                 // The strips hold r - mean r: sum r z = sum (r - mean r) z + mean r sum z.
                 if (threadIdx.x == 0)

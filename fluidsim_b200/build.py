@@ -9,7 +9,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIBRARY = os.path.join(HERE, "libfluidcuda.so")
 SOURCES = ["fc_engine.cu", "fc_server.cpp"]
-HEADERS = ["fc_device.cuh", "fc_pcg.cuh", "fc_multigrid.cuh", "fc_smooth.cuh", "fc_advect.cuh", "fc_tension.cuh", "fc_viscosity.cuh", "fc_json.h", "fc_errors.h"]
+# Every header beside the sources: a change to any of them rebuilds the library.
+HEADERS = sorted(f for f in os.listdir(CSRC) if f.endswith((".cuh", ".h")))
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -262,6 +262,57 @@ __device__ bool arrive_last(const GridDesc& g, int tile_index, int tiles, double
     return true;
 }
 
+// Arrival of a persistent kernel's run of `run_tiles` tiles of one grid whose partial pairs are
+// already written to `pairs` (`entries` slots in all, indexed by tile). The CTA counts the run
+// once instead of once per tile; the last CTA to arrive folds all pairs in slot order (each
+// thread a contiguous run, loads batched; deterministic), leaves the sums in total->x, total->y
+// (thread 0) and resets the counter. Must be called by all threads.
+template <int NT>
+__device__ bool arrive_run(const GridDesc& g, const double2* pairs, int run_tiles, int grid_tiles, int entries,
+    double4* total)
+{
+    __shared__ int is_last;
+    __threadfence(); // the writers' partials before the count
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        const unsigned int ticket = atomicAdd(g.counter, unsigned(run_tiles));
+        is_last = ticket + unsigned(run_tiles) == unsigned(grid_tiles);
+    }
+    __syncthreads();
+    if (!is_last)
+        return false;
+    __threadfence();
+    const int per = (entries + NT - 1) / NT;
+    const int first = threadIdx.x * per;
+    const int last = min(entries, first + per);
+    double sx = 0.0, sy = 0.0;
+    constexpr int kBatch = 8;
+    for (int e = first; e < last; e += kBatch)
+    {
+        double2 v[kBatch];
+#pragma unroll
+        for (int u = 0; u < kBatch; ++u)
+            v[u] = e + u < last ? __ldcg(pairs + e + u) : make_double2(0.0, 0.0);
+#pragma unroll
+        for (int u = 0; u < kBatch; ++u)
+            if (e + u < last)
+            {
+                sx += v[u].x;
+                sy += v[u].y;
+            }
+    }
+    const double4 out = block_reduce4<NT>(make_double4(sx, sy, 0.0, 0.0), 0);
+    if (threadIdx.x == 0)
+    {
+        *total = out;
+        *g.counter = 0u;
+        __threadfence();
+    }
+    __syncthreads();
+    return true;
+}
+
 __device__ __forceinline__ bool finite_d(double v) { return isfinite(v); }
 
 // Programmatic dependent launch. The kernels of the PCG loop are launched so that each may

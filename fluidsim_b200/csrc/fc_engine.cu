@@ -172,8 +172,9 @@ std::vector<HostLevel> build_levels(int W, int H)
                 if (value[k] == 0.0)
                     continue;
                 Gather& g = r[target[k]];
-                if (g.count >= 4)
-                    fail(FC_ERR_CUDA, "restriction stencil overflow");
+                // The smoothing kernels sum coarse cell c over fine cells 2c-1 .. 2c+2 only.
+                if (g.count >= 4 || f < 2 * target[k] - 1 || f > 2 * target[k] + 2)
+                    fail(FC_ERR_CUDA, "restriction stencil outside fine cells 2c-1 .. 2c+2");
                 g.index[g.count] = f;
                 g.weight[g.count] = value[k];
                 ++g.count;
@@ -423,10 +424,16 @@ size_t allocate_grid(Grid& g, bool allocate = true)
     const HostLevel& last = g.levels.back();
     d.ncoarse = last.w * last.h - 1;
     d.vec_tiles = ceil_div(W, kVecTileX) * ceil_div(H, kVecTileY);
-    // Partial slots for the most level-0 post tiles any plan can use (the short strips).
-    // The short regions have the most output tiles.
+    // The level-0 post kernel writes one (sum z, sum r z) pair per tile: slots for the most
+    // tiles any region shape gives (two pairs to a double4 slot).
     const TileSizes ts = tile_sizes(g.precision, kShapeShort);
     d.post_tiles = g.tail > 0 ? ceil_div(W, ts.post_x) * ceil_div(H, ts.post_y) : 0;
+    long long post_pairs = 0;
+    for (int shape = 0; shape < kShapes && g.tail > 0; ++shape)
+    {
+        const TileSizes t = tile_sizes(g.precision, shape);
+        post_pairs = std::max(post_pairs, (long long)ceil_div(W, t.post_x) * ceil_div(H, t.post_y));
+    }
 
     const size_t padded0 = size_t(g.S) * (H + 2);
     auto add = [&](void** where, size_t bytes) { slots.push_back({where, bytes}); };
@@ -443,7 +450,8 @@ size_t allocate_grid(Grid& g, bool allocate = true)
     add((void**)&d.coarse_inverse, size_t(std::max(1, d.ncoarse * d.ncoarse)) * sizeof(double));
     add((void**)&d.coarse, sizeof(CoarseInfo));
     add((void**)&d.state, sizeof(SolveState));
-    add((void**)&d.partial, size_t(std::max(std::max(d.vec_tiles, d.post_tiles), 1)) * sizeof(double4));
+    add((void**)&d.partial, size_t(std::max<long long>(std::max<long long>(d.vec_tiles, (post_pairs + 1) / 2), 1)) *
+                                sizeof(double4));
     add((void**)&d.counter, sizeof(unsigned int) * 4);
     add((void**)&d.density, g.cells * sizeof(double));
     add((void**)&g.fraction, g.cells * sizeof(double));
@@ -872,13 +880,13 @@ std::unique_ptr<Plan> make_plan(const std::vector<Grid*>& grids, cudaStream_t st
             return count;
         };
         // Tall regions need two waves of their two CTAs per SM; short strips halve each CTA's
-        // latency on the small levels. The post-smoothing kernel also has a wide shape (FP32,
-        // one 16-warp CTA per SM, the least halo per output cell), used with four waves of
-        // regions; the pre-smoothing kernel, heavier in barriers, runs faster as two tall CTAs.
+        // latency on the small levels. In FP32 the wide shape (one 16-warp CTA per SM, the
+        // least halo per output cell) takes levels with four waves of regions.
         const int base = tiles_of(kShapeTall) >= 2LL * sms ? kShapeTall : kShapeShort;
-        plan->shape_pre[l] = base;
-        plan->shape_post[l] =
+        const int shape =
             plan->precision != FC_PRECISION_FP64 && tiles_of(kShapeWide) >= 4LL * sms ? kShapeWide : base;
+        plan->shape_pre[l] = shape;
+        plan->shape_post[l] = shape;
         const TileSizes tp = tile_sizes(plan->precision, plan->shape_pre[l]);
         const TileSizes tq = tile_sizes(plan->precision, plan->shape_post[l]);
         add(plan->pre[l], [&]

@@ -63,7 +63,8 @@ template <typename T, int K> struct Strip
 {
     T a[K], b[K];   // solution at columns 2j, 2j+1
     T ra[K], rb[K]; // right-hand side (zero where a cell has no open face)
-    T wl[K];        // face between columns 2j-1 and 2j
+    // The face between columns 2j-1 and 2j is the left lane's wr: its products come from there
+    // by shuffle, which keeps eight registers per strip free.
     T wm[K];        // face between 2j and 2j+1
     T wr[K];        // face between 2j+1 and 2j+2
     T da[K], db[K]; // lower faces (row k to k+1)
@@ -93,10 +94,10 @@ __device__ __forceinline__ void strip_finish(Strip<T, K>& s, const StripRaw<T, K
     for (int k = 0; k < K; ++k)
     {
         const T shifted = __shfl_up_sync(0xffffffffu, s.wr[k], 1);
-        s.wl[k] = lane == 0 ? raw.wl0[k] : shifted;
+        const T wl = lane == 0 ? raw.wl0[k] : shifted;
         const T up_a = k == 0 ? s.ua : s.da[k - 1];
         const T up_b = k == 0 ? s.ub : s.db[k - 1];
-        const T diag_a = ((s.wl[k] + s.wm[k]) + up_a) + s.da[k];
+        const T diag_a = ((wl + s.wm[k]) + up_a) + s.da[k];
         const T diag_b = ((s.wm[k] + s.wr[k]) + up_b) + s.db[k];
         s.ia[k] = diag_a > T(0) ? reciprocal(diag_a) : T(0);
         s.ib[k] = diag_b > T(0) ? reciprocal(diag_b) : T(0);
@@ -131,12 +132,13 @@ __device__ __forceinline__ void strip_sweep(Strip<T, K>& s, Edges<T, WARPS>& e, 
                 s.a[k] = s.ra[k] * s.ia[k];
             else
             {
-                T left = __shfl_up_sync(0xffffffffu, s.b[k], 1);
+                // wl * left, formed on the left lane as its wr * b (zero left of the region).
+                T left = __shfl_up_sync(0xffffffffu, s.wr[k] * s.b[k], 1);
                 left = lane == 0 ? T(0) : left;
                 const T up = k == 0 ? above : s.a[k - 1];
                 const T dn = k == K - 1 ? below : s.a[k + 1];
                 const T wu = k == 0 ? s.ua : s.da[k - 1];
-                s.a[k] = (s.ra[k] + ((s.wl[k] * left + s.wm[k] * s.b[k]) + (wu * up + s.da[k] * dn))) * s.ia[k];
+                s.a[k] = (s.ra[k] + ((left + s.wm[k] * s.b[k]) + (wu * up + s.da[k] * dn))) * s.ia[k];
             }
         }
         else

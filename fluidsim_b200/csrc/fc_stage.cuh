@@ -205,6 +205,52 @@ __device__ __forceinline__ bool stage_failed(bool ok, SolveState* state)
     return false;
 }
 
+// One axis of the transpose-bilinear restriction for coarse cell c: the weights of fine cells
+// 2c-1, 2c, 2c+1, 2c+2 (bit p of `mask` set when fine cell 2c-1+p contributes). The table lists
+// its fine cells in ascending order, so summing by offset keeps the table's order; the host
+// checks that no entry falls outside the four offsets.
+template <typename T> struct RestrictAxis
+{
+    T w[4];
+    unsigned mask;
+};
+
+template <typename T> __device__ __forceinline__ RestrictAxis<T> restrict_axis(const Gather* table, int c)
+{
+    RestrictAxis<T> r;
+    r.mask = 0;
+    const Gather g = table[c];
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+    {
+        r.w[p] = T(0);
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+            if (e < g.count && g.index[e] == 2 * c - 1 + p)
+            {
+                r.w[p] = T(g.weight[e]);
+                r.mask |= 1u << p;
+            }
+    }
+    return r;
+}
+
+// sum over the set offsets of w[p] * v[p], accumulated in offset order from zero.
+template <typename T>
+__device__ __forceinline__ T restrict_sum(const RestrictAxis<T>& r, T v0, T v1, T v2, T v3)
+{
+    T s = T(0);
+    if (r.mask & 1u)
+        s += r.w[0] * v0;
+    if (r.mask & 2u)
+        s += r.w[1] * v1;
+    if (r.mask & 4u)
+        s += r.w[2] * v2;
+    if (r.mask & 8u)
+        s += r.w[3] * v3;
+    return s;
+}
+
 // Pre-smoothing of `count` tiles (tiles[0 .. count)): four sweeps from zero, the residual, the
 // pre-smoothed solution of the output cells and the transpose-bilinear restriction into the
 // coarse right-hand side (PressureMultigrid.cpp:398-402, 204-231, 233-276).
@@ -214,13 +260,16 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
 {
     using Shape = TileShape<T, K, true, WARPS>;
     using S = Stage<T, W, K, true, WARPS>;
-    constexpr int NT = 32 * WARPS;
     extern __shared__ __align__(128) char stage[];
     __shared__ uint64_t bar;
     __shared__ Edges<T, WARPS> edges;
-    __shared__ __align__(16) T res[Shape::RY][Shape::RX]; // written as pairs
     constexpr int OCX = Shape::OX / 2, OCY = Shape::OY / 2;
-    __shared__ Gather gather_x[OCX], gather_y[OCY];
+    // The restriction runs in two passes. Along x, lane L sums fine columns 2L-1 .. 2L+2 of
+    // every row from registers into lines[row][L]: that is coarse column L - HALO/2 of the
+    // tile. Along y, coarse row q sums lines HALO-1+2q .. HALO+2+2q.
+    static_assert(Shape::HALO % 2 == 0 && Shape::HALO / 2 >= 2 && OCX + Shape::HALO / 2 <= 31, "restriction lanes");
+    __shared__ T lines[Shape::RY][32];
+    __shared__ RestrictAxis<T> along_y[OCY];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     allow_dependents();
     // TMA writes shared memory at 128-byte aligned addresses only; a misplaced staging buffer is
@@ -262,18 +311,15 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
         const LevelDesc& C = g.lev[level + 1];
         const int X0 = t.x0 - Shape::HALO, Y0 = t.y0 - Shape::HALO;
         const int cx0 = t.x0 / 2, cy0 = t.y0 / 2;
-        // The restriction tables of the tile's coarse cells, while its boxes land.
-        Gather gt{};
-        if (threadIdx.x < OCX)
-        {
-            if (cx0 + int(threadIdx.x) < C.w)
-                gt = L.rx[cx0 + threadIdx.x];
-        }
-        else if (threadIdx.x < OCX + OCY)
-        {
-            if (cy0 + int(threadIdx.x) - OCX < C.h)
-                gt = L.ry[cy0 + threadIdx.x - OCX];
-        }
+        // The restriction weights of the tile's coarse cells, while its boxes land.
+        const int qx = lane - Shape::HALO / 2, cx = cx0 + qx;
+        const bool column = qx >= 0 && qx < OCX && cx < C.w;
+        RestrictAxis<T> along_x{};
+        if (column)
+            along_x = restrict_axis<T>(L.rx, cx);
+        RestrictAxis<T> row_weights{};
+        if (threadIdx.x < OCY && cy0 + int(threadIdx.x) < C.h)
+            row_weights = restrict_axis<T>(L.ry, cy0 + threadIdx.x);
         const bool done = g.state->done != 0;
         const double mean_r = level == 0 ? g.state->mean_r : 0.0;
         const bool ok = mbarrier_wait(&bar, parity);
@@ -309,8 +355,8 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
             strip_sweep<T, K, WARPS>(s, edges, 0, false, 0, lane, warp);
             strip_sweep<T, K, WARPS>(s, edges, 1, false, 1, lane, warp);
         }
-        // Residual of every cell into shared memory; the edge buffers hold the final values:
-        // buffer 0 colour 0, buffer 1 colour 1.
+        // Residual of every cell, summed along x into the lines; the edge buffers hold the final
+        // values: buffer 0 colour 0, buffer 1 colour 1.
         const T above_a = edges.bottom[1][warp][lane], above_b = edges.bottom[0][warp][lane];
         const T below_a = edges.top[0][warp + 2][lane], below_b = edges.top[1][warp + 2][lane];
         T* pre = static_cast<T*>(L.pre);
@@ -329,13 +375,19 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
             const T wua = k == 0 ? s.ua : s.da[k - 1];
             const T wub = k == 0 ? s.ub : s.db[k - 1];
             const T a = s.a[k], b = s.b[k];
-            const T pa = (s.wl[k] * (a - left) + s.wm[k] * (a - b)) + (wua * (a - ua) + s.da[k] * (a - na));
+            // Lane 0's cells are halo columns whose residual neither the output nor the
+            // restriction reads (its first lane, HALO/2, takes columns from HALO - 1 on).
+            T wl = __shfl_up_sync(0xffffffffu, s.wr[k], 1); // every lane takes part
+            wl = lane == 0 ? T(0) : wl;
+            const T pa = (wl * (a - left) + s.wm[k] * (a - b)) + (wua * (a - ua) + s.da[k] * (a - na));
             const T pb = (s.wm[k] * (b - a) + s.wr[k] * (b - right)) + (wub * (b - ub) + s.db[k] * (b - nb));
             const int y = warp * K + k;
-            typename Pair<T>::type rr;
-            rr.x = s.ia[k] > T(0) ? s.ra[k] - pa : T(0);
-            rr.y = s.ib[k] > T(0) ? s.rb[k] - pb : T(0);
-            *reinterpret_cast<typename Pair<T>::type*>(&res[y][2 * lane]) = rr;
+            const T res_a = s.ia[k] > T(0) ? s.ra[k] - pa : T(0);
+            const T res_b = s.ib[k] > T(0) ? s.rb[k] - pb : T(0);
+            // Lanes 0 and 31 hold no coarse column, so the wrapped shuffles are never summed.
+            const T res_left = __shfl_up_sync(0xffffffffu, res_b, 1);
+            const T res_right = __shfl_down_sync(0xffffffffu, res_a, 1);
+            lines[y][lane] = restrict_sum(along_x, res_left, res_a, res_b, res_right);
             const int gy = Y0 + y;
             if (y >= Shape::HALO && y < Shape::HALO + Shape::OY && 2 * lane >= Shape::HALO &&
                 2 * lane < Shape::HALO + Shape::OX && gy < L.h && gx < L.w)
@@ -352,33 +404,25 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
                     pre[idx] = a;
             }
         }
-        if (threadIdx.x < OCX)
-            gather_x[threadIdx.x] = gt;
-        else if (threadIdx.x < OCX + OCY)
-            gather_y[threadIdx.x - OCX] = gt;
+        if (threadIdx.x < OCY)
+            along_y[threadIdx.x] = row_weights;
         __syncthreads();
-        // Transpose-bilinear restriction onto the tile's coarse cells.
+        // Along y onto the tile's coarse cells: warp w takes coarse rows w, w + WARPS, ...
+        // The next tile rewrites lines and along_y only after its first barrier, which every
+        // thread reaches after finishing here.
         T* crhs = static_cast<T*>(C.rhs);
-        for (int q = threadIdx.x; q < OCX * OCY; q += NT)
+        if (column)
         {
-            const int qx = q % OCX, qy = q / OCX;
-            const int cx = cx0 + qx, cy = cy0 + qy;
-            if (cx >= C.w || cy >= C.h)
-                continue;
-            const Gather& gxr = gather_x[qx];
-            const Gather& gyr = gather_y[qy];
-            T value = T(0);
-            for (int iy = 0; iy < gyr.count; ++iy)
+            for (int qy = warp; qy < OCY; qy += WARPS)
             {
-                const int y = gyr.index[iy] - Y0;
-                T line = T(0);
-                for (int ix = 0; ix < gxr.count; ++ix)
-                    line += T(gxr.weight[ix]) * res[y][gxr.index[ix] - X0];
-                value += T(gyr.weight[iy]) * line;
+                const int cy = cy0 + qy;
+                if (cy >= C.h)
+                    break;
+                const int r = Shape::HALO - 1 + 2 * qy;
+                crhs[padded_index32(C.S, cx, cy)] =
+                    restrict_sum(along_y[qy], lines[r][lane], lines[r + 1][lane], lines[r + 2][lane], lines[r + 3][lane]);
             }
-            crhs[padded_index32(C.S, cx, cy)] = value;
         }
-        __syncthreads(); // res and the gather tables are rewritten by the next tile
     }
 }
 
@@ -397,6 +441,7 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
     __shared__ Edges<T, WARPS> edges;
     __shared__ Interp interp_y[Shape::RY];
     __shared__ double4 total;
+    __shared__ double2 warp_pairs[WARPS];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     allow_dependents();
     // TMA writes shared memory at 128-byte aligned addresses only; a misplaced staging buffer is
@@ -430,6 +475,7 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
         stage_issue_data<T, W, K, false, WARPS>(grids[t.grid], level, set, t.x0 - Shape::HALO, t.y0 - Shape::HALO, stage, &bar);
     }
     unsigned parity = 0;
+    int run = 0; // level 0: tiles of the current grid finished since the last count
     for (; i < count; i += gridDim.x)
     {
         const Tile t = tiles[i];
@@ -567,11 +613,35 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
         }
         if (level == 0)
         {
-            if (arrive_last<NT>(g, t.index, g.post_tiles, block_reduce4<NT>(make_double4(sz, srz, 0, 0), 0), &total, 0))
+            // One (sum z, sum r z) pair per tile, the warps' sums added in warp order; the CTA
+            // counts its tiles of this grid once, when its next tile belongs to another grid or
+            // it has none left. warp_pairs is rewritten only after the next tile's barriers.
+            double2* pairs = reinterpret_cast<double2*>(g.partial);
+            const double wz = warp_sum(sz), wrz = warp_sum(srz);
+            if (lane == 0)
+                warp_pairs[warp] = make_double2(wz, wrz);
+            __syncthreads();
+            if (threadIdx.x == 0)
             {
-                // The strips hold r - mean r: sum r z = sum (r - mean r) z + mean r sum z.
-                if (threadIdx.x == 0)
-                    finish_preconditioner(state, total.x, total.y + state.mean_r * total.x);
+                double2 acc = warp_pairs[0];
+#pragma unroll
+                for (int w = 1; w < WARPS; ++w)
+                {
+                    acc.x += warp_pairs[w].x;
+                    acc.y += warp_pairs[w].y;
+                }
+                pairs[t.index] = acc;
+            }
+            ++run;
+            if (next >= count || tiles[next].grid != t.grid)
+            {
+                if (arrive_run<NT>(g, pairs, run, g.post_tiles, g.post_tiles, &total))
+                {
+                    // The strips hold r - mean r: sum r z = sum (r - mean r) z + mean r sum z.
+                    if (threadIdx.x == 0)
+                        finish_preconditioner(state, total.x, total.y + state.mean_r * total.x);
+                }
+                run = 0;
             }
         }
     }

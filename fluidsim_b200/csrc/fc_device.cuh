@@ -115,6 +115,10 @@ struct LevelDesc
     const void* right_h;
     const void* down_h;
     float wscale;
+    // Inverse diagonal of the levels the strip kernels smooth, in the working precision: 1 / the
+    // sum of a cell's four face weights (as the kernels decode them), 0 for a cell with no open
+    // face and in the padding. Written by the rebuild.
+    void* inv;
     void* rhs;           // levels >= 1 (level 0 reads the PCG residual minus its mean)
     void* pre;           // pre-smoothed solution, read by the post-smoothing of the same level
     void* sol;           // final solution of the level (level 0: the PCG vector z)
@@ -173,6 +177,10 @@ template <typename T> __device__ __forceinline__ T load_as(const void* base, lon
 {
     return static_cast<const T*>(base)[i];
 }
+
+// Correctly rounded reciprocal in the working precision.
+__device__ __forceinline__ float reciprocal(float v) { return __frcp_rn(v); }
+__device__ __forceinline__ double reciprocal(double v) { return 1.0 / v; }
 
 __device__ __forceinline__ double warp_sum(double v)
 {

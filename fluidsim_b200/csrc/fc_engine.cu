@@ -247,17 +247,20 @@ struct Grid
 };
 
 // Strip heights of the smoothing kernels: tall strips (less halo overhead) on levels with
-// enough tiles to fill the GPU twice, short ones (half the per-CTA latency) below that.
+// enough tiles to fill the GPU twice, short ones (half the per-CTA latency) below that, and the
+// strips of the 16-warp wide regions (FP32 only).
 template <typename T> struct Tiling;
 template <> struct Tiling<float>
 {
     static constexpr int big = 8;
     static constexpr int small = 4;
+    static constexpr int wide = 8;
 };
 template <> struct Tiling<double>
 {
     static constexpr int big = 6;
     static constexpr int small = 4;
+    static constexpr int wide = 6;
 };
 
 struct TileSizes
@@ -280,7 +283,7 @@ TileSizes tile_sizes(int precision, int shape)
     if (shape == kShapeShort)
         return tile_sizes_of<float, Tiling<float>::small, 8>();
     if (shape == kShapeWide)
-        return tile_sizes_of<float, Tiling<float>::big, 16>();
+        return tile_sizes_of<float, Tiling<float>::wide, 16>();
     return tile_sizes_of<float, Tiling<float>::big, 8>();
 }
 
@@ -356,8 +359,9 @@ void encode_stage_maps(Grid& g)
     const CUtensorMapDataType vt = fp64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
     const int big = fp64 ? Tiling<double>::big : Tiling<float>::big;
     const int small = fp64 ? Tiling<double>::small : Tiling<float>::small;
+    const int wide = fp64 ? Tiling<double>::wide : Tiling<float>::wide;
     // Strip rows of a region per shape: warps x strip height.
-    const int rows[kShapes] = {8 * big, 8 * small, 16 * big};
+    const int rows[kShapes] = {8 * big, 8 * small, 16 * wide};
     std::vector<CUtensorMap> maps(g.levels.size() * kShapes * kMapsPerSet);
     std::memset(maps.data(), 0, maps.size() * sizeof(CUtensorMap));
     const GridDesc& d = g.desc;
@@ -382,6 +386,7 @@ void encode_stage_maps(Grid& g)
                 encode_box(m[kMapDown], L.down, vt, g.elem, L.S, L.h + 2, 72, bh);
             }
             encode_box(m[kMapVector], l == 0 ? d.r : L.rhs, vt, g.elem, L.S, L.h + 2, 72, bh);
+            encode_box(m[kMapInverse], L.inv, vt, g.elem, L.S, L.h + 2, 72, bh);
             encode_box(m[kMapPre], L.pre, vt, g.elem, L.S, L.h + 2, 72, bh);
             encode_box(m[kMapCoarse], C.sol, vt, g.elem, C.S, C.h + 2, 40, rows[set] / 2 + 4);
         }
@@ -473,6 +478,8 @@ size_t allocate_grid(Grid& g, bool allocate = true)
         const size_t padded = size_t(L.S) * (L.h + 2);
         add(&ld.right, padded * elem);
         add(&ld.down, padded * elem);
+        if (l + 1 < g.levels.size())
+            add(&ld.inv, padded * elem);
         // Mixed precision: FP16 copies of the weights of the coarse levels the strip kernels
         // smooth (the fine level keeps FP32 weights).
         if (g.precision == FC_PRECISION_MIXED && l >= 1 && l + 1 < g.levels.size())
@@ -930,6 +937,8 @@ template <typename T> void launch_rebuild(Plan& p)
     if (p.precision == FC_PRECISION_MIXED)
         for (int l = 1; l < p.max_tail; ++l)
             FC_LAUNCH(k_weights_half, dim3(ceil_div(p.padded_max[l], 256), p.n()), 256, 0, s, p.d_desc, l);
+    for (int l = 0; l + 1 < p.max_levels; ++l)
+        FC_LAUNCH(k_inverse_diagonal<T>, dim3(ceil_div(p.padded_max[l], 256), p.n()), 256, 0, s, p.d_desc, l);
 }
 
 // Resident CTAs of the persistent smoothing kernels: two per SM in FP32, one in FP64 (their
@@ -971,12 +980,12 @@ void launch_smooth_kernel(Plan& p, int level, int set, bool dependent, cudaStrea
 
 template <typename T, typename W, bool PRE> void launch_smooth_shape(Plan& p, int level, bool dependent, cudaStream_t s)
 {
-    constexpr int KB = Tiling<T>::big, KS = Tiling<T>::small;
+    constexpr int KB = Tiling<T>::big, KS = Tiling<T>::small, KW = Tiling<T>::wide;
     const int shape = PRE ? p.shape_pre[level] : p.shape_post[level];
     if constexpr (sizeof(T) == 4)
     {
         if (shape == kShapeWide)
-            return launch_smooth_kernel<T, KB, W, PRE, 16>(p, level, shape, dependent, s);
+            return launch_smooth_kernel<T, KW, W, PRE, 16>(p, level, shape, dependent, s);
     }
     if (shape == kShapeShort)
         launch_smooth_kernel<T, KS, W, PRE, 8>(p, level, shape, dependent, s);

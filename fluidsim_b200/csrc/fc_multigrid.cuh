@@ -103,6 +103,57 @@ __global__ void k_weights_half(const GridDesc* grids, int level)
     }
 }
 
+// Inverse diagonal of a level the strip kernels smooth (blockIdx.y = grid): for each cell
+// 1 / (((left + right) + up) + down) over its face weights, decoded as the kernels decode them
+// (the FP16 copies times the level scale on mixed-precision coarse levels), 0 where the sum is
+// not positive and in the padding. The kernels formed it per region before; the sum and the
+// reciprocal are the same, so the smoothing is unchanged (PressureMultigrid.cpp:104-117).
+template <typename T> __global__ void k_inverse_diagonal(const GridDesc* grids, int level)
+{
+    const GridDesc& g = grids[blockIdx.y];
+    if (level + 1 >= g.levels)
+        return;
+    const LevelDesc& L = g.lev[level];
+    const int n = L.S * (L.h + 2);
+    T* inv = static_cast<T*>(L.inv);
+    bool half = false;
+    if constexpr (sizeof(T) == 4)
+        half = L.right_h != nullptr && level >= 1 && level < g.tail;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        const int x = i % L.S - kPadX, y = i / L.S - 1;
+        T value = T(0);
+        if (x >= 0 && x < L.w && y >= 0 && y < L.h)
+        {
+            T wl, wr, wu, wd;
+            if constexpr (sizeof(T) == 4)
+            {
+                if (half)
+                {
+                    const __half* rh = static_cast<const __half*>(L.right_h);
+                    const __half* dh = static_cast<const __half*>(L.down_h);
+                    wl = __half2float(rh[i - 1]) * L.wscale;
+                    wr = __half2float(rh[i]) * L.wscale;
+                    wu = __half2float(dh[i - L.S]) * L.wscale;
+                    wd = __half2float(dh[i]) * L.wscale;
+                }
+            }
+            if (!half)
+            {
+                const T* right = static_cast<const T*>(L.right);
+                const T* down = static_cast<const T*>(L.down);
+                wl = right[i - 1];
+                wr = right[i];
+                wu = down[i - L.S];
+                wd = down[i];
+            }
+            const T diag = ((wl + wr) + wu) + wd;
+            value = diag > T(0) ? reciprocal(diag) : T(0);
+        }
+        inv[i] = value;
+    }
+}
+
 // Coarse level `level + 1` from `level`. PressureMultigrid.cpp:142-202 (coarsen) and
 // :104-117 (the diagonal is recomputed on the fly wherever it is needed).
 template <typename T> __global__ void k_coarsen(const GridDesc* grids, const Tile* tiles, int level)

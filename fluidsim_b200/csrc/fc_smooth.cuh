@@ -50,8 +50,6 @@ template <> struct Pair<double>
     using type = double2;
 };
 
-__device__ __forceinline__ float reciprocal(float v) { return __frcp_rn(v); }
-__device__ __forceinline__ double reciprocal(double v) { return 1.0 / v; }
 
 // r - mean in the working precision (FP64 keeps the reference's exact subtraction).
 __device__ __forceinline__ float minus_mean(float r, double mean) { return r - float(mean); }
@@ -79,38 +77,26 @@ template <typename T, int WARPS = 8> struct Edges
     T bottom[2][WARPS + 2][32];
 };
 
-// Strip assembly: the staged loads (fc_stage.cuh) fill the weights, right-hand side and the
-// raw left weight of lane 0; strip_finish forms the left weights, inverse diagonals and the
-// masked right-hand side.
-template <typename T, int K> struct StripRaw
-{
-    T wl0[K];
-};
-
+// Strip assembly: the staged loads (fc_stage.cuh) fill the weights, inverse diagonals and
+// right-hand side; strip_finish masks the right-hand side (and on the fine level subtracts the
+// residual's mean).
 template <typename T, int K>
-__device__ __forceinline__ void strip_finish(Strip<T, K>& s, const StripRaw<T, K>& raw, int level, int lane, double mean_r)
+__device__ __forceinline__ void strip_finish(Strip<T, K>& s, int level, double mean_r)
 {
 #pragma unroll
     for (int k = 0; k < K; ++k)
     {
-        const T shifted = __shfl_up_sync(0xffffffffu, s.wr[k], 1);
-        const T wl = lane == 0 ? raw.wl0[k] : shifted;
-        const T up_a = k == 0 ? s.ua : s.da[k - 1];
-        const T up_b = k == 0 ? s.ub : s.db[k - 1];
-        const T diag_a = ((wl + s.wm[k]) + up_a) + s.da[k];
-        const T diag_b = ((s.wm[k] + s.wr[k]) + up_b) + s.db[k];
-        s.ia[k] = diag_a > T(0) ? reciprocal(diag_a) : T(0);
-        s.ib[k] = diag_b > T(0) ? reciprocal(diag_b) : T(0);
-        // A cell with no open face takes no part (inside obstacles, a 1x1 grid, the padding).
+        // A cell with no open face takes no part (inside obstacles, a 1x1 grid, the padding):
+        // its inverse diagonal is zero.
         if (level == 0)
         {
-            s.ra[k] = diag_a > T(0) ? minus_mean(s.ra[k], mean_r) : T(0);
-            s.rb[k] = diag_b > T(0) ? minus_mean(s.rb[k], mean_r) : T(0);
+            s.ra[k] = s.ia[k] > T(0) ? minus_mean(s.ra[k], mean_r) : T(0);
+            s.rb[k] = s.ib[k] > T(0) ? minus_mean(s.rb[k], mean_r) : T(0);
         }
         else
         {
-            s.ra[k] = diag_a > T(0) ? s.ra[k] : T(0);
-            s.rb[k] = diag_b > T(0) ? s.rb[k] : T(0);
+            s.ra[k] = s.ia[k] > T(0) ? s.ra[k] : T(0);
+            s.rb[k] = s.ib[k] > T(0) ? s.rb[k] : T(0);
         }
     }
 }

@@ -31,16 +31,16 @@ template <typename T, typename W, int K, bool PRE, int WARPS = 8> struct Stage
     static constexpr size_t WB = round(size_t(BW) * BH * sizeof(W));
     static constexpr size_t VB = round(size_t(BW) * BH * sizeof(T));
     static constexpr size_t CB = PRE ? 0 : round(size_t(CBW) * CBH * sizeof(T));
-    static constexpr size_t right = 0, down = WB, vec = 2 * WB, pre = 2 * WB + VB;
+    static constexpr size_t right = 0, down = WB, inv = 2 * WB, vec = 2 * WB + VB, pre = 2 * WB + 2 * VB;
     static constexpr size_t coarse = PRE ? pre : pre + VB;
     static constexpr size_t bytes = coarse + CB;
     // Bytes the boxes of one tile deliver (full boxes, zero-filled parts included).
-    static constexpr unsigned tx = unsigned(2 * BW * BH * sizeof(W) + (PRE ? 1 : 2) * BW * BH * sizeof(T) +
+    static constexpr unsigned tx = unsigned(2 * BW * BH * sizeof(W) + (PRE ? 2 : 3) * BW * BH * sizeof(T) +
                                             (PRE ? 0 : CBW * CBH * sizeof(T)));
 };
 
 // Tensor maps of a grid: per level, per region shape (kShapeTall, kShapeShort, kShapeWide),
-// five maps.
+// six maps.
 enum RegionShape
 {
     kShapeTall = 0,  // 8 warps of the larger strip height
@@ -56,7 +56,8 @@ enum StageMap
     kMapVector = 2, // level 0: the PCG residual r; coarser levels: the restricted rhs
     kMapPre = 3,
     kMapCoarse = 4, // the next level's solution (post)
-    kMapsPerSet = 5
+    kMapInverse = 5, // the level's inverse diagonal
+    kMapsPerSet = 6
 };
 constexpr int kTensorMapBytes = 128;
 
@@ -72,9 +73,9 @@ template <typename E> __host__ __device__ __forceinline__ int box_start(int v)
     return sizeof(E) >= 4 ? (v & ~3) : (v & ~7);
 }
 
-// Issues the boxes of the tile whose region starts at (X0, Y0); one thread. The weights are
-// written by no kernel of the projection, so a kernel may issue them before waiting on its
-// predecessor (stage_issue_weights); the other boxes follow (stage_issue_data). The barrier
+// Issues the boxes of the tile whose region starts at (X0, Y0); one thread. The weights and the
+// inverse diagonal are written by no kernel of the projection, so a kernel may issue them before
+// waiting on its predecessor (stage_issue_weights); the other boxes follow (stage_issue_data). The barrier
 // expects the bytes of all of them from the first call.
 template <typename T, typename W, int K, bool PRE, int WARPS>
 __device__ __forceinline__ void stage_issue_weights(const GridDesc& g, int level, int set, int X0, int Y0, char* stage,
@@ -87,6 +88,7 @@ __device__ __forceinline__ void stage_issue_weights(const GridDesc& g, int level
     mbarrier_expect_tx(bar, S::tx);
     tma_load_2d(stage + S::right, stage_map(g, level, set, kMapRight), bw, by, bar);
     tma_load_2d(stage + S::down, stage_map(g, level, set, kMapDown), bw, by, bar);
+    tma_load_2d(stage + S::inv, stage_map(g, level, set, kMapInverse), box_start<T>(X0 + 1), by, bar);
 }
 
 template <typename T, typename W, int K, bool PRE, int WARPS>
@@ -122,18 +124,10 @@ template <> __device__ __forceinline__ float2 weight_pair<__half>(const __half* 
     const float2 v = __half22float2(*reinterpret_cast<const __half2*>(p));
     return make_float2(v.x * scale, v.y * scale);
 }
-template <typename W> __device__ __forceinline__ float weight_one(const W* p, float scale);
-template <> __device__ __forceinline__ float weight_one<float>(const float* p, float) { return *p; }
-template <> __device__ __forceinline__ float weight_one<__half>(const __half* p, float scale)
-{
-    return __half2float(*p) * scale;
-}
 
-// Strip registers from the staged boxes: weights, inverse-diagonal inputs and right-hand side
-// (the values strip_weights and strip_rhs read from global memory).
+// Strip registers from the staged boxes: weights, inverse diagonals and right-hand side.
 template <typename T, typename W, int K, bool PRE, int WARPS>
-__device__ __forceinline__ void stage_strip(Strip<T, K>& s, StripRaw<T, K>& raw, const char* stage, int X0,
-    float wscale, int lane, int warp)
+__device__ __forceinline__ void stage_strip(Strip<T, K>& s, const char* stage, int X0, float wscale, int lane, int warp)
 {
     using S = Stage<T, W, K, PRE, WARPS>;
     using P = typename Pair<T>::type;
@@ -143,6 +137,7 @@ __device__ __forceinline__ void stage_strip(Strip<T, K>& s, StripRaw<T, K>& raw,
     const W* right = reinterpret_cast<const W*>(stage + S::right);
     const W* down = reinterpret_cast<const W*>(stage + S::down);
     const T* vec = reinterpret_cast<const T*>(stage + S::vec);
+    const T* inv = reinterpret_cast<const T*>(stage + S::inv);
 #pragma unroll
     for (int k = 0; k < K; ++k)
     {
@@ -156,7 +151,6 @@ __device__ __forceinline__ void stage_strip(Strip<T, K>& s, StripRaw<T, K>& raw,
             s.wr[k] = w2.y;
             s.da[k] = d2.x;
             s.db[k] = d2.y;
-            raw.wl0[k] = lane == 0 ? T(right[rw - 1]) : T(0);
         }
         else
         {
@@ -166,11 +160,13 @@ __device__ __forceinline__ void stage_strip(Strip<T, K>& s, StripRaw<T, K>& raw,
             s.wr[k] = w2.y;
             s.da[k] = d2.x;
             s.db[k] = d2.y;
-            raw.wl0[k] = lane == 0 ? weight_one<W>(right + rw - 1, wscale) : 0.0f;
         }
         const P r2 = *reinterpret_cast<const P*>(vec + r);
         s.ra[k] = r2.x;
         s.rb[k] = r2.y;
+        const P i2 = *reinterpret_cast<const P*>(inv + r);
+        s.ia[k] = i2.x;
+        s.ib[k] = i2.y;
     }
     const int u = (warp * K) * S::BW + cw;
     if constexpr (sizeof(T) == 8)
@@ -327,11 +323,10 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
             return;
         parity ^= 1u;
         Strip<T, K> s;
-        StripRaw<T, K> raw;
         if (!done)
         {
-            stage_strip<T, W, K, true, WARPS>(s, raw, stage, X0, L.wscale, lane, warp);
-            strip_finish<T, K>(s, raw, level, lane, mean_r);
+            stage_strip<T, W, K, true, WARPS>(s, stage, X0, L.wscale, lane, warp);
+            strip_finish<T, K>(s, level, mean_r);
         }
         __syncthreads();
         // The staging buffer is free: the next tile's boxes stream in while this one sweeps.
@@ -506,12 +501,11 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
             return;
         parity ^= 1u;
         Strip<T, K> s;
-        StripRaw<T, K> raw;
         if (threadIdx.x < Shape::RY)
             interp_y[threadIdx.x] = iy;
         if (!done)
         {
-            stage_strip<T, W, K, false, WARPS>(s, raw, stage, X0, L.wscale, lane, warp);
+            stage_strip<T, W, K, false, WARPS>(s, stage, X0, L.wscale, lane, warp);
             // The pre-smoothed values of the strip.
             const T* pre = reinterpret_cast<const T*>(stage + S::pre);
             const int c = (X0 + 2 - box_start<T>(X0 + 1)) + 2 * lane;
@@ -523,7 +517,7 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
                 s.a[k] = ab.x;
                 s.b[k] = ab.y;
             }
-            strip_finish<T, K>(s, raw, level, lane, mean_r);
+            strip_finish<T, K>(s, level, mean_r);
         }
         __syncthreads();
         if (!done)

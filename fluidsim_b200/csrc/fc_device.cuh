@@ -226,9 +226,51 @@ template <int NT> __device__ double4 block_reduce4(double4 v, int max_mask)
     return out;
 }
 
+// The last block's fold of a grid's per-tile partials, in tile order (deterministic): each
+// thread folds a contiguous run (loads batched ahead of the sums, read from L2), then the runs
+// are combined by block_reduce4. Leaves the result in *total (thread 0's view) and resets the
+// counter. Must be called by all threads of the block, after the arrival's fence.
+template <int NT> __device__ void fold_partials(const GridDesc& g, int tiles, double4* total, int max_mask)
+{
+    double4 acc = make_double4(0, 0, 0, 0);
+    const int per = (tiles + NT - 1) / NT;
+    const int first = threadIdx.x * per;
+    const int last = min(tiles, first + per);
+    constexpr int kBatch = 4;
+    const double2* slots = reinterpret_cast<const double2*>(g.partial);
+    for (int t0 = first; t0 < last; t0 += kBatch)
+    {
+        double2 lo[kBatch], hi[kBatch];
+#pragma unroll
+        for (int u = 0; u < kBatch; ++u)
+            if (t0 + u < last)
+            {
+                lo[u] = __ldcg(slots + 2 * (t0 + u));
+                hi[u] = __ldcg(slots + 2 * (t0 + u) + 1);
+            }
+#pragma unroll
+        for (int u = 0; u < kBatch; ++u)
+            if (t0 + u < last)
+            {
+                acc.x = (max_mask & 1) ? fmax(acc.x, lo[u].x) : acc.x + lo[u].x;
+                acc.y = (max_mask & 2) ? fmax(acc.y, lo[u].y) : acc.y + lo[u].y;
+                acc.z = (max_mask & 4) ? fmax(acc.z, hi[u].x) : acc.z + hi[u].x;
+                acc.w = (max_mask & 8) ? fmax(acc.w, hi[u].y) : acc.w + hi[u].y;
+            }
+    }
+    const double4 out = block_reduce4<NT>(acc, max_mask);
+    if (threadIdx.x == 0)
+    {
+        *total = out;
+        *g.counter = 0u;
+        __threadfence();
+    }
+    __syncthreads();
+}
+
 // Publishes this tile's partial and reports whether this block is the last of its grid to
-// arrive; the last block then reads every partial in tile order (deterministic) and resets
-// the counter. Must be called by all threads of the block.
+// arrive; the last block then folds every partial (fold_partials). Must be called by all
+// threads of the block.
 template <int NT>
 __device__ bool arrive_last(const GridDesc& g, int tile_index, int tiles, double4 mine, double4* total, int max_mask)
 {
@@ -244,29 +286,29 @@ __device__ bool arrive_last(const GridDesc& g, int tile_index, int tiles, double
     if (!is_last)
         return false;
     __threadfence();
-    // The last block folds the partials in fixed order.
-    double4 acc = make_double4(0, 0, 0, 0);
-    // Each thread folds a contiguous run, then runs are combined in order.
-    const int per = (tiles + NT - 1) / NT;
-    const int first = threadIdx.x * per;
-    const int last = min(tiles, first + per);
-    for (int t = first; t < last; ++t)
-    {
-        const volatile double* slot = reinterpret_cast<const volatile double*>(&g.partial[t]);
-        const double4 s = make_double4(slot[0], slot[1], slot[2], slot[3]);
-        acc.x = (max_mask & 1) ? fmax(acc.x, s.x) : acc.x + s.x;
-        acc.y = (max_mask & 2) ? fmax(acc.y, s.y) : acc.y + s.y;
-        acc.z = (max_mask & 4) ? fmax(acc.z, s.z) : acc.z + s.z;
-        acc.w = (max_mask & 8) ? fmax(acc.w, s.w) : acc.w + s.w;
-    }
-    const double4 out = block_reduce4<NT>(acc, max_mask);
+    fold_partials<NT>(g, tiles, total, max_mask);
+    return true;
+}
+
+// Arrival of a persistent kernel's run of `run_tiles` tiles of one grid whose partials thread 0
+// already wrote to g.partial[tile]: the CTA counts the run once instead of once per tile, and
+// the last CTA to arrive folds all `tiles` partials (fold_partials). Must be called by all
+// threads of the block.
+template <int NT>
+__device__ bool arrive_count(const GridDesc& g, int run_tiles, int tiles, double4* total, int max_mask)
+{
+    __shared__ int is_last;
     if (threadIdx.x == 0)
     {
-        *total = out;
-        *g.counter = 0u;
-        __threadfence();
+        __threadfence(); // the partials before the count
+        const unsigned int ticket = atomicAdd(g.counter, unsigned(run_tiles));
+        is_last = ticket + unsigned(run_tiles) == unsigned(tiles);
     }
     __syncthreads();
+    if (!is_last)
+        return false;
+    __threadfence();
+    fold_partials<NT>(g, tiles, total, max_mask);
     return true;
 }
 

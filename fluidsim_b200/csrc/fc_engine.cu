@@ -943,7 +943,7 @@ template <typename T> void launch_rebuild(Plan& p)
 
 // Resident CTAs of the persistent smoothing kernels: two per SM in FP32, one in FP64 (their
 // launch bounds and shared-memory staging).
-int smoothing_ctas(bool fp64)
+int sm_count()
 {
     static int sms = 0;
     if (!sms)
@@ -952,8 +952,10 @@ int smoothing_ctas(bool fp64)
         check(cudaGetDevice(&device), "device");
         check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "SM count");
     }
-    return sms * (fp64 ? 1 : 2);
+    return sms;
 }
+
+int smoothing_ctas(bool fp64) { return sm_count() * (fp64 ? 1 : 2); }
 
 template <typename T, int K, typename W, bool PRE, int WARPS>
 void launch_smooth_kernel(Plan& p, int level, int set, bool dependent, cudaStream_t s)
@@ -1029,7 +1031,8 @@ template <typename T> void launch_iteration(Plan& p, bool use_mg, int parity)
 {
     cudaStream_t s = p.stream;
     FC_LAUNCH_DEP(k_direction_operator<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec), parity);
-    FC_LAUNCH_DEP(k_update<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec), parity);
+    FC_LAUNCH_DEP(k_update<T>, std::min(p.vec.count, kUpdateCtasPerSm * sm_count()), kVecThreads, 0, s, p.d_desc,
+        p.at(p.vec), p.vec.count, parity);
     FC_LAUNCH_DEP(k_true_residual<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec), 0);
     launch_precondition<T>(p, use_mg);
 }

@@ -491,8 +491,11 @@ __global__ void __launch_bounds__(kVecThreads) k_direction_operator(const GridDe
 
 // p += alpha d ; r -= alpha q ; residual stats. FluidGridCPU.cpp:1600-1641.
 // The padded halo and row padding of d, q, r and p are zero, so the update runs over the whole
-// padded array as one flat stream: tile t of the grid takes the t-th equal slice, four cells per
-// thread and load, every load of the slice issued before the arithmetic.
+// padded array as one flat stream cut into one equal slice per vector tile. The kernel is
+// persistent (three CTAs per SM walk the slices of every grid), each thread takes two quads of
+// four cells per step with every load of the step issued before the arithmetic, and a CTA
+// counts its slices of a grid once; the per-slice partials and their fold are those of one CTA
+// per slice.
 template <typename T> struct Quad;
 template <> struct Quad<float>
 {
@@ -503,90 +506,106 @@ template <> struct Quad<double>
     using type = double4;
 };
 
+constexpr int kUpdateCtasPerSm = 2;
+
 template <typename T>
-__global__ void __launch_bounds__(kVecThreads) k_update(const GridDesc* grids, const Tile* tiles, int parity)
+__global__ void __launch_bounds__(kVecThreads, kUpdateCtasPerSm)
+    k_update(const GridDesc* grids, const Tile* tiles, int count, int parity)
 {
     using Q = typename Quad<T>::type;
-    constexpr int U = 4; // quads per thread
+    constexpr int U = 2; // quads per thread and step
     allow_dependents();
-    const Tile t = tiles[blockIdx.x];
-    const GridDesc& g = grids[t.grid];
-    SolveState& s = *g.state;
     dependency_wait();
-    if (s.done)
-        return;
-    const T* d = static_cast<const T*>(g.d[parity ^ 1]);
-    const T* q = static_cast<const T*>(g.q);
-    T* r = static_cast<T*>(g.r);
-    const double alpha = s.rz / s.dq;
-    // The padded length S * (H + 2) is a multiple of 8; slices are whole quads.
-    const long long quads = (long long)g.S * (g.H + 2) / 4;
-    const long long per = (quads + g.vec_tiles - 1) / g.vec_tiles;
-    const long long first = per * t.index;
-    const long long last = min(quads, first + per);
-    double sum = 0.0, mx = 0.0, sq = 0.0;
-    for (long long base = first + threadIdx.x; base < last; base += (long long)kVecThreads * U)
-    {
-        Q dv[U], qv[U], rv[U];
-        double4 pv[U];
-#pragma unroll
-        for (int u = 0; u < U; ++u)
-        {
-            const long long j = base + (long long)u * kVecThreads;
-            if (j < last)
-            {
-                dv[u] = reinterpret_cast<const Q*>(d)[j];
-                qv[u] = reinterpret_cast<const Q*>(q)[j];
-                rv[u] = reinterpret_cast<const Q*>(r)[j];
-                pv[u] = reinterpret_cast<const double4*>(g.p)[j];
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < U; ++u)
-        {
-            const long long j = base + (long long)u * kVecThreads;
-            if (j >= last)
-                continue;
-            double4 pp = pv[u];
-            pp.x += alpha * double(dv[u].x);
-            pp.y += alpha * double(dv[u].y);
-            pp.z += alpha * double(dv[u].z);
-            pp.w += alpha * double(dv[u].w);
-            Q rr;
-            rr.x = T(double(rv[u].x) - alpha * double(qv[u].x));
-            rr.y = T(double(rv[u].y) - alpha * double(qv[u].y));
-            rr.z = T(double(rv[u].z) - alpha * double(qv[u].z));
-            rr.w = T(double(rv[u].w) - alpha * double(qv[u].w));
-            reinterpret_cast<double4*>(g.p)[j] = pp;
-            reinterpret_cast<Q*>(r)[j] = rr;
-            const double e[4] = {double(rr.x), double(rr.y), double(rr.z), double(rr.w)};
-#pragma unroll
-            for (int c = 0; c < 4; ++c)
-            {
-                sum += e[c];
-                mx = fmax(mx, fabs(e[c]));
-                sq += e[c] * e[c];
-            }
-        }
-    }
     __shared__ double4 total;
-    if (arrive_last<kVecThreads>(g, t.index, g.vec_tiles, block_reduce4<kVecThreads>(make_double4(sum, mx, sq, 0), 2), &total, 2))
+    int run = 0; // slices of the current grid finished since the last count
+    for (int i = blockIdx.x; i < count; i += gridDim.x)
     {
-        if (threadIdx.x == 0)
+        const Tile t = tiles[i];
+        const GridDesc& g = grids[t.grid];
+        SolveState& s = *g.state;
+        if (s.done)
+            continue;
+        const T* d = static_cast<const T*>(g.d[parity ^ 1]);
+        const T* q = static_cast<const T*>(g.q);
+        T* r = static_cast<T*>(g.r);
+        const double alpha = s.rz / s.dq;
+        // The padded length S * (H + 2) is a multiple of 8; slices are whole quads.
+        const long long quads = (long long)g.S * (g.H + 2) / 4;
+        const long long per = (quads + g.vec_tiles - 1) / g.vec_tiles;
+        const long long first = per * t.index;
+        const long long last = min(quads, first + per);
+        double sum = 0.0, mx = 0.0, sq = 0.0;
+        for (long long base = first + threadIdx.x; base < last; base += (long long)kVecThreads * U)
         {
-            s.iterations += 1;
-            const double maximum = isfinite(total.x) ? total.y : INFINITY;
-            s.sum_r = total.x;
-            s.max_r = maximum;
-            s.sumsq_r = total.z;
-            s.mean_r = total.x * s.inv_cells;
-            if (stop_rule_met(s, maximum, total.z))
-                s.verify = 1;
-            else if (s.iterations >= s.max_iterations)
+            Q dv[U], qv[U], rv[U];
+            double4 pv[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u)
             {
-                s.status = kIterationLimit;
-                s.done = 1;
+                const long long j = base + (long long)u * kVecThreads;
+                if (j < last)
+                {
+                    dv[u] = reinterpret_cast<const Q*>(d)[j];
+                    qv[u] = reinterpret_cast<const Q*>(q)[j];
+                    rv[u] = reinterpret_cast<const Q*>(r)[j];
+                    pv[u] = reinterpret_cast<const double4*>(g.p)[j];
+                }
             }
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+            {
+                const long long j = base + (long long)u * kVecThreads;
+                if (j >= last)
+                    continue;
+                double4 pp = pv[u];
+                pp.x += alpha * double(dv[u].x);
+                pp.y += alpha * double(dv[u].y);
+                pp.z += alpha * double(dv[u].z);
+                pp.w += alpha * double(dv[u].w);
+                Q rr;
+                rr.x = T(double(rv[u].x) - alpha * double(qv[u].x));
+                rr.y = T(double(rv[u].y) - alpha * double(qv[u].y));
+                rr.z = T(double(rv[u].z) - alpha * double(qv[u].z));
+                rr.w = T(double(rv[u].w) - alpha * double(qv[u].w));
+                reinterpret_cast<double4*>(g.p)[j] = pp;
+                reinterpret_cast<Q*>(r)[j] = rr;
+                const double e[4] = {double(rr.x), double(rr.y), double(rr.z), double(rr.w)};
+#pragma unroll
+                for (int c = 0; c < 4; ++c)
+                {
+                    sum += e[c];
+                    mx = fmax(mx, fabs(e[c]));
+                    sq += e[c] * e[c];
+                }
+            }
+        }
+        const double4 part = block_reduce4<kVecThreads>(make_double4(sum, mx, sq, 0), 2);
+        if (threadIdx.x == 0)
+            g.partial[t.index] = part;
+        ++run;
+        const int next = i + gridDim.x;
+        if (next >= count || tiles[next].grid != t.grid)
+        {
+            if (arrive_count<kVecThreads>(g, run, g.vec_tiles, &total, 2))
+            {
+                if (threadIdx.x == 0)
+                {
+                    s.iterations += 1;
+                    const double maximum = isfinite(total.x) ? total.y : INFINITY;
+                    s.sum_r = total.x;
+                    s.max_r = maximum;
+                    s.sumsq_r = total.z;
+                    s.mean_r = total.x * s.inv_cells;
+                    if (stop_rule_met(s, maximum, total.z))
+                        s.verify = 1;
+                    else if (s.iterations >= s.max_iterations)
+                    {
+                        s.status = kIterationLimit;
+                        s.done = 1;
+                    }
+                }
+            }
+            run = 0;
         }
     }
 }

@@ -30,10 +30,10 @@ METRIC = "MAC cells projected/s at 1e-6 residual"
 UNIT = "cells/s"
 L2_FLUSH_BYTES = 256 << 20
 # Algorithmic bytes per fine cell of the two fused fine-level smoothing kernels (FP32):
-# pre reads r, right, down and writes the pre-smoothed solution plus a quarter cell of coarse
-# rhs; post reads the pre-smoothed solution, a quarter cell of coarse solution, r, right, down
-# and writes z.
-ALGORITHMIC_BYTES = {0: 4 + 4 + 4 + 4 + 1, 1: 4 + 1 + 4 + 4 + 4 + 4}
+# pre reads r, right, down and the inverse diagonal and writes the pre-smoothed solution plus a
+# quarter cell of coarse rhs; post reads the pre-smoothed solution, a quarter cell of coarse
+# solution, r, right, down and the inverse diagonal and writes z.
+ALGORITHMIC_BYTES = {0: 4 + 4 + 4 + 4 + 4 + 1, 1: 4 + 1 + 4 + 4 + 4 + 4 + 4}
 KERNEL_NAMES = {0: "k_smooth_pre (fine level)", 1: "k_smooth_post (fine level)"}
 
 
@@ -50,6 +50,8 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-serve", action="store_true", help="skip the serving (continuous batching) measurement")
     p.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision comparison")
+    p.add_argument("--tail-cells", type=int, default=0,
+                   help="multigrid tail threshold in cells (0: autotuned); pins the schedule for profiling")
     p.add_argument("--serve-requests", type=int, default=16)
     p.add_argument("--serve-steps", type=int, default=300)
     p.add_argument("--launch", choices=["graph", "stream"], default="graph",
@@ -217,9 +219,14 @@ def run_cuda(args, world, rank, local_rank):
     work = FluidGrid(size, size, scene.cell_size, "fp32")
     work.configureMaterials([scene.liquid_density], [scene.gas_density])
     work.setGravityY(scene.gravity)
-    # The multigrid schedule picked by the autotuner (timed V-cycles, outside the timed steps).
+    # The multigrid schedule picked by the autotuner (timed V-cycles, outside the timed steps),
+    # or the one --tail-cells pins.
     work.copyStateFrom(pristine)
-    tail_cells, vcycle_ms = work.autotune(10)
+    if args.tail_cells > 0:
+        work.setTailCells(args.tail_cells)
+        tail_cells, vcycle_ms = args.tail_cells, None
+    else:
+        tail_cells, vcycle_ms = work.autotune(10)
     stream = torch.cuda.ExternalStream(work.stream())
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
 

@@ -292,7 +292,8 @@ TileSizes tile_sizes(int precision, int shape)
 void choose_tail(Grid& g)
 {
     const int limit_cells = g.elem == 4 ? g.tail_cells : std::min(g.tail_cells, 1024);
-    const size_t limit_bytes = 200 * 1024;
+    // Dynamic shared memory of the tail; its register strips' edge rows take up to 35 KB more.
+    const size_t limit_bytes = 184 * 1024;
     std::vector<int> w, h;
     for (auto& l : g.levels)
         w.push_back(l.w), h.push_back(l.h);
@@ -300,7 +301,9 @@ void choose_tail(Grid& g)
     for (int l = 0; l < n; ++l)
     {
         const size_t bytes = tail_bytes(w.data(), h.data(), l, n, g.elem);
-        if (w[l] * h[l] <= limit_cells && bytes <= limit_bytes)
+        // The tail's register strips hold levels of up to kTailMaxSide x kTailMaxSide cells (the
+        // coarsest level, at most 64 cells, always fits).
+        if (w[l] * h[l] <= limit_cells && w[l] <= kTailMaxSide && h[l] <= kTailMaxSide && bytes <= limit_bytes)
         {
             g.tail = l;
             g.tail_smem = bytes;
@@ -1039,9 +1042,9 @@ template <typename T> void launch_iteration(Plan& p, bool use_mg, int parity)
 
 template <typename T> void set_kernel_attributes(Plan& p)
 {
-    if (p.tail_smem > 48 * 1024)
-        check(cudaFuncSetAttribute(k_mg_tail<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(p.tail_smem)),
-            "tail shared memory");
+    // Always opted in: the tail's static edge rows count against the 48 KB default as well.
+    check(cudaFuncSetAttribute(k_mg_tail<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(p.tail_smem)),
+        "tail shared memory");
 }
 
 // Projection set-up: states, right-hand side, warm start, first residual, first z.
@@ -2030,10 +2033,10 @@ double time_kernel(Grid& g, int kernel, int repeats)
     running.done = 0;
     running.restart = 1;
     check(cudaMemcpyAsync(g.desc.state, &running, sizeof(running), cudaMemcpyHostToDevice, p.stream), "state");
-    cudaEvent_t start, stop;
-    check(cudaEventCreate(&start), "event");
-    check(cudaEventCreate(&stop), "event");
-    float ms = 0.0f;
+    // One event pair per launch: the state reset between launches stays outside the timing.
+    std::vector<cudaEvent_t> marks(2 * size_t(repeats));
+    for (cudaEvent_t& e : marks)
+        check(cudaEventCreate(&e), "event");
     dispatch(g.precision, [&](auto zero)
     {
         using T = decltype(zero);
@@ -2049,19 +2052,25 @@ double time_kernel(Grid& g, int kernel, int repeats)
             }
         };
         launch(); // warm
-        check(cudaEventRecord(start, p.stream), "event");
         for (int i = 0; i < repeats; ++i)
         {
             // The level-0 post kernel folds a reduction that may mark the solve done.
             check(cudaMemcpyAsync(&g.desc.state->done, &running.done, sizeof(int), cudaMemcpyHostToDevice, p.stream), "state");
+            check(cudaEventRecord(marks[2 * i], p.stream), "event");
             launch();
+            check(cudaEventRecord(marks[2 * i + 1], p.stream), "event");
         }
-        check(cudaEventRecord(stop, p.stream), "event");
     });
-    check(cudaEventSynchronize(stop), "event");
-    check(cudaEventElapsedTime(&ms, start, stop), "event");
-    cudaEventDestroy(start);
-    cudaEventDestroy(stop);
+    check(cudaEventSynchronize(marks.back()), "event");
+    double ms = 0.0;
+    for (int i = 0; i < repeats; ++i)
+    {
+        float one = 0.0f;
+        check(cudaEventElapsedTime(&one, marks[2 * i], marks[2 * i + 1]), "event");
+        ms += one;
+    }
+    for (cudaEvent_t e : marks)
+        cudaEventDestroy(e);
     check(cudaMemcpyAsync(g.desc.state, &saved, sizeof(saved), cudaMemcpyHostToDevice, p.stream), "state");
     check(cudaStreamSynchronize(p.stream), "state");
     return double(ms) / repeats;

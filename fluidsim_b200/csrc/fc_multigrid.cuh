@@ -15,6 +15,7 @@
 #pragma once
 
 #include "fc_device.cuh"
+#include "fc_smooth.cuh"
 
 namespace fc
 {
@@ -361,91 +362,196 @@ __host__ __device__ inline size_t tail_bytes(const int* w, const int* h, int fir
     return bytes;
 }
 
-// One half-sweep pair (a full red-black sweep) over a tail level; warp = row, lane = column pair.
-template <typename T> __device__ void tail_smooth(const TailLevel<T> L, bool reverse, bool from_zero)
+// The tail smooths each level as register strips, the same arithmetic as the strip kernels
+// (fc_smooth.cuh) with the whole level resident: warp w holds rows 2w and 2w + 1, lane j columns
+// 2j and 2j + 1, so a level of up to 64 x 64 cells fits the 32 warps (the tail only takes such
+// levels). Rows and columns outside the level hold zero weights, inverse diagonals and values,
+// and the edge rows of the warps pass through shared memory once per half-sweep.
+constexpr int kTailK = 2;
+constexpr int kTailMaxSide = 2 * 32;
+static_assert(kTailWarps * kTailK == kTailMaxSide, "tail strips cover 64 rows");
+
+template <typename T> using TailEdges = Edges<T, kTailWarps>;
+
+// Strip registers of level L: weights, inverse diagonals, masked right-hand side and, for the
+// post-smoothing, the pre-smoothed solution.
+template <typename T>
+__device__ __forceinline__ void tail_load_strip(const TailLevel<T>& L, Strip<T, kTailK>& s, bool with_solution, int lane,
+    int warp)
 {
-    T* const m = tail_array<T>();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int pass = 0; pass < 2; ++pass)
+    const T* m = tail_array<T>();
+    const int x = 2 * lane;
+    const bool col_a = x < L.w, col_b = x + 1 < L.w;
+    const int y0 = kTailK * warp;
+    s.ua = col_a && y0 < L.h ? m[L.down + L.at(x, y0 - 1)] : T(0);
+    s.ub = col_b && y0 < L.h ? m[L.down + L.at(x + 1, y0 - 1)] : T(0);
+#pragma unroll
+    for (int k = 0; k < kTailK; ++k)
     {
-        const int colour = reverse ? 1 - pass : pass;
-        const bool skip = from_zero && pass == 0;
-        for (int y = warp; y < L.h; y += kTailWarps)
-        {
-            for (int x = 2 * lane + ((colour + y) & 1); x < L.w; x += 64)
-            {
-                const int i = L.at(x, y);
-                T value = m[L.rhs + i];
-                if (!skip)
-                    value = value + ((m[L.right + i - 1] * m[L.sol + i - 1] + m[L.right + i] * m[L.sol + i + 1]) +
-                                        (m[L.down + i - L.s] * m[L.sol + i - L.s] + m[L.down + i] * m[L.sol + i + L.s]));
-                m[L.sol + i] = value * m[L.inv + i];
-            }
-        }
-        __syncthreads();
+        const int y = y0 + k;
+        const bool in_a = col_a && y < L.h, in_b = col_b && y < L.h;
+        const int i = in_a ? L.at(x, y) : 0;
+        s.wm[k] = in_a ? m[L.right + i] : T(0);
+        s.da[k] = in_a ? m[L.down + i] : T(0);
+        s.ia[k] = in_a ? m[L.inv + i] : T(0);
+        s.ra[k] = in_a && s.ia[k] > T(0) ? m[L.rhs + i] : T(0);
+        s.a[k] = in_a && with_solution ? m[L.sol + i] : T(0);
+        s.wr[k] = in_b ? m[L.right + i + 1] : T(0);
+        s.db[k] = in_b ? m[L.down + i + 1] : T(0);
+        s.ib[k] = in_b ? m[L.inv + i + 1] : T(0);
+        s.rb[k] = in_b && s.ib[k] > T(0) ? m[L.rhs + i + 1] : T(0);
+        s.b[k] = in_b && with_solution ? m[L.sol + i + 1] : T(0);
     }
 }
 
-template <typename T> __device__ void tail_restrict(const TailLevel<T> F, const TailLevel<T> Cl)
+template <typename T>
+__device__ __forceinline__ void tail_store_solution(const TailLevel<T>& L, const Strip<T, kTailK>& s, int lane, int warp)
+{
+    T* m = tail_array<T>();
+    const int x = 2 * lane;
+#pragma unroll
+    for (int k = 0; k < kTailK; ++k)
+    {
+        const int y = kTailK * warp + k;
+        if (y >= L.h || x >= L.w)
+            continue;
+        const int i = L.at(x, y);
+        m[L.sol + i] = s.a[k];
+        if (x + 1 < L.w)
+            m[L.sol + i + 1] = s.b[k];
+    }
+}
+
+// Pre-smoothing of tail level L: four red-black sweeps from zero, the residual, and its
+// transpose-bilinear restriction into C's right-hand side (PressureMultigrid.cpp:398-402,
+// 204-231, 233-276). The pre-smoothed solution stays in L.sol for the post-smoothing.
+template <typename T>
+__device__ void tail_pre(const TailLevel<T> L, const TailLevel<T> C, TailEdges<T>& edges, int lane, int warp)
 {
     T* const m = tail_array<T>();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int y = warp; y < F.h; y += kTailWarps)
+    Strip<T, kTailK> s;
+    tail_load_strip(L, s, false, lane, warp);
+    strip_sweep<T, kTailK, kTailWarps>(s, edges, 0, true, 0, lane, warp);
+    strip_sweep<T, kTailK, kTailWarps>(s, edges, 1, false, 1, lane, warp);
+#pragma unroll 1
+    for (int sweep = 1; sweep < 4; ++sweep)
     {
-        for (int x = lane; x < F.w; x += 32)
+        strip_sweep<T, kTailK, kTailWarps>(s, edges, 0, false, 0, lane, warp);
+        strip_sweep<T, kTailK, kTailWarps>(s, edges, 1, false, 1, lane, warp);
+    }
+    // Residual from registers; the edge buffers hold the final values (buffer 0 colour 0,
+    // buffer 1 colour 1). Cells without an open face pass no residual down.
+    const T above_a = edges.bottom[1][warp][lane], above_b = edges.bottom[0][warp][lane];
+    const T below_a = edges.top[0][warp + 2][lane], below_b = edges.top[1][warp + 2][lane];
+    const int x = 2 * lane;
+#pragma unroll
+    for (int k = 0; k < kTailK; ++k)
+    {
+        T left = __shfl_up_sync(0xffffffffu, s.b[k], 1);
+        T right = __shfl_down_sync(0xffffffffu, s.a[k], 1);
+        T wl = __shfl_up_sync(0xffffffffu, s.wr[k], 1);
+        left = lane == 0 ? T(0) : left;
+        right = lane == 31 ? T(0) : right;
+        wl = lane == 0 ? T(0) : wl;
+        const T ua = k == 0 ? above_a : s.a[k - 1];
+        const T ub = k == 0 ? above_b : s.b[k - 1];
+        const T na = k == kTailK - 1 ? below_a : s.a[k + 1];
+        const T nb = k == kTailK - 1 ? below_b : s.b[k + 1];
+        const T wua = k == 0 ? s.ua : s.da[k - 1];
+        const T wub = k == 0 ? s.ub : s.db[k - 1];
+        const T a = s.a[k], b = s.b[k];
+        const T pa = (wl * (a - left) + s.wm[k] * (a - b)) + (wua * (a - ua) + s.da[k] * (a - na));
+        const T pb = (s.wm[k] * (b - a) + s.wr[k] * (b - right)) + (wub * (b - ub) + s.db[k] * (b - nb));
+        const int y = kTailK * warp + k;
+        if (y >= L.h || x >= L.w)
+            continue;
+        const int i = L.at(x, y);
+        m[L.sol + i] = a;
+        m[L.res + i] = s.ia[k] > T(0) ? s.ra[k] - pa : T(0);
+        if (x + 1 < L.w)
         {
-            const int i = F.at(x, y);
-            const T center = m[F.sol + i];
-            const T product =
-                (m[F.right + i - 1] * (center - m[F.sol + i - 1]) + m[F.right + i] * (center - m[F.sol + i + 1])) +
-                (m[F.down + i - F.s] * (center - m[F.sol + i - F.s]) + m[F.down + i] * (center - m[F.sol + i + F.s]));
-            // Cells without an open face pass no residual down (keeps the cycle symmetric).
-            m[F.res + i] = m[F.inv + i] > T(0) ? m[F.rhs + i] - product : T(0);
+            m[L.sol + i + 1] = b;
+            m[L.res + i + 1] = s.ib[k] > T(0) ? s.rb[k] - pb : T(0);
         }
     }
     __syncthreads();
-    const Gather* rx = tail_table<const Gather>(F.rx);
-    const Gather* ry = tail_table<const Gather>(F.ry);
-    for (int cy = warp; cy < Cl.h; cy += kTailWarps)
+    // Restriction: coarse cell (cx, cy) sums fine rows 2cy-1 .. 2cy+2 of the x-sums of fine
+    // columns 2cx-1 .. 2cx+2 (only the offsets its tables list are read).
+    const Gather* rx = tail_table<const Gather>(L.rx);
+    const Gather* ry = tail_table<const Gather>(L.ry);
+    for (int q = threadIdx.x; q < C.w * C.h; q += kTailThreads)
     {
-        const Gather gy = ry[cy];
-        for (int cx = lane; cx < Cl.w; cx += 32)
+        const int cx = q % C.w, cy = q / C.w;
+        const RestrictAxis<T> ax = restrict_axis<T>(rx, cx), ay = restrict_axis<T>(ry, cy);
+        T line[4];
+#pragma unroll
+        for (int p = 0; p < 4; ++p)
         {
-            const Gather& gx = rx[cx];
-            double value = 0.0;
-            for (int iy = 0; iy < gy.count; ++iy)
+            line[p] = T(0);
+            if (ay.mask & (1u << p))
             {
-                double line = 0.0;
-                for (int ix = 0; ix < gx.count; ++ix)
-                    line += gx.weight[ix] * double(m[F.res + F.at(gx.index[ix], gy.index[iy])]);
-                value += gy.weight[iy] * line;
+                const int row = L.res + L.at(2 * cx - 1, 2 * cy - 1 + p);
+                T v[4];
+#pragma unroll
+                for (int e = 0; e < 4; ++e)
+                    v[e] = (ax.mask & (1u << e)) ? m[row + e] : T(0);
+                line[p] = restrict_sum(ax, v[0], v[1], v[2], v[3]);
             }
-            m[Cl.rhs + Cl.at(cx, cy)] = T(value);
         }
+        m[C.rhs + C.at(cx, cy)] = restrict_sum(ay, line[0], line[1], line[2], line[3]);
     }
     __syncthreads();
 }
 
-template <typename T> __device__ void tail_prolong(const TailLevel<T> Cl, const TailLevel<T> F)
+// Post-smoothing of tail level L: the bilinear prolongation of C's solution added to the
+// pre-smoothed solution, then four sweeps in reversed colour order (PressureMultigrid.cpp:
+// 403-407, 278-298). The result replaces L.sol.
+template <typename T>
+__device__ void tail_post(const TailLevel<T> C, const TailLevel<T> L, TailEdges<T>& edges, int lane, int warp)
 {
-    T* const m = tail_array<T>();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const Interp* px = tail_table<const Interp>(F.px);
-    const Interp* pys = tail_table<const Interp>(F.py);
-    for (int y = warp; y < F.h; y += kTailWarps)
+    const T* m = tail_array<T>();
+    Strip<T, kTailK> s;
+    tail_load_strip(L, s, true, lane, warp);
+    const Interp* px = tail_table<const Interp>(L.px);
+    const Interp* py = tail_table<const Interp>(L.py);
+    const int x = 2 * lane;
+    const bool col_a = x < L.w, col_b = x + 1 < L.w;
+    const Interp pa = col_a ? px[x] : Interp{0, 0, 0.0};
+    const Interp pb = col_b ? px[x + 1] : Interp{0, 0, 0.0};
+    const T wxa = T(pa.weight), wxb = T(pb.weight);
+#pragma unroll
+    for (int k = 0; k < kTailK; ++k)
     {
-        const Interp py = pys[y];
-        for (int x = lane; x < F.w; x += 32)
+        const int y = kTailK * warp + k;
+        if (y >= L.h)
+            continue;
+        const Interp iy = py[y];
+        const T wy = T(iy.weight);
+        const int top = C.sol + C.at(0, iy.first), bottom = C.sol + C.at(0, iy.second);
+        if (col_a)
         {
-            const Interp& p = px[x];
-            const double a = (1.0 - p.weight) * double(m[Cl.sol + Cl.at(p.first, py.first)]) +
-                             p.weight * double(m[Cl.sol + Cl.at(p.second, py.first)]);
-            const double b = (1.0 - p.weight) * double(m[Cl.sol + Cl.at(p.first, py.second)]) +
-                             p.weight * double(m[Cl.sol + Cl.at(p.second, py.second)]);
-            const int i = F.at(x, y);
-            m[F.sol + i] = T(double(m[F.sol + i]) + ((1.0 - py.weight) * a + py.weight * b));
+            const T u = (T(1) - wxa) * m[top + pa.first] + wxa * m[top + pa.second];
+            const T d = (T(1) - wxa) * m[bottom + pa.first] + wxa * m[bottom + pa.second];
+            s.a[k] = s.a[k] + ((T(1) - wy) * u + wy * d);
+        }
+        if (col_b)
+        {
+            const T u = (T(1) - wxb) * m[top + pb.first] + wxb * m[top + pb.second];
+            const T d = (T(1) - wxb) * m[bottom + pb.first] + wxb * m[bottom + pb.second];
+            s.b[k] = s.b[k] + ((T(1) - wy) * u + wy * d);
         }
     }
+    // The first half-sweep (colour 1) reads colour-0 edges from buffer 1.
+    edges.top[1][warp + 1][lane] = s.a[0];
+    edges.bottom[1][warp + 1][lane] = s.b[kTailK - 1];
+    __syncthreads();
+#pragma unroll 1
+    for (int sweep = 0; sweep < 4; ++sweep)
+    {
+        strip_sweep<T, kTailK, kTailWarps>(s, edges, 1, false, 0, lane, warp);
+        strip_sweep<T, kTailK, kTailWarps>(s, edges, 0, false, 1, lane, warp);
+    }
+    tail_store_solution(L, s, lane, warp);
     __syncthreads();
 }
 
@@ -566,6 +672,8 @@ template <typename T> __global__ void __launch_bounds__(kTailThreads) k_mg_tail(
     // zero.
     for (int i = threadIdx.x; i < array_elements; i += blockDim.x)
         m[i] = T(0);
+    __shared__ TailEdges<T> edges;
+    edges_clear<T, kTailK, kTailWarps>(edges);
     __shared__ CoarseInfo info;
     if (threadIdx.x < int(sizeof(CoarseInfo) / sizeof(int)))
         reinterpret_cast<int*>(&info)[threadIdx.x] = reinterpret_cast<const int*>(g.coarse)[threadIdx.x];
@@ -646,19 +754,10 @@ template <typename T> __global__ void __launch_bounds__(kTailThreads) k_mg_tail(
     __syncthreads();
 
     for (int l = first; l < last; ++l)
-    {
-        tail_smooth(lv[l], false, true);
-        for (int sweep = 1; sweep < 4; ++sweep)
-            tail_smooth(lv[l], false, false);
-        tail_restrict(lv[l], lv[l + 1]);
-    }
+        tail_pre(lv[l], lv[l + 1], edges, lane, warp);
     tail_solve_coarsest(lv[last], inverse_offset, vectors_offset, info);
     for (int l = last - 1; l >= first; --l)
-    {
-        tail_prolong(lv[l + 1], lv[l]);
-        for (int sweep = 0; sweep < 4; ++sweep)
-            tail_smooth(lv[l], true, false);
-    }
+        tail_post(lv[l + 1], lv[l], edges, lane, warp);
 
     // Hand the first tail level's solution to the finer post-smoothing (or to z).
     const TailLevel<T> F = lv[first];

@@ -201,52 +201,6 @@ __device__ __forceinline__ bool stage_failed(bool ok, SolveState* state)
     return false;
 }
 
-// One axis of the transpose-bilinear restriction for coarse cell c: the weights of fine cells
-// 2c-1, 2c, 2c+1, 2c+2 (bit p of `mask` set when fine cell 2c-1+p contributes). The table lists
-// its fine cells in ascending order, so summing by offset keeps the table's order; the host
-// checks that no entry falls outside the four offsets.
-template <typename T> struct RestrictAxis
-{
-    T w[4];
-    unsigned mask;
-};
-
-template <typename T> __device__ __forceinline__ RestrictAxis<T> restrict_axis(const Gather* table, int c)
-{
-    RestrictAxis<T> r;
-    r.mask = 0;
-    const Gather g = table[c];
-#pragma unroll
-    for (int p = 0; p < 4; ++p)
-    {
-        r.w[p] = T(0);
-#pragma unroll
-        for (int e = 0; e < 4; ++e)
-            if (e < g.count && g.index[e] == 2 * c - 1 + p)
-            {
-                r.w[p] = T(g.weight[e]);
-                r.mask |= 1u << p;
-            }
-    }
-    return r;
-}
-
-// sum over the set offsets of w[p] * v[p], accumulated in offset order from zero.
-template <typename T>
-__device__ __forceinline__ T restrict_sum(const RestrictAxis<T>& r, T v0, T v1, T v2, T v3)
-{
-    T s = T(0);
-    if (r.mask & 1u)
-        s += r.w[0] * v0;
-    if (r.mask & 2u)
-        s += r.w[1] * v1;
-    if (r.mask & 4u)
-        s += r.w[2] * v2;
-    if (r.mask & 8u)
-        s += r.w[3] * v3;
-    return s;
-}
-
 // Pre-smoothing of `count` tiles (tiles[0 .. count)): four sweeps from zero, the residual, the
 // pre-smoothed solution of the output cells and the transpose-bilinear restriction into the
 // coarse right-hand side (PressureMultigrid.cpp:398-402, 204-231, 233-276).

@@ -363,6 +363,24 @@ __device__ bool arrive_run(const GridDesc& g, const double2* pairs, int run_tile
     return true;
 }
 
+__device__ __forceinline__ void stage_failed_at(SolveState* state)
+{
+    state->status = kBreakdown;
+    state->done = 1;
+}
+
+// Records a failed wait (the staged data never arrived) on the tile's grid; returns true then.
+__device__ __forceinline__ bool stage_failed(bool ok, SolveState* state)
+{
+    if (__syncthreads_or(!ok))
+    {
+        if (threadIdx.x == 0)
+            stage_failed_at(state);
+        return true;
+    }
+    return false;
+}
+
 __device__ __forceinline__ bool finite_d(double v) { return isfinite(v); }
 
 // Programmatic dependent launch. The kernels of the PCG loop are launched so that each may

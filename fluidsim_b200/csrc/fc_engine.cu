@@ -292,8 +292,9 @@ TileSizes tile_sizes(int precision, int shape)
 void choose_tail(Grid& g)
 {
     const int limit_cells = g.elem == 4 ? g.tail_cells : std::min(g.tail_cells, 1024);
-    // Dynamic shared memory of the tail; its register strips' edge rows take up to 35 KB more.
-    const size_t limit_bytes = 184 * 1024;
+    // Dynamic shared memory of the tail, within the 227 KB a CTA may hold beside its static
+    // shared memory (the register strips' edge rows: 19 KB in FP32, 36 KB in FP64).
+    const size_t limit_bytes = (g.elem == 4 ? 208 : 188) * 1024;
     std::vector<int> w, h;
     for (auto& l : g.levels)
         w.push_back(l.w), h.push_back(l.h);

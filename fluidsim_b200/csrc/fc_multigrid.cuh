@@ -16,6 +16,7 @@
 
 #include "fc_device.cuh"
 #include "fc_smooth.cuh"
+#include "fc_tma.cuh"
 
 namespace fc
 {
@@ -331,12 +332,14 @@ constexpr int kTailWarps = kTailThreads / 32;
 // every access is a shared-memory access.
 extern __shared__ __align__(16) unsigned char tail_smem[];
 
+// A tail level in shared memory: its arrays keep the global padded layout (stride s = the
+// level's padded stride, halo row and columns of zeros), so that whole arrays arrive by bulk copy.
 template <typename T> struct TailLevel
 {
-    int w, h, s;                      // s = w + 2, one zero halo cell
+    int w, h, s;
     int right, down, inv, rhs, sol, res; // element offsets of the level's arrays
     int px, py, rx, ry;               // byte offsets of the transfer tables
-    __device__ int at(int x, int y) const { return (y + 1) * s + x + 1; }
+    __device__ int at(int x, int y) const { return (y + 1) * s + x + kPadX; }
 };
 
 template <typename T> __device__ __forceinline__ T* tail_array() { return reinterpret_cast<T*>(tail_smem); }
@@ -349,15 +352,16 @@ __host__ __device__ inline size_t align16(size_t n) { return (n + 15) / 16 * 16;
 __host__ __device__ inline int padded_index32_tail(int S, int x, int y) { return (y + 1) * S + x + kPadX; }
 
 // Shared-memory layout of the tail of a grid starting at level `first` (host and device
-// agree): per level six padded arrays, then the transfer tables, then the coarsest inverse and
-// two vectors of the coarsest solve.
+// agree): per level six padded arrays, then per smoothed level its four transfer tables (each
+// 16-byte aligned), then the coarsest inverse and two vectors of the coarsest solve.
 __host__ __device__ inline size_t tail_bytes(const int* w, const int* h, int first, int levels, size_t elem)
 {
     size_t bytes = 0;
     for (int l = first; l < levels; ++l)
-        bytes += align16(size_t(w[l] + 2) * (h[l] + 2) * 6 * elem);
+        bytes += align16(size_t(padded_stride(w[l])) * (h[l] + 2) * 6 * elem);
     for (int l = first; l + 1 < levels; ++l)
-        bytes += align16((w[l] + h[l]) * sizeof(Interp)) + align16((w[l + 1] + h[l + 1]) * sizeof(Gather));
+        bytes += align16(w[l] * sizeof(Interp)) + align16(h[l] * sizeof(Interp)) + align16(w[l + 1] * sizeof(Gather)) +
+                 align16(h[l + 1] * sizeof(Gather));
     bytes += align16(size_t(kMaxCoarse) * kMaxCoarse * sizeof(double)) + 2 * kMaxCoarse * sizeof(double);
     return bytes;
 }
@@ -373,11 +377,12 @@ static_assert(kTailWarps * kTailK == kTailMaxSide, "tail strips cover 64 rows");
 
 template <typename T> using TailEdges = Edges<T, kTailWarps>;
 
-// Strip registers of level L: weights, inverse diagonals, masked right-hand side and, for the
-// post-smoothing, the pre-smoothed solution.
+// Strip registers of level L: weights, inverse diagonals, masked right-hand side (less `mean`:
+// the residual's mean on the fine level, zero elsewhere) and, for the post-smoothing, the
+// pre-smoothed solution.
 template <typename T>
-__device__ __forceinline__ void tail_load_strip(const TailLevel<T>& L, Strip<T, kTailK>& s, bool with_solution, int lane,
-    int warp)
+__device__ __forceinline__ void tail_load_strip(const TailLevel<T>& L, Strip<T, kTailK>& s, bool with_solution,
+    double mean, int lane, int warp)
 {
     const T* m = tail_array<T>();
     const int x = 2 * lane;
@@ -394,12 +399,12 @@ __device__ __forceinline__ void tail_load_strip(const TailLevel<T>& L, Strip<T, 
         s.wm[k] = in_a ? m[L.right + i] : T(0);
         s.da[k] = in_a ? m[L.down + i] : T(0);
         s.ia[k] = in_a ? m[L.inv + i] : T(0);
-        s.ra[k] = in_a && s.ia[k] > T(0) ? m[L.rhs + i] : T(0);
+        s.ra[k] = in_a && s.ia[k] > T(0) ? minus_mean(m[L.rhs + i], mean) : T(0);
         s.a[k] = in_a && with_solution ? m[L.sol + i] : T(0);
         s.wr[k] = in_b ? m[L.right + i + 1] : T(0);
         s.db[k] = in_b ? m[L.down + i + 1] : T(0);
         s.ib[k] = in_b ? m[L.inv + i + 1] : T(0);
-        s.rb[k] = in_b && s.ib[k] > T(0) ? m[L.rhs + i + 1] : T(0);
+        s.rb[k] = in_b && s.ib[k] > T(0) ? minus_mean(m[L.rhs + i + 1], mean) : T(0);
         s.b[k] = in_b && with_solution ? m[L.sol + i + 1] : T(0);
     }
 }
@@ -426,11 +431,11 @@ __device__ __forceinline__ void tail_store_solution(const TailLevel<T>& L, const
 // transpose-bilinear restriction into C's right-hand side (PressureMultigrid.cpp:398-402,
 // 204-231, 233-276). The pre-smoothed solution stays in L.sol for the post-smoothing.
 template <typename T>
-__device__ void tail_pre(const TailLevel<T> L, const TailLevel<T> C, TailEdges<T>& edges, int lane, int warp)
+__device__ void tail_pre(const TailLevel<T> L, const TailLevel<T> C, double mean, TailEdges<T>& edges, int lane, int warp)
 {
     T* const m = tail_array<T>();
     Strip<T, kTailK> s;
-    tail_load_strip(L, s, false, lane, warp);
+    tail_load_strip(L, s, false, mean, lane, warp);
     strip_sweep<T, kTailK, kTailWarps>(s, edges, 0, true, 0, lane, warp);
     strip_sweep<T, kTailK, kTailWarps>(s, edges, 1, false, 1, lane, warp);
 #pragma unroll 1
@@ -507,11 +512,12 @@ __device__ void tail_pre(const TailLevel<T> L, const TailLevel<T> C, TailEdges<T
 // pre-smoothed solution, then four sweeps in reversed colour order (PressureMultigrid.cpp:
 // 403-407, 278-298). The result replaces L.sol.
 template <typename T>
-__device__ void tail_post(const TailLevel<T> C, const TailLevel<T> L, TailEdges<T>& edges, int lane, int warp)
+__device__ void tail_post(const TailLevel<T> C, const TailLevel<T> L, double mean, TailEdges<T>& edges, int lane,
+    int warp)
 {
     const T* m = tail_array<T>();
     Strip<T, kTailK> s;
-    tail_load_strip(L, s, true, lane, warp);
+    tail_load_strip(L, s, true, mean, lane, warp);
     const Interp* px = tail_table<const Interp>(L.px);
     const Interp* py = tail_table<const Interp>(L.py);
     const int x = 2 * lane;
@@ -640,7 +646,7 @@ template <typename T> __global__ void __launch_bounds__(kTailThreads) k_mg_tail(
         TailLevel<T>& L = lv[l];
         L.w = g.lev[l].w;
         L.h = g.lev[l].h;
-        L.s = L.w + 2;
+        L.s = g.lev[l].S;
         const int cells = L.s * (L.h + 2);
         const int base = cursor / int(sizeof(T));
         L.right = base;
@@ -655,109 +661,118 @@ template <typename T> __global__ void __launch_bounds__(kTailThreads) k_mg_tail(
     {
         TailLevel<T>& L = lv[l];
         L.px = cursor;
-        L.py = cursor + L.w * int(sizeof(Interp));
-        cursor += int(align16((L.w + L.h) * sizeof(Interp)));
+        cursor += int(align16(L.w * sizeof(Interp)));
+        L.py = cursor;
+        cursor += int(align16(L.h * sizeof(Interp)));
         L.rx = cursor;
-        L.ry = cursor + lv[l + 1].w * int(sizeof(Gather));
-        cursor += int(align16((lv[l + 1].w + lv[l + 1].h) * sizeof(Gather)));
+        cursor += int(align16(lv[l + 1].w * sizeof(Gather)));
+        L.ry = cursor;
+        cursor += int(align16(lv[l + 1].h * sizeof(Gather)));
     }
     const int inverse_offset = cursor;
     cursor += int(align16(size_t(kMaxCoarse) * kMaxCoarse * sizeof(double)));
     const int vectors_offset = cursor;
-    const int array_elements = lv[last].res + (lv[last].s * (lv[last].h + 2)) - lv[first].right;
 
-    // Everything the cycle touches except the right-hand side is written by no kernel of the
-    // projection (coefficients, transfer tables, the coarsest inverse and its unknown map), so it
-    // is copied in before waiting on the previous kernel; halos and the other arrays start at
-    // zero.
-    for (int i = threadIdx.x; i < array_elements; i += blockDim.x)
-        m[i] = T(0);
+    // Everything the cycle reads except the right-hand side is written by no kernel of the
+    // projection (weights, inverse diagonals, transfer tables, the coarsest inverse and its
+    // unknown map), so it is copied in by bulk copies before waiting on the previous kernel. The
+    // global arrays are 256-byte aligned slots of one allocation, so rounding a copy up to 16
+    // bytes stays inside it; every shared region is rounded the same way. The arrays that no
+    // copy fills are written before they are read (solutions, residuals, coarse right-hand
+    // sides), and only their in-level cells are read.
+    __shared__ uint64_t bar;
     __shared__ TailEdges<T> edges;
-    edges_clear<T, kTailK, kTailWarps>(edges);
     __shared__ CoarseInfo info;
+    if (threadIdx.x == 0)
+    {
+        mbarrier_init(&bar, 1);
+        fence_async_shared();
+    }
+    edges_clear<T, kTailK, kTailWarps>(edges);
     if (threadIdx.x < int(sizeof(CoarseInfo) / sizeof(int)))
         reinterpret_cast<int*>(&info)[threadIdx.x] = reinterpret_cast<const int*>(g.coarse)[threadIdx.x];
     __syncthreads();
-    for (int l = first; l <= last; ++l)
+    // Bulk copies write 16-byte aligned shared addresses only: a misplaced buffer is reported.
+    if ((smem_address(tail_smem) & 15u) != 0)
     {
-        const TailLevel<T> L = lv[l];
-        const LevelDesc& D = g.lev[l];
-        const T* right = static_cast<const T*>(D.right);
-        const T* down = static_cast<const T*>(D.down);
-        for (int y = warp; y < L.h; y += kTailWarps)
-        {
-            for (int x = lane; x < L.w; x += 32)
-            {
-                const int i = padded_index32_tail(D.S, x, y);
-                const int j = L.at(x, y);
-                m[L.right + j] = right[i];
-                m[L.down + j] = down[i];
-            }
-        }
-        if (l < last)
-        {
-            Interp* px = tail_table<Interp>(L.px);
-            Interp* py = tail_table<Interp>(L.py);
-            Gather* rx = tail_table<Gather>(L.rx);
-            Gather* ry = tail_table<Gather>(L.ry);
-            for (int i = threadIdx.x; i < L.w; i += blockDim.x)
-                px[i] = D.px[i];
-            for (int i = threadIdx.x; i < L.h; i += blockDim.x)
-                py[i] = D.py[i];
-            for (int i = threadIdx.x; i < lv[l + 1].w; i += blockDim.x)
-                rx[i] = D.rx[i];
-            for (int i = threadIdx.x; i < lv[l + 1].h; i += blockDim.x)
-                ry[i] = D.ry[i];
-        }
+        if (threadIdx.x == 0)
+            stage_failed_at(g.state);
+        return;
     }
+    if (threadIdx.x == 0)
     {
-        double* inverse = tail_table<double>(inverse_offset);
-        const int n = info.n;
-        for (int i = threadIdx.x; i < n * n; i += blockDim.x)
-            inverse[i] = g.coarse_inverse[i];
-    }
-    __syncthreads();
-    for (int l = first; l <= last; ++l)
-    {
-        const TailLevel<T> L = lv[l];
-        for (int y = warp; y < L.h; y += kTailWarps)
+        auto rounded = [](size_t bytes) { return unsigned(align16(bytes)); };
+        unsigned total = 0;
+        for (int l = first; l < last; ++l)
         {
-            for (int x = lane; x < L.w; x += 32)
-            {
-                const int j = L.at(x, y);
-                const T diag = ((m[L.right + j - 1] + m[L.right + j]) + m[L.down + j - L.s]) + m[L.down + j];
-                m[L.inv + j] = diag > T(0) ? T(1) / diag : T(0);
-            }
+            const size_t cells = size_t(lv[l].s) * (lv[l].h + 2);
+            total += 3 * rounded(cells * sizeof(T));
+            total += rounded(lv[l].w * sizeof(Interp)) + rounded(lv[l].h * sizeof(Interp)) +
+                     rounded(lv[l + 1].w * sizeof(Gather)) + rounded(lv[l + 1].h * sizeof(Gather));
         }
+        total += rounded(size_t(info.n) * info.n * sizeof(double));
+        mbarrier_expect_tx(&bar, total);
+        for (int l = first; l < last; ++l)
+        {
+            const TailLevel<T>& L = lv[l];
+            const LevelDesc& D = g.lev[l];
+            const unsigned bytes = rounded(size_t(L.s) * (L.h + 2) * sizeof(T));
+            bulk_load(m + L.right, D.right, bytes, &bar);
+            bulk_load(m + L.down, D.down, bytes, &bar);
+            bulk_load(m + L.inv, D.inv, bytes, &bar);
+            bulk_load(tail_smem + L.px, D.px, rounded(L.w * sizeof(Interp)), &bar);
+            bulk_load(tail_smem + L.py, D.py, rounded(L.h * sizeof(Interp)), &bar);
+            bulk_load(tail_smem + L.rx, D.rx, rounded(lv[l + 1].w * sizeof(Gather)), &bar);
+            bulk_load(tail_smem + L.ry, D.ry, rounded(lv[l + 1].h * sizeof(Gather)), &bar);
+        }
+        if (info.n > 0)
+            bulk_load(tail_smem + inverse_offset, g.coarse_inverse, rounded(size_t(info.n) * info.n * sizeof(double)), &bar);
     }
+    if (stage_failed(mbarrier_wait(&bar, 0), g.state))
+        return;
 
     // The right-hand side of the first tail level comes from the previous kernel.
     dependency_wait();
     if (state.done)
         return;
+    const double mean_r = first == 0 ? state.mean_r : 0.0;
     {
         const TailLevel<T> L = lv[first];
         const LevelDesc& D = g.lev[first];
         const T* rhs = first == 0 ? static_cast<const T*>(g.r) : static_cast<const T*>(D.rhs);
-        const double mean_r = first == 0 ? state.mean_r : 0.0;
-        for (int y = warp; y < L.h; y += kTailWarps)
+        if (first < last)
         {
-            for (int x = lane; x < L.w; x += 32)
+            // Raw; the strips mask it and take off the residual's mean (level 0).
+            if (threadIdx.x == 0)
             {
-                const int j = L.at(x, y);
-                const T b = rhs[padded_index32_tail(D.S, x, y)];
-                // Cells with no open face take no part.
-                m[L.rhs + j] = m[L.inv + j] > T(0) ? (first == 0 ? T(double(b) - mean_r) : b) : T(0);
+                const unsigned bytes = unsigned(align16(size_t(L.s) * (L.h + 2) * sizeof(T)));
+                mbarrier_expect_tx(&bar, bytes);
+                bulk_load(m + L.rhs, rhs, bytes, &bar);
             }
+            if (stage_failed(mbarrier_wait(&bar, 1), g.state))
+                return;
+        }
+        else
+        {
+            // A grid of at most 64 cells: the coarsest solve reads the masked right-hand side.
+            const T* right = static_cast<const T*>(D.right);
+            const T* down = static_cast<const T*>(D.down);
+            for (int q = threadIdx.x; q < L.w * L.h; q += kTailThreads)
+            {
+                const int x = q % L.w, y = q / L.w;
+                const int i = padded_index32_tail(D.S, x, y);
+                const T diag = ((right[i - 1] + right[i]) + down[i - D.S]) + down[i];
+                m[L.rhs + L.at(x, y)] = diag > T(0) ? (first == 0 ? minus_mean(rhs[i], mean_r) : rhs[i]) : T(0);
+            }
+            __syncthreads();
         }
     }
-    __syncthreads();
 
     for (int l = first; l < last; ++l)
-        tail_pre(lv[l], lv[l + 1], edges, lane, warp);
+        tail_pre(lv[l], lv[l + 1], l == 0 ? mean_r : 0.0, edges, lane, warp);
     tail_solve_coarsest(lv[last], inverse_offset, vectors_offset, info);
     for (int l = last - 1; l >= first; --l)
-        tail_post(lv[l + 1], lv[l], edges, lane, warp);
+        tail_post(lv[l + 1], lv[l], l == 0 ? mean_r : 0.0, edges, lane, warp);
 
     // Hand the first tail level's solution to the finer post-smoothing (or to z).
     const TailLevel<T> F = lv[first];

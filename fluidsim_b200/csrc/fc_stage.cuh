@@ -183,24 +183,6 @@ __device__ __forceinline__ void stage_strip(Strip<T, K>& s, const char* stage, i
     }
 }
 
-__device__ __forceinline__ void stage_failed_at(SolveState* state)
-{
-    state->status = kBreakdown;
-    state->done = 1;
-}
-
-// Records a failed wait (the staged data never arrived) on the tile's grid; returns true then.
-__device__ __forceinline__ bool stage_failed(bool ok, SolveState* state)
-{
-    if (__syncthreads_or(!ok))
-    {
-        if (threadIdx.x == 0)
-            stage_failed_at(state);
-        return true;
-    }
-    return false;
-}
-
 // Pre-smoothing of `count` tiles (tiles[0 .. count)): four sweeps from zero, the residual, the
 // pre-smoothed solution of the output cells and the transpose-bilinear restriction into the
 // coarse right-hand side (PressureMultigrid.cpp:398-402, 204-231, 233-276).

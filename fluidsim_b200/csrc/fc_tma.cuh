@@ -65,6 +65,16 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const void* map, int x, i
         : "memory");
 }
 
+// A contiguous copy of `bytes` from global into shared memory, counted on the barrier. Both
+// addresses must be 16-byte aligned and `bytes` a multiple of 16.
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, uint64_t* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_address(dst)),
+        "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(smem_address(bar))
+        : "memory");
+}
+
 __device__ __forceinline__ void prefetch_tensormap(const void* map)
 {
     asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");

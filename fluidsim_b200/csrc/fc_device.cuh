@@ -128,6 +128,10 @@ struct LevelDesc
     const Interp* py;
     const Gather* rx;    // coarse (l+1) cell -> fine cells of l
     const Gather* ry;
+    // The same per coarse column / row as offset weights in the working precision
+    // (RestrictAxis<T>, fc_smooth.cuh), built by the host from rx / ry.
+    const void* rwx;
+    const void* rwy;
 };
 
 struct GridDesc

@@ -120,7 +120,28 @@ struct HostLevel
     std::vector<double> cx, cy;
     std::vector<Interp> px, py; // this level -> next
     std::vector<Gather> rx, ry; // next level's cells -> this level
+    std::vector<unsigned char> rwx, rwy; // rx, ry as RestrictAxis<T> of the grid's precision
 };
+
+// Offset weights of a restriction table (what restrict_axis forms on the device).
+template <typename T> std::vector<unsigned char> restrict_weights(const std::vector<Gather>& table)
+{
+    std::vector<unsigned char> bytes(table.size() * sizeof(RestrictAxis<T>));
+    RestrictAxis<T>* out = reinterpret_cast<RestrictAxis<T>*>(bytes.data());
+    for (size_t c = 0; c < table.size(); ++c)
+    {
+        RestrictAxis<T> r{};
+        for (int p = 0; p < 4; ++p)
+            for (int e = 0; e < table[c].count; ++e)
+                if (table[c].index[e] == 2 * int(c) - 1 + p)
+                {
+                    r.w[p] = T(table[c].weight[e]);
+                    r.mask |= 1u << p;
+                }
+        out[c] = r;
+    }
+    return bytes;
+}
 
 // Halving until at most 64 cells; cell centres keep a shorter last cell on odd sizes.
 // PressureMultigrid.cpp:24-62.
@@ -471,7 +492,7 @@ size_t allocate_grid(Grid& g, bool allocate = true)
     add((void**)&g.mask, g.cells);
     add((void**)&d.lev[0].pre, padded0 * elem);
     std::vector<void*> cx(g.levels.size()), cy(g.levels.size()), px(g.levels.size()), py(g.levels.size()),
-        rx(g.levels.size()), ry(g.levels.size());
+        rx(g.levels.size()), ry(g.levels.size()), rwx(g.levels.size()), rwy(g.levels.size());
     for (size_t l = 0; l < g.levels.size(); ++l)
     {
         const HostLevel& L = g.levels[l];
@@ -505,6 +526,11 @@ size_t allocate_grid(Grid& g, bool allocate = true)
             add(&py[l], L.py.size() * sizeof(Interp));
             add(&rx[l], L.rx.size() * sizeof(Gather));
             add(&ry[l], L.ry.size() * sizeof(Gather));
+            HostLevel& H = g.levels[l];
+            H.rwx = g.elem == 8 ? restrict_weights<double>(L.rx) : restrict_weights<float>(L.rx);
+            H.rwy = g.elem == 8 ? restrict_weights<double>(L.ry) : restrict_weights<float>(L.ry);
+            add(&rwx[l], H.rwx.size());
+            add(&rwy[l], H.rwy.size());
         }
     }
     // TMA maps: per level, kShapes region shapes, kMapsPerSet maps of 128 bytes.
@@ -542,6 +568,10 @@ size_t allocate_grid(Grid& g, bool allocate = true)
             ld.py = static_cast<const Interp*>(py[l]);
             ld.rx = static_cast<const Gather*>(rx[l]);
             ld.ry = static_cast<const Gather*>(ry[l]);
+            check(cudaMemcpyAsync(rwx[l], L.rwx.data(), L.rwx.size(), cudaMemcpyHostToDevice, g.stream), "tables");
+            check(cudaMemcpyAsync(rwy[l], L.rwy.data(), L.rwy.size(), cudaMemcpyHostToDevice, g.stream), "tables");
+            ld.rwx = rwx[l];
+            ld.rwy = rwy[l];
         }
     }
     d.solid = nullptr;

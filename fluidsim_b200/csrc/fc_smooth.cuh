@@ -159,8 +159,9 @@ __device__ __forceinline__ void edges_clear(Edges<T, WARPS>& e)
 // One axis of the transpose-bilinear restriction for coarse cell c: the weights of fine cells
 // 2c-1, 2c, 2c+1, 2c+2 (bit p of `mask` set when fine cell 2c-1+p contributes). The table lists
 // its fine cells in ascending order, so summing by offset keeps the table's order; the host
-// checks that no entry falls outside the four offsets.
-template <typename T> struct RestrictAxis
+// checks that no entry falls outside the four offsets. The strip kernels read these per coarse
+// cell precomputed (LevelDesc::rwx, rwy); the tail forms them from its staged tables.
+template <typename T> struct alignas(16) RestrictAxis
 {
     T w[4];
     unsigned mask;

@@ -106,6 +106,18 @@ __device__ __forceinline__ void stage_issue_data(const GridDesc& g, int level, i
     }
 }
 
+// Fetches the descriptors of the data maps ahead of the data copies (one thread): their first
+// use after the dependency wait then costs only the copy.
+template <bool PRE> __device__ __forceinline__ void stage_prefetch_data_maps(const GridDesc& g, int level, int set)
+{
+    prefetch_tensormap(stage_map(g, level, set, kMapVector));
+    if (!PRE)
+    {
+        prefetch_tensormap(stage_map(g, level, set, kMapPre));
+        prefetch_tensormap(stage_map(g, level, set, kMapCoarse));
+    }
+}
+
 template <typename T, typename W, int K, bool PRE, int WARPS>
 __device__ __forceinline__ void stage_issue(const GridDesc& g, int level, int set, int X0, int Y0, char* stage,
     uint64_t* bar)
@@ -221,6 +233,7 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
         const Tile t = tiles[i];
         stage_issue_weights<T, W, K, true, WARPS>(grids[t.grid], level, set, t.x0 - Shape::HALO, t.y0 - Shape::HALO, stage,
             &bar);
+        stage_prefetch_data_maps<true>(grids[t.grid], level, set);
     }
     dependency_wait();
     if (misplaced)
@@ -246,12 +259,13 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
         // The restriction weights of the tile's coarse cells, while its boxes land.
         const int qx = lane - Shape::HALO / 2, cx = cx0 + qx;
         const bool column = qx >= 0 && qx < OCX && cx < C.w;
+        // Plain loads first used after the sweeps, so their latency stays off the tile's path.
         RestrictAxis<T> along_x{};
         if (column)
-            along_x = restrict_axis<T>(L.rx, cx);
+            along_x = static_cast<const RestrictAxis<T>*>(L.rwx)[cx];
         RestrictAxis<T> row_weights{};
         if (threadIdx.x < OCY && cy0 + int(threadIdx.x) < C.h)
-            row_weights = restrict_axis<T>(L.ry, cy0 + threadIdx.x);
+            row_weights = static_cast<const RestrictAxis<T>*>(L.rwy)[cy0 + threadIdx.x];
         const bool done = g.state->done != 0;
         const double mean_r = level == 0 ? g.state->mean_r : 0.0;
         const bool ok = mbarrier_wait(&bar, parity);
@@ -392,6 +406,7 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
         const Tile t = tiles[i];
         stage_issue_weights<T, W, K, false, WARPS>(grids[t.grid], level, set, t.x0 - Shape::HALO, t.y0 - Shape::HALO, stage,
             &bar);
+        stage_prefetch_data_maps<false>(grids[t.grid], level, set);
     }
     dependency_wait();
     if (misplaced)

@@ -492,7 +492,7 @@ __global__ void __launch_bounds__(kVecThreads) k_direction_operator(const GridDe
 // p += alpha d ; r -= alpha q ; residual stats. FluidGridCPU.cpp:1600-1641.
 // The padded halo and row padding of d, q, r and p are zero, so the update runs over the whole
 // padded array as one flat stream cut into one equal slice per vector tile. The kernel is
-// persistent (three CTAs per SM walk the slices of every grid), each thread takes two quads of
+// persistent (two CTAs per SM walk the slices of every grid), each thread takes two quads of
 // four cells per step with every load of the step issued before the arithmetic, and a CTA
 // counts its slices of a grid once; the per-slice partials and their fold are those of one CTA
 // per slice.

@@ -31,9 +31,13 @@ template <typename T, typename W, int K, bool PRE, int WARPS = 8> struct Stage
     static constexpr size_t WB = round(size_t(BW) * BH * sizeof(W));
     static constexpr size_t VB = round(size_t(BW) * BH * sizeof(T));
     static constexpr size_t CB = PRE ? 0 : round(size_t(CBW) * CBH * sizeof(T));
+    // Post: the prolongation tables of the region's rows and columns (Interp, 16 bytes each).
+    static constexpr size_t IY = PRE ? 0 : round(size_t(WARPS) * K * sizeof(Interp));
+    static constexpr size_t IX = PRE ? 0 : round(64 * sizeof(Interp));
     static constexpr size_t right = 0, down = WB, inv = 2 * WB, vec = 2 * WB + VB, pre = 2 * WB + 2 * VB;
     static constexpr size_t coarse = PRE ? pre : pre + VB;
-    static constexpr size_t bytes = coarse + CB;
+    static constexpr size_t rows = coarse + CB, cols = rows + IY;
+    static constexpr size_t bytes = cols + IX;
     // Bytes the boxes of one tile deliver (full boxes, zero-filled parts included).
     static constexpr unsigned tx = unsigned(2 * BW * BH * sizeof(W) + (PRE ? 2 : 3) * BW * BH * sizeof(T) +
                                             (PRE ? 0 : CBW * CBH * sizeof(T)));
@@ -85,7 +89,23 @@ __device__ __forceinline__ void stage_issue_weights(const GridDesc& g, int level
     // Padded coordinates: column gx + 2, row gy + 1. The region needs columns X0-1 .. X0+63 and
     // rows Y0-1 .. Y0+WARPS*K-1.
     const int bw = box_start<W>(X0 + 1), by = Y0;
-    mbarrier_expect_tx(bar, S::tx);
+    if constexpr (!PRE)
+    {
+        // The prolongation tables of the region's in-level rows and columns, by bulk copy into
+        // slots indexed by region row / column (the kernel reads in-level slots only).
+        const LevelDesc& L = g.lev[level];
+        const int r0 = max(Y0, 0), r1 = min(Y0 + WARPS * K, L.h);
+        const int c0 = max(X0, 0), c1 = min(X0 + 64, L.w);
+        const unsigned row_bytes = r1 > r0 ? unsigned(r1 - r0) * sizeof(Interp) : 0u;
+        const unsigned col_bytes = c1 > c0 ? unsigned(c1 - c0) * sizeof(Interp) : 0u;
+        mbarrier_expect_tx(bar, S::tx + row_bytes + col_bytes);
+        if (row_bytes)
+            bulk_load(stage + S::rows + size_t(r0 - Y0) * sizeof(Interp), L.py + r0, row_bytes, bar);
+        if (col_bytes)
+            bulk_load(stage + S::cols + size_t(c0 - X0) * sizeof(Interp), L.px + c0, col_bytes, bar);
+    }
+    else
+        mbarrier_expect_tx(bar, S::tx);
     tma_load_2d(stage + S::right, stage_map(g, level, set, kMapRight), bw, by, bar);
     tma_load_2d(stage + S::down, stage_map(g, level, set, kMapDown), bw, by, bar);
     tma_load_2d(stage + S::inv, stage_map(g, level, set, kMapInverse), box_start<T>(X0 + 1), by, bar);
@@ -384,7 +404,6 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
     extern __shared__ __align__(128) char stage[];
     __shared__ uint64_t bar;
     __shared__ Edges<T, WARPS> edges;
-    __shared__ Interp interp_y[Shape::RY];
     __shared__ double4 total;
     __shared__ double2 warp_pairs[WARPS];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -430,21 +449,8 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
         const LevelDesc& L = g.lev[level];
         const int X0 = t.x0 - Shape::HALO, Y0 = t.y0 - Shape::HALO;
         const int CX0 = X0 / 2 - 1, CY0 = Y0 / 2 - 1;
-        // Interpolation tables of the tile's rows and columns, while its boxes land.
-        Interp iy{0, 0, 0.0};
-        if (threadIdx.x < Shape::RY)
-        {
-            const int gy = Y0 + int(threadIdx.x);
-            if (gy >= 0 && gy < L.h)
-                iy = L.py[gy];
-        }
         const int gx = X0 + 2 * lane;
         const bool in_a = gx >= 0 && gx < L.w, in_b = gx + 1 >= 0 && gx + 1 < L.w;
-        Interp pa{0, 0, 0.0}, pb{0, 0, 0.0};
-        if (in_a)
-            pa = L.px[gx];
-        if (in_b)
-            pb = L.px[gx + 1];
         const bool done = state.done != 0;
         const double mean_r = level == 0 ? state.mean_r : 0.0;
         const bool ok = mbarrier_wait(&bar, parity);
@@ -452,8 +458,6 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
             return;
         parity ^= 1u;
         Strip<T, K> s;
-        if (threadIdx.x < Shape::RY)
-            interp_y[threadIdx.x] = iy;
         if (!done)
         {
             stage_strip<T, W, K, false, WARPS>(s, stage, X0, L.wscale, lane, warp);
@@ -473,7 +477,12 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
         __syncthreads();
         if (!done)
         {
-            // Add the prolonged coarse correction, in-level cells only.
+            // Add the prolonged coarse correction, in-level cells only; the tables arrived with
+            // the tile's boxes.
+            const Interp* interp_y = reinterpret_cast<const Interp*>(stage + S::rows);
+            const Interp* interp_x = reinterpret_cast<const Interp*>(stage + S::cols);
+            const Interp pa = in_a ? interp_x[2 * lane] : Interp{0, 0, 0.0};
+            const Interp pb = in_b ? interp_x[2 * lane + 1] : Interp{0, 0, 0.0};
             const T* coarse = reinterpret_cast<const T*>(stage + S::coarse);
             const int coff = CX0 + 2 - box_start<T>(CX0 + 2);
             const T wxa = T(pa.weight), wxb = T(pb.weight);

@@ -782,7 +782,6 @@ struct Plan
     int* d_body_count = nullptr;
     Range vec;
     Range faces; // tiles over the (W+1) x (H+1) face index space
-    Range coarsen[kMaxLevels];
     Range pre[kMaxLevels];
     Range post[kMaxLevels];
     // Region shape (RegionShape) of each level's pre- and post-smoothing kernels.
@@ -895,18 +894,6 @@ std::unique_ptr<Plan> make_plan(const std::vector<Grid*>& grids, cudaStream_t st
         for (size_t l = 0; l < g->levels.size(); ++l)
             plan->padded_max[l] = std::max(plan->padded_max[l], g->levels[l].S * (g->levels[l].h + 2));
     }
-    for (int l = 0; l + 1 < plan->max_levels; ++l)
-    {
-        add(plan->coarsen[l], [&]
-        {
-            for (int i = 0; i < n; ++i)
-            {
-                const auto& L = grids[i]->levels;
-                if (l + 1 < int(L.size()))
-                    append_tiles(tiles, i, L[l + 1].w, L[l + 1].h, kVecTileX, kVecTileY);
-            }
-        });
-    }
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, grids.front()->device);
     for (int l = 0; l < plan->max_tail; ++l)
@@ -966,8 +953,15 @@ template <typename T> void launch_rebuild(Plan& p)
     FC_LAUNCH(k_density, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
     FC_LAUNCH(k_coefficients<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
     for (int l = 0; l + 1 < p.max_levels; ++l)
-        FC_LAUNCH(k_coarsen<T>, p.coarsen[l].count, kVecThreads, 0, s, p.d_desc, p.at(p.coarsen[l]), l);
-    FC_LAUNCH(k_coarse_inverse<T>, p.n(), 256, 0, s, p.d_desc);
+        FC_LAUNCH(k_coarsen<T>, dim3(ceil_div(p.padded_max[l + 1], 256), p.n()), 256, 0, s, p.d_desc, l);
+    static const bool inverse_configured = [&]
+    {
+        check(cudaFuncSetAttribute(k_coarse_inverse<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kCoarseInverseSmem)),
+            "coarse inverse shared memory");
+        return true;
+    }();
+    (void)inverse_configured;
+    FC_LAUNCH(k_coarse_inverse<T>, p.n(), kCoarseThreads, kCoarseInverseSmem, s, p.d_desc);
     if (p.precision == FC_PRECISION_MIXED)
         for (int l = 1; l < p.max_tail; ++l)
             FC_LAUNCH(k_weights_half, dim3(ceil_div(p.padded_max[l], 256), p.n()), 256, 0, s, p.d_desc, l);

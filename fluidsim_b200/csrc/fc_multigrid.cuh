@@ -158,85 +158,103 @@ template <typename T> __global__ void k_inverse_diagonal(const GridDesc* grids, 
 
 // Coarse level `level + 1` from `level`. PressureMultigrid.cpp:142-202 (coarsen) and
 // :104-117 (the diagonal is recomputed on the fly wherever it is needed).
-template <typename T> __global__ void k_coarsen(const GridDesc* grids, const Tile* tiles, int level)
+// One thread per coarse cell (blockIdx.y = grid): the FP64 divisions of a cell form a long
+// dependent chain, so the kernel needs many cells in flight rather than many cells per thread.
+template <typename T> __global__ void k_coarsen(const GridDesc* grids, int level)
 {
-    const Tile t = tiles[blockIdx.x];
-    const GridDesc& g = grids[t.grid];
+    const GridDesc& g = grids[blockIdx.y];
+    if (level + 1 >= g.levels)
+        return;
     const LevelDesc& f = g.lev[level];
     const LevelDesc& c = g.lev[level + 1];
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= c.w * c.h)
+        return;
+    const int x = q % c.w, y = q / c.w;
     const T* fr = static_cast<const T*>(f.right);
     const T* fd = static_cast<const T*>(f.down);
     T* cr = static_cast<T*>(c.right);
     T* cd = static_cast<T*>(c.down);
-    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-    for (int k = 0; k < kVecCells; ++k)
+    double right = 0.0, down = 0.0;
+    if (x + 1 < c.w)
     {
-        const int x = t.x0 + tx + 32 * (k & 1), y = t.y0 + ty + 8 * (k >> 1);
-        if (x >= c.w || y >= c.h)
-            continue;
-        double right = 0.0, down = 0.0;
-        if (x + 1 < c.w)
+        const int e = 2 * x + 2;
+        const double a = (f.cx[e - 1] - c.cx[x]) / (f.cx[e - 1] - f.cx[e - 2]);
+        const double b = e + 1 < f.w ? (c.cx[x + 1] - f.cx[e]) / (f.cx[e + 1] - f.cx[e]) : 0.0;
+        const int fy_end = min(2 * y + 2, f.h);
+        for (int fy = 2 * y; fy < fy_end; ++fy)
         {
-            const int e = 2 * x + 2;
-            const double a = (f.cx[e - 1] - c.cx[x]) / (f.cx[e - 1] - f.cx[e - 2]);
-            const double b = e + 1 < f.w ? (c.cx[x + 1] - f.cx[e]) / (f.cx[e + 1] - f.cx[e]) : 0.0;
-            const int fy_end = min(2 * y + 2, f.h);
-            for (int fy = 2 * y; fy < fy_end; ++fy)
-            {
-                const long long i = padded_index(f.S, e - 1, fy); // fine cell 2x+1: its right face is the coarse face
-                double resistance = a / double(fr[i - 1]) + 1.0 / double(fr[i]);
-                if (b != 0.0)
-                    resistance += b / double(fr[i + 1]);
-                right += 1.0 / resistance;
-            }
+            const long long i = padded_index(f.S, e - 1, fy); // fine cell 2x+1: its right face is the coarse face
+            double resistance = a / double(fr[i - 1]) + 1.0 / double(fr[i]);
+            if (b != 0.0)
+                resistance += b / double(fr[i + 1]);
+            right += 1.0 / resistance;
         }
-        if (y + 1 < c.h)
-        {
-            const int e = 2 * y + 2;
-            const double a = (f.cy[e - 1] - c.cy[y]) / (f.cy[e - 1] - f.cy[e - 2]);
-            const double b = e + 1 < f.h ? (c.cy[y + 1] - f.cy[e]) / (f.cy[e + 1] - f.cy[e]) : 0.0;
-            const int fx_end = min(2 * x + 2, f.w);
-            for (int fx = 2 * x; fx < fx_end; ++fx)
-            {
-                const long long i = padded_index(f.S, fx, e - 1); // fine cell 2y+1: its lower face is the coarse face
-                double resistance = a / double(fd[i - f.S]) + 1.0 / double(fd[i]);
-                if (b != 0.0)
-                    resistance += b / double(fd[i + f.S]);
-                down += 1.0 / resistance;
-            }
-        }
-        const long long ci = padded_index(c.S, x, y);
-        cr[ci] = T(right);
-        cd[ci] = T(down);
     }
+    if (y + 1 < c.h)
+    {
+        const int e = 2 * y + 2;
+        const double a = (f.cy[e - 1] - c.cy[y]) / (f.cy[e - 1] - f.cy[e - 2]);
+        const double b = e + 1 < f.h ? (c.cy[y + 1] - f.cy[e]) / (f.cy[e + 1] - f.cy[e]) : 0.0;
+        const int fx_end = min(2 * x + 2, f.w);
+        for (int fx = 2 * x; fx < fx_end; ++fx)
+        {
+            const long long i = padded_index(f.S, fx, e - 1); // fine cell 2y+1: its lower face is the coarse face
+            double resistance = a / double(fd[i - f.S]) + 1.0 / double(fd[i]);
+            if (b != 0.0)
+                resistance += b / double(fd[i + f.S]);
+            down += 1.0 / resistance;
+        }
+    }
+    const long long ci = padded_index(c.S, x, y);
+    cr[ci] = T(right);
+    cd[ci] = T(down);
 }
 
 // Dense pinned operator of the coarsest level, its Cholesky factor and the explicit inverse,
 // in FP64; one CTA per grid. PressureMultigrid.cpp:300-345 (factorCoarsest). A non-positive
 // or non-finite pivot marks the preconditioner invalid (the reference's breakdown, :334-335).
+//
+// The factor is formed right-looking: every entry receives the same subtractions in the same
+// order as the reference's column-by-column loop (products of columns 0, 1, ... in turn, then
+// the division by the pivot), so it is the same factor bit for bit, with the work of each step
+// spread over the CTA. Y = L^-1 by forward substitution (likewise right-looking, each entry
+// keeping the left-looking order), and the inverse A^-1 = Y^T Y as independent dot products.
 constexpr int kMaxCoarse = 64;
+constexpr int kCoarseThreads = 512;
+// Dynamic shared memory: the factor L and Y, n x n doubles each.
+constexpr size_t kCoarseInverseSmem = 2 * size_t(kMaxCoarse) * kMaxCoarse * sizeof(double);
 
-template <typename T> __global__ void __launch_bounds__(256) k_coarse_inverse(const GridDesc* grids)
+template <typename T> __global__ void __launch_bounds__(kCoarseThreads) k_coarse_inverse(const GridDesc* grids)
 {
     const GridDesc& g = grids[blockIdx.x];
     const int last = g.levels - 1;
     const LevelDesc& l = g.lev[last];
     const int cells = l.w * l.h;
-    __shared__ double a[kMaxCoarse * kMaxCoarse];
+    extern __shared__ double coarse_smem[];
+    double* a = coarse_smem;                         // operator, then its factor (lower triangle)
+    double* yi = coarse_smem + kMaxCoarse * kMaxCoarse; // L^-1 (lower triangle)
     __shared__ int map[kMaxCoarse];
+    __shared__ unsigned char open[kMaxCoarse];
     __shared__ int failed, n_shared, pinned_shared;
     const T* right = static_cast<const T*>(l.right);
     const T* down = static_cast<const T*>(l.down);
+    // Unknowns in cell order: open cells after the first one (pinned). The cells' diagonals
+    // are read in parallel, the numbering is one pass over the flags.
+    for (int cell = threadIdx.x; cell < cells; cell += blockDim.x)
+    {
+        const long long i = padded_index(l.S, cell % l.w, cell / l.w);
+        const double diag = ((double(right[i - 1]) + double(right[i])) + double(down[i - l.S])) + double(down[i]);
+        open[cell] = diag > 0.0 ? 1 : 0;
+    }
+    __syncthreads();
     if (threadIdx.x == 0)
     {
-        // Unknowns in cell order: open cells after the first one (pinned).
         int n = 0, pinned = -1;
         for (int cell = 0; cell < cells; ++cell)
         {
-            const long long i = padded_index(l.S, cell % l.w, cell / l.w);
-            const double diag = ((double(right[i - 1]) + double(right[i])) + double(down[i - l.S])) + double(down[i]);
             map[cell] = -1;
-            if (!(diag > 0.0))
+            if (!open[cell])
                 continue;
             if (pinned < 0)
                 pinned = cell;
@@ -250,7 +268,10 @@ template <typename T> __global__ void __launch_bounds__(256) k_coarse_inverse(co
     __syncthreads();
     const int n = n_shared;
     for (int i = threadIdx.x; i < n * n; i += blockDim.x)
+    {
         a[i] = 0.0;
+        yi[i] = (i / n == i % n) ? 1.0 : 0.0;
+    }
     __syncthreads();
     for (int cell = threadIdx.x; cell < cells; cell += blockDim.x)
     {
@@ -266,49 +287,55 @@ template <typename T> __global__ void __launch_bounds__(256) k_coarse_inverse(co
             a[row * n + map[cell - l.w]] = -double(down[i - l.S]);
     }
     __syncthreads();
-    // Cholesky of the lower triangle, column by column (same arithmetic as row by row).
-    for (int col = 0; col < n; ++col)
+    // Cholesky, right-looking: at step k the pivot and column k are final; the trailing lower
+    // triangle then takes its k-th product.
+    for (int k = 0; k < n; ++k)
     {
         if (threadIdx.x == 0)
         {
-            double value = a[col * n + col];
-            for (int k = 0; k < col; ++k)
-                value -= a[col * n + k] * a[col * n + k];
+            const double value = a[k * n + k];
             if (!(value > 0.0) || !isfinite(value))
                 failed = 1;
-            a[col * n + col] = sqrt(value);
+            a[k * n + k] = sqrt(value);
         }
         __syncthreads();
-        const double pivot = a[col * n + col];
-        for (int row = col + 1 + threadIdx.x; row < n; row += blockDim.x)
+        const double pivot = a[k * n + k];
+        for (int row = k + 1 + threadIdx.x; row < n; row += blockDim.x)
+            a[row * n + k] = a[row * n + k] / pivot;
+        __syncthreads();
+        const int m = n - 1 - k; // trailing rows and columns k+1 .. n-1
+        for (int e = threadIdx.x; e < m * m; e += blockDim.x)
         {
-            double value = a[row * n + col];
-            for (int k = 0; k < col; ++k)
-                value -= a[row * n + k] * a[col * n + k];
-            a[row * n + col] = value / pivot;
+            const int row = k + 1 + e / m, col = k + 1 + e % m;
+            if (col <= row)
+                a[row * n + col] -= a[row * n + k] * a[col * n + k];
         }
         __syncthreads();
     }
-    // inverse = L^-T L^-1, one column of the identity per thread.
-    for (int c = threadIdx.x; c < n; c += blockDim.x)
+    // Y = L^-1, right-looking forward substitution: row k of Y is final after its division;
+    // the rows below then take its product.
+    for (int k = 0; k < n; ++k)
     {
-        double y[kMaxCoarse];
-        for (int row = 0; row < n; ++row)
+        const double pivot = a[k * n + k];
+        for (int col = threadIdx.x; col <= k; col += blockDim.x)
+            yi[k * n + col] = yi[k * n + col] / pivot;
+        __syncthreads();
+        const int m = n - 1 - k;
+        for (int e = threadIdx.x; e < m * (k + 1); e += blockDim.x)
         {
-            double value = row == c ? 1.0 : 0.0;
-            for (int k = 0; k < row; ++k)
-                value -= a[row * n + k] * y[k];
-            y[row] = value / a[row * n + row];
+            const int row = k + 1 + e / (k + 1), col = e % (k + 1);
+            yi[row * n + col] -= a[row * n + k] * yi[k * n + col];
         }
-        for (int row = n - 1; row >= 0; --row)
-        {
-            double value = y[row];
-            for (int k = row + 1; k < n; ++k)
-                value -= a[k * n + row] * y[k];
-            y[row] = value / a[row * n + row];
-        }
-        for (int row = 0; row < n; ++row)
-            g.coarse_inverse[row * n + c] = y[row];
+        __syncthreads();
+    }
+    // A^-1 = Y^T Y: entry (r, c) sums Y[k][r] Y[k][c] over k >= max(r, c).
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x)
+    {
+        const int r = e / n, c = e % n;
+        double value = 0.0;
+        for (int k = max(r, c); k < n; ++k)
+            value += yi[k * n + r] * yi[k * n + c];
+        g.coarse_inverse[e] = value;
     }
     for (int cell = threadIdx.x; cell < kMaxCoarse; cell += blockDim.x)
         g.coarse->map[cell] = cell < cells ? map[cell] : -1;

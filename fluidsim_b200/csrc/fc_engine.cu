@@ -787,6 +787,11 @@ struct Plan
     // Region shape (RegionShape) of each level's pre- and post-smoothing kernels.
     int shape_pre[kMaxLevels] = {};
     int shape_post[kMaxLevels] = {};
+    // The fine level's post-smoothing folds each grid's z sums per region, so its regions take
+    // each grid's own shape (the one the grid would have alone): results then do not depend on
+    // which grids share the plan. post0[shape] holds the regions of the grids of that shape.
+    Range post0[kShapes];
+    std::vector<int> post0_shape; // per grid
     int max_levels = 0;
     int max_tail = 0;
     int padded_max[kMaxLevels] = {}; // largest padded level array of any grid, per level
@@ -843,17 +848,30 @@ void append_tiles(std::vector<Tile>& tiles, int grid, int w, int h, int tx, int 
 void upload_descriptors(Plan& plan)
 {
     std::vector<GridDesc> descs(plan.n());
-    const TileSizes ts = tile_sizes(plan.precision, plan.shape_post[0]);
     for (int i = 0; i < plan.n(); ++i)
     {
         descs[i] = plan.grids[i]->desc;
-        // Level-0 post tiles of this grid in this plan: the count its z reduction waits for.
+        // Level-0 post regions of this grid (its own shape): the count its z reduction waits for.
         const Grid& g = *plan.grids[i];
+        const int shape = i < int(plan.post0_shape.size()) ? plan.post0_shape[i] : kShapeShort;
+        const TileSizes ts = tile_sizes(plan.precision, shape);
         descs[i].post_tiles = g.tail > 0 ? ceil_div(g.W, ts.post_x) * ceil_div(g.H, ts.post_y) : 0;
     }
     check(cudaMemcpyAsync(plan.d_desc, descs.data(), descs.size() * sizeof(GridDesc), cudaMemcpyHostToDevice, plan.stream),
         "plan descriptors");
     check(cudaStreamSynchronize(plan.stream), "plan descriptors");
+}
+
+// Region shape of a level from its region counts in the tall and wide shapes: tall regions once
+// there is one for every other SM (a tall region costs less than the two short ones it
+// replaces: the per-region latency is paid once, with less halo); short strips, which halve
+// each CTA's latency, on the smaller levels; in FP32 the wide shape (one 16-warp CTA per SM,
+// the least halo per output cell) for levels with four waves of regions.
+int region_shape(int precision, long long tall_regions, long long wide_regions, int sms)
+{
+    if (precision != FC_PRECISION_FP64 && wide_regions >= 4LL * sms)
+        return kShapeWide;
+    return 2 * tall_regions >= sms ? kShapeTall : kShapeShort;
 }
 
 std::unique_ptr<Plan> make_plan(const std::vector<Grid*>& grids, cudaStream_t stream)
@@ -898,21 +916,32 @@ std::unique_ptr<Plan> make_plan(const std::vector<Grid*>& grids, cudaStream_t st
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, grids.front()->device);
     for (int l = 0; l < plan->max_tail; ++l)
     {
-        auto tiles_of = [&](int shape)
+        auto tiles_of = [&](int shape, int only)
         {
             const TileSizes t = tile_sizes(plan->precision, shape);
             long long count = 0;
             for (int i = 0; i < n; ++i)
-                if (l < grids[i]->tail)
+                if (l < grids[i]->tail && (only < 0 || i == only))
                     count += (long long)ceil_div(grids[i]->levels[l].w, t.pre_x) * ceil_div(grids[i]->levels[l].h, t.pre_y);
             return count;
         };
-        // Tall regions need two waves of their two CTAs per SM; short strips halve each CTA's
-        // latency on the small levels. In FP32 the wide shape (one 16-warp CTA per SM, the
-        // least halo per output cell) takes levels with four waves of regions.
-        const int base = tiles_of(kShapeTall) >= 2LL * sms ? kShapeTall : kShapeShort;
-        const int shape =
-            plan->precision != FC_PRECISION_FP64 && tiles_of(kShapeWide) >= 4LL * sms ? kShapeWide : base;
+        const int shape = region_shape(plan->precision, tiles_of(kShapeTall, -1), tiles_of(kShapeWide, -1), sms);
+        if (l == 0)
+        {
+            plan->post0_shape.assign(n, kShapeShort);
+            for (int i = 0; i < n; ++i)
+                plan->post0_shape[i] = region_shape(plan->precision, tiles_of(kShapeTall, i), tiles_of(kShapeWide, i), sms);
+            for (int set = 0; set < kShapes; ++set)
+            {
+                const TileSizes tq = tile_sizes(plan->precision, set);
+                add(plan->post0[set], [&]
+                {
+                    for (int i = 0; i < n; ++i)
+                        if (grids[i]->tail > 0 && plan->post0_shape[i] == set)
+                            append_tiles(tiles, i, grids[i]->W, grids[i]->H, tq.post_x, tq.post_y);
+                });
+            }
+        }
         plan->shape_pre[l] = shape;
         plan->shape_post[l] = shape;
         const TileSizes tp = tile_sizes(plan->precision, plan->shape_pre[l]);
@@ -923,12 +952,13 @@ std::unique_ptr<Plan> make_plan(const std::vector<Grid*>& grids, cudaStream_t st
                 if (l < grids[i]->tail)
                     append_tiles(tiles, i, grids[i]->levels[l].w, grids[i]->levels[l].h, tp.pre_x, tp.pre_y);
         });
-        add(plan->post[l], [&]
-        {
-            for (int i = 0; i < n; ++i)
-                if (l < grids[i]->tail)
-                    append_tiles(tiles, i, grids[i]->levels[l].w, grids[i]->levels[l].h, tq.post_x, tq.post_y);
-        });
+        if (l > 0)
+            add(plan->post[l], [&]
+            {
+                for (int i = 0; i < n; ++i)
+                    if (l < grids[i]->tail)
+                        append_tiles(tiles, i, grids[i]->levels[l].w, grids[i]->levels[l].h, tq.post_x, tq.post_y);
+            });
     }
     check(cudaMalloc(&plan->d_tiles, std::max<size_t>(1, tiles.size()) * sizeof(Tile)), "plan tiles");
     check(cudaMemcpy(plan->d_tiles, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice), "plan tiles");
@@ -986,10 +1016,9 @@ int sm_count()
 int smoothing_ctas(bool fp64) { return sm_count() * (fp64 ? 1 : 2); }
 
 template <typename T, int K, typename W, bool PRE, int WARPS>
-void launch_smooth_kernel(Plan& p, int level, int set, bool dependent, cudaStream_t s)
+void launch_smooth_kernel(Plan& p, const Range& r, int level, int set, bool dependent, cudaStream_t s)
 {
     using St = Stage<T, W, K, PRE, WARPS>;
-    const Range& r = PRE ? p.pre[level] : p.post[level];
     if (r.count <= 0)
         return;
     auto kernel = PRE ? k_smooth_pre<T, K, W, WARPS> : k_smooth_post<T, K, W, WARPS>;
@@ -1008,35 +1037,45 @@ void launch_smooth_kernel(Plan& p, int level, int set, bool dependent, cudaStrea
         FC_LAUNCH(kernel, ctas, 32 * WARPS, St::bytes, s, p.d_desc, p.at(r), r.count, level, set);
 }
 
-template <typename T, typename W, bool PRE> void launch_smooth_shape(Plan& p, int level, bool dependent, cudaStream_t s)
+template <typename T, typename W, bool PRE>
+void launch_smooth_shape(Plan& p, const Range& r, int level, int shape, bool dependent, cudaStream_t s)
 {
     constexpr int KB = Tiling<T>::big, KS = Tiling<T>::small, KW = Tiling<T>::wide;
-    const int shape = PRE ? p.shape_pre[level] : p.shape_post[level];
     if constexpr (sizeof(T) == 4)
     {
         if (shape == kShapeWide)
-            return launch_smooth_kernel<T, KW, W, PRE, 16>(p, level, shape, dependent, s);
+            return launch_smooth_kernel<T, KW, W, PRE, 16>(p, r, level, shape, dependent, s);
     }
     if (shape == kShapeShort)
-        launch_smooth_kernel<T, KS, W, PRE, 8>(p, level, shape, dependent, s);
+        launch_smooth_kernel<T, KS, W, PRE, 8>(p, r, level, shape, dependent, s);
     else
-        launch_smooth_kernel<T, KB, W, PRE, 8>(p, level, shape, dependent, s);
+        launch_smooth_kernel<T, KB, W, PRE, 8>(p, r, level, shape, dependent, s);
 }
 
 // The pre- or post-smoothing kernel of one level in the plan's region shape, with FP16 weights
 // on the coarse levels of a mixed-precision plan.
 template <typename T> void launch_smooth(Plan& p, int level, bool pre, bool dependent, cudaStream_t s)
 {
+    if (!pre && level == 0)
+    {
+        // One launch per region shape the plan's grids take on the fine level.
+        for (int shape = 0; shape < kShapes; ++shape)
+            launch_smooth_shape<T, T, false>(p, p.post0[shape], 0, shape, dependent, s);
+        return;
+    }
+    const Range& r = pre ? p.pre[level] : p.post[level];
+    const int shape = pre ? p.shape_pre[level] : p.shape_post[level];
     if constexpr (sizeof(T) == 4)
     {
         if (p.precision == FC_PRECISION_MIXED && level >= 1)
         {
-            pre ? launch_smooth_shape<T, __half, true>(p, level, dependent, s)
-                : launch_smooth_shape<T, __half, false>(p, level, dependent, s);
+            pre ? launch_smooth_shape<T, __half, true>(p, r, level, shape, dependent, s)
+                : launch_smooth_shape<T, __half, false>(p, r, level, shape, dependent, s);
             return;
         }
     }
-    pre ? launch_smooth_shape<T, T, true>(p, level, dependent, s) : launch_smooth_shape<T, T, false>(p, level, dependent, s);
+    pre ? launch_smooth_shape<T, T, true>(p, r, level, shape, dependent, s)
+        : launch_smooth_shape<T, T, false>(p, r, level, shape, dependent, s);
 }
 
 // One application of the preconditioner to r: z, mean z, r.z and beta.

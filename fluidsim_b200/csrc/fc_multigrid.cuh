@@ -454,6 +454,28 @@ __device__ __forceinline__ void tail_store_solution(const TailLevel<T>& L, const
     }
 }
 
+// Warps of the tail CTA that hold rows of level L, and the strips barrier for them: the whole
+// CTA when every warp does, else named barrier 1 over those warps (the others wait for the
+// level at the next CTA barrier). The last of them reads the row below its strip from the
+// edge slot of the first idle warp, which a taller level may have written: it clears it.
+template <typename T> struct TailWarps
+{
+    int active, threads;
+    __device__ TailWarps(const TailLevel<T>& L)
+    {
+        active = (L.h + kTailK - 1) / kTailK;
+        threads = active == kTailWarps ? 0 : active * 32;
+    }
+    __device__ void clear_below(TailEdges<T>& edges, int lane, int warp) const
+    {
+        if (warp == active - 1 && active < kTailWarps)
+        {
+            edges.top[0][active + 1][lane] = T(0);
+            edges.top[1][active + 1][lane] = T(0);
+        }
+    }
+};
+
 // Pre-smoothing of tail level L: four red-black sweeps from zero, the residual, and its
 // transpose-bilinear restriction into C's right-hand side (PressureMultigrid.cpp:398-402,
 // 204-231, 233-276). The pre-smoothed solution stays in L.sol for the post-smoothing.
@@ -461,15 +483,19 @@ template <typename T>
 __device__ void tail_pre(const TailLevel<T> L, const TailLevel<T> C, double mean, TailEdges<T>& edges, int lane, int warp)
 {
     T* const m = tail_array<T>();
+    const TailWarps<T> tw(L);
+    if (warp < tw.active)
+    {
     Strip<T, kTailK> s;
     tail_load_strip(L, s, false, mean, lane, warp);
-    strip_sweep<T, kTailK, kTailWarps>(s, edges, 0, true, 0, lane, warp);
-    strip_sweep<T, kTailK, kTailWarps>(s, edges, 1, false, 1, lane, warp);
+    tw.clear_below(edges, lane, warp);
+    strip_sweep<T, kTailK, kTailWarps>(s, edges, 0, true, 0, lane, warp, tw.threads);
+    strip_sweep<T, kTailK, kTailWarps>(s, edges, 1, false, 1, lane, warp, tw.threads);
 #pragma unroll 1
     for (int sweep = 1; sweep < 4; ++sweep)
     {
-        strip_sweep<T, kTailK, kTailWarps>(s, edges, 0, false, 0, lane, warp);
-        strip_sweep<T, kTailK, kTailWarps>(s, edges, 1, false, 1, lane, warp);
+        strip_sweep<T, kTailK, kTailWarps>(s, edges, 0, false, 0, lane, warp, tw.threads);
+        strip_sweep<T, kTailK, kTailWarps>(s, edges, 1, false, 1, lane, warp, tw.threads);
     }
     // Residual from registers; the edge buffers hold the final values (buffer 0 colour 0,
     // buffer 1 colour 1). Cells without an open face pass no residual down.
@@ -505,6 +531,7 @@ __device__ void tail_pre(const TailLevel<T> L, const TailLevel<T> C, double mean
             m[L.sol + i + 1] = b;
             m[L.res + i + 1] = s.ib[k] > T(0) ? s.rb[k] - pb : T(0);
         }
+    }
     }
     __syncthreads();
     // Restriction: coarse cell (cx, cy) sums fine rows 2cy-1 .. 2cy+2 of the x-sums of fine
@@ -543,8 +570,12 @@ __device__ void tail_post(const TailLevel<T> C, const TailLevel<T> L, double mea
     int warp)
 {
     const T* m = tail_array<T>();
+    const TailWarps<T> tw(L);
+    if (warp < tw.active)
+    {
     Strip<T, kTailK> s;
     tail_load_strip(L, s, true, mean, lane, warp);
+    tw.clear_below(edges, lane, warp);
     const Interp* px = tail_table<const Interp>(L.px);
     const Interp* py = tail_table<const Interp>(L.py);
     const int x = 2 * lane;
@@ -577,14 +608,15 @@ __device__ void tail_post(const TailLevel<T> C, const TailLevel<T> L, double mea
     // The first half-sweep (colour 1) reads colour-0 edges from buffer 1.
     edges.top[1][warp + 1][lane] = s.a[0];
     edges.bottom[1][warp + 1][lane] = s.b[kTailK - 1];
-    __syncthreads();
+    strips_barrier(tw.threads);
 #pragma unroll 1
     for (int sweep = 0; sweep < 4; ++sweep)
     {
-        strip_sweep<T, kTailK, kTailWarps>(s, edges, 1, false, 0, lane, warp);
-        strip_sweep<T, kTailK, kTailWarps>(s, edges, 0, false, 1, lane, warp);
+        strip_sweep<T, kTailK, kTailWarps>(s, edges, 1, false, 0, lane, warp, tw.threads);
+        strip_sweep<T, kTailK, kTailWarps>(s, edges, 0, false, 1, lane, warp, tw.threads);
     }
     tail_store_solution(L, s, lane, warp);
+    }
     __syncthreads();
 }
 

@@ -101,11 +101,23 @@ __device__ __forceinline__ void strip_finish(Strip<T, K>& s, int level, double m
     }
 }
 
+// Barrier of the warps that hold strips: the whole CTA (threads == 0), or, where only the first
+// threads / 32 warps hold a level's rows, those warps alone on named barrier 1 (threads a multiple
+// of 32; every one of them reaches each barrier).
+__device__ __forceinline__ void strips_barrier(int threads)
+{
+    if (threads == 0)
+        __syncthreads();
+    else
+        asm volatile("bar.sync 1, %0;" ::"r"(threads) : "memory");
+}
+
 // One red-black half-sweep of colour c over the strip; publishes the strip's edge rows of that
-// colour into buffer `buf` and reads the neighbours' edges from buffer buf ^ 1.
+// colour into buffer `buf` and reads the neighbours' edges from buffer buf ^ 1. `threads` selects
+// the barrier (strips_barrier).
 template <typename T, int K, int WARPS = 8>
 __device__ __forceinline__ void strip_sweep(Strip<T, K>& s, Edges<T, WARPS>& e, int c, bool from_zero, int buf, int lane,
-    int warp)
+    int warp, int threads = 0)
 {
     const T above = from_zero ? T(0) : e.bottom[buf ^ 1][warp][lane];
     const T below = from_zero ? T(0) : e.top[buf ^ 1][warp + 2][lane];
@@ -145,7 +157,7 @@ __device__ __forceinline__ void strip_sweep(Strip<T, K>& s, Edges<T, WARPS>& e, 
     // Row 0 is even: colour c sits in a when c == 0. Row K-1 is odd: in a when c == 1.
     e.top[buf][warp + 1][lane] = c == 0 ? s.a[0] : s.b[0];
     e.bottom[buf][warp + 1][lane] = c == 1 ? s.a[K - 1] : s.b[K - 1];
-    __syncthreads();
+    strips_barrier(threads);
 }
 
 template <typename T, int K, int WARPS = 8>

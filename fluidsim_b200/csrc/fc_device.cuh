@@ -177,11 +177,6 @@ struct Tile
     int index;
 };
 
-template <typename T> __device__ __forceinline__ T load_as(const void* base, long long i)
-{
-    return static_cast<const T*>(base)[i];
-}
-
 // Correctly rounded reciprocal in the working precision.
 __device__ __forceinline__ float reciprocal(float v) { return __frcp_rn(v); }
 __device__ __forceinline__ double reciprocal(double v) { return 1.0 / v; }
@@ -384,8 +379,6 @@ __device__ __forceinline__ bool stage_failed(bool ok, SolveState* state)
     }
     return false;
 }
-
-__device__ __forceinline__ bool finite_d(double v) { return isfinite(v); }
 
 // Programmatic dependent launch. The kernels of the PCG loop are launched so that each may
 // start while its predecessor finishes: allow_dependents() lets the next kernel's CTAs be

@@ -10,8 +10,12 @@
 //  * k_smooth_pre / k_smooth_post (fc_stage.cuh): temporally blocked smoothing of one level per launch,
 //    with the residual and restriction fused into the pre kernel and the prolongation and the
 //    fine-level z reductions fused into the post kernel.
-//  * k_mg_tail: the coarse levels that fit in shared memory are cycled by one CTA per grid,
-//    including the coarsest direct solve (explicit FP64 inverse of the pinned Cholesky system).
+//  * k_mg_tail: the coarse levels of at most 64 x 64 cells that fit in shared memory are cycled
+//    by one CTA per grid as register strips, their inputs bulk-copied in before the dependency
+//    wait, including the coarsest direct solve (explicit FP64 inverse of the pinned Cholesky
+//    system).
+//  * The rebuild: k_coarsen (one coarse cell per thread), k_inverse_diagonal, k_weights_half
+//    (mixed precision) and k_coarse_inverse (right-looking factor, the reference's arithmetic).
 #pragma once
 
 #include "fc_device.cuh"

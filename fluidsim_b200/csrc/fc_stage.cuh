@@ -9,9 +9,11 @@
 //   issue tile i+1's boxes -> sweep tile i from registers -> write tile i's outputs
 //
 // so the HBM latency of one tile hides behind the arithmetic of the previous one. The boxes are
-// 2D tiles of the padded level arrays (72 columns x 8K+1 rows: the strip rows and the row above,
-// the column left of the region, rounded out to 16-byte alignment); coordinates outside an array
-// read as zero, which is what the direct loads of the first form read there.
+// 2D tiles of the padded level arrays: weights, inverse diagonal, the level's vector (and for
+// the post kernel the pre-smoothed solution and the coarse solution), 72 columns x WARPS*K+1
+// rows (the strip rows and the row above, the column left of the region, rounded out to 16-byte
+// alignment); coordinates outside an array read as zero, as the padded halo does. The post kernel
+// also bulk-copies the region's rows and columns of the prolongation tables.
 #pragma once
 
 #include "fc_smooth.cuh"

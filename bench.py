@@ -50,6 +50,7 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-serve", action="store_true", help="skip the serving (continuous batching) measurement")
     p.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision comparison")
+    p.add_argument("--no-steps", action="store_true", help="skip the full-step (transport + projection) measurement")
     p.add_argument("--tail-cells", type=int, default=0,
                    help="multigrid tail threshold in cells (0: autotuned); pins the schedule for profiling")
     p.add_argument("--serve-requests", type=int, default=16)
@@ -319,6 +320,8 @@ def run_cuda(args, world, rank, local_rank):
             line["batched"] = batched
     if rank == 0 and not args.no_serve:
         line["serve"] = serve_measure(args)
+    if rank == 0 and not args.no_steps:
+        line["steps"] = steps_measure(args, torch)
     return line
 
 
@@ -414,6 +417,45 @@ def e2e_measure(args, scene, torch):
     ms = statistics.mean(times)
     return {"value": scene.cells / (ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
             "ms_per_step": ms}
+
+
+def steps_measure(args, torch, steps=20, warmup=3, size=1024):
+    """Full time steps of the dam break with obstacles: a 1024x1024 scene, 16 seeded circular
+    obstacles of radii 8..40 cells, gravity -9.8, dt 1/120. Each step runs RK2 semi-Lagrangian
+    transport of u and v, the body force and the MG-PCG projection (FluidGrid.step, the
+    reference's step order) to the 1e-6 stop rule; a step is accepted as the reference accepts
+    it (converged, or precision-limited: the solver met its stop rule and only the FP32 rounding
+    of the face velocities is left in the divergence). The scene evolves from step to step, timed
+    with CUDA events on the grid's stream; the projection's unfused byte model gives a GB/s
+    figure beside it."""
+    from fluidsim_b200 import FluidGrid, scenes
+
+    scene = scenes.dam_break(size, size, seed=11, obstacles=16, velocity=0.0)
+    g = FluidGrid(size, size, scene.cell_size, "fp32")
+    scenes.upload_scene(g, scene)
+    stream = torch.cuda.ExternalStream(g.stream())
+    times, iters, statuses, accepted = [], [], {}, True
+    for i in range(warmup + steps):
+        with torch.cuda.stream(stream):
+            start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            start.record(stream)
+        r = g.step(scene.dt, 200, args.tolerance)
+        stop.record(stream)
+        stop.synchronize()
+        if i >= warmup:
+            times.append(start.elapsed_time(stop))
+            iters.append(r.iterations)
+            statuses[r.solve_status] = statuses.get(r.solve_status, 0) + 1
+            accepted = accepted and r.accepted()
+    g.destroy()
+    ms = statistics.mean(times)
+    mean_iters = statistics.mean(iters)
+    model_bytes = scene.cells * (70 + 306 * mean_iters)
+    return {"workload": f"dam_break_{size}x{size}, 16 obstacles, {steps} steps after {warmup}", "value": scene.cells / (ms / 1e3),
+            "unit": UNIT, "ms_per_step": ms, "p50_ms": statistics.median(times), "max_ms": max(times),
+            "iterations_per_step": mean_iters, "max_iterations": max(iters), "solve_status": statuses,
+            "all_accepted": accepted,
+            "projection_model_gbs": model_bytes / (ms / 1e3) / 1e9}
 
 
 def batched_measure(args, torch, world=1, rank=0, count=256):

@@ -320,3 +320,33 @@ def test_large_grid_converges_relative():
     assert r.iterations < 80
     # divergence falls by orders of magnitude (FP32 velocity storage sets the floor)
     assert r.divergence_l2 < 1e-3 * r.rhs_l2 / (s.cell_size * s.cell_size / s.dt) + 1e-3
+
+
+@pytest.mark.parametrize("rule", ["absolute", "relative"])
+def test_fp32_converges_from_a_poor_warm_start(rule):
+    """A warm start far from the solution (random pressure of amplitude 1e3) leaves an initial
+    residual many orders above the stop rule. FP32 rounding then gives the recurrence residual a
+    mean that no iteration removes; the solve must still verify and converge like FP64, not run
+    to its iteration cap."""
+    s = scenes.dam_break(256, 256, seed=3, obstacles=4, velocity=1.0)
+    warm = np.random.default_rng(5).uniform(-1e3, 1e3, (s.height, s.width))
+    results, outs = {}, {}
+    for precision in ("fp64", "fp32"):
+        g = FluidGrid(s.width, s.height, s.cell_size, precision)
+        scenes.upload_scene(g, s, pressure=warm)
+        if rule == "absolute":
+            r = g.project(s.dt, 200, 1e-6)
+        else:
+            r = g.project(s.dt, 200, 1e-6, relative_tolerance=1e-6)
+        results[precision], outs[precision] = r, g.download()
+    r32, r64 = results["fp32"], results["fp64"]
+    assert r64.solve_status == "converged"
+    assert r32.solve_status == "converged", r32
+    assert r32.iterations <= 2 * r64.iterations + 10
+    if rule == "relative":
+        assert r32.residual_l2 <= 1.0001e-6 * r32.rhs_l2
+    else:
+        assert r32.accepted()
+    scale = max(np.abs(outs["fp64"].u).max(), np.abs(outs["fp64"].v).max())
+    assert np.abs(outs["fp32"].u - outs["fp64"].u).max() <= 1e-4 * scale
+    assert np.abs(outs["fp32"].v - outs["fp64"].v).max() <= 1e-4 * scale

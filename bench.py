@@ -51,6 +51,8 @@ def parse():
     p.add_argument("--no-serve", action="store_true", help="skip the serving (continuous batching) measurement")
     p.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision comparison")
     p.add_argument("--no-steps", action="store_true", help="skip the full-step (transport + projection) measurement")
+    p.add_argument("--no-viscous", action="store_true",
+                   help="skip the 4096x4096 variable-viscosity comparison of FP32 and mixed precision")
     p.add_argument("--tail-cells", type=int, default=0,
                    help="multigrid tail threshold in cells (0: autotuned); pins the schedule for profiling")
     p.add_argument("--serve-requests", type=int, default=16)
@@ -322,6 +324,13 @@ def run_cuda(args, world, rank, local_rank):
         line["serve"] = serve_measure(args)
     if rank == 0 and not args.no_steps:
         line["steps"] = steps_measure(args, torch)
+    if rank == 0 and not args.no_viscous:
+        from fluidsim_b200 import FluidCudaError
+
+        try:
+            line["viscous"] = viscous_measure(args, torch, flush)
+        except FluidCudaError as e:  # a solver that did not converge is reported, not hidden
+            line["viscous"] = {"error": str(e)}
     return line
 
 
@@ -419,7 +428,7 @@ def e2e_measure(args, scene, torch):
             "ms_per_step": ms}
 
 
-def steps_measure(args, torch, steps=20, warmup=3, size=1024):
+def steps_measure(args, torch, steps=100, warmup=3, size=1024):
     """Full time steps of the dam break with obstacles: a 1024x1024 scene, 16 seeded circular
     obstacles of radii 8..40 cells, gravity -9.8, dt 1/120. Each step runs RK2 semi-Lagrangian
     transport of u and v, the body force and the MG-PCG projection (FluidGrid.step, the
@@ -456,6 +465,65 @@ def steps_measure(args, torch, steps=20, warmup=3, size=1024):
             "iterations_per_step": mean_iters, "max_iterations": max(iters), "solve_status": statuses,
             "all_accepted": accepted,
             "projection_model_gbs": model_bytes / (ms / 1e3) / 1e9}
+
+
+def viscous_measure(args, torch, flush, size=4096, steps=3, warmup=1):
+    """Variable-viscosity flow at 4096x4096 (scenes.viscous_blob: a fractal liquid blob over 60 %
+    of the domain, 1000:1 density ratio, viscosity log-uniform in [1e-3, 10] along a smooth noise
+    field, U[-1, 1] FP32 velocities). One step is the implicit viscosity solve (V-cycle
+    preconditioned CG to the reference's 1e-4 relative residual) and then the MG-PCG projection
+    to the 1e-6 stop rule, from the same initial state every time, timed with CUDA events on the
+    grid's stream after an L2 flush. Plain FP32 and mixed precision (FP16 coarse-level pressure
+    weights) are each compared with an FP64 device solve of the same step: the viscosity to the
+    same 1e-4 stop rule (a tighter viscosity solve moves the velocities by a few percent of their
+    scale, which would hide the precision), then the pressure to a 1e-12 relative residual."""
+    from fluidsim_b200 import FluidGrid, scenes
+
+    scene = scenes.viscous_blob(size, size, seed=5)
+    ref = FluidGrid(size, size, scene.cell_size, "fp64")
+    scenes.upload_scene(ref, scene)
+    ref_visc, _ = ref.applyViscosity(scene.dt, 1e-4, 4000)
+    ref_proj = ref.project(scene.dt, 4000, 1e-12, relative_tolerance=1e-12)
+    exact = ref.download()
+    ref.destroy()
+    scale = max(np.abs(exact.u).max(), np.abs(exact.v).max())
+    out = {"workload": f"viscous_blob_{size}x{size}: viscosity then projection, {steps} steps after {warmup}",
+           "fp64_reference": {"viscosity_iterations": ref_visc, "pressure_iterations": ref_proj.iterations,
+                              "tolerances": "viscosity 1e-4 (the reference's rule), pressure 1e-12 relative"}}
+    for precision in ("fp32", "mixed"):
+        pristine = FluidGrid(size, size, scene.cell_size, precision)
+        scenes.upload_scene(pristine, scene)
+        work = FluidGrid(size, size, scene.cell_size, precision)
+        scenes.configure_grid(work, scene)
+        stream = torch.cuda.ExternalStream(work.stream())
+        total, visc_ms, visc_it, proj_it = [], [], [], []
+        for i in range(warmup + steps):
+            work.copyStateFrom(pristine)
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+                events = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+                events[0].record(stream)
+            it, _ = work.applyViscosity(scene.dt, 1e-4, 4000)
+            events[1].record(stream)
+            r = work.project(scene.dt, 400, args.tolerance, relative_tolerance=args.tolerance)
+            events[2].record(stream)
+            events[2].synchronize()
+            if i >= warmup:
+                total.append(events[0].elapsed_time(events[2]))
+                visc_ms.append(events[0].elapsed_time(events[1]))
+                visc_it.append(it)
+                proj_it.append(r.iterations)
+        s = work.download()
+        err = max(np.abs(s.u - exact.u).max(), np.abs(s.v - exact.v).max()) / scale
+        ms = statistics.mean(total)
+        out[precision] = {"value": scene.cells / (ms / 1e3), "unit": UNIT, "ms_per_step": ms,
+                          "viscosity_ms": statistics.mean(visc_ms), "viscosity_iterations": statistics.mean(visc_it),
+                          "pressure_iterations": statistics.mean(proj_it), "pressure_status": r.solve_status,
+                          "relative_residual": r.relative_residual, "velocity_error_vs_fp64": err}
+        work.destroy()
+        pristine.destroy()
+    out["speedup_vs_fp32"] = out["fp32"]["ms_per_step"] / out["mixed"]["ms_per_step"]
+    return out
 
 
 def batched_measure(args, torch, world=1, rank=0, count=256):

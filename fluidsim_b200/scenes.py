@@ -33,6 +33,9 @@ class Scene:
     name: str = ""
     liquid_mass: List[np.ndarray] = field(default_factory=list)
     gas_mass: List[np.ndarray] = field(default_factory=list)
+    # Per-component viscosities (liquid components, then gas); None leaves the grid inviscid.
+    liquid_viscosity: Optional[List[float]] = None
+    gas_viscosity: Optional[List[float]] = None
 
     def __post_init__(self):
         area = self.cell_size * self.cell_size
@@ -172,6 +175,59 @@ def random_pool(width, height, seed=0, dt=1.0 / 60.0, liquid_density=1000.0, gas
                  name=f"pool_{width}x{height}")
 
 
+def _fractal_noise(rng, w, h, octaves=7, base=4):
+    """Value noise: octave k is a (base * 2^k + 1)^2 lattice of U[0, 1) values, bilinearly
+    interpolated to the cell centres (along x on the lattice rows, then along y), with
+    amplitude 2^-k."""
+    total = np.zeros((h, w))
+    for k in range(octaves):
+        n = base << k
+        lattice = rng.random((n + 1, n + 1))
+        xs = (np.arange(w) + 0.5) * (n / w)
+        x0 = np.minimum(xs.astype(int), n - 1)
+        tx = xs - x0
+        rows = lattice[:, x0] * (1 - tx) + lattice[:, x0 + 1] * tx
+        ys = (np.arange(h) + 0.5) * (n / h)
+        y0 = np.minimum(ys.astype(int), n - 1)
+        ty = (ys - y0)[:, None]
+        total += (rows[y0] * (1 - ty) + rows[y0 + 1] * ty) * 0.5 ** k
+    return total
+
+
+def _uniform_ranks(a):
+    """Maps values to U(0, 1] by rank."""
+    ranks = np.empty(a.size)
+    ranks[np.argsort(a, axis=None)] = np.arange(1, a.size + 1)
+    return ranks / a.size
+
+
+def viscous_blob(width=4096, height=4096, seed=0, dt=1.0 / 120.0, cover=0.6, mu_range=(1e-3, 10.0),
+                 liquid_density=1000.0, gas_density=1.0) -> Scene:
+    """Variable-viscosity flow: a fractal-noise liquid blob over `cover` of the domain in air
+    (1000:1 density ratio), i.i.d. U[-1, 1] FP32 face velocities with the walls closed, no
+    gravity. Inside the liquid the viscosity is log-uniform over `mu_range` along a second
+    smooth noise field. The liquid is two components of equal density with the end viscosities;
+    the volume-weighted blend of their viscosities (FluidSim/UniformWebGPU/FluidGridGPU.cpp:172-217)
+    gives each cell its target. Air has the lower viscosity. The cell size is 1/width."""
+    rng = np.random.default_rng(seed)
+    blob = _fractal_noise(rng, width, height)
+    fraction = (blob >= np.quantile(blob, 1.0 - cover)).astype(float)
+    lo, hi = mu_range
+    liquid_cells = fraction > 0
+    mu = np.full((height, width), lo)
+    mu[liquid_cells] = lo * (hi / lo) ** _uniform_ranks(_fractal_noise(rng, width, height)[liquid_cells])
+    share = (mu - lo) / (hi - lo)  # volume share of the viscous component in the liquid
+    u, v = _random_faces(rng, width, height)
+    _close_walls(u, v)
+    dx = 1.0 / width
+    area = dx * dx
+    liquid = [liquid_density * fraction * (1.0 - share) * area, liquid_density * fraction * share * area]
+    return Scene(width, height, dx, dt, liquid_density, gas_density, fraction, u, v,
+                 name=f"viscous_blob_{width}x{height}", liquid_mass=liquid,
+                 gas_mass=[gas_density * (1.0 - fraction) * area], liquid_viscosity=[lo, hi],
+                 gas_viscosity=[lo])
+
+
 def uneven_batch(count=256, seed=0, min_side=64, max_side=1024, max_aspect=2.0, obstacles=True) -> List[Scene]:
     """Independent scenes with log-uniform sides, aspect up to 2:1, fill in [0.3, 0.9],
     0-8 circular obstacles and U[-1, 1] FP32 velocities."""
@@ -189,13 +245,20 @@ def uneven_batch(count=256, seed=0, min_side=64, max_side=1024, max_aspect=2.0, 
     return scenes
 
 
-def upload_scene(grid, scene: Scene, pressure=None):
-    """Configures materials, obstacles and state of a FluidGrid from a scene."""
-    from .grid import FluidGridState
-
-    grid.configureMaterials([scene.liquid_density], [scene.gas_density])
+def configure_grid(grid, scene: Scene):
+    """Configures a FluidGrid's materials, gravity, surface tension and obstacles from a scene.
+    Every component of a phase has the phase's density."""
+    grid.configureMaterials([scene.liquid_density] * len(scene.liquid_mass), [scene.gas_density] * len(scene.gas_mass),
+                            scene.liquid_viscosity, scene.gas_viscosity)
     grid.setGravityY(scene.gravity)
     if scene.surface_tension:
         grid.setSurfaceTension(scene.surface_tension)
     grid.setObstacles(scene.solid)
+
+
+def upload_scene(grid, scene: Scene, pressure=None):
+    """Configures materials, obstacles and state of a FluidGrid from a scene."""
+    from .grid import FluidGridState
+
+    configure_grid(grid, scene)
     grid.upload(FluidGridState(scene.fraction, scene.u, scene.v, pressure, scene.liquid_mass, scene.gas_mass))

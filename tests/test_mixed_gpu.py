@@ -78,3 +78,53 @@ def test_mixed_weight_scale_covers_extreme_densities(oracle):
     assert r.solve_status == "converged"
     scale = max(np.abs(uo).max(), np.abs(vo).max())
     assert max(np.abs(out.u - uo).max(), np.abs(out.v - vo).max()) <= 1e-4 * scale
+
+
+def _viscous_restatement(oracle, s):
+    """The variable-viscosity step in the FP64 restatement: viscosity to the reference's 1e-4
+    relative residual, then the projection to 1e-12."""
+    material = oracle.viscosity_material(s.liquid_mass + s.gas_mass, [s.liquid_density] * len(s.liquid_mass)
+                                         + [s.gas_density] * len(s.gas_mass),
+                                         s.liquid_viscosity + s.gas_viscosity, s.cell_size)
+    it, u, v, _ = oracle.Viscosity(s.width, s.height).solve(s.u, s.v, material, s.dt, s.cell_size, 1e-4)
+    o = oracle.OracleGrid(s.width, s.height, s.cell_size)
+    o.upload(s.density(), u, v, None, s.solid)
+    o.project(s.dt, 2000, 1e-12, relative_tolerance=1e-12)
+    return it, (u, v), o.download()
+
+
+@pytest.mark.parametrize("size", [(96, 80), (128, 128)], ids=lambda s: f"{s[0]}x{s[1]}")
+def test_viscous_blob_against_restatement(oracle, size):
+    """The variable-viscosity workload (fractal liquid blob, 1000:1 densities, viscosity
+    log-uniform in [1e-3, 10] from two liquid components) at small sizes. FP64 on the device
+    follows the restatement step by step; the viscosity solve is the same FP32 code in plain FP32
+    and in mixed precision, and both end close to the FP64 step."""
+    w, h = size
+    s = scenes.viscous_blob(w, h, seed=9)
+    it_o, (uv_o, vv_o), (uo, vo, _) = _viscous_restatement(oracle, s)
+    scale = max(np.abs(uo).max(), np.abs(vo).max())
+
+    g = _grid(s, "fp64")
+    it, _ = g.applyViscosity(s.dt, 1e-4, 4000)
+    mid = g.download()
+    assert it == it_o
+    assert max(np.abs(mid.u - uv_o).max(), np.abs(mid.v - vv_o).max()) <= 1e-10 * scale
+    r = g.project(s.dt, 2000, 1e-12, relative_tolerance=1e-12)
+    out = g.download()
+    assert r.solve_status == "converged"
+    assert max(np.abs(out.u - uo).max(), np.abs(out.v - vo).max()) <= 1e-8 * scale
+
+    runs = {}
+    for precision in ("fp32", "mixed"):
+        g = _grid(s, precision)
+        it, _ = g.applyViscosity(s.dt, 1e-4, 4000)
+        mid = g.download()
+        r = g.project(s.dt, 500, 1e-6, relative_tolerance=1e-6)
+        out = g.download()
+        assert r.solve_status == "converged" and r.residual_l2 <= 1.0001e-6 * r.rhs_l2, (precision, r)
+        runs[precision] = (it, mid, max(np.abs(out.u - uo).max(), np.abs(out.v - vo).max()) / scale)
+    (it32, mid32, err32), (itm, midm, errm) = runs["fp32"], runs["mixed"]
+    assert it32 == itm == it_o
+    assert np.array_equal(mid32.u, midm.u) and np.array_equal(mid32.v, midm.v)
+    # FP32 viscosity and a 1e-6 projection against the FP64 step: 1e-4 of the scale.
+    assert err32 <= 1e-4 and errm <= 1e-4

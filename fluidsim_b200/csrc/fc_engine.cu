@@ -1734,9 +1734,12 @@ size_t viscosity_layout(const Grid& g, ViscWork* work, char* base)
     for (void*& p : vecs)
         p = take(nodes0 * 2 * e);
     void* state = take(sizeof(ViscState));
+    // visc_arrive_last: one partial per block and per group of kViscThreads blocks, a counter
+    // per group and one for the groups.
     const int blocks = ceil_div(int(nodes0), kViscThreads);
-    void* partial = take(size_t(blocks) * sizeof(double4));
-    void* counter = take(sizeof(unsigned int) * 4);
+    const int groups = ceil_div(blocks, kViscThreads);
+    void* partial = take(size_t(blocks + groups) * sizeof(double4));
+    void* counter = take(sizeof(unsigned int) * (1 + groups));
     void* comp = take(size_t(std::max(g.components(), 1)) * sizeof(double2));
     if (work)
     {

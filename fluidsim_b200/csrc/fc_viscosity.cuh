@@ -82,33 +82,59 @@ template <typename T> struct Nodes
     __device__ T4 coeff(const void* c, int x, int y) const { return static_cast<const T4*>(c)[at(x, y)]; }
 };
 
-// Deterministic block-then-grid reduction: each block stores its partial; the last block to
-// arrive folds them in index order.
+// Deterministic two-level reduction. Blocks arrive in fixed groups of NT consecutive blocks:
+// the last block of a group to arrive folds the group's partials (one per thread, then
+// block_reduce4's fixed tree) into a group sum, and the last group to finish folds the group
+// sums (each thread a contiguous run, in index order). No serial chain is longer than two
+// loads per thread, and the order of every sum is set by the block indices, not by arrival.
+// partial holds blocks + groups slots; counter[0] counts finished groups and counter[1 + g] the
+// arrivals in group g (viscosity_layout sizes both).
 template <int NT>
 __device__ bool visc_arrive_last(double4* partial, unsigned int* counter, int index, int blocks, double4 mine,
     double4* total, int max_mask)
 {
     __shared__ int is_last;
+    const int group = index / NT, groups = (blocks + NT - 1) / NT;
+    const int first = group * NT, members = min(NT, blocks - first);
     if (threadIdx.x == 0)
     {
         partial[index] = mine;
         __threadfence();
-        is_last = atomicAdd(counter, 1u) == unsigned(blocks - 1);
+        is_last = atomicAdd(counter + 1 + group, 1u) == unsigned(members - 1);
     }
     __syncthreads();
     if (!is_last)
         return false;
     __threadfence();
-    const int per = (blocks + NT - 1) / NT;
-    const int first = threadIdx.x * per, last = min(blocks, first + per);
-    double4 acc = make_double4(0, 0, 0, 0);
-    for (int t = first; t < last; ++t)
+    const double2* slots = reinterpret_cast<const double2*>(partial);
+    double4 v = make_double4(0, 0, 0, 0);
+    if (int(threadIdx.x) < members)
     {
-        const volatile double* slot = reinterpret_cast<const volatile double*>(&partial[t]);
-        acc.x = (max_mask & 1) ? fmax(acc.x, slot[0]) : acc.x + slot[0];
-        acc.y = (max_mask & 2) ? fmax(acc.y, slot[1]) : acc.y + slot[1];
-        acc.z = (max_mask & 4) ? fmax(acc.z, slot[2]) : acc.z + slot[2];
-        acc.w = (max_mask & 8) ? fmax(acc.w, slot[3]) : acc.w + slot[3];
+        const double2 lo = __ldcg(slots + 2 * (first + threadIdx.x)), hi = __ldcg(slots + 2 * (first + threadIdx.x) + 1);
+        v = make_double4(lo.x, lo.y, hi.x, hi.y);
+    }
+    const double4 group_total = block_reduce4<NT>(v, max_mask);
+    if (threadIdx.x == 0)
+    {
+        partial[blocks + group] = group_total;
+        counter[1 + group] = 0u;
+        __threadfence();
+        is_last = atomicAdd(counter, 1u) == unsigned(groups - 1);
+    }
+    __syncthreads();
+    if (!is_last)
+        return false;
+    __threadfence();
+    const int per = (groups + NT - 1) / NT;
+    const int a = threadIdx.x * per, b = min(groups, a + per);
+    double4 acc = make_double4(0, 0, 0, 0);
+    for (int t = a; t < b; ++t)
+    {
+        const double2 lo = __ldcg(slots + 2 * (blocks + t)), hi = __ldcg(slots + 2 * (blocks + t) + 1);
+        acc.x = (max_mask & 1) ? fmax(acc.x, lo.x) : acc.x + lo.x;
+        acc.y = (max_mask & 2) ? fmax(acc.y, lo.y) : acc.y + lo.y;
+        acc.z = (max_mask & 4) ? fmax(acc.z, hi.x) : acc.z + hi.x;
+        acc.w = (max_mask & 8) ? fmax(acc.w, hi.y) : acc.w + hi.y;
     }
     const double4 out = block_reduce4<NT>(acc, max_mask);
     if (threadIdx.x == 0)
@@ -468,20 +494,35 @@ __global__ void __launch_bounds__(kViscThreads) k_visc_restrict(ViscLevel fine, 
     double value[2] = {0.0, 0.0};
     if (!visc_stopped(state))
     {
+        // The 4 x 4 fine nodes 2p - 1 .. 2p + 2 cover both components' stencils; they are loaded
+        // together (indices clamped into the lattice, the clamped copies unused), then summed in
+        // the stencil's row order, skipping nodes outside the lattice.
         const T2* res = static_cast<const T2*>(fine.res);
+        T2 q[4][4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+            {
+                const int qx = clampi(2 * px + i - 1, 0, fine.w), qy = clampi(2 * py + j - 1, 0, fine.h);
+                q[j][i] = res[(long long)qy * (fine.w + 1) + qx];
+            }
+#pragma unroll
         for (int component = 0; component < 2; ++component)
         {
             if ((component == 0 && (px == 0 || px == coarse.w || py == coarse.h)) ||
                 (component == 1 && (py == 0 || py == coarse.h || px == coarse.w)))
                 continue;
             const int ex = component == 1 ? 2 : 1, ey = component == 1 ? 1 : 2;
-            for (int y = -1; y <= ey; ++y)
-                for (int x = -1; x <= ex; ++x)
+#pragma unroll
+            for (int y = -1; y <= 2; ++y)
+#pragma unroll
+                for (int x = -1; x <= 2; ++x)
                 {
                     const int qx = 2 * px + x, qy = 2 * py + y;
-                    if (qx < 0 || qy < 0 || qx > fine.w || qy > fine.h)
+                    if (x > ex || y > ey || qx < 0 || qy < 0 || qx > fine.w || qy > fine.h)
                         continue;
-                    const T2 r = res[(long long)qy * (fine.w + 1) + qx];
+                    const T2 r = q[y + 1][x + 1];
                     value[component] += transfer_weight(qx, qy, px, py, component, coarse.w, coarse.h) *
                                         double(component == 0 ? r.x : r.y);
                 }

@@ -1846,9 +1846,10 @@ template <typename T> ViscResult viscosity_solve(Grid& g, double dt, double tole
     const unsigned char* solid = g.has_solid ? g.solid : nullptr;
     const int nodes = (g.W + 1) * (g.H + 1);
     const int blocks = ceil_div(nodes, kViscThreads);
+    const int reduce_blocks = ceil_div(nodes, kViscThreads * kViscReduceNodes);
     ViscLevel& L0 = w.lev[0];
     FC_LAUNCH(k_visc_pack<T>, blocks, kViscThreads, 0, s, g.W, g.H, g.desc.u, g.desc.v, L0.coeff, solid, w.solution, w.rhs);
-    FC_LAUNCH((k_visc_residual<T, kResidualInitial>), blocks, kViscThreads, 0, s, L0, dt, solid, w.solution, w.rhs,
+    FC_LAUNCH((k_visc_residual<T, kResidualInitial>), reduce_blocks, kViscThreads, 0, s, L0, dt, solid, w.solution, w.rhs,
         w.residual, w.state, w.partial, w.counter, tolerance);
     ViscState h{};
     auto read_state = [&]
@@ -1870,16 +1871,16 @@ template <typename T> ViscResult viscosity_solve(Grid& g, double dt, double tole
         for (int i = 0; i < batch; ++i)
         {
             viscosity_cycle<T>(w, 0, w.residual, dt, solid, s);
-            FC_LAUNCH(k_visc_dot_rz<T>, blocks, kViscThreads, 0, s, nodes, L0.coeff, w.residual, L0.x, w.state,
+            FC_LAUNCH(k_visc_dot_rz<T>, reduce_blocks, kViscThreads, 0, s, nodes, L0.coeff, w.residual, L0.x, w.state,
                 w.partial, w.counter);
             FC_LAUNCH(k_visc_direction<T>, blocks, kViscThreads, 0, s, nodes, L0.x, w.direction, w.state);
-            FC_LAUNCH((k_visc_apply<T, true>), blocks, kViscThreads, 0, s, L0, dt, solid, w.direction, w.product,
+            FC_LAUNCH((k_visc_apply<T, true>), reduce_blocks, kViscThreads, 0, s, L0, dt, solid, w.direction, w.product,
                 w.state, w.partial, w.counter);
             FC_LAUNCH(k_visc_update<T>, blocks, kViscThreads, 0, s, nodes, w.solution, w.residual, w.direction,
                 w.product, w.state);
         }
         result.iterations += batch;
-        FC_LAUNCH((k_visc_residual<T, kResidualTruth>), blocks, kViscThreads, 0, s, L0, dt, solid, w.solution, w.rhs,
+        FC_LAUNCH((k_visc_residual<T, kResidualTruth>), reduce_blocks, kViscThreads, 0, s, L0, dt, solid, w.solution, w.rhs,
             w.truth, w.state, w.partial, w.counter, tolerance);
         read_state();
         result.relative_residual = std::sqrt(h.truth / std::max(h.energy, 1e-30));

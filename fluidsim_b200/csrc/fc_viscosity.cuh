@@ -20,6 +20,10 @@ namespace fc
 
 constexpr int kViscThreads = 256;
 constexpr int kViscCoarseNodes = 256; // the coarsest level fits one block
+// Nodes per thread of the kernels that end in a grid reduction: a block covers this many runs
+// of kViscThreads consecutive nodes, so the per-block reduction, fence and atomic are paid a
+// quarter as often.
+constexpr int kViscReduceNodes = 4;
 
 template <typename T> struct Vec;
 template <> struct Vec<float>
@@ -290,12 +294,16 @@ __global__ void __launch_bounds__(kViscThreads) k_visc_apply(ViscLevel lv, doubl
     const void* f, void* out, ViscState* state, double4* partial, unsigned int* counter)
 {
     using T2 = typename Vec<T>::two;
+    constexpr int kNodes = kDot ? kViscReduceNodes : 1;
     const Nodes<T> L{lv.w, lv.h};
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
     const bool stopped = visc_stopped(state);
     double dq = 0.0;
-    if (n < (lv.w + 1) * (lv.h + 1))
+#pragma unroll 1
+    for (int k = 0; k < kNodes; ++k)
     {
+        const int n = (blockIdx.x * kNodes + k) * blockDim.x + threadIdx.x;
+        if (n >= (lv.w + 1) * (lv.h + 1))
+            break;
         const int x = n % (lv.w + 1), y = n / (lv.w + 1);
         T2 r;
         r.x = r.y = T(0);
@@ -307,7 +315,7 @@ __global__ void __launch_bounds__(kViscThreads) k_visc_apply(ViscLevel lv, doubl
             r.x = m.u ? ax : T(0);
             r.y = m.v ? ay : T(0);
             const T2 d = static_cast<const T2*>(f)[n];
-            dq = double(d.x) * double(r.x) + double(d.y) * double(r.y);
+            dq += double(d.x) * double(r.x) + double(d.y) * double(r.y);
         }
         static_cast<T2*>(out)[n] = r;
     }
@@ -385,17 +393,22 @@ __global__ void __launch_bounds__(kViscThreads) k_visc_residual(ViscLevel lv, do
     double tolerance)
 {
     using T2 = typename Vec<T>::two;
+    constexpr int kNodes = kMode == kResidualPlain ? 1 : kViscReduceNodes;
     const Nodes<T> L{lv.w, lv.h};
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (kMode == kResidualPlain && visc_stopped(state))
     {
+        const int n = blockIdx.x * blockDim.x + threadIdx.x;
         if (n < (lv.w + 1) * (lv.h + 1))
             static_cast<T2*>(out)[n] = T2{T(0), T(0)};
         return;
     }
     double4 mine = make_double4(0, 0, 0, 0);
-    if (n < (lv.w + 1) * (lv.h + 1))
+#pragma unroll 1
+    for (int k = 0; k < kNodes; ++k)
     {
+        const int n = (blockIdx.x * kNodes + k) * blockDim.x + threadIdx.x;
+        if (n >= (lv.w + 1) * (lv.h + 1))
+            break;
         const int x = n % (lv.w + 1), y = n / (lv.w + 1);
         const FaceMask m = face_mask(lv.w, lv.h, x, y, solid);
         T ax, ay;
@@ -409,12 +422,12 @@ __global__ void __launch_bounds__(kViscThreads) k_visc_residual(ViscLevel lv, do
         {
             const auto c = L.coeff(lv.coeff, x, y);
             const double rx = r.x, ry = r.y;
-            mine.x = rx / double(c.z) * rx + ry / double(c.w) * ry;
+            mine.x += rx / double(c.z) * rx + ry / double(c.w) * ry;
             if (kMode == kResidualInitial)
             {
                 const T2 v = static_cast<const T2*>(f)[n];
-                mine.y = double(c.z) * double(v.x) * double(v.x) + double(c.w) * double(v.y) * double(v.y);
-                mine.z = double(c.z) + double(c.w);
+                mine.y += double(c.z) * double(v.x) * double(v.x) + double(c.w) * double(v.y) * double(v.y);
+                mine.z += double(c.z) + double(c.w);
             }
         }
     }
@@ -455,8 +468,6 @@ __global__ void __launch_bounds__(kViscThreads) k_visc_residual(ViscLevel lv, do
 // exact transpose, with the reference's tangential clamps.
 // ---------------------------------------------------------------------------------------------
 
-__device__ __forceinline__ double transfer_offset_x(int component) { return component == 1 ? 0.5 : 0.0; }
-__device__ __forceinline__ double transfer_offset_y(int component) { return component == 1 ? 0.0 : 0.5; }
 
 __device__ __forceinline__ void transfer_clamp(int bx, int by, int component, int cw, int ch, int& cx, int& cy)
 {
@@ -464,12 +475,29 @@ __device__ __forceinline__ void transfer_clamp(int bx, int by, int component, in
     cy = clampi(by, 0, ch - (component == 1 ? 0 : 1));
 }
 
+// Coarse coordinate of fine index f along an axis with face offset `half` (0 or 1/2):
+// l = (f + half) / 2 - half, returned as b = floor(l) and t = l - b. Both are exact in integer
+// arithmetic: t is 0 or 1/2 without the offset, 3/4 or 1/4 with it.
+__device__ __forceinline__ void transfer_axis(int f, bool half, int& b, double& t)
+{
+    if (half)
+    {
+        b = (f - 1) >> 1; // arithmetic shift: floor((f - 1) / 2)
+        t = (f & 1) ? 0.25 : 0.75;
+    }
+    else
+    {
+        b = f >> 1;
+        t = (f & 1) ? 0.5 : 0.0;
+    }
+}
+
 __device__ __forceinline__ double transfer_weight(int fx, int fy, int px, int py, int component, int cw, int ch)
 {
-    const double lx = (fx + transfer_offset_x(component)) * 0.5 - transfer_offset_x(component);
-    const double ly = (fy + transfer_offset_y(component)) * 0.5 - transfer_offset_y(component);
-    const int bx = int(floor(lx)), by = int(floor(ly));
-    const double tx = lx - bx, ty = ly - by;
+    int bx, by;
+    double tx, ty;
+    transfer_axis(fx, component == 1, bx, tx);
+    transfer_axis(fy, component == 0, by, ty);
     double result = 0.0;
     for (int y = 0; y < 2; ++y)
         for (int x = 0; x < 2; ++x)
@@ -507,6 +535,25 @@ __global__ void __launch_bounds__(kViscThreads) k_visc_restrict(ViscLevel fine, 
                 const int qx = clampi(2 * px + i - 1, 0, fine.w), qy = clampi(2 * py + j - 1, 0, fine.h);
                 q[j][i] = res[(long long)qy * (fine.w + 1) + qx];
             }
+        if (px >= 2 && py >= 2 && px <= coarse.w - 3 && py <= coarse.h - 3)
+        {
+            // No clamp reaches a node two or more from every edge: each stencil weight is the
+            // product of the 1D weights (1/2, 1, 1/2) along the face's own axis and
+            // (1/4, 3/4, 3/4, 1/4) across it, exactly transfer_weight's value.
+            constexpr double kNear[3] = {0.5, 1.0, 0.5};
+            constexpr double kFar[4] = {0.25, 0.75, 0.75, 0.25};
+#pragma unroll
+            for (int y = 0; y < 4; ++y)
+#pragma unroll
+                for (int x = 0; x < 3; ++x)
+                    value[0] += kNear[x] * kFar[y] * double(q[y][x].x);
+#pragma unroll
+            for (int y = 0; y < 3; ++y)
+#pragma unroll
+                for (int x = 0; x < 4; ++x)
+                    value[1] += kFar[x] * kNear[y] * double(q[y][x].y);
+        }
+        else
 #pragma unroll
         for (int component = 0; component < 2; ++component)
         {
@@ -551,13 +598,16 @@ __global__ void __launch_bounds__(kViscThreads) k_visc_prolong(ViscLevel fine, V
         const T2 own = static_cast<const T2*>(fine.x)[n];
         const T2* c = static_cast<const T2*>(coarse.x);
         T value[2] = {own.x, own.y};
+#pragma unroll
         for (int component = 0; component < 2; ++component)
         {
-            const double lx = (px + transfer_offset_x(component)) * 0.5 - transfer_offset_x(component);
-            const double ly = (py + transfer_offset_y(component)) * 0.5 - transfer_offset_y(component);
-            const int bx = int(floor(lx)), by = int(floor(ly));
-            const double tx = lx - bx, ty = ly - by;
+            int bx, by;
+            double tx, ty;
+            transfer_axis(px, component == 1, bx, tx);
+            transfer_axis(py, component == 0, by, ty);
+#pragma unroll
             for (int y = 0; y < 2; ++y)
+#pragma unroll
                 for (int x = 0; x < 2; ++x)
                 {
                     int cx, cy;
@@ -644,14 +694,32 @@ __global__ void __launch_bounds__(kViscThreads) k_visc_dot_rz(int nodes, const v
 {
     using T2 = typename Vec<T>::two;
     using T4 = typename Vec<T>::four;
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
     double4 mine = make_double4(0, 0, 0, 0);
-    if (n < nodes && !visc_stopped(state))
+    if (!visc_stopped(state))
     {
-        const T2 a = static_cast<const T2*>(r)[n], b = static_cast<const T2*>(z)[n];
-        const T4 c = static_cast<const T4*>(coeff)[n];
-        mine.x = double(a.x) * double(b.x) + double(a.y) * double(b.y);
-        mine.y = double(a.x) / double(c.z) * double(a.x) + double(a.y) / double(c.w) * double(a.y);
+        T2 a[kViscReduceNodes], b[kViscReduceNodes];
+        T4 c[kViscReduceNodes];
+#pragma unroll
+        for (int k = 0; k < kViscReduceNodes; ++k)
+        {
+            const int n = (blockIdx.x * kViscReduceNodes + k) * blockDim.x + threadIdx.x;
+            if (n < nodes)
+            {
+                a[k] = static_cast<const T2*>(r)[n];
+                b[k] = static_cast<const T2*>(z)[n];
+                c[k] = static_cast<const T4*>(coeff)[n];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kViscReduceNodes; ++k)
+        {
+            const int n = (blockIdx.x * kViscReduceNodes + k) * blockDim.x + threadIdx.x;
+            if (n < nodes)
+            {
+                mine.x += double(a[k].x) * double(b[k].x) + double(a[k].y) * double(b[k].y);
+                mine.y += double(a[k].x) / double(c[k].z) * double(a[k].x) + double(a[k].y) / double(c[k].w) * double(a[k].y);
+            }
+        }
     }
     double4 total;
     if (visc_arrive_last<kViscThreads>(partial, counter, blockIdx.x, gridDim.x, block_reduce4<kViscThreads>(mine, 0),

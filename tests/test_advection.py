@@ -194,3 +194,21 @@ def test_gpu_step_transports_then_projects(oracle):
     sa, sb = a.download(), b.download()
     for x, y in ((sa.u, sb.u), (sa.v, sb.v), (sa.pressure, sb.pressure), (sa.liquid_fraction, sb.liquid_fraction)):
         assert np.array_equal(x, y)
+
+
+@pytest.mark.gpu
+def test_gpu_steps_of_a_dam_break_are_all_accepted():
+    """Sixty whole FP32 steps of a 256x256 dam break with obstacles, with the reference's step
+    defaults (200 iterations, divergence 1e-6): every projection is accepted under the
+    reference's result contract, and none runs to its iteration cap."""
+    from fluidsim_b200 import scenes
+
+    sc = scenes.dam_break(256, 256, seed=11, obstacles=8, velocity=0.0)
+    g = _grid(sc.width, sc.height, sc.cell_size, "fp32")
+    scenes.upload_scene(g, sc)
+    for step in range(60):
+        r = g.step(sc.dt, 200, 1e-6)
+        assert r.solve_status == "converged" and r.accepted(), (step, r)
+        assert r.iterations < 200
+    s = g.download()
+    assert np.isfinite(s.u).all() and np.isfinite(s.v).all()

@@ -1785,22 +1785,22 @@ template <typename T> void viscosity_cycle(ViscWork& w, size_t l, void* b, doubl
     {
         ViscLevel c = L;
         c.rhs = b;
-        FC_LAUNCH(k_visc_coarse<T>, 1, kViscCoarseNodes, 0, s, c, dt, mask, w.state);
+        FC_LAUNCH_DEP(k_visc_coarse<T>, 1, kViscCoarseNodes, 0, s, c, dt, mask, w.state);
         return;
     }
     auto smooth = [&](int zero)
     {
-        FC_LAUNCH(k_visc_smooth<T>, blocks, kViscThreads, 0, s, L, dt, mask, b, zero, w.state);
+        FC_LAUNCH_DEP(k_visc_smooth<T>, blocks, kViscThreads, 0, s, L, dt, mask, b, zero, w.state);
         std::swap(L.x, L.next);
     };
     smooth(1);
     smooth(0);
-    FC_LAUNCH((k_visc_residual<T, kResidualPlain>), blocks, kViscThreads, 0, s, L, dt, mask, L.x, b, L.res, w.state,
+    FC_LAUNCH_DEP((k_visc_residual<T, kResidualPlain>), blocks, kViscThreads, 0, s, L, dt, mask, L.x, b, L.res, w.state,
         w.partial, w.counter, 0.0);
     ViscLevel& C = w.lev[l + 1];
-    FC_LAUNCH(k_visc_restrict<T>, ceil_div((C.w + 1) * (C.h + 1), kViscThreads), kViscThreads, 0, s, L, C, w.state);
+    FC_LAUNCH_DEP(k_visc_restrict<T>, ceil_div((C.w + 1) * (C.h + 1), kViscThreads), kViscThreads, 0, s, L, C, w.state);
     viscosity_cycle<T>(w, l + 1, C.rhs, dt, solid, s);
-    FC_LAUNCH(k_visc_prolong<T>, blocks, kViscThreads, 0, s, L, C, mask, w.state);
+    FC_LAUNCH_DEP(k_visc_prolong<T>, blocks, kViscThreads, 0, s, L, C, mask, w.state);
     std::swap(L.x, L.next);
     smooth(0);
     smooth(0);
@@ -1871,16 +1871,16 @@ template <typename T> ViscResult viscosity_solve(Grid& g, double dt, double tole
         for (int i = 0; i < batch; ++i)
         {
             viscosity_cycle<T>(w, 0, w.residual, dt, solid, s);
-            FC_LAUNCH(k_visc_dot_rz<T>, reduce_blocks, kViscThreads, 0, s, nodes, L0.coeff, w.residual, L0.x, w.state,
+            FC_LAUNCH_DEP(k_visc_dot_rz<T>, reduce_blocks, kViscThreads, 0, s, nodes, L0.coeff, w.residual, L0.x, w.state,
                 w.partial, w.counter);
-            FC_LAUNCH(k_visc_direction<T>, blocks, kViscThreads, 0, s, nodes, L0.x, w.direction, w.state);
-            FC_LAUNCH((k_visc_apply<T, true>), reduce_blocks, kViscThreads, 0, s, L0, dt, solid, w.direction, w.product,
+            FC_LAUNCH_DEP(k_visc_direction<T>, blocks, kViscThreads, 0, s, nodes, L0.x, w.direction, w.state);
+            FC_LAUNCH_DEP((k_visc_apply<T, true>), reduce_blocks, kViscThreads, 0, s, L0, dt, solid, w.direction, w.product,
                 w.state, w.partial, w.counter);
-            FC_LAUNCH(k_visc_update<T>, blocks, kViscThreads, 0, s, nodes, w.solution, w.residual, w.direction,
+            FC_LAUNCH_DEP(k_visc_update<T>, blocks, kViscThreads, 0, s, nodes, w.solution, w.residual, w.direction,
                 w.product, w.state);
         }
         result.iterations += batch;
-        FC_LAUNCH((k_visc_residual<T, kResidualTruth>), reduce_blocks, kViscThreads, 0, s, L0, dt, solid, w.solution, w.rhs,
+        FC_LAUNCH_DEP((k_visc_residual<T, kResidualTruth>), reduce_blocks, kViscThreads, 0, s, L0, dt, solid, w.solution, w.rhs,
             w.truth, w.state, w.partial, w.counter, tolerance);
         read_state();
         result.relative_residual = std::sqrt(h.truth / std::max(h.energy, 1e-30));
@@ -1889,7 +1889,7 @@ template <typename T> ViscResult viscosity_solve(Grid& g, double dt, double tole
         if (h.truth <= h.target)
             break;
         if (h.stopped)
-            FC_LAUNCH(k_visc_refresh<T>, blocks, kViscThreads, 0, s, nodes, w.truth, w.residual, w.state);
+            FC_LAUNCH_DEP(k_visc_refresh<T>, blocks, kViscThreads, 0, s, nodes, w.truth, w.residual, w.state);
     }
     FC_LAUNCH(k_visc_unpack<T>, blocks, kViscThreads, 0, s, g.W, g.H, w.solution, g.desc.u, g.desc.v);
     check(cudaStreamSynchronize(s), "viscosity");

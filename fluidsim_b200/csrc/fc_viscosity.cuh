@@ -10,7 +10,9 @@
 // Layout: the (w+1) x (h+1) node lattice of a level, row-major; node p holds u face p (x) and v
 // face p (y) as one 2-vector, and 4 coefficients (cell mu, vertex mu, u-face mass, v-face mass).
 // Reads outside a field clamp to its edge, as the reference's field accessor does. One thread
-// per node, 1D blocks of kViscThreads.
+// per node, 1D blocks of kViscThreads. The V-cycle and CG kernels are launched as programmatic
+// dependents of their predecessor and wait for it (dependency_wait) before their first memory
+// access, so only the launch itself overlaps the kernel before.
 #pragma once
 
 #include "fc_device.cuh"
@@ -293,6 +295,8 @@ template <typename T, bool kDot>
 __global__ void __launch_bounds__(kViscThreads) k_visc_apply(ViscLevel lv, double dt, const unsigned char* solid,
     const void* f, void* out, ViscState* state, double4* partial, unsigned int* counter)
 {
+    allow_dependents();
+    dependency_wait();
     using T2 = typename Vec<T>::two;
     constexpr int kNodes = kDot ? kViscReduceNodes : 1;
     const Nodes<T> L{lv.w, lv.h};
@@ -344,6 +348,8 @@ template <typename T>
 __global__ void __launch_bounds__(kViscThreads) k_visc_smooth(ViscLevel lv, double dt, const unsigned char* solid,
     const void* b, int zero, const ViscState* state)
 {
+    allow_dependents();
+    dependency_wait();
     using T2 = typename Vec<T>::two;
     const Nodes<T> L{lv.w, lv.h};
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
@@ -392,6 +398,8 @@ __global__ void __launch_bounds__(kViscThreads) k_visc_residual(ViscLevel lv, do
     const void* f, const void* b, void* out, ViscState* state, double4* partial, unsigned int* counter,
     double tolerance)
 {
+    allow_dependents();
+    dependency_wait();
     using T2 = typename Vec<T>::two;
     constexpr int kNodes = kMode == kResidualPlain ? 1 : kViscReduceNodes;
     const Nodes<T> L{lv.w, lv.h};
@@ -514,6 +522,8 @@ __device__ __forceinline__ double transfer_weight(int fx, int fy, int px, int py
 template <typename T>
 __global__ void __launch_bounds__(kViscThreads) k_visc_restrict(ViscLevel fine, ViscLevel coarse, const ViscState* state)
 {
+    allow_dependents();
+    dependency_wait();
     using T2 = typename Vec<T>::two;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= (coarse.w + 1) * (coarse.h + 1))
@@ -586,6 +596,8 @@ template <typename T>
 __global__ void __launch_bounds__(kViscThreads) k_visc_prolong(ViscLevel fine, ViscLevel coarse,
     const unsigned char* solid, const ViscState* state)
 {
+    allow_dependents();
+    dependency_wait();
     using T2 = typename Vec<T>::two;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= (fine.w + 1) * (fine.h + 1))
@@ -629,6 +641,8 @@ template <typename T>
 __global__ void __launch_bounds__(kViscCoarseNodes) k_visc_coarse(ViscLevel lv, double dt, const unsigned char* solid,
     const ViscState* state)
 {
+    allow_dependents();
+    dependency_wait();
     using T2 = typename Vec<T>::two;
     using T4 = typename Vec<T>::four;
     __shared__ T2 sx[kViscCoarseNodes];
@@ -692,6 +706,8 @@ template <typename T>
 __global__ void __launch_bounds__(kViscThreads) k_visc_dot_rz(int nodes, const void* coeff, const void* r, const void* z,
     ViscState* state, double4* partial, unsigned int* counter)
 {
+    allow_dependents();
+    dependency_wait();
     using T2 = typename Vec<T>::two;
     using T4 = typename Vec<T>::four;
     double4 mine = make_double4(0, 0, 0, 0);
@@ -747,6 +763,8 @@ __global__ void __launch_bounds__(kViscThreads) k_visc_dot_rz(int nodes, const v
 template <typename T>
 __global__ void __launch_bounds__(kViscThreads) k_visc_direction(int nodes, const void* z, void* d, const ViscState* state)
 {
+    allow_dependents();
+    dependency_wait();
     using T2 = typename Vec<T>::two;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= nodes || visc_stopped(state))
@@ -768,6 +786,8 @@ template <typename T>
 __global__ void __launch_bounds__(kViscThreads) k_visc_update(int nodes, void* x, void* r, const void* d, const void* q,
     const ViscState* state)
 {
+    allow_dependents();
+    dependency_wait();
     using T2 = typename Vec<T>::two;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= nodes || visc_stopped(state))
@@ -823,6 +843,8 @@ __global__ void __launch_bounds__(kViscThreads) k_visc_unpack(int w, int h, cons
 template <typename T>
 __global__ void __launch_bounds__(kViscThreads) k_visc_refresh(int nodes, const void* truth, void* r, ViscState* state)
 {
+    allow_dependents();
+    dependency_wait();
     using T2 = typename Vec<T>::two;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n < nodes)

@@ -148,3 +148,46 @@ def test_restatement_matches_live_reference(oracle, size):
     assert gr.iterations == rr.iterations and gr.converged == rr.converged
     assert np.abs(ug - ur).max() <= 1e-8 * max(1.0, np.abs(ur).max())
     assert np.abs(pg - pr).max() <= 1e-8 * np.abs(pr).max()
+
+
+@pytest.mark.parametrize("size", [(1, 129), (131, 1), (2, 67), (65, 47), (128, 128)], ids=lambda s: f"{s[0]}x{s[1]}")
+def test_restatement_multigrid_matches_diagonal(oracle, size):
+    """FluidGridTests.cpp:627-660: both preconditioners give the same velocities within 2e-6."""
+    s = scenes.sloped_pool(*size)
+    out = []
+    for multigrid in (True, False):
+        g = oracle.OracleGrid(s.width, s.height, s.cell_size)
+        g.set_preconditioner(multigrid)
+        g.upload(s.density(), s.u, s.v)
+        assert g.project(1.0 / 120.0, 4000, 1e-8).converged
+        out.append(g.download())
+    assert np.abs(out[0][0] - out[1][0]).max() < 2e-6 and np.abs(out[0][1] - out[1][1]).max() < 2e-6
+
+
+def test_restatement_large_mixed_pressure_within_default_budget(oracle):
+    """FluidGridTests.cpp:662-681: the 512x512 sloped pool converges within 200 iterations."""
+    s = scenes.sloped_pool(512, 512)
+    g = oracle.OracleGrid(512, 512, s.cell_size)
+    g.upload(s.density(), s.u, s.v)
+    r = g.project(1.0 / 120.0)
+    assert r.converged and r.max_divergence <= 1e-6
+
+
+def test_restatement_matches_live_reference_on_odd_grid(oracle):
+    """FluidGridTests.cpp:683-708's 513x257 grid: the restatement and the reference engine itself
+    agree within the reference test's 2e-7."""
+    w, h = 513, 257
+    y, x = np.mgrid[0:h, 0:w]
+    f = np.clip(y + 1.0 - (0.3 * x + 30.0), 0.0, 1.0)
+    u = np.sin(np.arange((w + 1) * h) * 0.03).reshape(h, w + 1)
+    v = np.cos(np.arange(w * (h + 1)) * 0.017).reshape(h + 1, w)
+    ref = oracle.ReferenceGrid(w, h, 1.0, 100.0, 0.1)
+    ref.upload(f, u, v, None, 100.0 * f, 0.1 * (1.0 - f))
+    rr = ref.project(0.004, 2000, 1e-8)
+    _, ur, vr, _ = ref.download()
+    g = oracle.OracleGrid(w, h, 1.0)
+    g.upload(100.0 * f + 0.1 * (1.0 - f), u, v)
+    gr = g.project(0.004, 2000, 1e-8)
+    ug, vg, _ = g.download()
+    assert rr.converged and gr.converged
+    assert np.abs(ug - ur).max() < 2e-7 and np.abs(vg - vr).max() < 2e-7

@@ -280,8 +280,8 @@ def run_cuda(args, world, rank, local_rank):
                 "traffic": None if traffic is None else traffic * scene.cells,
                 "kernel": KERNEL_NAMES[dominant], "kernel_ms": kernel_ms[dominant],
                 "algorithmic_bytes": algorithmic, "peak_source": f"{peak_kind} hbm_gbs (copy, burst)"}
-    # Whole-projection bandwidth against the survey's per-iteration byte model (306 B/cell per
-    # PCG iteration plus 70 B/cell of set-up), for reference beside the kernel figure.
+    # Whole-projection bandwidth against the byte model of an unfused projection (306 B/cell per
+    # PCG iteration plus 70 B/cell of set-up), for comparison beside the kernel figure.
     mean_iters = statistics.mean(r.iterations for r in results)
     model_bytes = scene.cells * (70 + 306 * mean_iters)
     projection_model = {"iterations": mean_iters, "bytes": model_bytes,

@@ -81,3 +81,53 @@ def test_cpp_adapter_compiles_against_reference_contract(tmp_path):
         cmd.insert(2, f"-I{nlohmann}")
     out = subprocess.run(cmd, capture_output=True, text=True)
     assert out.returncode == 0, out.stderr[-2000:]
+
+
+def _prototypes():
+    """extern "C" prototypes of include/fluidcuda.h: name -> (return type, [parameter types])."""
+    import re
+
+    text = open(os.path.join(os.path.dirname(__file__), "..", "include", "fluidcuda.h")).read()
+    text = re.sub(r"/\*.*?\*/", " ", text, flags=re.S)
+    text = re.sub(r"//[^\n]*", " ", text)
+    out = {}
+    for ret, name, params in re.findall(r"([A-Za-z_][\w \*]*?)\s*\b(fc_\w+)\s*\(([^;{]*?)\)\s*;", text):
+        types = []
+        for p in (q.strip() for q in params.split(",")):
+            if not p or p == "void":
+                continue
+            p = re.sub(r"\s*\b\w+\s*(\[\s*\])?$", "", p) if not p.endswith("*") else p
+            types.append(" ".join(p.replace("*", " * ").split()))
+        out[name] = (" ".join(ret.replace("*", " * ").split()), types)
+    return out
+
+
+def _category(ctype_or_c):
+    """A coarse ABI category shared by a C type name and a ctypes type."""
+    import ctypes as C
+
+    if isinstance(ctype_or_c, str):
+        t = ctype_or_c.replace("const ", "")
+        if "*" in t:
+            return "pointer"
+        return {"int": "int", "double": "double", "size_t": "size_t", "long long": "longlong"}.get(t, t)
+    if ctype_or_c in (C.c_void_p, C.c_char_p) or hasattr(ctype_or_c, "contents") or \
+            getattr(ctype_or_c, "_type_", None) is not None and issubclass(ctype_or_c, C._Pointer):
+        return "pointer"
+    return {C.c_int: "int", C.c_double: "double", C.c_size_t: "size_t", C.c_longlong: "longlong"}.get(ctype_or_c, "?")
+
+
+def test_ctypes_signatures_match_the_header():
+    """Every entry point the Python mirror binds has the header's return type and parameter
+    categories (int, double, size_t, long long or pointer), so no argument is passed in the
+    wrong register or width."""
+    from fluidsim_b200 import _native as N
+
+    protos = _prototypes()
+    for name, (res, args) in N.SIGNATURES.items():
+        assert name in protos, name
+        ret, params = protos[name]
+        assert len(params) == len(args), (name, params)
+        for c_type, py_type in zip(params, args):
+            assert _category(c_type) == _category(py_type), (name, c_type, py_type)
+        assert _category(ret) == _category(res), (name, ret, res)

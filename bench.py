@@ -2,14 +2,17 @@
 
 Workload (one step): a 2048 x 2048 two-phase dam break (liquid 1000 / gas 1, liquid below half
 height plus a seeded 200x300 block, face velocities U[-1, 1] in FP32), gravity -9.8 applied,
-then one pressure projection (coefficients and multigrid rebuilt from the step's masses, PCG
-to ||r|| <= 1e-6 ||b||, velocity update, divergence check). Inputs are seeded synthetic data;
-the reference publishes no dataset for this path.
+then one pressure projection: coefficients and multigrid rebuilt from the step's masses, MG-PCG
+to the reference's own stop rule (max |r| <= 1e-6 dx^2/dt on the FP64 residual,
+FluidGridCPU.cpp:1093), velocity update, divergence check. The reference arm runs the same
+scene, rule and config, so the two lines measure the same work. Inputs are seeded synthetic
+data; the reference publishes no dataset for this path.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuda|reference]
 
-N > 1 runs under torchrun, one rank per GPU, each projecting its own grid (independent
-replicas: the path has no exchange step). Rank 0 prints one JSON line.
+With N > 1 and no WORLD_SIZE in the environment the script starts itself under
+torch.distributed.run, one rank per GPU, each projecting its own grid (independent replicas:
+the path has no exchange step). Rank 0 prints one JSON line.
 """
 from __future__ import annotations
 
@@ -19,6 +22,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -51,6 +55,8 @@ def parse():
     p.add_argument("--no-serve", action="store_true", help="skip the serving (continuous batching) measurement")
     p.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision comparison")
     p.add_argument("--no-steps", action="store_true", help="skip the full-step (transport + projection) measurement")
+    p.add_argument("--no-rules", action="store_true",
+                   help="skip the relative-rule FP32 and reference-rule FP64 legs of the headline scene")
     p.add_argument("--no-viscous", action="store_true",
                    help="skip the 4096x4096 variable-viscosity comparison of FP32 and mixed precision")
     p.add_argument("--tail-cells", type=int, default=0,
@@ -96,11 +102,10 @@ class ClockSampler:
     def __init__(self, device_index):
         self.device = device_index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{device_index}.csv")
+        self.path = os.path.join(tempfile.gettempdir(), f"fluidsim_clocks_{os.getpid()}_rank{device_index}.csv")
 
     def __enter__(self):
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.file = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
@@ -175,6 +180,16 @@ def host_threads():
         return os.cpu_count() or 1
 
 
+RULE = "reference: max |r| <= tolerance * dx^2 / dt on the FP64 residual (FluidGridCPU.cpp:1093)"
+
+
+def workload_config(size, tolerance):
+    """The `config` of both arms' lines: the same scene, stop rule and tolerance."""
+    return {"workload": f"dam_break_{size}x{size} projection (gravity + MG-PCG to the reference's stop rule)",
+            "cells": size * size, "tolerance": tolerance, "stop_rule": RULE, "density_ratio": "1000:1",
+            "l2": "GPU: flushed (256 MiB write) before every timed step; host: inputs larger than L2"}
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return None
@@ -193,8 +208,7 @@ def run_reference(args, world, rank):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_step * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"dam_break_{size}x{size} projection", "cells": scene.cells,
-                   "tolerance": args.tolerance, "l2": "inputs larger than L2 on the host"},
+        "config": workload_config(size, args.tolerance),
         "iterations": statistics.mean(iters),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
                          "sample": f"{args.steps} projections of the {size}x{size} workload, FluidGridCPU::project"},
@@ -207,46 +221,97 @@ def run_reference(args, world, rank):
 # CUDA arm
 # ---------------------------------------------------------------------------------------------
 
+class ProjectionTimer:
+    """Times gravity + one projection of a scene from the same initial state every step: the
+    state is copied back from a pristine grid, the L2 flushed, and the step timed with CUDA
+    events on the grid's stream."""
+
+    def __init__(self, scene, precision, torch, flush, tail_cells=0, tune=True):
+        from fluidsim_b200 import FluidGrid, scenes
+
+        self.scene, self.torch, self.flush = scene, torch, flush
+        self.pristine = FluidGrid(scene.width, scene.height, scene.cell_size, precision)
+        scenes.upload_scene(self.pristine, scene)
+        self.work = FluidGrid(scene.width, scene.height, scene.cell_size, precision)
+        self.work.configureMaterials([scene.liquid_density], [scene.gas_density])
+        self.work.setGravityY(scene.gravity)
+        self.work.copyStateFrom(self.pristine)
+        self.tail_cells, self.vcycle_ms = tail_cells, None
+        if tail_cells > 0:
+            self.work.setTailCells(tail_cells)
+        elif tune:
+            # The multigrid schedule picked by the autotuner (timed V-cycles, outside the timed steps).
+            self.tail_cells, self.vcycle_ms = self.work.autotune(10)
+        self.stream = torch.cuda.ExternalStream(self.work.stream())
+
+    def step(self, tolerance, relative):
+        torch, scene = self.torch, self.scene
+        self.work.copyStateFrom(self.pristine)
+        with torch.cuda.stream(self.stream):
+            self.flush.fill_(1.0)
+            start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            start.record(self.stream)
+        self.work.applyGravity(scene.dt)
+        if relative:
+            r = self.work.project(scene.dt, 400, tolerance, relative_tolerance=tolerance)
+        else:
+            r = self.work.project(scene.dt, 400, tolerance)
+        stop.record(self.stream)
+        stop.synchronize()
+        return start.elapsed_time(stop), r
+
+    def run(self, steps, warmup, tolerance, relative):
+        for _ in range(warmup):
+            self.step(tolerance, relative)
+        times, results = [], []
+        for _ in range(steps):
+            ms, r = self.step(tolerance, relative)
+            times.append(ms)
+            results.append(r)
+        return times, results
+
+    def destroy(self):
+        self.work.destroy()
+        self.pristine.destroy()
+
+
+def solved(r, tolerance, relative):
+    """The solver met its stop rule (FP32 velocities may still be precision-limited)."""
+    if relative:
+        return r.solve_status == "converged" and r.residual_l2 <= tolerance * r.rhs_l2 * 1.0001
+    return r.solve_status in ("converged", "no_work") and r.accepted()
+
+
+def leg_summary(scene, times, results, tolerance, relative):
+    ms = statistics.mean(times)
+    iters = statistics.mean(r.iterations for r in results)
+    model_bytes = scene.cells * (70 + 306 * iters)
+    return {"value": scene.cells / (ms / 1e3), "unit": UNIT, "ms_per_step": ms, "iterations": iters,
+            "solved": all(solved(r, tolerance, relative) for r in results),
+            "converged": all(r.converged for r in results),
+            "precision_limited": any(r.precision_limited for r in results),
+            "max_divergence": max(r.max_divergence for r in results),
+            "relative_residual": max(r.relative_residual for r in results),
+            "restarts": max(r.restarts for r in results),
+            "projection_model_gbs": model_bytes / (ms / 1e3) / 1e9}
+
+
 def run_cuda(args, world, rank, local_rank):
     import torch
 
-    from fluidsim_b200 import FluidGrid, FluidGridState, ProjectionBatch, kernel_launches, scenes
+    from fluidsim_b200 import kernel_launches
     from fluidsim_b200 import _native
 
     torch.cuda.set_device(local_rank)
     _native.set_launch_mode(args.launch)
     size = args.size
     scene = scene_for(size, rank)
-    pristine = FluidGrid(size, size, scene.cell_size, "fp32")
-    scenes.upload_scene(pristine, scene)
-    work = FluidGrid(size, size, scene.cell_size, "fp32")
-    work.configureMaterials([scene.liquid_density], [scene.gas_density])
-    work.setGravityY(scene.gravity)
-    # The multigrid schedule picked by the autotuner (timed V-cycles, outside the timed steps),
-    # or the one --tail-cells pins.
-    work.copyStateFrom(pristine)
-    if args.tail_cells > 0:
-        work.setTailCells(args.tail_cells)
-        tail_cells, vcycle_ms = args.tail_cells, None
-    else:
-        tail_cells, vcycle_ms = work.autotune(10)
-    stream = torch.cuda.ExternalStream(work.stream())
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
-
-    def one_step(timed):
-        work.copyStateFrom(pristine)
-        with torch.cuda.stream(stream):
-            flush.fill_(1.0)
-            start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            start.record(stream)
-        work.applyGravity(scene.dt)
-        r = work.project(scene.dt, 200, args.tolerance, relative_tolerance=args.tolerance)
-        stop.record(stream)
-        stop.synchronize()
-        return start.elapsed_time(stop), r
+    timer = ProjectionTimer(scene, "fp32", torch, flush, args.tail_cells)
+    tail_cells, vcycle_ms, work = timer.tail_cells, timer.vcycle_ms, timer.work
 
     for _ in range(args.warmup):
-        one_step(False)
+        timer.step(args.tolerance, False)
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
@@ -254,7 +319,7 @@ def run_cuda(args, world, rank, local_rank):
     launches_before = kernel_launches()
     with ClockSampler(local_rank) as clocks:
         for _ in range(args.steps):
-            ms, r = one_step(True)
+            ms, r = timer.step(args.tolerance, False)
             times.append(ms)
             results.append(r)
     torch.cuda.synchronize()
@@ -265,8 +330,6 @@ def run_cuda(args, world, rank, local_rank):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         total_ms = float(t.item())
     value = world * scene.cells * args.steps / (total_ms / 1e3)
-    converged = all(r.solve_status == "converged" and r.residual_l2 <= args.tolerance * r.rhs_l2 * 1.0001
-                    for r in results)
 
     # Live roofline of the fused fine-level smoothing kernels (CUDA events on the grid stream).
     peak, peak_kind = measured_peaks()
@@ -278,34 +341,39 @@ def run_cuda(args, world, rank, local_rank):
     traffic = traffic_per_cell.get(dominant)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": None if traffic is None else traffic * scene.cells,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per fine cell of this kernel "
+                                  "(profiles/roofline_traffic.json, a 2048x2048 capture) times the cells; "
+                                  "not measured in this run",
                 "kernel": KERNEL_NAMES[dominant], "kernel_ms": kernel_ms[dominant],
                 "algorithmic_bytes": algorithmic, "peak_source": f"{peak_kind} hbm_gbs (copy, burst)"}
-    # Whole-projection bandwidth against the byte model of an unfused projection (306 B/cell per
-    # PCG iteration plus 70 B/cell of set-up), for comparison beside the kernel figure.
-    mean_iters = statistics.mean(r.iterations for r in results)
-    model_bytes = scene.cells * (70 + 306 * mean_iters)
-    projection_model = {"iterations": mean_iters, "bytes": model_bytes,
-                        "gbs": model_bytes / (total_ms / args.steps / 1e3) / 1e9 / (world if world > 1 else 1)}
+    timer.destroy()
+    headline = leg_summary(scene, times, results, args.tolerance, False)
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "launch": args.launch,
-        "config": {"workload": f"dam_break_{size}x{size} projection (gravity + PCG-MG to 1e-6 relative)",
-                   "cells": scene.cells, "tolerance": args.tolerance, "density_ratio": "1000:1",
-                   "l2": "flushed (256 MiB write) before every timed step", "parallelism": f"replicas x{world}"},
-        "iterations": mean_iters,
+        "launch": args.launch, "parallelism": f"replicas x{world}",
+        "config": workload_config(size, args.tolerance),
+        "iterations": headline["iterations"],
         "autotune": {"tail_cells": tail_cells, "vcycle_ms": vcycle_ms},
-        "converged": converged,
-        "relative_residual": max(r.relative_residual for r in results),
-        "restarts": max(r.restarts for r in results),
+        "solved": headline["solved"],
+        "converged": headline["converged"],
+        "precision_limited": headline["precision_limited"],
+        "max_divergence": headline["max_divergence"],
+        "relative_residual": headline["relative_residual"],
+        "restarts": headline["restarts"],
         "roofline": roofline,
-        "projection_bandwidth_model": projection_model,
+        "projection_bandwidth_model": {"iterations": headline["iterations"],
+                                       "bytes": scene.cells * (70 + 306 * headline["iterations"]),
+                                       "gbs": headline["projection_model_gbs"]},
         "clocks": clocks.summary(),
         "gpu_launches": launches,
     }
 
+    if rank == 0 and not args.no_rules:
+        line["relative_rule"] = rule_measure(args, scene, torch, flush, "fp32", True, tail_cells)
+        line["reference_rule_fp64"] = rule_measure(args, scene, torch, flush, "fp64", False, 0)
     if rank == 0 and not args.no_mixed:
         line["mixed"] = mixed_measure(args, scene, torch, flush)
     if rank == 0 and not args.no_e2e:
@@ -323,7 +391,7 @@ def run_cuda(args, world, rank, local_rank):
     if rank == 0 and not args.no_serve:
         line["serve"] = serve_measure(args)
     if rank == 0 and not args.no_steps:
-        line["steps"] = steps_measure(args, torch)
+        line["step_leg"] = steps_measure(args, torch)
     if rank == 0 and not args.no_viscous:
         from fluidsim_b200 import FluidCudaError
 
@@ -332,6 +400,19 @@ def run_cuda(args, world, rank, local_rank):
         except FluidCudaError as e:  # a solver that did not converge is reported, not hidden
             line["viscous"] = {"error": str(e)}
     return line
+
+
+def rule_measure(args, scene, torch, flush, precision, relative, tail_cells, steps=5, warmup=2):
+    """The headline scene under another stop rule or precision: FP32 to the relative residual
+    ||r|| <= tol ||b|| (the target form of the projection), and FP64 under the reference's own
+    rule (the reference engine's arithmetic on the device)."""
+    timer = ProjectionTimer(scene, precision, torch, flush, tail_cells, tune=tail_cells == 0)
+    times, results = timer.run(steps, warmup, args.tolerance, relative)
+    timer.destroy()
+    out = leg_summary(scene, times, results, args.tolerance, relative)
+    out["precision"] = precision
+    out["stop_rule"] = "relative: ||r||_2 <= tolerance * ||b||_2" if relative else RULE
+    return out
 
 
 def mixed_measure(args, scene, torch, flush, steps=5, warmup=2):
@@ -379,6 +460,7 @@ def mixed_measure(args, scene, torch, flush, steps=5, warmup=2):
         work.destroy()
         pristine.destroy()
     out["speedup_vs_fp32"] = out["fp32"]["ms_per_step"] / out["mixed"]["ms_per_step"]
+    out["stop_rule"] = "relative: ||r||_2 <= tolerance * ||b||_2"
     return out
 
 
@@ -414,7 +496,7 @@ def e2e_measure(args, scene, torch):
         start.record(stream)
         g.upload(state)
         g.applyGravity(scene.dt)
-        g.project(scene.dt, 200, args.tolerance, relative_tolerance=args.tolerance)
+        g.project(scene.dt, 400, args.tolerance)
         download_uvp()
         stop.record(stream)
         stop.synchronize()
@@ -425,7 +507,7 @@ def e2e_measure(args, scene, torch):
     d2h = 8 * (nu + nv + n)
     ms = statistics.mean(times)
     return {"value": scene.cells / (ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-            "ms_per_step": ms}
+            "ms_per_step": ms, "stop_rule": RULE}
 
 
 def steps_measure(args, torch, steps=100, warmup=3, size=1024):
@@ -652,11 +734,29 @@ def serve_measure(args, rate=200.0, budget=150 * 10**9):
             "speedup_vs_plain": served / plain}
 
 
+def spawn_ranks(args):
+    """Runs this script under torch.distributed.run with one rank per GPU (the caller asked
+    for N > 1 GPUs without starting the ranks); returns its exit code."""
+    import socket
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
 def main():
     args = parse()
+    if "WORLD_SIZE" not in os.environ and args.gpus > 1:
+        sys.exit(spawn_ranks(args))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != args.gpus:
+        print(f"bench.py: --gpus {args.gpus} but WORLD_SIZE is {world}", file=sys.stderr)
+        sys.exit(2)
     if args.impl == "reference":
         line = run_reference(args, world, rank)
         if line is not None:

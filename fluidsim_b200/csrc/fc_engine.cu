@@ -2384,22 +2384,38 @@ void load_checkpoint(Grid& g, const char* metadata, const void* payload, size_t 
             fail(FC_ERR_INVALID_ARGUMENT, "checkpoint metadata lacks a valid \"%s\"", key);
         return *v;
     };
+    // A number the loader casts to an integer: finite, integral and within [lo, hi] first, so
+    // no out-of-range value reaches a cast.
+    auto integer = [&](const char* key, double lo, double hi) -> long long
+    {
+        const double x = need(key, json::Value::Number).number;
+        if (!std::isfinite(x) || x != std::floor(x) || x < lo || x > hi)
+            fail(FC_ERR_INVALID_ARGUMENT, "checkpoint \"%s\" is not an integer in range", key);
+        return (long long)x;
+    };
+    auto finite = [&](const json::Value& v, const char* what) -> double
+    {
+        if (v.kind != json::Value::Number || !std::isfinite(v.number))
+            fail(FC_ERR_INVALID_ARGUMENT, "checkpoint %s is not a finite number", what);
+        return v.number;
+    };
     if (need("backend", json::Value::String).text != "cuda-uniform")
         fail(FC_ERR_INVALID_ARGUMENT, "checkpoint was written by another backend");
-    if (int(need("version", json::Value::Number).number) != kCheckpointVersion)
+    if (integer("version", 0, 1e6) != kCheckpointVersion)
         fail(FC_ERR_INVALID_ARGUMENT, "unsupported checkpoint version");
     const bool little = [] { const unsigned one = 1; return *reinterpret_cast<const unsigned char*>(&one) == 1; }();
     if (need("byte_order", json::Value::String).text != (little ? "little" : "big"))
         fail(FC_ERR_INVALID_ARGUMENT, "checkpoint byte order differs from this host");
     if (need("scalar", json::Value::String).text != (g.elem == 8 ? "float64" : "float32") ||
-        int(need("precision", json::Value::Number).number) != g.precision)
+        integer("precision", 0, 16) != g.precision)
         fail(FC_ERR_INVALID_ARGUMENT, "checkpoint precision differs from the grid's");
-    if (int(need("width", json::Value::Number).number) != g.W || int(need("height", json::Value::Number).number) != g.H ||
+    if (integer("width", 1, 1 << 30) != g.W || integer("height", 1, 1 << 30) != g.H ||
         need("cell_size", json::Value::Number).number != g.dx)
         fail(FC_ERR_INVALID_ARGUMENT, "checkpoint geometry differs from the grid's");
     const json::Value& origin = need("origin", json::Value::Array);
-    if (origin.items.size() != 2 || origin.items[0].kind != json::Value::Number || origin.items[1].kind != json::Value::Number)
+    if (origin.items.size() != 2)
         fail(FC_ERR_INVALID_ARGUMENT, "checkpoint origin is malformed");
+    const double origin_x = finite(origin.items[0], "origin"), origin_y = finite(origin.items[1], "origin");
     auto mixture = [&](const char* key, std::vector<double>& density, std::vector<double>& viscosity)
     {
         density.clear();
@@ -2408,7 +2424,7 @@ void load_checkpoint(Grid& g, const char* metadata, const void* payload, size_t 
         {
             const json::Value* d = c.find("density");
             const json::Value* mu = c.find("dynamic_viscosity");
-            if (!d || d->kind != json::Value::Number || !(d->number > 0.0))
+            if (!d || d->kind != json::Value::Number || !(d->number > 0.0) || !std::isfinite(d->number))
                 fail(FC_ERR_INVALID_ARGUMENT, "checkpoint mixture component is malformed");
             density.push_back(d->number);
             viscosity.push_back(mu && mu->kind == json::Value::Number ? mu->number : 0.0);
@@ -2423,11 +2439,11 @@ void load_checkpoint(Grid& g, const char* metadata, const void* payload, size_t 
     for (double mu : gv)
         if (!std::isfinite(mu) || mu < 0.0)
             fail(FC_ERR_INVALID_ARGUMENT, "Invalid saved material viscosity");
-    const int preconditioner = int(need("preconditioner", json::Value::Number).number);
+    const long long preconditioner = integer("preconditioner", -1e6, 1e6);
     if (preconditioner != FC_PRECONDITIONER_DIAGONAL && preconditioner != FC_PRECONDITIONER_MULTIGRID)
         fail(FC_ERR_INVALID_ARGUMENT, "checkpoint preconditioner is unknown");
     const bool solid = need("obstacles", json::Value::Bool).boolean;
-    const double gravity = need("gravity_y", json::Value::Number).number;
+    const double gravity = finite(need("gravity_y", json::Value::Number), "gravity_y");
     // Older checkpoints carry no surface tension: zero, the engine default.
     double tension = 0.0;
     if (const json::Value* st = m.find("surface_tension"))
@@ -2445,7 +2461,7 @@ void load_checkpoint(Grid& g, const char* metadata, const void* payload, size_t 
         transport = int(tr->number);
     }
     const PayloadLayout layout = payload_layout(g, int(ld.size() + gd.size()), solid);
-    if (size_t(need("payload_bytes", json::Value::Number).number) != layout.total || payload_bytes != layout.total)
+    if (integer("payload_bytes", 0, 9.0e15) != (long long)layout.total || payload_bytes != layout.total)
         fail(FC_ERR_INVALID_ARGUMENT, "checkpoint payload has %zu bytes, %zu expected", payload_bytes, layout.total);
 
     // Validated: apply.
@@ -2454,12 +2470,12 @@ void load_checkpoint(Grid& g, const char* metadata, const void* payload, size_t 
     g.gas_density = gd;
     g.gas_viscosity = gv;
     g.configured = true;
-    g.preconditioner = preconditioner;
+    g.preconditioner = int(preconditioner);
     g.gravity_y = gravity;
     g.surface_tension = tension;
     g.transport = transport;
-    g.origin_x = origin.items[0].number;
-    g.origin_y = origin.items[1].number;
+    g.origin_x = origin_x;
+    g.origin_y = origin_y;
     allocate_masses(g);
     g.has_solid = solid;
     const char* in = static_cast<const char*>(payload);
@@ -2569,8 +2585,12 @@ __global__ void __launch_bounds__(kVecThreads) k_divergence_noalloc(const T* u, 
     }
 }
 
-// Device address of the scratch array, looked up once per device (with that device current).
-void* noalloc_address()
+// Device address of the scratch array on the current device. Outside stream capture it is
+// looked up on every call, so a device or primary-context reset by the host (which unloads the
+// module and with it the array) never leaves a stale address behind. During capture the last
+// address looked up on that device is used, as a capture must not load modules; the header
+// asks for one call before any capture.
+void* noalloc_address(cudaStream_t stream)
 {
     static std::mutex lock;
     static void* addresses[64] = {};
@@ -2578,8 +2598,15 @@ void* noalloc_address()
     check(cudaGetDevice(&device), "current device");
     if (device < 0 || device >= 64)
         fail(FC_ERR_UNSUPPORTED, "device index %d out of range", device);
+    int stream_device = device;
+    check(cudaStreamGetDevice(stream, &stream_device), "stream device");
+    if (stream_device != device)
+        fail(FC_ERR_INVALID_ARGUMENT, "the stream belongs to device %d, but device %d is current; make the stream's "
+            "device current before the call", stream_device, device);
+    cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+    check(cudaStreamIsCapturing(stream, &capture), "stream capture status");
     std::lock_guard<std::mutex> guard(lock);
-    if (!addresses[device])
+    if (capture == cudaStreamCaptureStatusNone || !addresses[device])
     {
         void* address = nullptr;
         check(cudaGetSymbolAddress(&address, noalloc_scratch), "scratch symbol address");
@@ -3255,8 +3282,8 @@ int fc_divergence_noalloc(const void* u, const void* v, int width, int height, d
             fail(FC_ERR_INVALID_ARGUMENT,
                 "a %dx%d grid needs %lld tiles of 32x32 cells; the no-allocation path holds at most %d "
                 "(4,194,304 cells)", width, height, tiles, fc::kNoAllocMaxTiles);
-        unsigned char* scratch = static_cast<unsigned char*>(fc::noalloc_address());
         cudaStream_t s = static_cast<cudaStream_t>(stream);
+        unsigned char* scratch = static_cast<unsigned char*>(fc::noalloc_address(s));
         // The arrival counter must start at zero; the partial slots are overwritten.
         check(cudaMemsetAsync(scratch + fc::kNoAllocCounterOffset, 0, sizeof(unsigned int), s), "scratch clear");
         if (precision == FC_PRECISION_FP64)

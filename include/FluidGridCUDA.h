@@ -2,7 +2,7 @@
 //
 // Header-only adapter from fluid::FluidGridBase (FluidSim/FluidGridBase.h:20-147) to the C ABI
 // in fluidcuda.h. A FluidSim build adds it as one more backend of FluidGrid::selectBackend
-// (FluidSim/FluidGrid.cpp:37-90); see INTEGRATION.md for the selection branch. Status codes
+// (FluidSim/FluidGrid.cpp:37-90), next to the CPU and WebGPU branches. Status codes
 // become the reference's exception types: std::invalid_argument, std::logic_error,
 // std::runtime_error; a non-converged projection is a result, not an exception.
 #pragma once

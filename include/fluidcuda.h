@@ -256,13 +256,17 @@ int fc_time_kernel(fc_grid* grid, int kernel, int repeats, double* mean_ms);
  * float for FC_PRECISION_FP32 or double for FC_PRECISION_FP64. stats is a device array of 3
  * doubles receiving max |div u| (1/s; +inf if any cell is non-finite), the largest excess of
  * |div u| over the cell's float rounding allowance, and the sum of div u squared. The work is
- * queued on `stream` (a cudaStream_t, 0 for the legacy stream); the call does not wait.
+ * queued on `stream` (a cudaStream_t, 0 for the legacy stream); the call does not wait. The
+ * stream must belong to the current device; another device's stream is rejected with
+ * FC_ERR_INVALID_ARGUMENT.
  *
  * This entry point allocates nothing: its scratch is a fixed 128 KiB device array that every
  * GPU loading this library keeps until process exit. Grids are limited to 4096 tiles of 32x32
  * cells (4,194,304 cells, e.g. 2048x2048); larger ones are rejected with
- * FC_ERR_INVALID_ARGUMENT. The first call on a device looks up the array's device address;
- * make that first call before any stream capture. All calls share the one array, so calls
+ * FC_ERR_INVALID_ARGUMENT. Each call outside stream capture looks up the array's device
+ * address (so a device reset by the host leaves nothing stale); a call during capture reuses
+ * the last address looked up on that device, so make one call before any stream capture, and
+ * again after a device reset. All calls share the one array, so calls
  * whose work overlaps on the GPU race: order them on one stream or synchronise between them. */
 int fc_divergence_noalloc(const void* u, const void* v, int width, int height, double cell_size, int precision,
     double* stats, void* stream);

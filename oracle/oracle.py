@@ -26,10 +26,39 @@ _dp = C.POINTER(C.c_double)
 _u8p = C.POINTER(C.c_uint8)
 
 
+def reference_checkout():
+    """Root of the reference checkout whose sources the reference build compiles: the
+    FLUIDSIM_REFERENCE environment variable, else the checkout beside this build's working
+    tree; None when neither holds FluidSim/UniformCPU/FluidGridCPU.cpp."""
+    for root in (os.environ.get("FLUIDSIM_REFERENCE"), "/root/reference"):
+        if root and os.path.isfile(os.path.join(root, "FluidSim", "UniformCPU", "FluidGridCPU.cpp")):
+            return root
+    return None
+
+
+def json_include_dir():
+    """A directory holding nlohmann/json.hpp (the JSON type bitloop's checkpoint metadata
+    follows), from the Python environment's site-packages; None when absent."""
+    import sysconfig
+
+    for base in {sysconfig.get_paths()["purelib"], sysconfig.get_paths()["platlib"]}:
+        d = os.path.join(base, "include", "cudnn_frontend", "thirdparty")
+        if os.path.isfile(os.path.join(d, "nlohmann", "json.hpp")):
+            return d
+    return None
+
+
 def build(reference: bool = True) -> None:
     """Compile the restatement, and the reference engine when its sources are present."""
     targets = ["all"] if reference else ["oracle"]
-    subprocess.run(["make", "-s", "-f", os.path.join(HERE, "Makefile")] + targets, check=True)
+    extra = []
+    root = reference_checkout() if reference else None
+    if root:
+        extra.append(f"REFERENCE={root}")
+        inc = json_include_dir()
+        if inc:
+            extra.append(f"JSON_INCLUDE={inc}")
+    subprocess.run(["make", "-s", "-f", os.path.join(HERE, "Makefile")] + targets + extra, check=True)
 
 
 def _ptr(a):

@@ -69,15 +69,18 @@ def test_no_silent_host_fallback_without_gpu():
 @pytest.mark.skipif(shutil.which("g++") is None, reason="no host compiler")
 def test_cpp_adapter_compiles_against_reference_contract(tmp_path):
     """include/FluidGridCUDA.h implements fluid::FluidGridBase from the reference headers."""
-    reference = "/root/reference/FluidSim"
-    if not os.path.isdir(reference):
+    from oracle import oracle
+
+    checkout = oracle.reference_checkout()
+    if checkout is None:
         pytest.skip("reference headers not present")
+    reference = os.path.join(checkout, "FluidSim")
     src = tmp_path / "adapter.cpp"
     src.write_text('#include "FluidGridCUDA.h"\nint main() { return fluid::FluidGridCUDA::kind() == 0; }\n')
     cmd = ["g++", "-std=c++23", "-fsyntax-only", f"-I{HEADER_DIR}", f"-I{reference}",
            f"-I{os.path.join(ROOT, 'oracle', 'ref_shim')}", str(src)]
-    nlohmann = "/opt/prime-rl/.venv/lib/python3.12/site-packages/include/cudnn_frontend/thirdparty"
-    if os.path.isdir(nlohmann):
+    nlohmann = oracle.json_include_dir()
+    if nlohmann:
         cmd.insert(2, f"-I{nlohmann}")
     out = subprocess.run(cmd, capture_output=True, text=True)
     assert out.returncode == 0, out.stderr[-2000:]

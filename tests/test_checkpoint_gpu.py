@@ -62,6 +62,18 @@ def test_checkpoint_rejects_incompatible_input_before_changing_state():
     rejected(dict(meta, scalar="float64"), payload)
     rejected(meta, payload[:-8])
     rejected("{not json", payload)
+    # Numbers are checked before any cast: finite, integral and in range.
+    rejected(dict(meta, width=1e300), payload)
+    rejected(dict(meta, version=-1), payload)
+    rejected(dict(meta, version=1.5), payload)
+    rejected(dict(meta, precision=2 ** 40), payload)
+    rejected(dict(meta, payload_bytes=-8), payload)
+    rejected(dict(meta, preconditioner=1e30), payload)
+    text = json.dumps(meta)
+    # 1e999 parses as infinity: a non-finite gravity, origin or density is refused.
+    rejected(text.replace('"gravity_y": ' + json.dumps(meta["gravity_y"]), '"gravity_y": 1e999'), payload)
+    rejected(json.dumps(dict(meta, origin=[0.0, "x"])), payload)
+    rejected(text.replace('"origin": ' + json.dumps(meta["origin"]), '"origin": [1e999, 0]'), payload)
     other = FluidGrid(64, 48, 1.0 / 64, "fp64")
     with pytest.raises(FluidInvalidArgument):
         other.loadCheckpoint(meta, payload)

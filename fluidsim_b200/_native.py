@@ -142,6 +142,7 @@ SIGNATURES = {
     "fc_apply_gravity": (_int, [_vp, _dbl]),
     "fc_max_divergence": (_int, [_vp, _dp]),
     "fc_classify": (_int, [_vp, C.POINTER(C.c_uint8)]),
+    "fc_download_coefficients": (_int, [_vp, _dp, _dp, _dp]),
     "fc_apply_preconditioner": (_int, [_vp, _dp, _dbl, _dp]),
     "fc_time_kernel": (_int, [_vp, _int, _int, _dp]),
     "fc_divergence_noalloc": (_int, [_vp, _vp, _int, _int, _dbl, _int, _vp, _vp]),

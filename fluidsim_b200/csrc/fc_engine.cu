@@ -3228,6 +3228,61 @@ int fc_classify(fc_grid* grid, unsigned char* mask)
     });
 }
 
+int fc_download_coefficients(fc_grid* grid, double* inv_u, double* inv_v, double* inv_diagonal)
+{
+    return guarded([&]
+    {
+        if (!grid || !inv_u || !inv_v)
+            fail(FC_ERR_INVALID_ARGUMENT, "null argument");
+        Grid& g = grid->impl;
+        fc::require_uploaded(g);
+        fc::Plan& p = fc::single_plan(g);
+        fc::rebuild_if_dirty(p);
+        const fc::LevelDesc& L = g.desc.lev[0];
+        if (inv_diagonal && !L.inv)
+            fail(FC_ERR_UNSUPPORTED, "a single-level grid keeps no inverse diagonal");
+        const size_t padded = size_t(g.S) * (g.H + 2);
+        std::vector<double> right(padded), down(padded), inv(inv_diagonal ? padded : 0);
+        auto fetch = [&](const void* device, std::vector<double>& host)
+        {
+            if (g.elem == 8)
+            {
+                check(cudaMemcpyAsync(host.data(), device, padded * sizeof(double), cudaMemcpyDeviceToHost, p.stream),
+                    "coefficients");
+                return;
+            }
+            std::vector<float> f(padded);
+            check(cudaMemcpyAsync(f.data(), device, padded * sizeof(float), cudaMemcpyDeviceToHost, p.stream),
+                "coefficients");
+            check(cudaStreamSynchronize(p.stream), "coefficients");
+            for (size_t i = 0; i < padded; ++i)
+                host[i] = double(f[i]);
+        };
+        fetch(L.right, right);
+        fetch(L.down, down);
+        if (inv_diagonal)
+            fetch(L.inv, inv);
+        check(cudaStreamSynchronize(p.stream), "coefficients");
+        // A cell stores the weights of its right and lower faces (padded layout); the reference's
+        // arrays hold every face, walls included (FluidGridTypes.h:10-20).
+        const int W = g.W, H = g.H;
+        for (int y = 0; y < H; ++y)
+        {
+            inv_u[size_t(y) * (W + 1)] = 0.0;
+            for (int x = 0; x < W; ++x)
+            {
+                const size_t i = size_t(fc::padded_index(g.S, x, y));
+                inv_u[size_t(y) * (W + 1) + x + 1] = right[i];
+                inv_v[size_t(y + 1) * W + x] = down[i];
+                if (inv_diagonal)
+                    inv_diagonal[size_t(y) * W + x] = inv[i];
+            }
+        }
+        for (int x = 0; x < W; ++x)
+            inv_v[x] = 0.0;
+    });
+}
+
 int fc_autotune(fc_grid* grid, int repeats, int* tail_cells, double* vcycle_ms)
 {
     return guarded([&]

@@ -318,6 +318,14 @@ class FluidGrid:
         N.check(N.lib().fc_classify(self.handle, mask.ctypes.data_as(C.POINTER(C.c_uint8))))
         return mask
 
+    def downloadCoefficients(self):
+        """The fine level's (inv_u, inv_v, inv_diagonal) in the reference's layout
+        (FluidGridCPU::rebuildPressureCoefficients, FluidGridCPU.cpp:1154-1205)."""
+        w, h = self.width, self.height
+        inv_u, inv_v, inv_d = np.zeros((h, w + 1)), np.zeros((h + 1, w)), np.zeros((h, w))
+        N.check(N.lib().fc_download_coefficients(self.handle, _ptr(inv_u), _ptr(inv_v), _ptr(inv_d)))
+        return inv_u, inv_v, inv_d
+
     def applyPreconditioner(self, residual: np.ndarray, residual_mean: float = 0.0) -> np.ndarray:
         r = _as_f64(residual, (self.height, self.width), "residual")
         z = np.empty((self.height, self.width))

@@ -239,6 +239,14 @@ int fc_classify(fc_grid* grid, unsigned char* mask);
  * keeps its constant component, like the reference's apply. Rebuilds coefficients if needed. */
 int fc_apply_preconditioner(fc_grid* grid, const double* residual, double residual_mean, double* correction);
 
+/* The fine level's face weights and inverse diagonal as the projection uses them, in the
+ * reference's layout: inv_u (width+1)*height, inv_v width*(height+1), inv_diagonal
+ * width*height (may be null), each in the grid's working precision widened to double. The
+ * coefficients are rebuilt from the current state first if it changed. Replaces reading
+ * FluidGridCPU's inv_density_u/v and inv_pressure_diagonal (FluidGridCPU.cpp:1154-1205) for
+ * parity checks. A single-level grid keeps no inverse diagonal: FC_ERR_UNSUPPORTED. */
+int fc_download_coefficients(fc_grid* grid, double* inv_u, double* inv_v, double* inv_diagonal);
+
 /* Times one kernel of the projection with CUDA events on the grid's stream, on the grid's
  * current data, and returns the mean duration of `repeats` launches in milliseconds. Kernels:
  * 0 fine-level pre-smoothing + restriction, 1 fine-level prolongation + post-smoothing,

@@ -64,6 +64,7 @@ struct SolveState
     double div_excess;  // max(0, |div u| - local float rounding allowance)
     double div_sumsq;   // sum of div^2
     double res_max, res_sumsq;
+    double refresh_max; // FP32: recurrence max-norm that triggers a refresh from the true residual (0: none)
     double dt;          // time step of the projection in flight
     int iterations;
     int restarts;       // true-residual checks that failed and restarted the directions

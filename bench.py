@@ -293,6 +293,7 @@ def leg_summary(scene, times, results, tolerance, relative):
             "max_divergence": max(r.max_divergence for r in results),
             "relative_residual": max(r.relative_residual for r in results),
             "restarts": max(r.restarts for r in results),
+            "refreshes": max(r.refreshes for r in results),
             "projection_model_gbs": model_bytes / (ms / 1e3) / 1e9}
 
 
@@ -363,6 +364,7 @@ def run_cuda(args, world, rank, local_rank):
         "max_divergence": headline["max_divergence"],
         "relative_residual": headline["relative_residual"],
         "restarts": headline["restarts"],
+        "refreshes": headline["refreshes"],
         "roofline": roofline,
         "projection_bandwidth_model": {"iterations": headline["iterations"],
                                        "bytes": scene.cells * (70 + 306 * headline["iterations"]),

@@ -45,6 +45,7 @@ class FcResult(C.Structure):
         ("divergence_l2", C.c_double),
         ("restarts", C.c_int),
         ("kernels", C.c_int),
+        ("refreshes", C.c_int),
     ]
 
 

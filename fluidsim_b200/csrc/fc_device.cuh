@@ -68,6 +68,7 @@ struct SolveState
     double dt;          // time step of the projection in flight
     int iterations;
     int restarts;       // true-residual checks that failed and restarted the directions
+    int refreshes;      // FP32 early restarts from the true residual (refresh_threshold)
     int max_iterations;
     int done;
     int status;

@@ -1290,6 +1290,7 @@ void fill_result(const Grid& g, const SolveState& s, double divergence_tolerance
     r.divergence_excess = s.div_excess;
     r.divergence_l2 = std::sqrt(s.div_sumsq);
     r.restarts = s.restarts;
+    r.refreshes = s.refreshes;
     if (s.status == kNoWork)
     {
         r.residual_max = s.bmax;

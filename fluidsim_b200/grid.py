@@ -65,6 +65,7 @@ class ProjectionResult:
     divergence_l2: float = float("nan")
     restarts: int = 0
     kernels: int = 0
+    refreshes: int = 0
 
     def accepted(self) -> bool:
         """FluidProjectionResult::accepted (FluidGridTypes.h:76)."""
@@ -80,7 +81,7 @@ class ProjectionResult:
                    bool(r.relaxed), r.max_volume_error, r.rms_volume_error, r.viscosity_iterations,
                    bool(r.precision_limited), N.SOLVE_STATUS.get(r.solve_status, str(r.solve_status)),
                    r.residual_max, r.residual_l2, r.rhs_l2, r.divergence_excess, r.divergence_l2,
-                   r.restarts, r.kernels)
+                   r.restarts, r.kernels, r.refreshes)
 
 
 class FluidGrid:

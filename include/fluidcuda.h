@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define FC_ABI_VERSION 1
+#define FC_ABI_VERSION 2
 
 typedef enum fc_status
 {
@@ -102,6 +102,7 @@ typedef struct fc_result
     double divergence_l2;      /* L2 norm of div u over cells */
     int restarts;              /* recurrences that drifted and were restarted from b - A p */
     int kernels;               /* kernels the projection launched on the device */
+    int refreshes;             /* FP32: early restarts from b - A p once the recurrence fell 1e-4 */
 } fc_result;
 
 /* Mirrors fluid::FluidStepTimings (FluidSim/FluidGridTypes.h:49-57); milliseconds. */

@@ -42,7 +42,7 @@ def test_abi_version_and_status_strings():
     from fluidsim_b200 import _native
 
     lib = _native.lib()
-    assert lib.fc_abi_version() == 1
+    assert lib.fc_abi_version() == 2
     assert lib.fc_status_string(1) == b"invalid argument"
 
 

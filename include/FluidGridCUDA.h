@@ -5,6 +5,11 @@
 // (FluidSim/FluidGrid.cpp:37-90), next to the CPU and WebGPU branches. Status codes
 // become the reference's exception types: std::invalid_argument, std::logic_error,
 // std::runtime_error; a non-converged projection is a result, not an exception.
+//
+// Lifecycle as the reference's engines have it (UniformWebGPU/FluidGridWebGPU.cpp:145-165):
+// destroy() releases the device grid; the configuration (materials, gravity, origin, transport)
+// stays on the host, and the next upload() builds a new device grid from it. Any other use of
+// device state between destroy() and upload() throws std::logic_error.
 #pragma once
 
 #include "FluidGridBase.h"
@@ -26,7 +31,7 @@ public:
     static constexpr int kind() { return 1; }
 
     FluidGridCUDA(int width, int height, double cell_size, int precision = FC_PRECISION_FP32)
-        : width(width), height(height), cell_size(cell_size)
+        : width(width), height(height), cell_size(cell_size), precision(precision)
     {
         check(fc_create(width, height, cell_size, precision, &grid));
     }
@@ -51,7 +56,8 @@ public:
     void setOrigin(bl::DVec2 position) override
     {
         origin = position;
-        check(fc_set_origin(live(), position.x, position.y));
+        if (grid)
+            check(fc_set_origin(grid, position.x, position.y));
     }
 
     bool requiresRenderThread() const override { return false; }
@@ -63,7 +69,8 @@ public:
             ld.push_back(c.density), lv.push_back(c.dynamic_viscosity);
         for (const auto& c : gas.components)
             gd.push_back(c.density), gv.push_back(c.dynamic_viscosity);
-        check(fc_configure_materials(live(), int(ld.size()), ld.data(), lv.data(), int(gd.size()), gd.data(), gv.data()));
+        if (grid)
+            check(fc_configure_materials(grid, int(ld.size()), ld.data(), lv.data(), int(gd.size()), gd.data(), gv.data()));
         substances = std::move(catalogue);
         liquid_mixture = std::move(liquid);
         gas_mixture = std::move(gas);
@@ -72,7 +79,10 @@ public:
     // setComponentViscosity (FluidGridBase.h:47-52): a coefficient edit; membership stays fixed.
     void setComponentViscosity(Phase phase, size_t component, double coefficient) override
     {
-        check(fc_set_component_viscosity(live(), phase == Phase::Liquid ? 0 : 1, int(component), coefficient));
+        if (grid)
+            check(fc_set_component_viscosity(grid, phase == Phase::Liquid ? 0 : 1, int(component), coefficient));
+        else if (!std::isfinite(coefficient) || coefficient < 0.0)
+            throw std::invalid_argument("FluidGridCUDA viscosity must be finite and non-negative");
         auto& mixture = phase == Phase::Liquid ? liquid_mixture : gas_mixture;
         mixture.components.at(component).dynamic_viscosity = coefficient;
     }
@@ -83,14 +93,27 @@ public:
 
     const FluidMixture& getGasMixture() const override { return gas_mixture; }
 
-    double getGravityY() const override
+    double getGravityY() const override { return gravity; }
+
+    void setGravityY(double acceleration) override
     {
-        double g = 0.0;
-        check(fc_get_gravity(grid, &g));
-        return g;
+        if (grid)
+            check(fc_set_gravity(grid, acceleration));
+        else if (!std::isfinite(acceleration))
+            throw std::invalid_argument("FluidGridCUDA gravity must be finite");
+        gravity = acceleration;
     }
 
-    void setGravityY(double acceleration) override { check(fc_set_gravity(live(), acceleration)); }
+    // The material transport of step(): FC_TRANSPORT_SEMI_LAGRANGIAN (the default) or
+    // FC_TRANSPORT_PLIC, the reference UniformCPU engine's conservative transport.
+    void setTransport(int scheme)
+    {
+        if (grid)
+            check(fc_set_transport(grid, scheme));
+        else if (scheme != FC_TRANSPORT_SEMI_LAGRANGIAN && scheme != FC_TRANSPORT_PLIC)
+            throw std::invalid_argument("FluidGridCUDA transport scheme is unknown");
+        transport = scheme;
+    }
 
     void upload(const State& state) override
     {
@@ -118,7 +141,7 @@ public:
         };
         const auto lm = components(state.liquid_mass, liquid_mixture.components.size());
         const auto gm = components(state.gas_mass, gas_mixture.components.size());
-        check(fc_upload(live(), f, u, v, p, lm.empty() ? nullptr : lm.data(), gm.empty() ? nullptr : gm.data()));
+        check(fc_upload(rebuilt(), f, u, v, p, lm.empty() ? nullptr : lm.data(), gm.empty() ? nullptr : gm.data()));
     }
 
     State download() const override
@@ -136,7 +159,7 @@ public:
             lm.push_back(m.data());
         for (auto& m : s.gas_mass)
             gm.push_back(m.data());
-        check(fc_download(grid, s.liquid_fraction.data(), s.u.data(), s.v.data(), s.pressure.data(),
+        check(fc_download(live(), s.liquid_fraction.data(), s.u.data(), s.v.data(), s.pressure.data(),
             lm.empty() ? nullptr : lm.data(), gm.empty() ? nullptr : gm.data()));
         return s;
     }
@@ -176,7 +199,7 @@ public:
     double maxDivergence() const override
     {
         double value = 0.0;
-        check(fc_max_divergence(grid, &value));
+        check(fc_max_divergence(live(), &value));
         return value;
     }
 
@@ -212,7 +235,7 @@ public:
     bool saveCheckpoint(FluidCheckpoint& checkpoint) const override
     {
         size_t meta_bytes = 0, payload_bytes = 0;
-        check(fc_save_checkpoint(grid, nullptr, 0, &meta_bytes, nullptr, 0, &payload_bytes));
+        check(fc_save_checkpoint(live(), nullptr, 0, &meta_bytes, nullptr, 0, &payload_bytes));
         std::string meta(meta_bytes, '\0');
         checkpoint.data.resize(payload_bytes);
         check(fc_save_checkpoint(grid, meta.data(), meta_bytes, &meta_bytes, checkpoint.data.data(), payload_bytes,
@@ -236,7 +259,9 @@ public:
     bool loadCheckpoint(const FluidCheckpoint& checkpoint) override
     {
         const auto& metadata = checkpoint.metadata;
-        check(fc_load_checkpoint(live(), metadata.dump().c_str(), checkpoint.data.data(), checkpoint.data.size()));
+        check(fc_load_checkpoint(rebuilt(), metadata.dump().c_str(), checkpoint.data.data(), checkpoint.data.size()));
+        if (metadata.contains("gravity_y"))
+            gravity = metadata["gravity_y"].template get<double>();
         if (metadata.contains("host"))
         {
             const auto& host = metadata["host"];
@@ -306,7 +331,38 @@ private:
     fc_grid* live() const
     {
         if (!grid)
-            throw std::logic_error("FluidGridCUDA used after destroy()");
+            throw std::logic_error("FluidGridCUDA: upload a state after destroy() before using the grid");
+        return grid;
+    }
+
+    // The device grid for an upload: after destroy(), a new one with the host-side
+    // configuration applied (the reference's re-initialisation by upload).
+    fc_grid* rebuilt()
+    {
+        if (grid)
+            return grid;
+        fc_grid* fresh = nullptr;
+        check(fc_create(width, height, cell_size, precision, &fresh));
+        try
+        {
+            std::vector<double> ld, lv, gd, gv;
+            for (const auto& c : liquid_mixture.components)
+                ld.push_back(c.density), lv.push_back(c.dynamic_viscosity);
+            for (const auto& c : gas_mixture.components)
+                gd.push_back(c.density), gv.push_back(c.dynamic_viscosity);
+            if (!ld.empty() || !gd.empty())
+                check(fc_configure_materials(fresh, int(ld.size()), ld.data(), lv.data(), int(gd.size()), gd.data(),
+                    gv.data()));
+            check(fc_set_gravity(fresh, gravity));
+            check(fc_set_origin(fresh, origin.x, origin.y));
+            check(fc_set_transport(fresh, transport));
+        }
+        catch (...)
+        {
+            fc_destroy(fresh);
+            throw;
+        }
+        grid = fresh;
         return grid;
     }
 
@@ -330,6 +386,9 @@ private:
     int width;
     int height;
     double cell_size;
+    int precision;
+    double gravity = 0.0;
+    int transport = FC_TRANSPORT_SEMI_LAGRANGIAN;
     bl::DVec2 origin{};
     SubstanceCatalogue substances;
     FluidMixture liquid_mixture;

@@ -131,7 +131,7 @@ template <typename E, typename F> bool throws(F&& body)
 }
 }
 
-int main(int argc, char** argv)
+int run(int argc, char** argv)
 {
     const bool fp64 = argc < 2 || std::strcmp(argv[1], "fp32") != 0;
     const int precision = fp64 ? FC_PRECISION_FP64 : FC_PRECISION_FP32;
@@ -223,7 +223,7 @@ int main(int argc, char** argv)
     // Status codes arrive as the reference's exception types, before any state changes.
     const auto before = api.download();
     FluidGridBase::State bad = initial;
-    bad.u.resize(bad.u.size() - 1);
+    bad.u.assign(size_t(33 + 1) * 25 - 1, 0.0); // one face short (an empty u means all zero)
     expect(throws<std::invalid_argument>([&] { direct.upload(bad); }) &&
                throws<std::invalid_argument>([&] { api.upload(bad); }),
         "a mis-sized upload is invalid_argument on both engines");
@@ -244,4 +244,19 @@ int main(int argc, char** argv)
 
     std::printf("%s: %d failure(s)\n", failures ? "FAILED" : "PASSED", failures);
     return failures ? 1 : 0;
+}
+
+int main(int argc, char** argv)
+{
+    // Unbuffered: every check's line is out before a later failure ends the process.
+    std::setvbuf(stdout, nullptr, _IONBF, 0);
+    try
+    {
+        return run(argc, argv);
+    }
+    catch (const std::exception& e)
+    {
+        std::printf("FAIL uncaught exception: %s\n", e.what());
+        return 2;
+    }
 }

@@ -190,6 +190,13 @@ __device__ __forceinline__ double warp_sum(double v)
     return v;
 }
 
+__device__ __forceinline__ float warp_sum(float v)
+{
+    for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
 __device__ __forceinline__ double warp_max(double v)
 {
     for (int o = 16; o > 0; o >>= 1)

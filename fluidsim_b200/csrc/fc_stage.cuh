@@ -36,6 +36,8 @@ template <typename T, typename W, int K, bool PRE, int WARPS = 8> struct Stage
     // Post: the prolongation tables of the region's rows and columns (Interp, 16 bytes each).
     static constexpr size_t IY = PRE ? 0 : round(size_t(WARPS) * K * sizeof(Interp));
     static constexpr size_t IX = PRE ? 0 : round(64 * sizeof(Interp));
+    // The inverse diagonal is staged rather than formed from the weights: a correctly rounded
+    // FP32 reciprocal per cell cost more time (2,300 cycles a tile) than its box's copy.
     static constexpr size_t right = 0, down = WB, inv = 2 * WB, vec = 2 * WB + VB, pre = 2 * WB + 2 * VB;
     static constexpr size_t coarse = PRE ? pre : pre + VB;
     static constexpr size_t rows = coarse + CB, cols = rows + IY;
@@ -67,9 +69,25 @@ enum StageMap
 };
 constexpr int kTensorMapBytes = 128;
 
-__device__ __forceinline__ const void* stage_map(const GridDesc& g, int level, int set, int which)
+__device__ __forceinline__ const void* stage_map(const char* maps, int level, int set, int which)
 {
-    return static_cast<const char*>(g.maps) + size_t((level * kShapes + set) * kMapsPerSet + which) * kTensorMapBytes;
+    return maps + size_t((level * kShapes + set) * kMapsPerSet + which) * kTensorMapBytes;
+}
+
+// What the issuing thread needs to start one tile's copies, read from the tile's grid
+// descriptor a tile ahead: the issue then waits on no global load.
+struct IssueArgs
+{
+    const char* maps;  // the grid's tensor maps
+    const Interp* py;  // post: the level's prolongation tables
+    const Interp* px;
+    int w, h;          // the level's size
+};
+
+__device__ __forceinline__ IssueArgs issue_args(const GridDesc& g, int level)
+{
+    const LevelDesc& L = g.lev[level];
+    return IssueArgs{static_cast<const char*>(g.maps), L.py, L.px, L.w, L.h};
 }
 
 // First box column of a region whose leftmost needed padded column is v: a TMA box must start
@@ -84,7 +102,7 @@ template <typename E> __host__ __device__ __forceinline__ int box_start(int v)
 // waiting on its predecessor (stage_issue_weights); the other boxes follow (stage_issue_data). The barrier
 // expects the bytes of all of them from the first call.
 template <typename T, typename W, int K, bool PRE, int WARPS>
-__device__ __forceinline__ void stage_issue_weights(const GridDesc& g, int level, int set, int X0, int Y0, char* stage,
+__device__ __forceinline__ void stage_issue_weights(const IssueArgs& g, int level, int set, int X0, int Y0, char* stage,
     uint64_t* bar)
 {
     using S = Stage<T, W, K, PRE, WARPS>;
@@ -95,53 +113,52 @@ __device__ __forceinline__ void stage_issue_weights(const GridDesc& g, int level
     {
         // The prolongation tables of the region's in-level rows and columns, by bulk copy into
         // slots indexed by region row / column (the kernel reads in-level slots only).
-        const LevelDesc& L = g.lev[level];
-        const int r0 = max(Y0, 0), r1 = min(Y0 + WARPS * K, L.h);
-        const int c0 = max(X0, 0), c1 = min(X0 + 64, L.w);
+        const int r0 = max(Y0, 0), r1 = min(Y0 + WARPS * K, g.h);
+        const int c0 = max(X0, 0), c1 = min(X0 + 64, g.w);
         const unsigned row_bytes = r1 > r0 ? unsigned(r1 - r0) * sizeof(Interp) : 0u;
         const unsigned col_bytes = c1 > c0 ? unsigned(c1 - c0) * sizeof(Interp) : 0u;
         mbarrier_expect_tx(bar, S::tx + row_bytes + col_bytes);
         if (row_bytes)
-            bulk_load(stage + S::rows + size_t(r0 - Y0) * sizeof(Interp), L.py + r0, row_bytes, bar);
+            bulk_load(stage + S::rows + size_t(r0 - Y0) * sizeof(Interp), g.py + r0, row_bytes, bar);
         if (col_bytes)
-            bulk_load(stage + S::cols + size_t(c0 - X0) * sizeof(Interp), L.px + c0, col_bytes, bar);
+            bulk_load(stage + S::cols + size_t(c0 - X0) * sizeof(Interp), g.px + c0, col_bytes, bar);
     }
     else
         mbarrier_expect_tx(bar, S::tx);
-    tma_load_2d(stage + S::right, stage_map(g, level, set, kMapRight), bw, by, bar);
-    tma_load_2d(stage + S::down, stage_map(g, level, set, kMapDown), bw, by, bar);
-    tma_load_2d(stage + S::inv, stage_map(g, level, set, kMapInverse), box_start<T>(X0 + 1), by, bar);
+    tma_load_2d(stage + S::right, stage_map(g.maps, level, set, kMapRight), bw, by, bar);
+    tma_load_2d(stage + S::down, stage_map(g.maps, level, set, kMapDown), bw, by, bar);
+    tma_load_2d(stage + S::inv, stage_map(g.maps, level, set, kMapInverse), box_start<T>(X0 + 1), by, bar);
 }
 
 template <typename T, typename W, int K, bool PRE, int WARPS>
-__device__ __forceinline__ void stage_issue_data(const GridDesc& g, int level, int set, int X0, int Y0, char* stage,
+__device__ __forceinline__ void stage_issue_data(const IssueArgs& g, int level, int set, int X0, int Y0, char* stage,
     uint64_t* bar)
 {
     using S = Stage<T, W, K, PRE, WARPS>;
     const int bx = box_start<T>(X0 + 1), by = Y0;
-    tma_load_2d(stage + S::vec, stage_map(g, level, set, kMapVector), bx, by, bar);
+    tma_load_2d(stage + S::vec, stage_map(g.maps, level, set, kMapVector), bx, by, bar);
     if (!PRE)
     {
-        tma_load_2d(stage + S::pre, stage_map(g, level, set, kMapPre), bx, by, bar);
+        tma_load_2d(stage + S::pre, stage_map(g.maps, level, set, kMapPre), bx, by, bar);
         const int CX0 = X0 / 2 - 1, CY0 = Y0 / 2 - 1;
-        tma_load_2d(stage + S::coarse, stage_map(g, level, set, kMapCoarse), box_start<T>(CX0 + 2), CY0 + 1, bar);
+        tma_load_2d(stage + S::coarse, stage_map(g.maps, level, set, kMapCoarse), box_start<T>(CX0 + 2), CY0 + 1, bar);
     }
 }
 
 // Fetches the descriptors of the data maps ahead of the data copies (one thread): their first
 // use after the dependency wait then costs only the copy.
-template <bool PRE> __device__ __forceinline__ void stage_prefetch_data_maps(const GridDesc& g, int level, int set)
+template <bool PRE> __device__ __forceinline__ void stage_prefetch_data_maps(const IssueArgs& g, int level, int set)
 {
-    prefetch_tensormap(stage_map(g, level, set, kMapVector));
+    prefetch_tensormap(stage_map(g.maps, level, set, kMapVector));
     if (!PRE)
     {
-        prefetch_tensormap(stage_map(g, level, set, kMapPre));
-        prefetch_tensormap(stage_map(g, level, set, kMapCoarse));
+        prefetch_tensormap(stage_map(g.maps, level, set, kMapPre));
+        prefetch_tensormap(stage_map(g.maps, level, set, kMapCoarse));
     }
 }
 
 template <typename T, typename W, int K, bool PRE, int WARPS>
-__device__ __forceinline__ void stage_issue(const GridDesc& g, int level, int set, int X0, int Y0, char* stage,
+__device__ __forceinline__ void stage_issue(const IssueArgs& g, int level, int set, int X0, int Y0, char* stage,
     uint64_t* bar)
 {
     stage_issue_weights<T, W, K, PRE, WARPS>(g, level, set, X0, Y0, stage, bar);
@@ -217,12 +234,24 @@ __device__ __forceinline__ void stage_strip(Strip<T, K>& s, const char* stage, i
     }
 }
 
+// (1 - w) lo + w hi with one explicit rounding order (a product, then a fused multiply-add),
+// so that every path of the prolongation rounds a value the same way.
+template <typename T> __device__ __forceinline__ T prolong_lerp(T w, T lo, T hi)
+{
+    return fma(w, hi, (T(1) - w) * lo);
+}
+
 // Pre-smoothing of `count` tiles (tiles[0 .. count)): four sweeps from zero, the residual, the
 // pre-smoothed solution of the output cells and the transpose-bilinear restriction into the
 // coarse right-hand side (PressureMultigrid.cpp:398-402, 204-231, 233-276).
+//
+// Descriptor fields a tile uses are copied into registers when the tile starts, and the next
+// tile's entry and copy arguments are read one tile ahead: the kernel's global stores cannot
+// alias them, but the compiler cannot know that and would reload them from memory after every
+// store, which put dependent global loads on each tile's path.
 template <typename T, int K, typename W, int WARPS>
 __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2 : 1)
-    k_smooth_pre(const GridDesc* grids, const Tile* tiles, int count, int level, int set)
+    k_smooth_pre(const GridDesc* __restrict__ grids, const Tile* __restrict__ tiles, int count, int level, int set)
 {
     using Shape = TileShape<T, K, true, WARPS>;
     using S = Stage<T, W, K, true, WARPS>;
@@ -249,68 +278,78 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
     edges_clear<T, K, WARPS>(edges);
     __syncthreads();
     int i = blockIdx.x;
+    Tile t = i < count ? tiles[i] : Tile{};
     // The first tile's weights stream in while the previous kernel finishes.
     if (threadIdx.x == 0 && i < count && !misplaced)
     {
-        const Tile t = tiles[i];
-        stage_issue_weights<T, W, K, true, WARPS>(grids[t.grid], level, set, t.x0 - Shape::HALO, t.y0 - Shape::HALO, stage,
-            &bar);
-        stage_prefetch_data_maps<true>(grids[t.grid], level, set);
+        const IssueArgs first = issue_args(grids[t.grid], level);
+        stage_issue_weights<T, W, K, true, WARPS>(first, level, set, t.x0 - Shape::HALO, t.y0 - Shape::HALO, stage, &bar);
+        stage_prefetch_data_maps<true>(first, level, set);
     }
     dependency_wait();
     if (misplaced)
     {
         if (threadIdx.x == 0 && i < count)
-            stage_failed_at(grids[tiles[i].grid].state);
+            stage_failed_at(grids[t.grid].state);
         return;
     }
     if (threadIdx.x == 0 && i < count)
-    {
-        const Tile t = tiles[i];
-        stage_issue_data<T, W, K, true, WARPS>(grids[t.grid], level, set, t.x0 - Shape::HALO, t.y0 - Shape::HALO, stage, &bar);
-    }
+        stage_issue_data<T, W, K, true, WARPS>(issue_args(grids[t.grid], level), level, set, t.x0 - Shape::HALO,
+            t.y0 - Shape::HALO, stage, &bar);
     unsigned parity = 0;
     for (; i < count; i += gridDim.x)
     {
-        const Tile t = tiles[i];
+        const int next = i + gridDim.x;
+        const Tile n = next < count ? tiles[next] : Tile{};
         const GridDesc& g = grids[t.grid];
-        const LevelDesc& L = g.lev[level];
-        const LevelDesc& C = g.lev[level + 1];
+        SolveState* const state = g.state;
+        const LevelDesc& Ld = g.lev[level];
+        const LevelDesc& Cd = g.lev[level + 1];
+        const int Lw = Ld.w, Lh = Ld.h, LS = Ld.S;
+        const int Cw = Cd.w, Ch = Cd.h, CS = Cd.S;
+        T* const pre = static_cast<T*>(Ld.pre);
+        T* const crhs = static_cast<T*>(Cd.rhs);
+        const float wscale = Ld.wscale;
         const int X0 = t.x0 - Shape::HALO, Y0 = t.y0 - Shape::HALO;
         const int cx0 = t.x0 / 2, cy0 = t.y0 / 2;
         // The restriction weights of the tile's coarse cells, while its boxes land.
         const int qx = lane - Shape::HALO / 2, cx = cx0 + qx;
-        const bool column = qx >= 0 && qx < OCX && cx < C.w;
+        const bool column = qx >= 0 && qx < OCX && cx < Cw;
         // Plain loads first used after the sweeps, so their latency stays off the tile's path.
         RestrictAxis<T> along_x{};
         if (column)
-            along_x = static_cast<const RestrictAxis<T>*>(L.rwx)[cx];
+            along_x = static_cast<const RestrictAxis<T>*>(Ld.rwx)[cx];
         RestrictAxis<T> row_weights{};
-        if (threadIdx.x < OCY && cy0 + int(threadIdx.x) < C.h)
-            row_weights = static_cast<const RestrictAxis<T>*>(L.rwy)[cy0 + threadIdx.x];
-        const bool done = g.state->done != 0;
-        const double mean_r = level == 0 ? g.state->mean_r : 0.0;
+        if (threadIdx.x < OCY && cy0 + int(threadIdx.x) < Ch)
+            row_weights = static_cast<const RestrictAxis<T>*>(Ld.rwy)[cy0 + threadIdx.x];
+        const bool done = state->done != 0;
+        const double mean_r = level == 0 ? state->mean_r : 0.0;
+        // The next tile's copy arguments, for the issuing thread.
+        IssueArgs na{};
+        if (threadIdx.x == 0 && next < count)
+            na = issue_args(grids[n.grid], level);
         const bool ok = mbarrier_wait(&bar, parity);
-        if (stage_failed(ok, g.state))
+        if (stage_failed(ok, state))
             return;
         parity ^= 1u;
         Strip<T, K> s;
         if (!done)
         {
-            stage_strip<T, W, K, true, WARPS>(s, stage, X0, L.wscale, lane, warp);
+            stage_strip<T, W, K, true, WARPS>(s, stage, X0, wscale, lane, warp);
             strip_finish<T, K>(s, level, mean_r);
         }
         __syncthreads();
         // The staging buffer is free: the next tile's boxes stream in while this one sweeps.
-        const int next = i + gridDim.x;
         if (threadIdx.x == 0 && next < count)
         {
             fence_async_shared();
-            const Tile n = tiles[next];
-            stage_issue<T, W, K, true, WARPS>(grids[n.grid], level, set, n.x0 - Shape::HALO, n.y0 - Shape::HALO, stage, &bar);
+            stage_issue<T, W, K, true, WARPS>(na, level, set, n.x0 - Shape::HALO, n.y0 - Shape::HALO, stage, &bar);
         }
         if (done)
+        {
+            t = n;
             continue;
+        }
 #pragma unroll
         for (int k = 0; k < K; ++k)
             s.a[k] = s.b[k] = T(0);
@@ -326,7 +365,6 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
         // values: buffer 0 colour 0, buffer 1 colour 1.
         const T above_a = edges.bottom[1][warp][lane], above_b = edges.bottom[0][warp][lane];
         const T below_a = edges.top[0][warp + 2][lane], below_b = edges.top[1][warp + 2][lane];
-        T* pre = static_cast<T*>(L.pre);
         const int gx = X0 + 2 * lane;
 #pragma unroll
         for (int k = 0; k < K; ++k)
@@ -337,8 +375,8 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
             right = lane == 31 ? T(0) : right;
             const T ua = k == 0 ? above_a : s.a[k - 1];
             const T ub = k == 0 ? above_b : s.b[k - 1];
-            const T na = k == K - 1 ? below_a : s.a[k + 1];
-            const T nb = k == K - 1 ? below_b : s.b[k + 1];
+            const T na_ = k == K - 1 ? below_a : s.a[k + 1];
+            const T nb_ = k == K - 1 ? below_b : s.b[k + 1];
             const T wua = k == 0 ? s.ua : s.da[k - 1];
             const T wub = k == 0 ? s.ub : s.db[k - 1];
             const T a = s.a[k], b = s.b[k];
@@ -346,8 +384,8 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
             // restriction reads (its first lane, HALO/2, takes columns from HALO - 1 on).
             T wl = __shfl_up_sync(0xffffffffu, s.wr[k], 1); // every lane takes part
             wl = lane == 0 ? T(0) : wl;
-            const T pa = (wl * (a - left) + s.wm[k] * (a - b)) + (wua * (a - ua) + s.da[k] * (a - na));
-            const T pb = (s.wm[k] * (b - a) + s.wr[k] * (b - right)) + (wub * (b - ub) + s.db[k] * (b - nb));
+            const T pa = (wl * (a - left) + s.wm[k] * (a - b)) + (wua * (a - ua) + s.da[k] * (a - na_));
+            const T pb = (s.wm[k] * (b - a) + s.wr[k] * (b - right)) + (wub * (b - ub) + s.db[k] * (b - nb_));
             const int y = warp * K + k;
             const T res_a = s.ia[k] > T(0) ? s.ra[k] - pa : T(0);
             const T res_b = s.ib[k] > T(0) ? s.rb[k] - pb : T(0);
@@ -357,10 +395,10 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
             lines[y][lane] = restrict_sum(along_x, res_left, res_a, res_b, res_right);
             const int gy = Y0 + y;
             if (y >= Shape::HALO && y < Shape::HALO + Shape::OY && 2 * lane >= Shape::HALO &&
-                2 * lane < Shape::HALO + Shape::OX && gy < L.h && gx < L.w)
+                2 * lane < Shape::HALO + Shape::OX && gy < Lh && gx < Lw)
             {
-                const int idx = padded_index32(L.S, gx, gy);
-                if (gx + 1 < L.w)
+                const int idx = padded_index32(LS, gx, gy);
+                if (gx + 1 < Lw)
                 {
                     typename Pair<T>::type ab;
                     ab.x = a;
@@ -377,28 +415,30 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
         // Along y onto the tile's coarse cells: warp w takes coarse rows w, w + WARPS, ...
         // The next tile rewrites lines and along_y only after its first barrier, which every
         // thread reaches after finishing here.
-        T* crhs = static_cast<T*>(C.rhs);
         if (column)
         {
             for (int qy = warp; qy < OCY; qy += WARPS)
             {
                 const int cy = cy0 + qy;
-                if (cy >= C.h)
+                if (cy >= Ch)
                     break;
                 const int r = Shape::HALO - 1 + 2 * qy;
-                crhs[padded_index32(C.S, cx, cy)] =
+                crhs[padded_index32(CS, cx, cy)] =
                     restrict_sum(along_y[qy], lines[r][lane], lines[r + 1][lane], lines[r + 2][lane], lines[r + 3][lane]);
             }
         }
+        t = n;
     }
 }
 
 // Post-smoothing of `count` tiles: the bilinear prolongation of the coarse solution added to
 // the pre-smoothed one, four sweeps in reversed colour order, and on the fine level sum(z) and
 // r.z for the PCG scalars (PressureMultigrid.cpp:403-407, 278-298; FluidGridCPU.cpp:1712-1726).
+// Descriptor fields are held in registers and the next tile's entry read a tile ahead, as in
+// k_smooth_pre.
 template <typename T, int K, typename W, int WARPS>
 __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2 : 1)
-    k_smooth_post(const GridDesc* grids, const Tile* tiles, int count, int level, int set)
+    k_smooth_post(const GridDesc* __restrict__ grids, const Tile* __restrict__ tiles, int count, int level, int set)
 {
     using Shape = TileShape<T, K, false, WARPS>;
     using S = Stage<T, W, K, false, WARPS>;
@@ -421,48 +461,53 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
     edges_clear<T, K, WARPS>(edges);
     __syncthreads();
     int i = blockIdx.x;
+    Tile t = i < count ? tiles[i] : Tile{};
     // The first tile's weights stream in while the previous kernel finishes.
     if (threadIdx.x == 0 && i < count && !misplaced)
     {
-        const Tile t = tiles[i];
-        stage_issue_weights<T, W, K, false, WARPS>(grids[t.grid], level, set, t.x0 - Shape::HALO, t.y0 - Shape::HALO, stage,
-            &bar);
-        stage_prefetch_data_maps<false>(grids[t.grid], level, set);
+        const IssueArgs first = issue_args(grids[t.grid], level);
+        stage_issue_weights<T, W, K, false, WARPS>(first, level, set, t.x0 - Shape::HALO, t.y0 - Shape::HALO, stage, &bar);
+        stage_prefetch_data_maps<false>(first, level, set);
     }
     dependency_wait();
     if (misplaced)
     {
         if (threadIdx.x == 0 && i < count)
-            stage_failed_at(grids[tiles[i].grid].state);
+            stage_failed_at(grids[t.grid].state);
         return;
     }
     if (threadIdx.x == 0 && i < count)
-    {
-        const Tile t = tiles[i];
-        stage_issue_data<T, W, K, false, WARPS>(grids[t.grid], level, set, t.x0 - Shape::HALO, t.y0 - Shape::HALO, stage, &bar);
-    }
+        stage_issue_data<T, W, K, false, WARPS>(issue_args(grids[t.grid], level), level, set, t.x0 - Shape::HALO,
+            t.y0 - Shape::HALO, stage, &bar);
     unsigned parity = 0;
     int run = 0; // level 0: tiles of the current grid finished since the last count
     for (; i < count; i += gridDim.x)
     {
-        const Tile t = tiles[i];
+        const int next = i + gridDim.x;
+        const Tile n = next < count ? tiles[next] : Tile{};
         const GridDesc& g = grids[t.grid];
-        SolveState& state = *g.state;
-        const LevelDesc& L = g.lev[level];
+        SolveState* const state = g.state;
+        const LevelDesc& Ld = g.lev[level];
+        const int Lw = Ld.w, Lh = Ld.h, LS = Ld.S;
+        T* const out = static_cast<T*>(Ld.sol);
+        const float wscale = Ld.wscale;
         const int X0 = t.x0 - Shape::HALO, Y0 = t.y0 - Shape::HALO;
         const int CX0 = X0 / 2 - 1, CY0 = Y0 / 2 - 1;
         const int gx = X0 + 2 * lane;
-        const bool in_a = gx >= 0 && gx < L.w, in_b = gx + 1 >= 0 && gx + 1 < L.w;
-        const bool done = state.done != 0;
-        const double mean_r = level == 0 ? state.mean_r : 0.0;
+        const bool in_a = gx >= 0 && gx < Lw, in_b = gx + 1 >= 0 && gx + 1 < Lw;
+        const bool done = state->done != 0;
+        const double mean_r = level == 0 ? state->mean_r : 0.0;
+        IssueArgs na{};
+        if (threadIdx.x == 0 && next < count)
+            na = issue_args(grids[n.grid], level);
         const bool ok = mbarrier_wait(&bar, parity);
-        if (stage_failed(ok, g.state))
+        if (stage_failed(ok, state))
             return;
         parity ^= 1u;
         Strip<T, K> s;
         if (!done)
         {
-            stage_strip<T, W, K, false, WARPS>(s, stage, X0, L.wscale, lane, warp);
+            stage_strip<T, W, K, false, WARPS>(s, stage, X0, wscale, lane, warp);
             // The pre-smoothed values of the strip.
             const T* pre = reinterpret_cast<const T*>(stage + S::pre);
             const int c = (X0 + 2 - box_start<T>(X0 + 1)) + 2 * lane;
@@ -475,56 +520,89 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
                 s.b[k] = ab.y;
             }
             strip_finish<T, K>(s, level, mean_r);
-        }
-        __syncthreads();
-        if (!done)
-        {
             // Add the prolonged coarse correction, in-level cells only; the tables arrived with
             // the tile's boxes.
             const Interp* interp_y = reinterpret_cast<const Interp*>(stage + S::rows);
             const Interp* interp_x = reinterpret_cast<const Interp*>(stage + S::cols);
-            const Interp pa = in_a ? interp_x[2 * lane] : Interp{0, 0, 0.0};
-            const Interp pb = in_b ? interp_x[2 * lane + 1] : Interp{0, 0, 0.0};
             const T* coarse = reinterpret_cast<const T*>(stage + S::coarse);
             const int coff = CX0 + 2 - box_start<T>(CX0 + 2);
+            const Interp pa = in_a ? interp_x[2 * lane] : Interp{CX0, CX0, 0.0};
+            const Interp pb = in_b ? interp_x[2 * lane + 1] : Interp{CX0, CX0, 0.0};
             const T wxa = T(pa.weight), wxb = T(pb.weight);
             const int fa = pa.first - CX0 + coff, sa = pa.second - CX0 + coff;
             const int fb = pb.first - CX0 + coff, sb = pb.second - CX0 + coff;
+            const int r0 = warp * K;
+            // Each coarse row the warp's rows read is interpolated along x once: K / 2 + 2 rows
+            // instead of 2K. The loads do not wait for the row tables: the box rows r0 / 2 ..
+            // r0 / 2 + K / 2 + 1 are inside the coarse box whatever the tables say.
+            T xa[K / 2 + 2], xb[K / 2 + 2];
+#pragma unroll
+            for (int j = 0; j < K / 2 + 2; ++j)
+            {
+                const T* row = coarse + (r0 / 2 + j) * S::CBW;
+                xa[j] = prolong_lerp(wxa, row[fa], row[sa]);
+                xb[j] = prolong_lerp(wxb, row[fb], row[sb]);
+            }
+            Interp py[K];
+            bool regular = true;
 #pragma unroll
             for (int k = 0; k < K; ++k)
             {
-                const int gy = Y0 + warp * K + k;
-                if (gy < 0 || gy >= L.h)
-                    continue;
-                const Interp& py = interp_y[warp * K + k];
-                const T* top = coarse + (py.first - CY0) * S::CBW;
-                const T* bottom = coarse + (py.second - CY0) * S::CBW;
-                const T wy = T(py.weight);
-                if (in_a)
+                const int gy = Y0 + r0 + k;
+                regular = regular && gy >= 0 && gy < Lh;
+                py[k] = regular ? interp_y[r0 + k] : Interp{CY0, CY0, 0.0};
+                // Away from the level's edges, fine rows 2m and 2m + 1 (the region origin is
+                // even) read coarse rows m - 1, m and m, m + 1: box rows r0 / 2 + (k + 1) / 2
+                // and the one below.
+                regular = regular && py[k].first - CY0 == r0 / 2 + (k + 1) / 2 && py[k].second == py[k].first + 1;
+            }
+            if (regular)
+            {
+#pragma unroll
+                for (int k = 0; k < K; ++k)
                 {
-                    const T u = (T(1) - wxa) * top[fa] + wxa * top[sa];
-                    const T d = (T(1) - wxa) * bottom[fa] + wxa * bottom[sa];
-                    s.a[k] = s.a[k] + ((T(1) - wy) * u + wy * d);
+                    const T wy = T(py[k].weight);
+                    const int f = (k + 1) / 2;
+                    if (in_a)
+                        s.a[k] = s.a[k] + prolong_lerp(wy, xa[f], xa[f + 1]);
+                    if (in_b)
+                        s.b[k] = s.b[k] + prolong_lerp(wy, xb[f], xb[f + 1]);
                 }
-                if (in_b)
+            }
+            else
+            {
+                // Rows at the level's edges: each fine row reads its two coarse rows.
+#pragma unroll
+                for (int k = 0; k < K; ++k)
                 {
-                    const T u = (T(1) - wxb) * top[fb] + wxb * top[sb];
-                    const T d = (T(1) - wxb) * bottom[fb] + wxb * bottom[sb];
-                    s.b[k] = s.b[k] + ((T(1) - wy) * u + wy * d);
+                    const int gy = Y0 + r0 + k;
+                    if (gy < 0 || gy >= Lh)
+                        continue;
+                    const Interp q = interp_y[r0 + k];
+                    const T* top = coarse + (q.first - CY0) * S::CBW;
+                    const T* bottom = coarse + (q.second - CY0) * S::CBW;
+                    const T wy = T(q.weight);
+                    if (in_a)
+                        s.a[k] = s.a[k] + prolong_lerp(wy, prolong_lerp(wxa, top[fa], top[sa]),
+                                              prolong_lerp(wxa, bottom[fa], bottom[sa]));
+                    if (in_b)
+                        s.b[k] = s.b[k] + prolong_lerp(wy, prolong_lerp(wxb, top[fb], top[sb]),
+                                              prolong_lerp(wxb, bottom[fb], bottom[sb]));
                 }
             }
         }
         __syncthreads();
         // The staging buffer is free: the next tile's boxes stream in while this one sweeps.
-        const int next = i + gridDim.x;
         if (threadIdx.x == 0 && next < count)
         {
             fence_async_shared();
-            const Tile n = tiles[next];
-            stage_issue<T, W, K, false, WARPS>(grids[n.grid], level, set, n.x0 - Shape::HALO, n.y0 - Shape::HALO, stage, &bar);
+            stage_issue<T, W, K, false, WARPS>(na, level, set, n.x0 - Shape::HALO, n.y0 - Shape::HALO, stage, &bar);
         }
         if (done)
+        {
+            t = n;
             continue;
+        }
         // The first half-sweep (colour 1) reads colour-0 edges from buffer 1.
         edges.top[1][warp + 1][lane] = s.a[0];
         edges.bottom[1][warp + 1][lane] = s.b[K - 1];
@@ -535,17 +613,20 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
             strip_sweep<T, K, WARPS>(s, edges, 1, false, 0, lane, warp);
             strip_sweep<T, K, WARPS>(s, edges, 0, false, 1, lane, warp);
         }
-        T* out = static_cast<T*>(L.sol);
-        double sz = 0.0, srz = 0.0;
+        // Fine level: the thread's sums of z and r z over its output cells. FP32 sums its at
+        // most 2K terms, and the warp's 32 threads, in FP32 and hands the warp's sums to the FP64
+        // reduction (FP64 arithmetic and conversions per cell made this phase as long as the
+        // sweeps); FP64 sums in FP64.
+        T tz = T(0), trz = T(0);
         const bool cols_out = 2 * lane >= Shape::HALO && 2 * lane < Shape::HALO + Shape::OX;
 #pragma unroll
         for (int k = 0; k < K; ++k)
         {
             const int y = warp * K + k;
             const int gy = Y0 + y;
-            if (!cols_out || y < Shape::HALO || y >= Shape::HALO + Shape::OY || gy >= L.h || !in_a)
+            if (!cols_out || y < Shape::HALO || y >= Shape::HALO + Shape::OY || gy >= Lh || !in_a)
                 continue;
-            const int idx = padded_index32(L.S, gx, gy);
+            const int idx = padded_index32(LS, gx, gy);
             if (in_b)
             {
                 typename Pair<T>::type ab;
@@ -558,12 +639,12 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
             if (level == 0)
             {
                 // Cells without an open face hold z = 0 and rhs = 0: they add nothing to either sum.
-                sz += double(s.a[k]);
-                srz += double(s.ra[k]) * double(s.a[k]);
+                tz += s.a[k];
+                trz += s.ra[k] * s.a[k];
                 if (in_b)
                 {
-                    sz += double(s.b[k]);
-                    srz += double(s.rb[k]) * double(s.b[k]);
+                    tz += s.b[k];
+                    trz += s.rb[k] * s.b[k];
                 }
             }
         }
@@ -573,7 +654,8 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
             // counts its tiles of this grid once, when its next tile belongs to another grid or
             // it has none left. warp_pairs is rewritten only after the next tile's barriers.
             double2* pairs = reinterpret_cast<double2*>(g.partial);
-            const double wz = warp_sum(sz), wrz = warp_sum(srz);
+            // The warp's sums in the working precision (FP32: a fixed shuffle tree of 32 terms).
+            const double wz = double(warp_sum(tz)), wrz = double(warp_sum(trz));
             if (lane == 0)
                 warp_pairs[warp] = make_double2(wz, wrz);
             __syncthreads();
@@ -589,17 +671,18 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
                 pairs[t.index] = acc;
             }
             ++run;
-            if (next >= count || tiles[next].grid != t.grid)
+            if (next >= count || n.grid != t.grid)
             {
                 if (arrive_run<NT>(g, pairs, run, g.post_tiles, g.post_tiles, &total))
                 {
                     // The strips hold r - mean r: sum r z = sum (r - mean r) z + mean r sum z.
                     if (threadIdx.x == 0)
-                        finish_preconditioner(state, total.x, total.y + state.mean_r * total.x);
+                        finish_preconditioner(*state, total.x, total.y + state->mean_r * total.x);
                 }
                 run = 0;
             }
         }
+        t = n;
     }
 }
 

@@ -394,6 +394,8 @@ def run_cuda(args, world, rank, local_rank):
         line["serve"] = serve_measure(args)
     if rank == 0 and not args.no_steps:
         line["step_leg"] = steps_measure(args, torch)
+        # The same 100 steps with the air held at p = 0 (the free-surface boundary the workload states).
+        line["step_leg_dirichlet"] = steps_measure(args, torch, air_model="dirichlet")
     if rank == 0 and not args.no_viscous:
         from fluidsim_b200 import FluidCudaError
 
@@ -512,7 +514,7 @@ def e2e_measure(args, scene, torch):
             "ms_per_step": ms, "stop_rule": RULE}
 
 
-def steps_measure(args, torch, steps=100, warmup=3, size=1024):
+def steps_measure(args, torch, steps=100, warmup=3, size=1024, air_model="gas"):
     """Full time steps of the dam break with obstacles: a 1024x1024 scene, 16 seeded circular
     obstacles of radii 8..40 cells, gravity -9.8, dt 1/120. Each step runs RK2 semi-Lagrangian
     transport of u and v, the body force and the MG-PCG projection (FluidGrid.step, the
@@ -524,6 +526,7 @@ def steps_measure(args, torch, steps=100, warmup=3, size=1024):
     from fluidsim_b200 import FluidGrid, scenes
 
     scene = scenes.dam_break(size, size, seed=11, obstacles=16, velocity=0.0)
+    scene.air_model = air_model
     g = FluidGrid(size, size, scene.cell_size, "fp32")
     scenes.upload_scene(g, scene)
     stream = torch.cuda.ExternalStream(g.stream())
@@ -544,7 +547,8 @@ def steps_measure(args, torch, steps=100, warmup=3, size=1024):
     ms = statistics.mean(times)
     mean_iters = statistics.mean(iters)
     model_bytes = scene.cells * (70 + 306 * mean_iters)
-    return {"workload": f"dam_break_{size}x{size}, 16 obstacles, {steps} steps after {warmup}", "value": scene.cells / (ms / 1e3),
+    return {"workload": f"dam_break_{size}x{size}, 16 obstacles, {steps} steps after {warmup}", "air_model": air_model,
+            "value": scene.cells / (ms / 1e3),
             "unit": UNIT, "ms_per_step": ms, "p50_ms": statistics.median(times), "max_ms": max(times),
             "iterations_per_step": mean_iters, "max_iterations": max(iters), "solve_status": statuses,
             "all_accepted": accepted,

@@ -21,6 +21,7 @@ STATUS_NAMES = {
 PRECISION = {"fp32": 0, "fp64": 1, "mixed": 2}
 PRECONDITIONER = {"diagonal": 0, "multigrid": 1}
 TRANSPORT = {"semi_lagrangian": 0, "plic": 1}
+AIR_MODEL = {"gas": 0, "dirichlet": 1}
 SOLVE_STATUS = {0: "running", 1: "converged", 2: "iteration_limit", 3: "stalled", 4: "no_work", 5: "breakdown"}
 
 
@@ -143,6 +144,9 @@ SIGNATURES = {
     "fc_apply_gravity": (_int, [_vp, _dbl]),
     "fc_max_divergence": (_int, [_vp, _dp]),
     "fc_classify": (_int, [_vp, C.POINTER(C.c_uint8)]),
+    "fc_set_air_model": (_int, [_vp, _int]),
+    "fc_get_air_model": (_int, [_vp, C.POINTER(_int)]),
+    "fc_extend_air_velocity": (_int, [_vp]),
     "fc_download_coefficients": (_int, [_vp, _dp, _dp, _dp]),
     "fc_apply_preconditioner": (_int, [_vp, _dp, _dbl, _dp]),
     "fc_time_kernel": (_int, [_vp, _int, _int, _dp]),

@@ -105,6 +105,7 @@ struct CoarseInfo
     int pinned;  // pinned cell, -1 when no cell is open
     int open;    // open cells (n + 1, or 0)
     int map[64]; // cell -> unknown index, -1 for the pinned and the closed cells
+    int dirichlet; // Dirichlet air: unknowns only, nothing pinned, no mean and no gauge
 };
 
 struct LevelDesc
@@ -164,6 +165,10 @@ struct GridDesc
     int vec_tiles;           // tiles of the fine vector kernels
     int post_tiles;          // tiles of the level-0 post-smoothing kernel (0 when tail == 0)
     unsigned char* solid;    // optional obstacle mask, W x H, unpadded (null: none)
+    // Dirichlet air model (null: the reference's gas model): 1 where a cell is air held at
+    // p = 0, neither solid nor liquid phase (f > 0.5). Written by k_coefficients from `fraction`.
+    unsigned char* air;
+    const double* fraction;  // liquid fraction, W x H, unpadded
     double* density;         // W x H, unpadded
     double* const* masses;   // device array of `components` W x H mass fields
     int components;

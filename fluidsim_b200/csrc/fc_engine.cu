@@ -258,6 +258,9 @@ struct Grid
     char* visc_arena = nullptr;    // viscosity solver workspace, allocated on first use
     size_t visc_bytes = 0;
     int transport = FC_TRANSPORT_SEMI_LAGRANGIAN;
+    int air_model = FC_AIR_GAS;
+    unsigned char* air = nullptr;  // Dirichlet air cells (written by k_coefficients)
+    unsigned char* air_faces = nullptr; // extension layers of the u then v faces (Dirichlet air)
     char* plic_arena = nullptr;    // PLIC transport workspace, allocated on first use
     size_t plic_bytes = 0;
 
@@ -477,7 +480,8 @@ size_t allocate_grid(Grid& g, bool allocate = true)
     add((void**)&d.b, padded0 * sizeof(double));
     add(&d.u, g.faces_u * elem);
     add(&d.v, g.faces_v * elem);
-    add((void**)&d.coarse_inverse, size_t(std::max(1, d.ncoarse * d.ncoarse)) * sizeof(double));
+    // Up to every coarsest cell is an unknown (Dirichlet air pins none).
+    add((void**)&d.coarse_inverse, size_t(std::max(1, (d.ncoarse + 1) * (d.ncoarse + 1))) * sizeof(double));
     add((void**)&d.coarse, sizeof(CoarseInfo));
     add((void**)&d.state, sizeof(SolveState));
     add((void**)&d.partial, size_t(std::max<long long>(std::max<long long>(d.vec_tiles, (post_pairs + 1) / 2), 1)) *
@@ -490,6 +494,8 @@ size_t allocate_grid(Grid& g, bool allocate = true)
     add(&g.v_next, g.faces_v * elem);
     add((void**)&g.solid, g.cells);
     add((void**)&g.mask, g.cells);
+    add((void**)&g.air, g.cells);
+    add((void**)&g.air_faces, g.faces_u + g.faces_v);
     add((void**)&d.lev[0].pre, padded0 * elem);
     std::vector<void*> cx(g.levels.size()), cy(g.levels.size()), px(g.levels.size()), py(g.levels.size()),
         rx(g.levels.size()), ry(g.levels.size()), rwx(g.levels.size()), rwy(g.levels.size());
@@ -673,7 +679,9 @@ __global__ void k_init_states(const GridDesc* grids, int n, const ProjectParams*
     s.rz = 1.0;
     s.dq = 1.0;
     s.dt = p.dt;
-    s.inv_cells = 1.0 / (double(g.W) * double(g.H));
+    // Dirichlet air: a non-singular system with no mean to take; a zero factor makes every mean
+    // of the solve (right-hand side, pressure, residual, preconditioned residual) zero.
+    s.inv_cells = g.air ? 0.0 : 1.0 / (double(g.W) * double(g.H));
     g.counter[0] = 0u;
 }
 
@@ -682,7 +690,7 @@ __global__ void __launch_bounds__(kVecThreads) k_count_open(const GridDesc* grid
 {
     const Tile t = tiles[blockIdx.x];
     const GridDesc& g = grids[t.grid];
-    if (!g.solid)
+    if (!g.solid || g.air)
         return;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     double open = 0.0;
@@ -738,6 +746,108 @@ template <typename T> __global__ void k_gravity(const GridDesc* grids, const Til
             continue;
         const long long f = (long long)y * g.W + x;
         v[f] = T(double(v[f]) + increment);
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Velocity extension into Dirichlet air (no reference counterpart)
+// ------------------------------------------------------------------------------------------
+//
+// Under Dirichlet air nothing constrains the face velocities between air cells: gravity keeps
+// accelerating them, and transport, which samples and moves the velocity field on both sides
+// of the surface, would carry that into the liquid. Before each substep the liquid's velocity
+// is therefore extended into the air layer by layer (the constant extrapolation of R. Bridson,
+// Fluid Simulation for Computer Graphics, 2nd ed., sec. 4.5): a face known to layer k - 1 keeps
+// its value, an unknown face beside known ones takes their mean and joins layer k, and after
+// kAirLayers layers the faces still unknown are set to zero. Faces of liquid cells, solid faces
+// and the walls form layer 0.
+constexpr int kAirLayers = 4;
+constexpr unsigned char kAirUnknown = 255;
+
+__device__ __forceinline__ bool liquid_cell(const GridDesc& g, int x, int y)
+{
+    const long long c = (long long)y * g.W + x;
+    return !(g.solid && g.solid[c]) && g.fraction[c] > 0.5;
+}
+
+__device__ __forceinline__ bool solid_cell(const GridDesc& g, int x, int y)
+{
+    return g.solid && g.solid[(long long)y * g.W + x];
+}
+
+// Layer 0 over the face tiles ((W + 1) x (H + 1) positions: u face (x, y) for y < H, v face
+// (x, y) for x < W).
+__global__ void k_air_faces_init(const GridDesc* grids, const Tile* tiles, unsigned char* known_u, unsigned char* known_v)
+{
+    const Tile t = tiles[blockIdx.x];
+    const GridDesc& g = grids[t.grid];
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (int k = 0; k < kVecCells; ++k)
+    {
+        const int x = t.x0 + tx + 32 * (k & 1), y = t.y0 + ty + 8 * (k >> 1);
+        if (x <= g.W && y < g.H)
+        {
+            const bool known = x == 0 || x == g.W || solid_cell(g, x - 1, y) || solid_cell(g, x, y) ||
+                               liquid_cell(g, x - 1, y) || liquid_cell(g, x, y);
+            known_u[(long long)y * (g.W + 1) + x] = known ? 0 : kAirUnknown;
+        }
+        if (x < g.W && y <= g.H)
+        {
+            const bool known = y == 0 || y == g.H || solid_cell(g, x, y - 1) || solid_cell(g, x, y) ||
+                               liquid_cell(g, x, y - 1) || liquid_cell(g, x, y);
+            known_v[(long long)y * g.W + x] = known ? 0 : kAirUnknown;
+        }
+    }
+}
+
+// Layer `layer` of one face array (nx x ny faces). Faces written in this pass were unknown and
+// are read by none of this pass's faces (they read faces of layers < `layer` only), so the
+// update is in place and independent of the order in which faces run.
+template <typename T>
+__device__ __forceinline__ void extend_face(T* value, unsigned char* known, int nx, int ny, int x, int y, int layer)
+{
+    const long long f = (long long)y * nx + x;
+    if (known[f] != kAirUnknown)
+        return;
+    double sum = 0.0;
+    int count = 0;
+    const int dx[4] = {-1, 1, 0, 0}, dy[4] = {0, 0, -1, 1};
+#pragma unroll
+    for (int n = 0; n < 4; ++n)
+    {
+        const int qx = x + dx[n], qy = y + dy[n];
+        if (qx < 0 || qx >= nx || qy < 0 || qy >= ny)
+            continue;
+        const long long q = (long long)qy * nx + qx;
+        if (known[q] < layer)
+        {
+            sum += double(value[q]);
+            ++count;
+        }
+    }
+    if (count > 0)
+    {
+        value[f] = T(sum / count);
+        known[f] = (unsigned char)layer;
+    }
+    else if (layer == kAirLayers)
+        value[f] = T(0);
+}
+
+template <typename T>
+__global__ void k_air_faces_extend(const GridDesc* grids, const Tile* tiles, unsigned char* known_u, unsigned char* known_v,
+    int layer)
+{
+    const Tile t = tiles[blockIdx.x];
+    const GridDesc& g = grids[t.grid];
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (int k = 0; k < kVecCells; ++k)
+    {
+        const int x = t.x0 + tx + 32 * (k & 1), y = t.y0 + ty + 8 * (k >> 1);
+        if (x <= g.W && y < g.H)
+            extend_face(static_cast<T*>(g.u), known_u, g.W + 1, g.H, x, y, layer);
+        if (x < g.W && y <= g.H)
+            extend_face(static_cast<T*>(g.v), known_v, g.W, g.H + 1, x, y, layer);
     }
 }
 
@@ -991,12 +1101,14 @@ template <typename T> void launch_rebuild(Plan& p)
         return true;
     }();
     (void)inverse_configured;
-    FC_LAUNCH(k_coarse_inverse<T>, p.n(), kCoarseThreads, kCoarseInverseSmem, s, p.d_desc);
     if (p.precision == FC_PRECISION_MIXED)
         for (int l = 1; l < p.max_tail; ++l)
             FC_LAUNCH(k_weights_half, dim3(ceil_div(p.padded_max[l], 256), p.n()), 256, 0, s, p.d_desc, l);
+    // Level by level: under Dirichlet air a coarse level's held cells follow from the finer
+    // level's inverse diagonal, and the coarsest factor from the level above it.
     for (int l = 0; l + 1 < p.max_levels; ++l)
         FC_LAUNCH(k_inverse_diagonal<T>, dim3(ceil_div(p.padded_max[l], 256), p.n()), 256, 0, s, p.d_desc, l);
+    FC_LAUNCH(k_coarse_inverse<T>, p.n(), kCoarseThreads, kCoarseInverseSmem, s, p.d_desc);
 }
 
 // Resident CTAs of the persistent smoothing kernels: two per SM in FP32, one in FP64 (their
@@ -1335,6 +1447,8 @@ void refresh_descriptor(Grid& g)
 {
     set_weight_scales(g);
     g.desc.solid = g.has_solid ? g.solid : nullptr;
+    g.desc.air = g.air_model == FC_AIR_DIRICHLET ? g.air : nullptr;
+    g.desc.fraction = g.fraction;
     g.desc.masses = g.mass_ptrs;
     g.desc.components = g.components();
     if (g.plan)
@@ -2071,7 +2185,7 @@ void apply_preconditioner(Grid& g, const double* residual, double residual_mean,
     s.mean_r = residual_mean;
     s.restart = 1;
     s.rz = 1.0;
-    s.inv_cells = 1.0 / double(g.cells);
+    s.inv_cells = g.air_model == FC_AIR_DIRICHLET ? 0.0 : 1.0 / double(g.cells);
     check(cudaMemcpyAsync(g.desc.state, &s, sizeof(s), cudaMemcpyHostToDevice, p.stream), "state");
     check(cudaMemcpyAsync(g.staging, residual, g.cells * sizeof(double), cudaMemcpyHostToDevice, p.stream), "residual");
     dispatch(g.precision, [&](auto zero)
@@ -2318,6 +2432,7 @@ std::string checkpoint_metadata(const Grid& g)
     m += ", \"gravity_y\": " + number(g.gravity_y);
     m += ", \"surface_tension\": " + number(g.surface_tension);
     m += ", \"transport\": " + std::to_string(g.transport);
+    m += ", \"air_model\": " + std::to_string(g.air_model);
     m += ", \"preconditioner\": " + std::to_string(g.preconditioner);
     m += ", \"liquid_mixture\": " + mixture(g.liquid_density, g.liquid_viscosity);
     m += ", \"gas_mixture\": " + mixture(g.gas_density, g.gas_viscosity);
@@ -2461,6 +2576,14 @@ void load_checkpoint(Grid& g, const char* metadata, const void* payload, size_t 
             fail(FC_ERR_INVALID_ARGUMENT, "checkpoint transport scheme is unknown");
         transport = int(tr->number);
     }
+    // Older checkpoints carry no air model: the gas model, the engine default.
+    int air_model = FC_AIR_GAS;
+    if (const json::Value* am = m.find("air_model"))
+    {
+        if (am->kind != json::Value::Number || (am->number != FC_AIR_GAS && am->number != FC_AIR_DIRICHLET))
+            fail(FC_ERR_INVALID_ARGUMENT, "checkpoint air model is unknown");
+        air_model = int(am->number);
+    }
     const PayloadLayout layout = payload_layout(g, int(ld.size() + gd.size()), solid);
     if (integer("payload_bytes", 0, 9.0e15) != (long long)layout.total || payload_bytes != layout.total)
         fail(FC_ERR_INVALID_ARGUMENT, "checkpoint payload has %zu bytes, %zu expected", payload_bytes, layout.total);
@@ -2475,6 +2598,7 @@ void load_checkpoint(Grid& g, const char* metadata, const void* payload, size_t 
     g.gravity_y = gravity;
     g.surface_tension = tension;
     g.transport = transport;
+    g.air_model = air_model;
     g.origin_x = origin_x;
     g.origin_y = origin_y;
     allocate_masses(g);
@@ -3067,6 +3191,33 @@ int fc_set_transport(fc_grid* grid, int transport)
     });
 }
 
+int fc_set_air_model(fc_grid* grid, int model)
+{
+    return guarded([&]
+    {
+        if (!grid)
+            fail(FC_ERR_INVALID_ARGUMENT, "null grid");
+        if (model != FC_AIR_GAS && model != FC_AIR_DIRICHLET)
+            fail(FC_ERR_INVALID_ARGUMENT, "unknown air model %d", model);
+        Grid& g = grid->impl;
+        if (g.air_model == model)
+            return;
+        g.air_model = model;
+        g.coefficients_dirty = true;
+        fc::refresh_descriptor(g);
+    });
+}
+
+int fc_get_air_model(const fc_grid* grid, int* model)
+{
+    return guarded([&]
+    {
+        if (!grid || !model)
+            fail(FC_ERR_INVALID_ARGUMENT, "null argument");
+        *model = grid->impl.air_model;
+    });
+}
+
 int fc_get_transport(const fc_grid* grid, int* transport)
 {
     return guarded([&]
@@ -3103,6 +3254,31 @@ int fc_apply_gravity(fc_grid* grid, double dt)
             FC_LAUNCH(fc::k_gravity<T>, p.vec.count, fc::kVecThreads, 0, p.stream, p.d_desc, p.at(p.vec), g.gravity_y * dt);
         });
         check(cudaStreamSynchronize(p.stream), "gravity");
+    });
+}
+
+// Dirichlet air: the liquid's face velocities extended into the air (k_air_faces_extend).
+int fc_extend_air_velocity(fc_grid* grid)
+{
+    return guarded([&]
+    {
+        if (!grid)
+            fail(FC_ERR_INVALID_ARGUMENT, "null grid");
+        Grid& g = grid->impl;
+        fc::require_uploaded(g);
+        fc::Plan& p = fc::single_plan(g);
+        unsigned char* known_u = g.air_faces;
+        unsigned char* known_v = g.air_faces + g.faces_u;
+        FC_LAUNCH(fc::k_air_faces_init, p.faces.count, fc::kVecThreads, 0, p.stream, p.d_desc, p.at(p.faces), known_u,
+            known_v);
+        fc::dispatch(g.precision, [&](auto zero)
+        {
+            using T = decltype(zero);
+            for (int layer = 1; layer <= fc::kAirLayers; ++layer)
+                FC_LAUNCH(fc::k_air_faces_extend<T>, p.faces.count, fc::kVecThreads, 0, p.stream, p.d_desc, p.at(p.faces),
+                    known_u, known_v, layer);
+        });
+        check(cudaStreamSynchronize(p.stream), "air velocity extension");
     });
 }
 
@@ -3150,6 +3326,9 @@ int fc_step(fc_grid* grid, double dt, int max_iterations, double divergence_tole
     };
     for (int i = 0; i < count; ++i)
     {
+        // Dirichlet air: transport sees the liquid's velocity extended into the air.
+        if (grid->impl.air_model == FC_AIR_DIRICHLET && (status = fc_extend_air_velocity(grid)) != FC_OK)
+            return status;
         if ((status = fc_advect(grid, step)) != FC_OK)
             return status;
         if (timings)

@@ -69,7 +69,7 @@ __global__ void __launch_bounds__(kVecThreads) k_precondition_diagonal(const Gri
         const long long i = padded_index(g.S, x, y);
         const double sum = ((double(right[i - 1]) + double(right[i])) + double(down[i - g.S])) + double(down[i]);
         const double inv = sum > 0.0 ? 1.0 / sum : 0.0;
-        const T value = T((double(r[i]) - mean_r) * inv);
+        const T value = g.air && g.air[(long long)y * g.W + x] ? T(0) : T((double(r[i]) - mean_r) * inv);
         z[i] = value;
         if (g.solid && g.solid[(long long)y * g.W + x])
             continue;
@@ -107,6 +107,26 @@ __global__ void k_weights_half(const GridDesc* grids, int level)
         rh[i] = __float2half_rn(fminf(right[i] * inv, 65504.0f));
         dh[i] = __float2half_rn(fminf(down[i] * inv, 65504.0f));
     }
+}
+
+// Dirichlet air (no reference counterpart): a cell held at zero. On the fine level the air
+// cells; on a coarse level the cells none of whose fine cells (2x .. 2x+1, 2y .. 2y+1 of the
+// level above, whose inverse diagonal is final) is an unknown. A held cell keeps its face
+// weights, so the unknowns beside it see the zero: the p = 0 boundary on every level.
+template <typename T> __device__ __forceinline__ bool held_cell(const GridDesc& g, int level, int x, int y)
+{
+    if (level == 0)
+        return g.air[(long long)y * g.W + x] != 0;
+    const LevelDesc& F = g.lev[level - 1];
+    const T* inv = static_cast<const T*>(F.inv);
+    for (int dy = 0; dy < 2; ++dy)
+        for (int dx = 0; dx < 2; ++dx)
+        {
+            const int fx = 2 * x + dx, fy = 2 * y + dy;
+            if (fx < F.w && fy < F.h && inv[padded_index(F.S, fx, fy)] > T(0))
+                return false;
+        }
+    return true;
 }
 
 // Inverse diagonal of a level the strip kernels smooth (blockIdx.y = grid): for each cell
@@ -155,6 +175,8 @@ template <typename T> __global__ void k_inverse_diagonal(const GridDesc* grids, 
             }
             const T diag = ((wl + wr) + wu) + wd;
             value = diag > T(0) ? reciprocal(diag) : T(0);
+            if (g.air && held_cell<T>(g, level, x, y))
+                value = T(0);
         }
         inv[i] = value;
     }
@@ -245,11 +267,12 @@ template <typename T> __global__ void __launch_bounds__(kCoarseThreads) k_coarse
     const T* down = static_cast<const T*>(l.down);
     // Unknowns in cell order: open cells after the first one (pinned). The cells' diagonals
     // are read in parallel, the numbering is one pass over the flags.
+    const bool dirichlet = g.air != nullptr;
     for (int cell = threadIdx.x; cell < cells; cell += blockDim.x)
     {
         const long long i = padded_index(l.S, cell % l.w, cell / l.w);
         const double diag = ((double(right[i - 1]) + double(right[i])) + double(down[i - l.S])) + double(down[i]);
-        open[cell] = diag > 0.0 ? 1 : 0;
+        open[cell] = diag > 0.0 && !(dirichlet && held_cell<T>(g, last, cell % l.w, cell / l.w)) ? 1 : 0;
     }
     __syncthreads();
     if (threadIdx.x == 0)
@@ -260,7 +283,8 @@ template <typename T> __global__ void __launch_bounds__(kCoarseThreads) k_coarse
             map[cell] = -1;
             if (!open[cell])
                 continue;
-            if (pinned < 0)
+            // Dirichlet air makes the system non-singular: nothing is pinned.
+            if (pinned < 0 && !dirichlet)
                 pinned = cell;
             else
                 map[cell] = n++;
@@ -347,7 +371,8 @@ template <typename T> __global__ void __launch_bounds__(kCoarseThreads) k_coarse
     {
         g.coarse->n = n;
         g.coarse->pinned = pinned_shared;
-        g.coarse->open = pinned_shared < 0 ? 0 : n + 1;
+        g.coarse->open = dirichlet ? n : (pinned_shared < 0 ? 0 : n + 1);
+        g.coarse->dirichlet = dirichlet ? 1 : 0;
         g.state->mg_valid = failed ? 0 : 1;
     }
 }
@@ -608,6 +633,10 @@ __device__ void tail_post(const TailLevel<T> C, const TailLevel<T> L, double mea
             const T d = (T(1) - wxb) * m[bottom + pb.first] + wxb * m[bottom + pb.second];
             s.b[k] = s.b[k] + ((T(1) - wy) * u + wy * d);
         }
+        // A cell that is no unknown keeps zero (Dirichlet air sees it; elsewhere such a cell
+        // has no open face and its value is never read).
+        s.a[k] = s.ia[k] > T(0) ? s.a[k] : T(0);
+        s.b[k] = s.ib[k] > T(0) ? s.b[k] : T(0);
     }
     // The first half-sweep (colour 1) reads colour-0 edges from buffer 1.
     edges.top[1][warp + 1][lane] = s.a[0];
@@ -644,7 +673,7 @@ __device__ void tail_solve_coarsest(const TailLevel<T> L, int inverse_offset, in
                 part += double(m[L.rhs + L.at(q % L.w, q / L.w)]);
         part = warp_sum(part);
         if (threadIdx.x == 0)
-            mean_shared = info.open > 0 ? part / info.open : 0.0;
+            mean_shared = info.open > 0 && !info.dirichlet ? part / info.open : 0.0;
     }
     __syncthreads();
     const double mean = mean_shared;
@@ -677,7 +706,7 @@ __device__ void tail_solve_coarsest(const TailLevel<T> L, int inverse_offset, in
             part += z[k];
         part = warp_sum(part);
         if (threadIdx.x == 0)
-            mean_shared = info.open > 0 ? part / info.open : 0.0;
+            mean_shared = info.open > 0 && !info.dirichlet ? part / info.open : 0.0;
     }
     __syncthreads();
     const double zmean = mean_shared;

@@ -81,6 +81,13 @@ __device__ __forceinline__ bool cell_solid(const GridDesc& g, int x, int y)
     return g.solid && g.solid[(long long)y * g.W + x];
 }
 
+// A cell that is no unknown of the pressure solve: solid, or air under the Dirichlet model
+// (held at p = 0; its faces keep their weights, so its liquid neighbours see the zero).
+__device__ __forceinline__ bool cell_held(const GridDesc& g, int x, int y)
+{
+    return cell_solid(g, x, y) || (g.air && g.air[(long long)y * g.W + x]);
+}
+
 #define FC_VEC_TILE_PROLOGUE                                                                       \
     const Tile t = tiles[blockIdx.x];                                                              \
     const GridDesc& g = grids[t.grid];                                                             \
@@ -121,6 +128,8 @@ template <typename T> __global__ void k_coefficients(const GridDesc* grids, cons
         const long long c = (long long)y * g.W + x;
         const long long i = padded_index(g.S, x, y);
         const bool solid = cell_solid(g, x, y);
+        if (g.air)
+            g.air[c] = !solid && !(g.fraction[c] > 0.5); // FluidGridCPU.cpp:1321-1322: liquid is f > 0.5
         double wr = 0.0, wd = 0.0;
         if (x + 1 < g.W && !solid && !cell_solid(g, x + 1, y))
             wr = 2.0 / (density[c] + density[c + 1]);
@@ -183,7 +192,7 @@ template <typename T> __global__ void __launch_bounds__(kVecThreads) k_rhs(const
         const double du = ur - ul;
         const double dv = vd - vu;
         double b = -(du + dv) / g.dx * scale;
-        if (cell_solid(g, x, y))
+        if (cell_held(g, x, y))
             b = 0.0;
         g.b[padded_index(g.S, x, y)] = b;
         sum += b;
@@ -205,7 +214,7 @@ template <typename T> __global__ void __launch_bounds__(kVecThreads) k_rhs_stats
     for (int k = 0; k < kVecCells; ++k)
     {
         const int x = t.x0 + tx + 32 * (k & 1), y = t.y0 + ty + 8 * (k >> 1);
-        if (x >= g.W || y >= g.H || cell_solid(g, x, y))
+        if (x >= g.W || y >= g.H || cell_held(g, x, y))
             continue;
         const double b = g.b[padded_index(g.S, x, y)] - mean;
         mx = fmax(mx, isfinite(b) ? fabs(b) : INFINITY);
@@ -243,7 +252,7 @@ __global__ void __launch_bounds__(kVecThreads) k_warm_start(const GridDesc* grid
         if (x >= g.W || y >= g.H)
             continue;
         const long long i = padded_index(g.S, x, y);
-        if (clear || cell_solid(g, x, y))
+        if (clear || cell_held(g, x, y))
         {
             g.p[i] = 0.0;
             g.p_prev[i] = 0.0;
@@ -273,7 +282,7 @@ __global__ void __launch_bounds__(kVecThreads) k_pressure_sum(const GridDesc* gr
     for (int k = 0; k < kVecCells; ++k)
     {
         const int x = t.x0 + tx + 32 * (k & 1), y = t.y0 + ty + 8 * (k >> 1);
-        if (x >= g.W || y >= g.H || cell_solid(g, x, y))
+        if (x >= g.W || y >= g.H || cell_held(g, x, y))
             continue;
         sum += g.p[padded_index(g.S, x, y)];
     }
@@ -298,8 +307,8 @@ __global__ void k_remove_pressure_mean(const GridDesc* grids, const Tile* tiles)
         if (x >= g.W || y >= g.H)
             continue;
         const long long i = padded_index(g.S, x, y);
-        // Pressure inside obstacles is held at zero.
-        g.p[i] = cell_solid(g, x, y) ? 0.0 : g.p[i] - mean;
+        // Pressure inside obstacles (and in Dirichlet air) is held at zero.
+        g.p[i] = cell_held(g, x, y) ? 0.0 : g.p[i] - mean;
     }
 }
 
@@ -335,7 +344,7 @@ __global__ void __launch_bounds__(kVecThreads) k_true_residual(const GridDesc* g
             continue;
         const long long i = padded_index(g.S, x, y);
         double value = 0.0;
-        if (!cell_solid(g, x, y))
+        if (!cell_held(g, x, y))
             value = (g.b[i] - mean_b) - apply_cell_fp64(right, down, g.p, i, g.S);
         const T stored = T(value);
         r[i] = stored;
@@ -504,9 +513,16 @@ __global__ void __launch_bounds__(kVecThreads) k_direction_operator(const GridDe
             {
                 const long long i = padded_index(S, gx, y);
                 const T ca = cur.x, cb = cur.y;
-                const T qa = (wl * (ca - left) + w[k].x * (ca - cb)) + (uw.x * (ca - prev.x) + dn[k].x * (ca - next.x));
-                const T qb =
-                    (w[k].x * (cb - ca) + w[k].y * (cb - right_d)) + (uw.y * (cb - prev.y) + dn[k].y * (cb - next.y));
+                T qa = (wl * (ca - left) + w[k].x * (ca - cb)) + (uw.x * (ca - prev.x) + dn[k].x * (ca - next.x));
+                T qb = (w[k].x * (cb - ca) + w[k].y * (cb - right_d)) + (uw.y * (cb - prev.y) + dn[k].y * (cb - next.y));
+                if (g.air)
+                {
+                    // Dirichlet air is no unknown: its direction is zero and its q stays zero,
+                    // so its residual stays zero.
+                    const unsigned char* air = g.air + (long long)y * g.W + gx;
+                    qa = air[0] ? T(0) : qa;
+                    qb = in_b && air[1] ? T(0) : qb;
+                }
                 if (in_b)
                 {
                     *reinterpret_cast<P*>(d_new + i) = cur;
@@ -732,6 +748,10 @@ template <typename T> __global__ void __launch_bounds__(kVecThreads) k_divergenc
     {
         const int x = t.x0 + tx + 32 * (k & 1), y = t.y0 + ty + 8 * (k >> 1);
         if (x >= g.W || y >= g.H)
+            continue;
+        // Dirichlet air: only the liquid is held divergence-free (classified from the current
+        // fraction, so a check between steps needs no coefficient rebuild).
+        if (g.air && (cell_solid(g, x, y) || !(g.fraction[(long long)y * g.W + x] > 0.5)))
             continue;
         const long long iu = (long long)y * (g.W + 1) + x;
         const long long iv = (long long)y * g.W + x;

@@ -590,6 +590,14 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
                                               prolong_lerp(wxb, bottom[fb], bottom[sb]));
                 }
             }
+            // A cell that is no unknown keeps zero: Dirichlet air is read by its liquid
+            // neighbours as p = 0; any other such cell has no open face and is never read.
+#pragma unroll
+            for (int k = 0; k < K; ++k)
+            {
+                s.a[k] = s.ia[k] > T(0) ? s.a[k] : T(0);
+                s.b[k] = s.ib[k] > T(0) ? s.b[k] : T(0);
+            }
         }
         __syncthreads();
         // The staging buffer is free: the next tile's boxes stream in while this one sweeps.

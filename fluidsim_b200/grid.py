@@ -243,6 +243,22 @@ class FluidGrid:
                                                 float(relative_tolerance), float(divergence_tolerance), C.byref(r)))
         return ProjectionResult.from_c(r)
 
+    def setAirModel(self, model: str):
+        """'gas' (the reference's two-phase model, default) or 'dirichlet' (air held at p = 0,
+        the free-surface boundary; see fc_set_air_model)."""
+        if model not in N.AIR_MODEL:
+            raise ValueError(f"unknown air model {model!r}")
+        N.check(N.lib().fc_set_air_model(self.handle, N.AIR_MODEL[model]))
+
+    def extendAirVelocity(self):
+        """The liquid's face velocities extended into Dirichlet air (fc_extend_air_velocity)."""
+        N.check(N.lib().fc_extend_air_velocity(self.handle))
+
+    def getAirModel(self) -> str:
+        m = C.c_int()
+        N.check(N.lib().fc_get_air_model(self.handle, C.byref(m)))
+        return {v: k for k, v in N.AIR_MODEL.items()}[m.value]
+
     def setTransport(self, scheme: str):
         """'semi_lagrangian' (default) or 'plic' (UniformCPU's conservative transport)."""
         N.check(N.lib().fc_set_transport(self.handle, N.TRANSPORT[scheme]))

@@ -36,6 +36,8 @@ class Scene:
     # Per-component viscosities (liquid components, then gas); None leaves the grid inviscid.
     liquid_viscosity: Optional[List[float]] = None
     gas_viscosity: Optional[List[float]] = None
+    # Air model of the pressure solve: "gas" (the reference's) or "dirichlet" (p = 0 in the air).
+    air_model: str = "gas"
 
     def __post_init__(self):
         area = self.cell_size * self.cell_size
@@ -251,6 +253,7 @@ def configure_grid(grid, scene: Scene):
     grid.configureMaterials([scene.liquid_density] * len(scene.liquid_mass), [scene.gas_density] * len(scene.gas_mass),
                             scene.liquid_viscosity, scene.gas_viscosity)
     grid.setGravityY(scene.gravity)
+    grid.setAirModel(scene.air_model)
     if scene.surface_tension:
         grid.setSurfaceTension(scene.surface_tension)
     grid.setObstacles(scene.solid)

@@ -55,6 +55,15 @@ typedef enum fc_transport
     FC_TRANSPORT_PLIC = 1             /* UniformCPU's conservative PLIC/MYC transport */
 } fc_transport;
 
+/* What the pressure solve makes of air. */
+typedef enum fc_air_model
+{
+    FC_AIR_GAS = 0,      /* the reference's two-phase model: air is a light gas component of the
+                            closed, mean-free system (FluidGridCPU.cpp:1063-1090); default */
+    FC_AIR_DIRICHLET = 1 /* free surface: cells neither solid nor liquid phase (f > 0.5) are held
+                            at p = 0 and only the liquid is made divergence-free */
+} fc_air_model;
+
 typedef enum fc_launch_mode
 {
     FC_LAUNCH_GRAPH = 0, /* one CUDA graph per projection with a device-side loop (default) */
@@ -192,6 +201,21 @@ int fc_advect(fc_grid* grid, double dt);
  * FP64 whatever the grid's precision. */
 int fc_set_transport(fc_grid* grid, int transport);
 int fc_get_transport(const fc_grid* grid, int* transport);
+/* Air model of the pressure solve (fc_air_model). No counterpart in the reference, whose air is
+ * always a gas component; FC_AIR_DIRICHLET replaces the closure of FluidGridCPU.cpp:1063-1090 by
+ * p = 0 in the air: no mean is removed, the liquid beside air sees the zero across the face (the
+ * face weight 2 / (rho_liquid + rho_air) and the velocity update stay the two-phase ones), every
+ * multigrid level holds the cells that cover no unknown at zero, the coarsest system pins no
+ * cell, and max_divergence runs over the liquid only. A grid without air cells then has a
+ * singular system: its coarsest factor breaks down. Set it before a batch holds the grid. */
+int fc_set_air_model(fc_grid* grid, int model);
+int fc_get_air_model(const fc_grid* grid, int* model);
+/* Under Dirichlet air nothing constrains the velocity between air cells, so fc_step extends the
+ * liquid's face velocities into the air before each substep's transport: faces of liquid cells,
+ * solid faces and walls are known; for 4 layers each unknown face beside known ones takes their
+ * mean; the faces left unknown are set to zero. No counterpart in the reference (its air is a
+ * gas the projection constrains). Exposed for checks; fc_step calls it itself. */
+int fc_extend_air_velocity(fc_grid* grid);
 /* FluidGridCPU::sampleVelocity (UniformCPU/FluidGridCPU.h:132, FluidGridCPU.cpp:465-471): the
  * staggered bilinear velocity at `count` world positions. positions and velocities are host
  * arrays of interleaved (x, y) pairs. */

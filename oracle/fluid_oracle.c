@@ -202,6 +202,10 @@ typedef struct
 struct or_mg
 {
     int pre_sweeps, post_sweeps; /* 4 and 4 in the reference (PressureMultigrid.cpp:396) */
+    /* Dirichlet air (no reference counterpart): cells of `air` hold p = 0 on the fine level;
+     * a coarse cell is held at zero when none of its fine cells is an unknown. Not owned. */
+    int dirichlet;
+    const unsigned char* air;
     int count;
     or_level* lev;
     int n;          /* coarsest unknowns: open cells - 1 (one pinned) */
@@ -403,6 +407,29 @@ static void level_coarsen(const or_level* f, or_level* c)
     level_diagonal(c);
 }
 
+/* Dirichlet air: a coarse cell none of whose fine cells is an unknown (inverse diagonal > 0)
+ * is held at zero, like the air cells it covers; its faces to the unknowns stay in their
+ * diagonals, which is the p = 0 boundary seen from the coarse level. No reference counterpart. */
+static void level_fix(const or_level* f, or_level* c)
+{
+    for (int y = 0; y < c->h; ++y)
+    {
+        for (int x = 0; x < c->w; ++x)
+        {
+            int unknown = 0;
+            for (int dy = 0; dy < 2; ++dy)
+                for (int dx = 0; dx < 2; ++dx)
+                {
+                    const int fx = 2 * x + dx, fy = 2 * y + dy;
+                    if (fx < f->w && fy < f->h && f->invd[(fy + 1) * f->s + fx + 1] > 0.0)
+                        unknown = 1;
+                }
+            if (!unknown)
+                c->invd[(y + 1) * c->s + x + 1] = 0.0;
+        }
+    }
+}
+
 /* Dense Cholesky of the coarsest operator with one cell pinned to zero.
  * PressureMultigrid.cpp:300-345 (factorCoarsest). The reference pins cell 0; here the pinned
  * cell is the first cell with an open face and cells without one (inside obstacles) are left
@@ -423,7 +450,13 @@ static int factor_coarsest(or_mg* mg)
         map[cell] = -1;
         if (!(diag > 0.0))
             continue;
-        if (mg->pinned < 0)
+        if (mg->dirichlet)
+        {
+            /* Dirichlet air: the held cells leave the system and nothing is pinned. */
+            if (l->invd[i] > 0.0)
+                map[cell] = n++;
+        }
+        else if (mg->pinned < 0)
             mg->pinned = cell;
         else
             map[cell] = n++;
@@ -480,8 +513,17 @@ int or_mg_rebuild(or_mg* mg, const double* inv_u, const double* inv_v)
         }
     }
     level_diagonal(f);
+    if (mg->dirichlet && mg->air)
+        for (int y = 0; y < f->h; ++y)
+            for (int x = 0; x < f->w; ++x)
+                if (mg->air[y * f->w + x])
+                    f->invd[(y + 1) * f->s + x + 1] = 0.0;
     for (int i = 0; i + 1 < mg->count; ++i)
+    {
         level_coarsen(&mg->lev[i], &mg->lev[i + 1]);
+        if (mg->dirichlet)
+            level_fix(&mg->lev[i], &mg->lev[i + 1]);
+    }
     return factor_coarsest(mg);
 }
 
@@ -549,7 +591,7 @@ static void level_restrict(or_level* f, or_level* c)
 
 /* Bilinear interpolation of the coarse correction, added to the fine solution.
  * PressureMultigrid.cpp:278-298 (prolongCorrection). */
-static void level_prolong(const or_level* c, or_level* f)
+static void level_prolong(const or_level* c, or_level* f, int dirichlet)
 {
     for (int y = 0; y < f->h; ++y)
     {
@@ -562,6 +604,10 @@ static void level_prolong(const or_level* c, or_level* f)
             const double a = (1.0 - px->weight) * top[px->first] + px->weight * top[px->second];
             const double b = (1.0 - px->weight) * bottom[px->first] + px->weight * bottom[px->second];
             f->sol[(y + 1) * f->s + x + 1] += (1.0 - py->weight) * a + py->weight * b;
+            /* Dirichlet air: cells held at zero stay at zero (the prolongation is masked, and the
+             * restriction, which passes no residual from them, is its transpose). */
+            if (dirichlet && !(f->invd[(y + 1) * f->s + x + 1] > 0.0))
+                f->sol[(y + 1) * f->s + x + 1] = 0.0;
         }
     }
 }
@@ -587,7 +633,8 @@ static void solve_coarsest(or_mg* mg)
         l->sol[(cell / l->w + 1) * l->s + cell % l->w + 1] = 0.0;
     if (open == 0)
         return;
-    mean /= open;
+    /* Dirichlet air: a non-singular system, solved as it stands (no mean, no gauge). */
+    mean = mg->dirichlet ? 0.0 : mean / open;
     for (int cell = 0; cell < cells; ++cell)
     {
         const int row = mg->map[cell];
@@ -608,8 +655,9 @@ static void solve_coarsest(or_mg* mg)
     double sum = 0.0;
     for (int k = 0; k < n; ++k)
         sum += z[k];
-    mean = sum / open;
-    l->sol[(mg->pinned / l->w + 1) * l->s + mg->pinned % l->w + 1] = -mean;
+    mean = mg->dirichlet ? 0.0 : sum / open;
+    if (mg->pinned >= 0)
+        l->sol[(mg->pinned / l->w + 1) * l->s + mg->pinned % l->w + 1] = -mean;
     for (int cell = 0; cell < cells; ++cell)
         if (mg->map[cell] >= 0)
             l->sol[(cell / l->w + 1) * l->s + cell % l->w + 1] = z[mg->map[cell]] - mean;
@@ -631,7 +679,7 @@ static void mg_cycle(or_mg* mg, int index)
         level_smooth(f, 0, 0);
     level_restrict(f, c);
     mg_cycle(mg, index + 1);
-    level_prolong(c, f);
+    level_prolong(c, f, mg->dirichlet);
     for (int sweep = 0; sweep < mg->post_sweeps; ++sweep)
         level_smooth(f, 1, 0);
 }
@@ -662,6 +710,7 @@ struct or_grid
     int w, h, n;
     int open;              /* cells outside obstacles */
     unsigned char* solid;  /* obstacle mask or NULL (no reference counterpart) */
+    unsigned char* air;    /* Dirichlet air cells (p = 0) or NULL: the gas model (no reference counterpart) */
     double dx;
     int preconditioner;
     double *density, *u, *v, *p, *p_prev;
@@ -696,6 +745,44 @@ or_grid* or_grid_create(int width, int height, double cell_size)
     return g;
 }
 
+/* Dirichlet air: the held cells take no part (inverse diagonal 0); their faces keep their
+ * weights, so the unknowns beside them see p = 0. */
+static void apply_air(or_grid* g)
+{
+    if (!g->air)
+        return;
+    for (int i = 0; i < g->n; ++i)
+        if (g->air[i])
+            g->inv_diag[i] = 0.0;
+    g->mg->dirichlet = 1;
+    g->mg->air = g->air;
+}
+
+void or_air_mask(int cells, const double* fraction, const unsigned char* solid, unsigned char* air)
+{
+    for (int i = 0; i < cells; ++i)
+        air[i] = !(solid && solid[i]) && !(fraction[i] > 0.5);
+}
+
+void or_grid_set_air(or_grid* g, const unsigned char* air)
+{
+    free(g->air);
+    g->air = NULL;
+    g->mg->dirichlet = 0;
+    g->mg->air = NULL;
+    if (air)
+    {
+        g->air = (unsigned char*)malloc((size_t)g->n);
+        for (int i = 0; i < g->n; ++i)
+            g->air[i] = air[i] ? 1 : 0;
+    }
+    or_coefficients(g->w, g->h, g->density, g->inv_u, g->inv_v, g->inv_diag);
+    or_face_flags(g->w, g->h, g->solid, g->inv_u, g->inv_v);
+    or_diagonal(g->w, g->h, g->inv_u, g->inv_v, g->inv_diag);
+    apply_air(g);
+    g->mg_valid = 0;
+}
+
 void or_grid_set_solid(or_grid* g, const unsigned char* solid)
 {
     free(g->solid);
@@ -714,6 +801,7 @@ void or_grid_set_solid(or_grid* g, const unsigned char* solid)
     or_coefficients(g->w, g->h, g->density, g->inv_u, g->inv_v, g->inv_diag);
     or_face_flags(g->w, g->h, g->solid, g->inv_u, g->inv_v);
     or_diagonal(g->w, g->h, g->inv_u, g->inv_v, g->inv_diag);
+    apply_air(g);
     g->mg_valid = 0;
 }
 
@@ -722,6 +810,7 @@ void or_grid_destroy(or_grid* g)
     if (!g)
         return;
     free(g->solid);
+    free(g->air);
     free(g->density), free(g->u), free(g->v), free(g->p), free(g->p_prev);
     free(g->inv_u), free(g->inv_v), free(g->inv_diag);
     free(g->b), free(g->r), free(g->z), free(g->d), free(g->q);
@@ -760,6 +849,7 @@ void or_grid_upload(or_grid* g, const double* density, const double* u, const do
         or_face_flags(g->w, g->h, g->solid, g->inv_u, g->inv_v);
         or_diagonal(g->w, g->h, g->inv_u, g->inv_v, g->inv_diag);
     }
+    apply_air(g);
     g->mg_valid = 0;
 }
 
@@ -791,6 +881,14 @@ static double sum_of(const double* x, int n)
 /* FluidGridCPU.cpp:1466-1474 (removeMean); obstacle cells are held at zero and excluded. */
 static void remove_mean(const or_grid* g, double* x)
 {
+    if (g->air)
+    {
+        /* Dirichlet air: a non-singular system; air cells hold zero. */
+        for (int i = 0; i < g->n; ++i)
+            if (g->air[i] || (g->solid && g->solid[i]))
+                x[i] = 0.0;
+        return;
+    }
     double sum = 0.0;
     for (int i = 0; i < g->n; ++i)
         if (!g->solid || !g->solid[i])
@@ -826,7 +924,7 @@ static or_stats true_residual(or_grid* g)
 {
     or_operator(g->w, g->h, g->inv_u, g->inv_v, g->p, g->q);
     for (int i = 0; i < g->n; ++i)
-        g->r[i] = g->b[i] - g->q[i];
+        g->r[i] = g->air && g->air[i] ? 0.0 : g->b[i] - g->q[i];
     return stats_of(g->r, g->n);
 }
 
@@ -842,7 +940,7 @@ static double precondition(or_grid* g, double residual_mean)
     for (int i = 0; i < g->n; ++i)
         if (!g->solid || !g->solid[i])
             zsum += g->z[i];
-    const double mean = zsum / g->open;
+    const double mean = g->air ? 0.0 : zsum / g->open;
     double dot = 0.0;
     for (int i = 0; i < g->n; ++i)
     {
@@ -891,13 +989,17 @@ static int solve_pressure(or_grid* g, int max_iterations, double tol_max, double
         if (!g->mg_valid)
             return -1;
     }
-    double residual_mean = initial.sum / g->open;
+    double residual_mean = g->air ? 0.0 : initial.sum / g->open;
     double rz = precondition(g, residual_mean);
     memcpy(g->d, g->z, n * sizeof(double));
     int iterations = 0;
     while (iterations < max_iterations && rz > 0.0 && isfinite(rz))
     {
         const double dq = or_operator(g->w, g->h, g->inv_u, g->inv_v, g->d, g->q);
+        if (g->air)
+            for (int i = 0; i < n; ++i)
+                if (g->air[i])
+                    g->q[i] = 0.0; /* air cells are no unknowns: their residual stays zero */
         if (dq <= 0.0 || !isfinite(dq))
             break;
         const double alpha = rz / dq;
@@ -909,7 +1011,7 @@ static int solve_pressure(or_grid* g, int max_iterations, double tol_max, double
             g->r[i] -= alpha * g->q[i];
         }
         or_stats s = stats_of(g->r, n);
-        residual_mean = s.sum / g->open;
+        residual_mean = g->air ? 0.0 : s.sum / g->open;
         ++iterations;
         int restart = 0;
         if (met(s, tol_max, tol_sumsq))
@@ -917,7 +1019,7 @@ static int solve_pressure(or_grid* g, int max_iterations, double tol_max, double
             const or_stats actual = true_residual(g);
             if (met(actual, tol_max, tol_sumsq))
                 break;
-            residual_mean = actual.sum / g->open;
+            residual_mean = g->air ? 0.0 : actual.sum / g->open;
             restart = 1;
         }
         const double next = precondition(g, residual_mean);
@@ -940,6 +1042,9 @@ double or_grid_max_divergence(const or_grid* g)
     {
         for (int x = 0; x < g->w; ++x)
         {
+            /* Dirichlet air: only the liquid is held divergence-free. */
+            if (g->air && (g->air[y * g->w + x] || (g->solid && g->solid[y * g->w + x])))
+                continue;
             const double div = ((g->u[(size_t)y * (g->w + 1) + x + 1] - g->u[(size_t)y * (g->w + 1) + x]) +
                                    (g->v[(size_t)(y + 1) * g->w + x] - g->v[(size_t)y * g->w + x])) /
                                g->dx;
@@ -975,7 +1080,7 @@ or_result or_grid_project(
                 }
     }
     or_rhs(w, h, g->dx, dt, g->u, g->v, g->b);
-    remove_mean(g, g->b);
+    remove_mean(g, g->b); /* Dirichlet air: b = 0 on air and solid cells, no mean taken */
     double bsq = 0.0;
     for (int i = 0; i < n; ++i)
         bsq += g->b[i] * g->b[i];

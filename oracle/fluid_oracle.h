@@ -40,6 +40,13 @@ void or_grid_set_preconditioner(or_grid* grid, int which);
  * excluded from every mean. NULL clears. Call after upload (it rebuilds the coefficients). */
 void or_grid_set_solid(or_grid* grid, const unsigned char* solid);
 
+/* Dirichlet air (no reference counterpart): cells of `air` hold p = 0 (the free-surface
+ * boundary), only the other cells are unknowns and divergence-free, and no mean is removed.
+ * NULL returns to the reference's gas model. Call after upload. or_air_mask classifies air as
+ * the cells that are neither solid nor liquid phase (f > 0.5, FluidGridCPU.cpp:1321-1322). */
+void or_grid_set_air(or_grid* grid, const unsigned char* air);
+void or_air_mask(int cells, const double* fraction, const unsigned char* solid, unsigned char* air);
+
 /* Upload: density per cell, face velocities and pressure (null = zero). Resets the warm-start
  * history to the uploaded pressure, like FluidGridCPU::upload. */
 void or_grid_upload(or_grid* grid, const double* density, const double* u, const double* v, const double* pressure);

@@ -107,6 +107,8 @@ def lib():
         L.or_grid_destroy.argtypes = [C.c_void_p]
         L.or_grid_set_preconditioner.argtypes = [C.c_void_p, C.c_int]
         L.or_grid_set_solid.argtypes = [C.c_void_p, _u8p]
+        L.or_grid_set_air.argtypes = [C.c_void_p, _u8p]
+        L.or_air_mask.argtypes = [C.c_int, _dp, _u8p, _u8p]
         L.or_grid_upload.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp]
         L.or_grid_download.argtypes = [C.c_void_p, _dp, _dp, _dp]
         L.or_grid_apply_gravity.argtypes = [C.c_void_p, C.c_double, C.c_double]
@@ -225,6 +227,15 @@ def classify(fraction, solid=None):
     return mask
 
 
+def air_mask(fraction, solid=None):
+    """Dirichlet air cells: neither solid nor liquid phase (f > 0.5)."""
+    f = _f64(fraction)
+    air = np.zeros(f.shape, dtype=np.uint8)
+    s = None if solid is None else np.ascontiguousarray(solid, dtype=np.uint8)
+    lib().or_air_mask(f.size, _ptr(f), None if s is None else s.ctypes.data_as(_u8p), air.ctypes.data_as(_u8p))
+    return air
+
+
 def close_solid_faces(inv_u, inv_v, solid):
     """Zero the face weights around solid cells (in place)."""
     s = np.ascontiguousarray(solid, dtype=np.uint8)
@@ -277,11 +288,14 @@ class OracleGrid:
     def set_sweeps(self, pre: int, post: int):
         lib().or_grid_set_sweeps(self.handle, pre, post)
 
-    def upload(self, density, u, v, pressure=None, solid=None):
+    def upload(self, density, u, v, pressure=None, solid=None, air=None):
+        """`air`: a mask of Dirichlet air cells (p = 0), or None for the reference's gas model."""
         lib().or_grid_upload(self.handle, _ptr(_f64(density)), _ptr(_f64(u)), _ptr(_f64(v)), _ptr(_f64(pressure)))
         if solid is not None:
             s = np.ascontiguousarray(solid, dtype=np.uint8)
             lib().or_grid_set_solid(self.handle, s.ctypes.data_as(_u8p))
+        self._air = None if air is None else np.ascontiguousarray(air, dtype=np.uint8)
+        lib().or_grid_set_air(self.handle, None if self._air is None else self._air.ctypes.data_as(_u8p))
 
     def download(self):
         u = np.zeros((self.h, self.w + 1))

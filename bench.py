@@ -686,12 +686,18 @@ def batched_measure(args, torch, world=1, rank=0, count=256):
             "max_iterations": max(r.iterations for r in res)}
 
 
-def serve_measure(args, rate=200.0, budget=150 * 10**9):
+SERVE_CLASSES = (256 * 256, 1024 * 1024)  # the server's default size classes (cells)
+
+
+def serve_measure(args, rate=200.0, budget=150 * 10**9, precision="mixed"):
     """Serving: Poisson arrivals (mean `rate` per second) of dam breaks with surface tension
     (sigma 0.07, liquid 1000, air 1), square sides log-uniform 64..2048, each run for
-    serve_steps steps of dt 1/120 to the max-norm rule at the bench tolerance, admitted by a
-    device-memory budget and batched as they arrive. The same simulations are then run one at a
-    time through fc_step (the plain path). A bounded sample: serve_requests requests."""
+    serve_steps steps of dt 1/120 to the max-norm rule at the bench tolerance, in mixed
+    precision, admitted by a device-memory budget and batched as they arrive in three size
+    classes (up to 256^2, up to 1024^2, larger cells), each stepped by its own worker. The same
+    simulations are then run one at a time through fc_step (the plain path, same precision).
+    Step latencies are reported per size class for both. A bounded sample: serve_requests
+    requests."""
     import time
 
     from fluidsim_b200 import FluidGrid, scenes
@@ -702,41 +708,62 @@ def serve_measure(args, rate=200.0, budget=150 * 10**9):
     steps = args.serve_steps
     cell_steps = steps * sum(s.cells for s in reqs)
     server = Server(budget, max_active=256)
-    out = serve(server, reqs, arrivals, steps, 200, args.tolerance)
-    stats = server.stats()
+    out = serve(server, reqs, arrivals, steps, 200, args.tolerance, precision=precision)
+    stats, per_class = server.stats(), server.class_stats()
     served_ok = all(st.state == "done" for st in out["statuses"])
+    failures = [{"side": s.width, "state": st.state, "error": server.error(sim)}
+                for s, sim, st in zip(reqs, out["ids"], out["statuses"]) if st.state != "done"]
+    if failures:
+        print(f"bench.py: served simulations failed: {failures}", file=sys.stderr)
     for sim in out["ids"]:
         server.release(sim)
     server.close()
 
-    plain_lat = []
+    def size_class(cells):
+        return sum(cells > b for b in SERVE_CLASSES)
+
+    plain_lat = [[] for _ in range(len(SERVE_CLASSES) + 1)]
+    plain_class_s = [0.0] * (len(SERVE_CLASSES) + 1)
     t0 = time.perf_counter()
     for s in reqs:
-        g = FluidGrid(s.width, s.height, s.cell_size, "fp32")
+        k = size_class(s.cells)
+        a0 = time.perf_counter()
+        g = FluidGrid(s.width, s.height, s.cell_size, precision)
         scenes.upload_scene(g, s)
         for _ in range(steps):
             a = time.perf_counter()
             g.step(s.dt, 200, args.tolerance)
-            plain_lat.append((time.perf_counter() - a) * 1e3)
+            plain_lat[k].append((time.perf_counter() - a) * 1e3)
         g.destroy()
+        plain_class_s[k] += time.perf_counter() - a0
     plain_s = time.perf_counter() - t0
-    plain_lat = np.sort(np.array(plain_lat))
 
     def pct(a, q):
-        return float(a[max(0, int(np.ceil(q * len(a))) - 1)])
+        a = np.sort(np.asarray(a))
+        return float(a[max(0, int(np.ceil(q * len(a))) - 1)]) if len(a) else None
 
+    classes = []
+    for k, c in enumerate(per_class):
+        members = [s for s in reqs if size_class(s.cells) == k]
+        classes.append({"max_cells": c["max_cells"] if k < len(SERVE_CLASSES) else None,
+                        "sizes": sorted(s.width for s in members),
+                        "served": {"step_p50_ms": c["step_p50_ms"], "step_p99_ms": c["step_p99_ms"],
+                                   "step_max_ms": c["step_max_ms"], "ticks": c["ticks"], "busy_s": c["busy_ms"] / 1e3},
+                        "plain": {"step_p50_ms": pct(plain_lat[k], 0.5), "step_p99_ms": pct(plain_lat[k], 0.99),
+                                  "wall_s": plain_class_s[k]}})
+    every = [x for lat in plain_lat for x in lat]
     served = cell_steps / out["wall_s"]
     plain = cell_steps / plain_s
-    return {"value": served, "unit": UNIT, "requests": len(reqs), "steps_per_request": steps,
+    return {"value": served, "unit": UNIT, "precision": precision, "requests": len(reqs), "steps_per_request": steps,
             "arrival_rate_per_s": rate, "sizes": sorted(s.width for s in reqs),
             "sample": f"{len(reqs)} requests (bounded sample of the Poisson stream), sides log-uniform 64..2048, "
                       f"dx 1/128, sigma 0.07, dt 1/120",
             "wall_s": out["wall_s"], "step_p50_ms": stats["step_p50_ms"], "step_p99_ms": stats["step_p99_ms"],
             "step_max_ms": stats["step_max_ms"], "peak_active": stats["peak_active"],
             "peak_device_bytes": stats["peak_bytes"], "budget_bytes": budget, "batch_plans_built": stats["batch_rebuilds"],
-            "all_done": served_ok,
-            "plain": {"value": plain, "unit": UNIT, "wall_s": plain_s, "step_p50_ms": pct(plain_lat, 0.5),
-                      "step_p99_ms": pct(plain_lat, 0.99)},
+            "all_done": served_ok, "failures": failures, "size_classes": classes,
+            "plain": {"value": plain, "unit": UNIT, "wall_s": plain_s, "step_p50_ms": pct(every, 0.5),
+                      "step_p99_ms": pct(every, 0.99)},
             "speedup_vs_plain": served / plain}
 
 

@@ -127,12 +127,16 @@ SIGNATURES = {
     "fc_grid_device_bytes": (_int, [_int, _int, _int, _int, _int, C.POINTER(C.c_size_t)]),
     "fc_get_device_bytes": (_int, [_vp, C.POINTER(C.c_size_t)]),
     "fc_server_create": (_int, [C.c_size_t, _int, C.POINTER(_vp)]),
+    "fc_server_create_classes": (_int, [C.c_size_t, _int, _int, C.POINTER(C.c_longlong), C.POINTER(_vp)]),
+    "fc_server_class_count": (_int, [_vp, C.POINTER(_int)]),
+    "fc_server_get_class_stats": (_int, [_vp, _int, C.POINTER(FcServerStats), C.POINTER(C.c_longlong)]),
     "fc_server_destroy": (_int, [_vp]),
     "fc_server_submit": (_int, [_vp, C.POINTER(FcSimDesc), C.POINTER(C.c_longlong)]),
     "fc_server_status": (_int, [_vp, C.c_longlong, C.POINTER(FcSimStatus)]),
     "fc_server_wait": (_int, [_vp, C.c_longlong, _dbl, C.POINTER(FcSimStatus)]),
     "fc_server_download": (_int, [_vp, C.c_longlong, _vp, _vp, _vp, _vp, _vp, _vp]),
     "fc_server_release": (_int, [_vp, C.c_longlong]),
+    "fc_server_error": (_int, [_vp, C.c_longlong, C.c_char_p, C.c_size_t]),
     "fc_server_get_stats": (_int, [_vp, C.POINTER(FcServerStats)]),
     "fc_server_step_latencies": (_int, [_vp, _vp, C.c_size_t, C.POINTER(C.c_size_t)]),
     "fc_get_surface_tension": (_int, [_vp, _dp]),
@@ -147,6 +151,8 @@ SIGNATURES = {
     "fc_set_air_model": (_int, [_vp, _int]),
     "fc_get_air_model": (_int, [_vp, C.POINTER(_int)]),
     "fc_extend_air_velocity": (_int, [_vp]),
+    "fc_advance_substep": (_int, [_vp, _dbl, C.POINTER(_int)]),
+    "fc_set_stream_priority": (_int, [_vp, _int]),
     "fc_download_coefficients": (_int, [_vp, _dp, _dp, _dp]),
     "fc_apply_preconditioner": (_int, [_vp, _dp, _dbl, _dp]),
     "fc_time_kernel": (_int, [_vp, _int, _int, _dp]),

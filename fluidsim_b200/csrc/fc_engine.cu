@@ -47,6 +47,9 @@ namespace fc
 
 thread_local std::string last_error;
 std::atomic<long long> launch_count{0};
+// Launches made by the calling thread: graph capture counts its captured kernels from this, so
+// kernels launched by other threads meanwhile are not counted as captured.
+thread_local long long thread_launches = 0;
 
 [[noreturn]] void fail(int status, const char* format, ...)
 {
@@ -80,6 +83,7 @@ inline long long launch_size(dim3 blocks) { return (long long)blocks.x * blocks.
             kernel<<<(blocks), (threads), (smem), (stream)>>>(__VA_ARGS__);                        \
             check(cudaGetLastError(), #kernel);                                                    \
             ::fc::launch_count.fetch_add(1, std::memory_order_relaxed);                            \
+            ++::fc::thread_launches;                                                               \
         }                                                                                          \
     } while (0)
 
@@ -103,6 +107,7 @@ void launch_dependent(const char* name, void (*kernel)(Params...), int blocks, i
     config.numAttrs = 1;
     check(cudaLaunchKernelEx(&config, kernel, static_cast<Params>(args)...), name);
     launch_count.fetch_add(1, std::memory_order_relaxed);
+    ++thread_launches;
 }
 
 #define FC_LAUNCH_DEP(kernel, blocks, threads, smem, stream, ...) \
@@ -239,6 +244,7 @@ struct Grid
     int tail_cells = 1024; // largest level the one-CTA tail takes (autotuned)
 
     cudaStream_t stream = nullptr;
+    int stream_priority = 0; // CUDA stream priority (lower runs first); batches take their members' highest
     char* arena = nullptr;
     size_t arena_bytes = 0;
     GridDesc desc{};
@@ -632,8 +638,12 @@ void allocate_masses(Grid& g)
         std::vector<double*> ptrs(k);
         for (int i = 0; i < k; ++i)
             ptrs[i] = g.masses + size_t(i) * g.cells;
-        check(cudaMemcpy(g.mass_ptrs, ptrs.data(), k * sizeof(double*), cudaMemcpyHostToDevice), "mass pointers");
-        check(cudaMemset(g.masses, 0, size_t(k) * g.cells * sizeof(double)), "mass clear");
+        // On the grid's stream: its kernels and uploads are ordered after both. (A copy or set on
+        // the legacy default stream is not ordered with the grid's non-blocking stream, and a
+        // pageable copy may return before its data lands.)
+        check(cudaMemcpyAsync(g.mass_ptrs, ptrs.data(), k * sizeof(double*), cudaMemcpyHostToDevice, g.stream),
+            "mass pointers");
+        check(cudaMemsetAsync(g.masses, 0, size_t(k) * g.cells * sizeof(double), g.stream), "mass clear");
     }
     g.desc.masses = g.mass_ptrs;
     g.desc.components = k;
@@ -993,7 +1003,10 @@ std::unique_ptr<Plan> make_plan(const std::vector<Grid*>& grids, cudaStream_t st
         plan->stream = stream;
     else
     {
-        check(cudaStreamCreateWithFlags(&plan->stream, cudaStreamNonBlocking), "plan stream");
+        int priority = 0;
+        for (const Grid* g : grids)
+            priority = std::min(priority, g->stream_priority);
+        check(cudaStreamCreateWithPriority(&plan->stream, cudaStreamNonBlocking, priority), "plan stream");
         plan->own_stream = true;
     }
     const int n = plan->n();
@@ -1071,7 +1084,10 @@ std::unique_ptr<Plan> make_plan(const std::vector<Grid*>& grids, cudaStream_t st
             });
     }
     check(cudaMalloc(&plan->d_tiles, std::max<size_t>(1, tiles.size()) * sizeof(Tile)), "plan tiles");
-    check(cudaMemcpy(plan->d_tiles, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice), "plan tiles");
+    // On the plan's stream, which every kernel reading the tiles runs on (a copy on the legacy
+    // default stream is not ordered with it and may return before its data lands).
+    check(cudaMemcpyAsync(plan->d_tiles, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice, plan->stream),
+        "plan tiles");
     check(cudaMalloc(&plan->d_desc, n * sizeof(GridDesc)), "plan descriptors");
     check(cudaMalloc(&plan->d_params, n * sizeof(ProjectParams)), "plan params");
     check(cudaMalloc(&plan->d_states, n * sizeof(SolveState)), "plan states");
@@ -1219,8 +1235,17 @@ template <typename T> void launch_iteration(Plan& p, bool use_mg, int parity)
 template <typename T> void set_kernel_attributes(Plan& p)
 {
     // Always opted in: the tail's static edge rows count against the 48 KB default as well.
-    check(cudaFuncSetAttribute(k_mg_tail<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(p.tail_smem)),
-        "tail shared memory");
+    // The limit only ever rises (to the largest tail any plan has launched), so plans driven
+    // from several threads never lower it under one another's launches.
+    static std::mutex lock;
+    static size_t opted = 0;
+    std::lock_guard<std::mutex> guard(lock);
+    if (p.tail_smem > opted)
+    {
+        check(cudaFuncSetAttribute(k_mg_tail<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(p.tail_smem)),
+            "tail shared memory");
+        opted = p.tail_smem;
+    }
 }
 
 // Projection set-up: states, right-hand side, warm start, first residual, first z.
@@ -1273,7 +1298,7 @@ template <typename T> void capture_projection(Plan& p, bool use_mg, int cap)
     p.graph = graph;
 
     // Set-up, captured into the outer graph.
-    const long long before_setup = launch_count.load();
+    const long long before_setup = thread_launches;
     check(cudaStreamBeginCaptureToGraph(s, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal), "capture");
     launch_setup<T>(p, use_mg);
 
@@ -1299,8 +1324,8 @@ template <typename T> void capture_projection(Plan& p, bool use_mg, int cap)
     launch_finish<T>(p);
     cudaGraph_t captured;
     check(cudaStreamEndCapture(s, &captured), "end capture");
-    p.setup_kernels = int(launch_count.load() - before_setup);
-    const long long before_body = launch_count.load();
+    p.setup_kernels = int(thread_launches - before_setup);
+    const long long before_body = thread_launches;
 
     // Loop body: two iterations (the direction buffers alternate) and the condition.
     cudaStream_t side;
@@ -1318,7 +1343,7 @@ template <typename T> void capture_projection(Plan& p, bool use_mg, int cap)
     cudaGraph_t body_captured;
     check(cudaStreamEndCapture(side, &body_captured), "body end capture");
     cudaStreamDestroy(side);
-    p.body_kernels = int(launch_count.load() - before_body);
+    p.body_kernels = int(thread_launches - before_body);
     // Captured launches are not executions: take them back out of the process counter, which
     // then advances by the executed kernels after each projection.
     launch_count.fetch_sub(p.setup_kernels + p.body_kernels);
@@ -1335,7 +1360,7 @@ template <typename T> long long run_projection(Plan& p, bool use_mg, int max_ite
     if (launch_mode.load() == FC_LAUNCH_STREAM)
     {
         set_kernel_attributes<T>(p);
-        const long long before = launch_count.load();
+        const long long before = thread_launches;
         check(cudaMemcpyAsync(p.d_params, p.h_params, p.n() * sizeof(ProjectParams), cudaMemcpyHostToDevice, p.stream),
             "params");
         launch_setup<T>(p, use_mg);
@@ -1360,7 +1385,7 @@ template <typename T> long long run_projection(Plan& p, bool use_mg, int max_ite
             "results");
         check(cudaStreamSynchronize(p.stream), "projection");
         p.h_bodies = bodies;
-        return launch_count.load() - before;
+        return thread_launches - before;
     }
     if (!p.exec || p.graph_cap != cap || p.graph_use_mg != (use_mg ? 1 : 0))
         capture_projection<T>(p, use_mg, cap);
@@ -1462,13 +1487,13 @@ void rebuild_if_dirty(Plan& p)
         dirty |= g->coefficients_dirty;
     if (!dirty)
         return;
-    const long long before = launch_count.load();
+    const long long before = thread_launches;
     dispatch(p.precision, [&](auto zero)
     {
         using T = decltype(zero);
         launch_rebuild<T>(p);
     });
-    p.rebuild_kernels = int(launch_count.load() - before);
+    p.rebuild_kernels = int(thread_launches - before);
     for (Grid* g : p.grids)
         g->coefficients_dirty = false;
 }
@@ -1642,7 +1667,7 @@ void download(Grid& g, double* fraction, double* u, double* v, double* pressure,
 // Semi-Lagrangian transport of the velocities, the liquid fraction and every component mass
 // through the velocity at the start of the step (fc_advect.cuh). Masses change, so the
 // pressure coefficients are rebuilt at the next projection.
-void advect_semi_lagrangian(Grid& g, double dt)
+void advect_semi_lagrangian(Grid& g, double dt, bool wait)
 {
     require_uploaded(g);
     Plan& p = single_plan(g);
@@ -1664,7 +1689,8 @@ void advect_semi_lagrangian(Grid& g, double dt)
         check(cudaMemcpyAsync(g.desc.u, g.u_next, g.faces_u * sizeof(T), cudaMemcpyDeviceToDevice, s), "advect");
         check(cudaMemcpyAsync(g.desc.v, g.v_next, g.faces_v * sizeof(T), cudaMemcpyDeviceToDevice, s), "advect");
     });
-    check(cudaStreamSynchronize(s), "advect");
+    if (wait)
+        check(cudaStreamSynchronize(s), "advect");
     g.coefficients_dirty = true;
 }
 
@@ -1740,7 +1766,7 @@ void launch_curvature(Grid& g, cudaStream_t s)
 
 // FluidGridCPU::applySurfaceTension (FluidGridCPU.cpp:862-926): curvature, then the capillary
 // force on every interior face with the pressure face weights of the current densities.
-void apply_surface_tension(Grid& g, double dt)
+void apply_surface_tension(Grid& g, double dt, bool wait = true)
 {
     require_uploaded(g);
     if (g.surface_tension == 0.0)
@@ -1755,7 +1781,8 @@ void apply_surface_tension(Grid& g, double dt)
         FC_LAUNCH(k_tension_force<T>, grid_dim, block, 0, p.stream, p.d_desc, 0, g.fraction, g.tension, g.surface_tension,
             dt);
     });
-    check(cudaStreamSynchronize(p.stream), "surface tension");
+    if (wait)
+        check(cudaStreamSynchronize(p.stream), "surface tension");
 }
 
 // Completed curvature per cell and its validity, for inspection.
@@ -2156,12 +2183,14 @@ void advect_plic(Grid& g, double dt)
     g.coefficients_dirty = true;
 }
 
-void advect(Grid& g, double dt)
+// Transport of one step. With wait false the semi-Lagrangian kernels are only enqueued on the
+// grid's stream (PLIC transport reads back its CFL substeps and always waits).
+void advect(Grid& g, double dt, bool wait = true)
 {
     if (g.transport == FC_TRANSPORT_PLIC)
         advect_plic(g, dt);
     else
-        advect_semi_lagrangian(g, dt);
+        advect_semi_lagrangian(g, dt, wait);
 }
 
 // One preconditioner application to a given residual (PressureMultigrid::apply,
@@ -2740,6 +2769,65 @@ void* noalloc_address(cudaStream_t stream)
     return addresses[device];
 }
 
+// Gravity on the vertical faces (FluidGridCPU.cpp:835-841 order: after transport).
+void apply_gravity(Grid& g, double dt, bool wait)
+{
+    require_uploaded(g);
+    Plan& p = single_plan(g);
+    dispatch(g.precision, [&](auto zero)
+    {
+        using T = decltype(zero);
+        FC_LAUNCH(k_gravity<T>, p.vec.count, kVecThreads, 0, p.stream, p.d_desc, p.at(p.vec), g.gravity_y * dt);
+    });
+    if (wait)
+        check(cudaStreamSynchronize(p.stream), "gravity");
+}
+
+// Dirichlet air: the liquid's face velocities extended into the air (k_air_faces_extend).
+void extend_air_velocity(Grid& g, bool wait)
+{
+    require_uploaded(g);
+    Plan& p = single_plan(g);
+    unsigned char* known_u = g.air_faces;
+    unsigned char* known_v = g.air_faces + g.faces_u;
+    FC_LAUNCH(k_air_faces_init, p.faces.count, kVecThreads, 0, p.stream, p.d_desc, p.at(p.faces), known_u, known_v);
+    dispatch(g.precision, [&](auto zero)
+    {
+        using T = decltype(zero);
+        for (int layer = 1; layer <= kAirLayers; ++layer)
+            FC_LAUNCH(k_air_faces_extend<T>, p.faces.count, kVecThreads, 0, p.stream, p.d_desc, p.at(p.faces), known_u,
+                known_v, layer);
+    });
+    if (wait)
+        check(cudaStreamSynchronize(p.stream), "air velocity extension");
+}
+
+// The reference's step runs the viscosity solve without an iteration cap; this bound only turns
+// a solve that cannot converge into an error instead of an endless loop.
+constexpr int kViscosityCap = 20000;
+
+// fc_step's physical substep before its projection (FluidGridCPU.cpp:300-360 order): the air
+// extension under Dirichlet air, transport, implicit viscosity when a component is viscous
+// (FluidGridGPU.cpp:1139-1146, 1e-4 relative), gravity and surface tension. With wait false the
+// kernels are only enqueued on the grid's stream; the viscosity solve and PLIC transport read
+// values back and wait regardless. Returns the viscosity iterations.
+int advance_substep(Grid& g, double dt, bool wait)
+{
+    if (g.air_model == FC_AIR_DIRICHLET)
+        extend_air_velocity(g, wait);
+    advect(g, dt, wait);
+    int viscous = 0;
+    if (has_viscosity(g))
+    {
+        const ViscResult r = apply_viscosity(g, dt, 1e-4, kViscosityCap);
+        viscous = r.iterations;
+    }
+    apply_gravity(g, dt, wait);
+    if (g.surface_tension > 0.0)
+        apply_surface_tension(g, dt, wait);
+    return viscous;
+}
+
 } // namespace fc
 
 // ==========================================================================================
@@ -3208,6 +3296,31 @@ int fc_set_air_model(fc_grid* grid, int model)
     });
 }
 
+int fc_set_stream_priority(fc_grid* grid, int priority)
+{
+    return guarded([&]
+    {
+        if (!grid)
+            fail(FC_ERR_INVALID_ARGUMENT, "null grid");
+        int least = 0, greatest = 0;
+        check(cudaDeviceGetStreamPriorityRange(&least, &greatest), "stream priority range");
+        if (priority > least || priority < greatest)
+            fail(FC_ERR_INVALID_ARGUMENT, "stream priority %d outside [%d, %d]", priority, greatest, least);
+        Grid& g = grid->impl;
+        if (priority == g.stream_priority)
+            return;
+        // The grid's single-grid plan runs on its stream: both are remade (the device state is
+        // kept); batches made later take the new priority.
+        check(cudaStreamSynchronize(g.stream), "stream priority");
+        g.plan.reset();
+        cudaStream_t fresh = nullptr;
+        check(cudaStreamCreateWithPriority(&fresh, cudaStreamNonBlocking, priority), "stream");
+        cudaStreamDestroy(g.stream);
+        g.stream = fresh;
+        g.stream_priority = priority;
+    });
+}
+
 int fc_get_air_model(const fc_grid* grid, int* model)
 {
     return guarded([&]
@@ -3245,15 +3358,7 @@ int fc_apply_gravity(fc_grid* grid, double dt)
     {
         if (!grid)
             fail(FC_ERR_INVALID_ARGUMENT, "null grid");
-        Grid& g = grid->impl;
-        fc::require_uploaded(g);
-        fc::Plan& p = fc::single_plan(g);
-        fc::dispatch(g.precision, [&](auto zero)
-        {
-            using T = decltype(zero);
-            FC_LAUNCH(fc::k_gravity<T>, p.vec.count, fc::kVecThreads, 0, p.stream, p.d_desc, p.at(p.vec), g.gravity_y * dt);
-        });
-        check(cudaStreamSynchronize(p.stream), "gravity");
+        fc::apply_gravity(grid->impl, dt, true);
     });
 }
 
@@ -3264,27 +3369,23 @@ int fc_extend_air_velocity(fc_grid* grid)
     {
         if (!grid)
             fail(FC_ERR_INVALID_ARGUMENT, "null grid");
-        Grid& g = grid->impl;
-        fc::require_uploaded(g);
-        fc::Plan& p = fc::single_plan(g);
-        unsigned char* known_u = g.air_faces;
-        unsigned char* known_v = g.air_faces + g.faces_u;
-        FC_LAUNCH(fc::k_air_faces_init, p.faces.count, fc::kVecThreads, 0, p.stream, p.d_desc, p.at(p.faces), known_u,
-            known_v);
-        fc::dispatch(g.precision, [&](auto zero)
-        {
-            using T = decltype(zero);
-            for (int layer = 1; layer <= fc::kAirLayers; ++layer)
-                FC_LAUNCH(fc::k_air_faces_extend<T>, p.faces.count, fc::kVecThreads, 0, p.stream, p.d_desc, p.at(p.faces),
-                    known_u, known_v, layer);
-        });
-        check(cudaStreamSynchronize(p.stream), "air velocity extension");
+        fc::extend_air_velocity(grid->impl, true);
     });
 }
 
-// The reference's step runs the viscosity solve without an iteration cap; this bound only turns
-// a solve that cannot converge into an error instead of an endless loop.
-constexpr int kViscosityCap = 20000;
+int fc_advance_substep(fc_grid* grid, double dt, int* viscosity_iterations)
+{
+    return guarded([&]
+    {
+        if (!grid)
+            fail(FC_ERR_INVALID_ARGUMENT, "null grid");
+        if (!(dt > 0.0) || !std::isfinite(dt))
+            fail(FC_ERR_INVALID_ARGUMENT, "time step must be positive and finite");
+        const int viscous = fc::advance_substep(grid->impl, dt, false);
+        if (viscosity_iterations)
+            *viscosity_iterations = viscous;
+    });
+}
 
 int fc_step(fc_grid* grid, double dt, int max_iterations, double divergence_tolerance, fc_result* result,
     fc_timings* timings)
@@ -3326,29 +3427,39 @@ int fc_step(fc_grid* grid, double dt, int max_iterations, double divergence_tole
     };
     for (int i = 0; i < count; ++i)
     {
-        // Dirichlet air: transport sees the liquid's velocity extended into the air.
-        if (grid->impl.air_model == FC_AIR_DIRICHLET && (status = fc_extend_air_velocity(grid)) != FC_OK)
-            return status;
-        if ((status = fc_advect(grid, step)) != FC_OK)
-            return status;
-        if (timings)
-            timings->transport_ms += elapsed();
-        // Implicit viscosity after transport (FluidGridGPU.cpp:1139-1146), 1e-4 relative.
-        if (fc::has_viscosity(grid->impl))
+        if (!timings)
         {
+            // The substep's kernels are enqueued without waiting; the projection orders after
+            // them on the grid's stream.
             int viscous = 0;
-            if ((status = fc_apply_viscosity(grid, step, 1e-4, kViscosityCap, &viscous, nullptr)) != FC_OK)
+            if ((status = guarded([&] { viscous = fc::advance_substep(grid->impl, step, false); })) != FC_OK)
                 return status;
             total.viscosity_iterations += viscous;
-            if (timings)
-                timings->viscosity_ms += elapsed();
         }
-        if ((status = fc_apply_gravity(grid, step)) != FC_OK)
-            return status;
-        if (tension && (status = fc_apply_surface_tension(grid, step)) != FC_OK)
-            return status;
-        if (timings)
+        else
+        {
+            // Timed: every stage waits for its kernels, so its time is its own.
+            // Dirichlet air: transport sees the liquid's velocity extended into the air.
+            if (grid->impl.air_model == FC_AIR_DIRICHLET && (status = fc_extend_air_velocity(grid)) != FC_OK)
+                return status;
+            if ((status = fc_advect(grid, step)) != FC_OK)
+                return status;
+            timings->transport_ms += elapsed();
+            // Implicit viscosity after transport (FluidGridGPU.cpp:1139-1146), 1e-4 relative.
+            if (fc::has_viscosity(grid->impl))
+            {
+                int viscous = 0;
+                if ((status = fc_apply_viscosity(grid, step, 1e-4, fc::kViscosityCap, &viscous, nullptr)) != FC_OK)
+                    return status;
+                total.viscosity_iterations += viscous;
+                timings->viscosity_ms += elapsed();
+            }
+            if ((status = fc_apply_gravity(grid, step)) != FC_OK)
+                return status;
+            if (tension && (status = fc_apply_surface_tension(grid, step)) != FC_OK)
+                return status;
             timings->forces_ms += elapsed();
+        }
         if ((status = fc_project(grid, step, max_iterations, divergence_tolerance, &one)) != FC_OK)
             return status;
         if (timings)

@@ -1,16 +1,18 @@
 // Serving loop of libfluidcuda.so: continuous batching of independent simulations on one GPU.
 //
 // Host runtime over the public C ABI (fluidcuda.h). The reference drives one grid per scene
-// from FluidScene::sceneProcess (FluidScene.inl:328-420): step, check accepted(), repeat. Here a
-// worker thread drives many grids at once. Each tick:
-//   1. admit queued simulations in arrival order while their device bytes fit the budget and a
-//      slot is free (create, configure, upload);
-//   2. run one physical (sub)step of transport and forces on every active grid;
-//   3. project all active grids in one batched solve (one launch per kernel for the batch);
+// from FluidScene::sceneProcess (FluidScene.inl:328-420): step, check accepted(), repeat. Here
+// simulations are sorted by grid size into classes (lanes), each driven by its own worker
+// thread, so a small simulation's step latency does not wait on a large grid's projection and
+// the GPU runs the classes' kernels side by side on their own streams. Each tick of a lane:
+//   1. admit the lane's queued simulations in arrival order while their device bytes fit the
+//      server's budget and a slot is free (create, configure, upload);
+//   2. enqueue one physical (sub)step of transport and forces on every active grid of the lane;
+//   3. project the lane's active grids in one batched solve (one launch per kernel for them);
 //   4. retire finished simulations: copy their final state to host memory, free the grid.
 // Substeps follow fc_step exactly (capillary subdivision, stop on a non-converged projection),
 // and the batched solve computes bit for bit what a single-grid solve computes, so a
-// simulation's result does not depend on what it was batched with.
+// simulation's result does not depend on what it was batched with or which lane ran it.
 #include "fc_errors.h"
 
 #include <cuda_runtime.h>
@@ -24,6 +26,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -47,6 +50,7 @@ struct Sim
     std::vector<double> liquid_densities, gas_densities;
     std::vector<unsigned char> solid;
     std::vector<double> fraction, u, v, pressure;
+    std::string error_text; // fc_last_error() of the call that failed it
     std::vector<std::vector<double>> liquid_mass, gas_mass;
     size_t bytes = 0;
 
@@ -82,16 +86,16 @@ struct Server
     int device = 0;
 
     std::mutex mutex;
-    std::condition_variable wake;     // the worker: new work or stop
+    std::condition_variable wake;     // the workers: new work, freed capacity or stop
     std::condition_variable changed;  // waiters: a simulation finished
     bool stop = false;
     long long next_id = 1;
-    std::deque<Sim*> queue;
     std::map<long long, std::unique_ptr<Sim>> sims;
-    size_t in_use = 0;
+    size_t in_use = 0;    // device bytes of admitted simulations (all lanes)
+    int running = 0;      // admitted simulations not yet retired (all lanes)
 
-    // Worker-owned. Grids are batched by what one batched solve must share: precision,
-    // iteration cap and tolerance. Each group keeps its plan while its membership holds.
+    // Grids are batched by what one batched solve must share: precision, iteration cap and
+    // tolerance. Each group keeps its plan while its membership holds.
     struct Group
     {
         int precision;
@@ -100,30 +104,73 @@ struct Server
         fc_batch* batch = nullptr;
         std::vector<Sim*> members;
     };
-    std::vector<Sim*> active;
-    std::vector<Group> groups;
+    // A size class of simulations with its own worker. queue, stats and latencies are guarded
+    // by mutex; active and groups belong to the worker.
+    struct Lane
+    {
+        long long max_cells = 0; // grids of at most this many cells (the last lane: any size)
+        int priority = 0;        // CUDA stream priority of its grids and batches
+        std::deque<Sim*> queue;
+        std::vector<Sim*> active;
+        std::vector<Group> groups;
+        fc_server_stats stats{};
+        std::vector<double> latencies;
+        bool busy = false;
+        Clock::time_point busy_since;
+        std::thread worker;
+    };
+    std::vector<std::unique_ptr<Lane>> lanes;
 
-    // Statistics (guarded by mutex).
-    fc_server_stats stats{};
-    std::vector<double> latencies;
-    bool busy = false;
+    // Whole-server statistics (guarded by mutex): peaks and the wall time with work.
+    int peak_active = 0;
+    size_t peak_bytes = 0;
+    int busy_lanes = 0;
+    double busy_ms = 0.0;
     Clock::time_point busy_since;
 
-    std::thread worker;
-
-    void run();
-    bool admit();
-    void tick();
-    bool project(std::vector<Sim*>& members, std::vector<fc_result>& results);
-    void retire(Sim* s, int error);
-    void release_groups();
+    Lane& lane_for(long long cells)
+    {
+        for (auto& l : lanes)
+            if (cells <= l->max_cells)
+                return *l;
+        return *lanes.back();
+    }
+    void set_busy(Lane& lane, bool busy); // with mutex held
+    void run(Lane& lane);
+    bool admit(Lane& lane);
+    void tick(Lane& lane);
+    bool project(Lane& lane, std::vector<Sim*>& members, std::vector<fc_result>& results);
+    void retire(Lane& lane, Sim* s, int error);
 };
 
-void Server::retire(Sim* s, int error)
+void Server::set_busy(Lane& lane, bool busy)
 {
-    // Called by the worker with the mutex released. A batch plan that holds this grid goes
-    // first: batches are destroyed before their grids, and no later membership may match it.
-    for (Group& g : groups)
+    if (lane.busy == busy)
+        return;
+    const Clock::time_point now = Clock::now();
+    lane.busy = busy;
+    if (busy)
+    {
+        lane.busy_since = now;
+        if (busy_lanes++ == 0)
+            busy_since = now;
+    }
+    else
+    {
+        lane.stats.busy_ms += ms_between(lane.busy_since, now);
+        if (--busy_lanes == 0)
+            busy_ms += ms_between(busy_since, now);
+    }
+}
+
+void Server::retire(Lane& lane, Sim* s, int error)
+{
+    // Called by the lane's worker with the mutex released, right after the failing call (if
+    // any): its message is still this thread's last error. A batch plan that holds this grid
+    // goes first: batches are destroyed before their grids, and no later membership may match.
+    if (error != FC_OK)
+        s->error_text = fc_last_error();
+    for (Group& g : lane.groups)
         if (std::find(g.members.begin(), g.members.end(), s) != g.members.end())
         {
             if (g.batch)
@@ -162,30 +209,24 @@ void Server::retire(Sim* s, int error)
     s->status.error = error;
     s->status.run_ms = ms_between(s->admitted, Clock::now());
     in_use -= s->bytes;
+    --running;
     changed.notify_all();
-}
-
-void Server::release_groups()
-{
-    for (Group& g : groups)
-        if (g.batch)
-            fc_batch_destroy(g.batch);
-    groups.clear();
+    wake.notify_all(); // freed capacity may admit another lane's queued simulation
 }
 
 // One batched solve for a set of grids that share precision, cap and tolerance; the group's
 // plan is rebuilt when its membership changed. Returns false on a failed solve.
-bool Server::project(std::vector<Sim*>& members, std::vector<fc_result>& results)
+bool Server::project(Lane& lane, std::vector<Sim*>& members, std::vector<fc_result>& results)
 {
     const fc_sim_desc& d = members.front()->desc;
     Group* group = nullptr;
-    for (Group& g : groups)
+    for (Group& g : lane.groups)
         if (g.precision == d.precision && g.max_iterations == d.max_iterations && g.tolerance == d.divergence_tolerance)
             group = &g;
     if (!group)
     {
-        groups.push_back({d.precision, d.max_iterations, d.divergence_tolerance, nullptr, {}});
-        group = &groups.back();
+        lane.groups.push_back({d.precision, d.max_iterations, d.divergence_tolerance, nullptr, {}});
+        group = &lane.groups.back();
     }
     if (group->members != members)
     {
@@ -200,7 +241,7 @@ bool Server::project(std::vector<Sim*>& members, std::vector<fc_result>& results
             return false;
         group->members = members;
         std::lock_guard<std::mutex> lock(mutex);
-        ++stats.batch_rebuilds;
+        ++lane.stats.batch_rebuilds;
     }
     std::vector<double> dts;
     for (Sim* s : members)
@@ -216,42 +257,45 @@ bool Server::project(std::vector<Sim*>& members, std::vector<fc_result>& results
     return true;
 }
 
-// Moves queued simulations to the active set while they fit. Returns whether any is active.
-bool Server::admit()
+// Moves the lane's queued simulations to its active set while they fit. Returns whether any is
+// active; waits while the lane has nothing to run.
+bool Server::admit(Lane& lane)
 {
     for (;;)
     {
         Sim* s = nullptr;
         {
             std::unique_lock<std::mutex> lock(mutex);
-            if (active.empty() && queue.empty())
+            const auto fits = [&]
             {
-                if (busy)
-                {
-                    stats.busy_ms += ms_between(busy_since, Clock::now());
-                    busy = false;
-                }
-                wake.wait(lock, [&] { return stop || !queue.empty(); });
+                return !lane.queue.empty() && running < max_active && in_use + lane.queue.front()->bytes <= budget;
+            };
+            if (lane.active.empty())
+            {
+                set_busy(lane, false);
+                wake.wait(lock, [&] { return stop || fits(); });
             }
             if (stop)
                 return false;
-            if (queue.empty() || int(active.size()) >= max_active || in_use + queue.front()->bytes > budget)
-                return !active.empty();
-            s = queue.front();
-            queue.pop_front();
+            if (!fits())
+                return !lane.active.empty();
+            s = lane.queue.front();
+            lane.queue.pop_front();
             in_use += s->bytes;
-            stats.peak_bytes = std::max(stats.peak_bytes, in_use);
-            if (!busy)
-            {
-                busy = true;
-                busy_since = Clock::now();
-            }
+            ++running;
+            peak_bytes = std::max(peak_bytes, in_use);
+            peak_active = std::max(peak_active, running);
+            lane.stats.peak_bytes = std::max(lane.stats.peak_bytes, in_use);
+            set_busy(lane, true);
         }
         s->admitted = Clock::now();
         const fc_sim_desc& d = s->desc;
         const int rc = guarded([&]
         {
             status_check(fc_create(d.width, d.height, d.cell_size, d.precision, &s->grid), "create");
+            // Smaller classes run at higher priority: their short kernels take SMs before the
+            // large grids' next ones when both wait.
+            status_check(fc_set_stream_priority(s->grid, lane.priority), "stream priority");
             status_check(fc_configure_materials(s->grid, int(s->liquid_densities.size()), s->liquid_densities.data(),
                              nullptr, int(s->gas_densities.size()), s->gas_densities.data(), nullptr),
                 "configure");
@@ -291,22 +335,23 @@ bool Server::admit()
         }
         if (rc != FC_OK)
         {
-            retire(s, rc);
+            retire(lane, s, rc);
             continue;
         }
         if (d.steps <= 0)
         {
-            retire(s, FC_OK);
+            retire(lane, s, FC_OK);
             continue;
         }
-        active.push_back(s);
+        lane.active.push_back(s);
         std::lock_guard<std::mutex> lock(mutex);
-        stats.peak_active = std::max(stats.peak_active, int(active.size()));
+        lane.stats.peak_active = std::max(lane.stats.peak_active, int(lane.active.size()));
     }
 }
 
-void Server::tick()
+void Server::tick(Lane& lane)
 {
+    std::vector<Sim*>& active = lane.active;
     const Clock::time_point start = Clock::now();
     // Transport and forces of the next physical step of every active grid (fc_step order).
     for (size_t i = 0; i < active.size();)
@@ -314,16 +359,12 @@ void Server::tick()
         Sim* s = active[i];
         if (s->substep == 0)
             s->step_started = start;
-        const int rc = guarded([&]
-        {
-            status_check(fc_advect(s->grid, s->sub_dt), "advect");
-            status_check(fc_apply_gravity(s->grid, s->sub_dt), "gravity");
-            if (s->desc.surface_tension > 0.0)
-                status_check(fc_apply_surface_tension(s->grid, s->sub_dt), "surface tension");
-        });
+        // Enqueued on the grid's stream without waiting: the grids' substeps run side by side
+        // and the batched projection waits for each member's stream.
+        const int rc = guarded([&] { status_check(fc_advance_substep(s->grid, s->sub_dt, nullptr), "substep"); });
         if (rc != FC_OK)
         {
-            retire(s, rc);
+            retire(lane, s, rc);
             active.erase(active.begin() + i);
             continue;
         }
@@ -349,21 +390,22 @@ void Server::tick()
             it->push_back(s);
     }
     // Plans of groups that no longer have members are released.
-    for (size_t g = 0; g < groups.size();)
+    for (size_t g = 0; g < lane.groups.size();)
     {
+        const Group& group = lane.groups[g];
         const bool used = std::any_of(parts.begin(), parts.end(), [&](const std::vector<Sim*>& p)
         {
             const fc_sim_desc& a = p.front()->desc;
-            return a.precision == groups[g].precision && a.max_iterations == groups[g].max_iterations &&
-                   a.divergence_tolerance == groups[g].tolerance;
+            return a.precision == group.precision && a.max_iterations == group.max_iterations &&
+                   a.divergence_tolerance == group.tolerance;
         });
         if (used)
             ++g;
         else
         {
-            if (groups[g].batch)
-                fc_batch_destroy(groups[g].batch);
-            groups.erase(groups.begin() + g);
+            if (group.batch)
+                fc_batch_destroy(group.batch);
+            lane.groups.erase(lane.groups.begin() + g);
         }
     }
     std::vector<std::pair<Sim*, fc_result>> done;
@@ -371,7 +413,7 @@ void Server::tick()
     for (auto& part : parts)
     {
         std::vector<fc_result> results;
-        if (project(part, results))
+        if (project(lane, part, results))
             for (size_t i = 0; i < part.size(); ++i)
                 done.push_back({part[i], results[i]});
         else
@@ -383,7 +425,8 @@ void Server::tick()
     std::vector<Sim*> finished;
     {
         std::lock_guard<std::mutex> lock(mutex);
-        ++stats.ticks;
+        fc_server_stats& st = lane.stats;
+        ++st.ticks;
         for (auto& [s, r] : done)
         {
             s->status.iterations += r.iterations;
@@ -391,15 +434,15 @@ void Server::tick()
             s->status.max_divergence = r.max_divergence;
             if (!r.converged)
                 s->status.converged = 0;
-            ++stats.physical_steps;
+            ++st.physical_steps;
             // A time step ends after its last substep, or early at a non-converged projection.
             if (++s->substep == s->substeps || !r.converged)
             {
                 s->substep = 0;
                 ++s->status.steps_done;
-                ++stats.steps;
-                stats.cell_steps += double(s->desc.width) * s->desc.height;
-                latencies.push_back(ms_between(s->step_started, end));
+                ++st.steps;
+                st.cell_steps += double(s->desc.width) * s->desc.height;
+                lane.latencies.push_back(ms_between(s->step_started, end));
                 if (s->status.steps_done == s->desc.steps)
                     finished.push_back(s);
             }
@@ -408,25 +451,44 @@ void Server::tick()
     for (Sim* s : failed)
     {
         active.erase(std::find(active.begin(), active.end(), s));
-        retire(s, failure);
+        retire(lane, s, failure);
     }
     for (Sim* s : finished)
     {
         active.erase(std::find(active.begin(), active.end(), s));
-        retire(s, FC_OK);
+        retire(lane, s, FC_OK);
     }
 }
 
-void Server::run()
+void Server::run(Lane& lane)
 {
     cudaSetDevice(device);
-    while (admit())
-        tick();
-    release_groups();
-    for (Sim* s : active)
+    while (admit(lane))
+        tick(lane);
+    for (Group& g : lane.groups)
+        if (g.batch)
+            fc_batch_destroy(g.batch);
+    lane.groups.clear();
+    for (Sim* s : lane.active)
         if (s->grid)
             fc_destroy(s->grid);
-    active.clear();
+    lane.active.clear();
+}
+
+// Nearest-rank percentiles and the maximum of step latencies into a stats record.
+void fill_latencies(std::vector<double> sorted, fc_server_stats& stats)
+{
+    std::sort(sorted.begin(), sorted.end());
+    auto percentile = [&](double q)
+    {
+        if (sorted.empty())
+            return 0.0;
+        const size_t rank = size_t(std::ceil(q * sorted.size()));
+        return sorted[std::min(sorted.size(), std::max<size_t>(rank, 1)) - 1];
+    };
+    stats.step_p50_ms = percentile(0.50);
+    stats.step_p99_ms = percentile(0.99);
+    stats.step_max_ms = sorted.empty() ? 0.0 : sorted.back();
 }
 
 } // namespace fc
@@ -441,12 +503,18 @@ using fc::guarded;
 
 extern "C" {
 
-int fc_server_create(size_t device_budget_bytes, int max_active, fc_server** out)
+int fc_server_create_classes(size_t device_budget_bytes, int max_active, int classes, const long long* max_cells,
+    fc_server** out)
 {
     return guarded([&]
     {
         if (!out || device_budget_bytes == 0 || max_active <= 0)
             fail(FC_ERR_INVALID_ARGUMENT, "server needs a positive budget and slot count");
+        if (classes < 1 || classes > 16 || (classes > 1 && !max_cells))
+            fail(FC_ERR_INVALID_ARGUMENT, "between 1 and 16 size classes, with classes - 1 bounds");
+        for (int k = 0; k + 1 < classes; ++k)
+            if (max_cells[k] <= 0 || (k > 0 && max_cells[k] <= max_cells[k - 1]))
+                fail(FC_ERR_INVALID_ARGUMENT, "size class bounds must be positive and increasing");
         *out = nullptr;
         auto server = std::make_unique<fc_server>();
         fc::Server& s = server->impl;
@@ -457,9 +525,31 @@ int fc_server_create(size_t device_budget_bytes, int max_active, fc_server** out
             cudaGetLastError();
             fail(FC_ERR_CUDA, "no CUDA device");
         }
-        s.worker = std::thread([&s] { s.run(); });
+        int least = 0, greatest = 0;
+        if (cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess)
+        {
+            cudaGetLastError();
+            least = greatest = 0;
+        }
+        for (int k = 0; k < classes; ++k)
+        {
+            s.lanes.push_back(std::make_unique<fc::Server::Lane>());
+            s.lanes.back()->max_cells = k + 1 < classes ? max_cells[k] : std::numeric_limits<long long>::max();
+            s.lanes.back()->priority = std::max(greatest, least - (classes - 1 - k));
+        }
+        for (auto& lane : s.lanes)
+        {
+            fc::Server::Lane* l = lane.get();
+            l->worker = std::thread([&s, l] { s.run(*l); });
+        }
         *out = server.release();
     });
+}
+
+int fc_server_create(size_t device_budget_bytes, int max_active, fc_server** out)
+{
+    const long long bounds[2] = {256LL * 256, 1024LL * 1024};
+    return fc_server_create_classes(device_budget_bytes, max_active, 3, bounds, out);
 }
 
 int fc_server_destroy(fc_server* server)
@@ -473,8 +563,9 @@ int fc_server_destroy(fc_server* server)
             server->impl.stop = true;
         }
         server->impl.wake.notify_all();
-        if (server->impl.worker.joinable())
-            server->impl.worker.join();
+        for (auto& lane : server->impl.lanes)
+            if (lane->worker.joinable())
+                lane->worker.join();
         delete server;
     });
 }
@@ -542,7 +633,7 @@ int fc_server_submit(fc_server* server, const fc_sim_desc* desc, long long* id)
                 fail(FC_ERR_LIFECYCLE, "server is stopping");
             sim->id = s.next_id++;
             *id = sim->id;
-            s.queue.push_back(sim.get());
+            s.lane_for((long long)cells).queue.push_back(sim.get());
             s.sims.emplace(sim->id, std::move(sim));
         }
         s.wake.notify_all();
@@ -616,6 +707,23 @@ int fc_server_download(fc_server* server, long long id, double* liquid_fraction,
     });
 }
 
+int fc_server_error(fc_server* server, long long id, char* text, size_t capacity)
+{
+    return guarded([&]
+    {
+        if (!server || (capacity && !text))
+            fail(FC_ERR_INVALID_ARGUMENT, "null argument");
+        std::lock_guard<std::mutex> lock(server->impl.mutex);
+        const fc::Sim* sim = find_sim(server->impl, id);
+        if (capacity)
+        {
+            const size_t n = std::min(capacity - 1, sim->error_text.size());
+            std::copy(sim->error_text.begin(), sim->error_text.begin() + n, text);
+            text[n] = '\0';
+        }
+    });
+}
+
 int fc_server_release(fc_server* server, long long id)
 {
     return guarded([&]
@@ -638,22 +746,52 @@ int fc_server_get_stats(fc_server* server, fc_server_stats* stats)
             fail(FC_ERR_INVALID_ARGUMENT, "null argument");
         fc::Server& s = server->impl;
         std::lock_guard<std::mutex> lock(s.mutex);
-        *stats = s.stats;
-        if (s.busy)
-            stats->busy_ms += fc::ms_between(s.busy_since, fc::Clock::now());
-        std::vector<double> sorted = s.latencies;
-        std::sort(sorted.begin(), sorted.end());
-        auto percentile = [&](double q)
+        fc_server_stats total{};
+        std::vector<double> latencies;
+        for (auto& lane : s.lanes)
         {
-            if (sorted.empty())
-                return 0.0;
-            // Nearest rank.
-            const size_t rank = size_t(std::ceil(q * sorted.size()));
-            return sorted[std::min(sorted.size(), std::max<size_t>(rank, 1)) - 1];
-        };
-        stats->step_p50_ms = percentile(0.50);
-        stats->step_p99_ms = percentile(0.99);
-        stats->step_max_ms = sorted.empty() ? 0.0 : sorted.back();
+            total.ticks += lane->stats.ticks;
+            total.steps += lane->stats.steps;
+            total.physical_steps += lane->stats.physical_steps;
+            total.cell_steps += lane->stats.cell_steps;
+            total.batch_rebuilds += lane->stats.batch_rebuilds;
+            latencies.insert(latencies.end(), lane->latencies.begin(), lane->latencies.end());
+        }
+        total.busy_ms = s.busy_ms + (s.busy_lanes > 0 ? fc::ms_between(s.busy_since, fc::Clock::now()) : 0.0);
+        total.peak_active = s.peak_active;
+        total.peak_bytes = s.peak_bytes;
+        fc::fill_latencies(std::move(latencies), total);
+        *stats = total;
+    });
+}
+
+int fc_server_class_count(fc_server* server, int* classes)
+{
+    return guarded([&]
+    {
+        if (!server || !classes)
+            fail(FC_ERR_INVALID_ARGUMENT, "null argument");
+        *classes = int(server->impl.lanes.size());
+    });
+}
+
+int fc_server_get_class_stats(fc_server* server, int size_class, fc_server_stats* stats, long long* max_cells)
+{
+    return guarded([&]
+    {
+        if (!server || !stats)
+            fail(FC_ERR_INVALID_ARGUMENT, "null argument");
+        fc::Server& s = server->impl;
+        if (size_class < 0 || size_class >= int(s.lanes.size()))
+            fail(FC_ERR_INVALID_ARGUMENT, "no size class %d", size_class);
+        std::lock_guard<std::mutex> lock(s.mutex);
+        const fc::Server::Lane& lane = *s.lanes[size_class];
+        *stats = lane.stats;
+        if (lane.busy)
+            stats->busy_ms += fc::ms_between(lane.busy_since, fc::Clock::now());
+        fc::fill_latencies(lane.latencies, *stats);
+        if (max_cells)
+            *max_cells = lane.max_cells;
     });
 }
 
@@ -664,9 +802,11 @@ int fc_server_step_latencies(fc_server* server, double* ms, size_t capacity, siz
         if (!server || !count || (capacity && !ms))
             fail(FC_ERR_INVALID_ARGUMENT, "null argument");
         std::lock_guard<std::mutex> lock(server->impl.mutex);
-        const auto& l = server->impl.latencies;
-        *count = l.size();
-        std::copy(l.begin(), l.begin() + std::min(capacity, l.size()), ms);
+        std::vector<double> all;
+        for (auto& lane : server->impl.lanes)
+            all.insert(all.end(), lane->latencies.begin(), lane->latencies.end());
+        *count = all.size();
+        std::copy(all.begin(), all.begin() + std::min(capacity, all.size()), ms);
     });
 }
 

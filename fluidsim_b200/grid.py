@@ -225,9 +225,11 @@ class FluidGrid:
     # -- stepping ---------------------------------------------------------------------------
     def step(self, dt: float, max_iterations: int = 200, divergence_tolerance: float = 1e-6,
              timings: Optional[dict] = None) -> ProjectionResult:
+        # Without a timings request the step enqueues each substep's stages without waiting
+        # between them; with one, every stage waits so that its time is its own.
         r, t = N.FcResult(), N.FcTimings()
         N.check(N.lib().fc_step(self.handle, float(dt), int(max_iterations), float(divergence_tolerance),
-                                C.byref(r), C.byref(t)))
+                                C.byref(r), C.byref(t) if timings is not None else None))
         if timings is not None:
             timings.update({k: getattr(t, k) for k, _ in N.FcTimings._fields_})
         return ProjectionResult.from_c(r)
@@ -253,6 +255,17 @@ class FluidGrid:
     def extendAirVelocity(self):
         """The liquid's face velocities extended into Dirichlet air (fc_extend_air_velocity)."""
         N.check(N.lib().fc_extend_air_velocity(self.handle))
+
+    def setStreamPriority(self, priority: int):
+        """CUDA stream priority of the grid's work (fc_set_stream_priority; lower runs first)."""
+        N.check(N.lib().fc_set_stream_priority(self.handle, int(priority)))
+
+    def advanceSubstep(self, dt: float) -> int:
+        """fc_step's substep before the projection, enqueued without waiting (fc_advance_substep);
+        returns the viscosity iterations."""
+        it = C.c_int()
+        N.check(N.lib().fc_advance_substep(self.handle, float(dt), C.byref(it)))
+        return it.value
 
     def getAirModel(self) -> str:
         m = C.c_int()

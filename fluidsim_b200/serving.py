@@ -1,9 +1,10 @@
 """Serving: many simulations on one GPU with continuous batching (fc_server_* in fluidcuda.h).
 
-The request loop lives in the native library (fluidsim_b200/csrc/fc_server.cpp): a worker thread
-admits simulations by device-memory budget, keeps their state on the device across steps and
-projects all running grids in one batched solve per tick. This module is its Python face, plus
-the Poisson arrival driver used by the serving measurement.
+The request loop lives in the native library (fluidsim_b200/csrc/fc_server.cpp): simulations are
+sorted by grid size into classes, and each class's worker thread admits simulations by the shared
+device-memory budget, keeps their state on the device across steps and projects its running
+grids in one batched solve per tick. This module is its Python face, plus the Poisson arrival
+driver used by the serving measurement.
 """
 from __future__ import annotations
 
@@ -51,11 +52,20 @@ def grid_device_bytes(width: int, height: int, precision: str = "fp32", componen
 
 
 class Server:
-    """Continuous-batching request loop over one GPU."""
+    """Continuous-batching request loop over one GPU.
 
-    def __init__(self, device_budget_bytes: int, max_active: int = 256):
+    size_classes: increasing cell-count bounds of the size classes (a class per bound plus one
+    for larger grids), each stepped by its own worker; None for the library's default (up to
+    256 x 256, up to 1024 x 1024, larger); [] for one class that steps everything in lockstep."""
+
+    def __init__(self, device_budget_bytes: int, max_active: int = 256, size_classes: Optional[Sequence[int]] = None):
         handle = C.c_void_p()
-        N.check(N.lib().fc_server_create(int(device_budget_bytes), int(max_active), C.byref(handle)))
+        if size_classes is None:
+            N.check(N.lib().fc_server_create(int(device_budget_bytes), int(max_active), C.byref(handle)))
+        else:
+            bounds = (C.c_longlong * max(1, len(size_classes)))(*[int(b) for b in size_classes])
+            N.check(N.lib().fc_server_create_classes(int(device_budget_bytes), int(max_active), len(size_classes) + 1,
+                                                     bounds, C.byref(handle)))
         self._h = handle
         self._shapes: Dict[int, tuple] = {}
 
@@ -131,6 +141,12 @@ class Server:
                                            C.cast(gt, C.c_void_p) if ng else None))
         return FluidGridState(f, u, v, p, lm, gm)
 
+    def error(self, sim: int) -> str:
+        """Why a simulation failed ('' unless it did)."""
+        buf = C.create_string_buffer(1024)
+        N.check(N.lib().fc_server_error(self._h, sim, buf, len(buf)))
+        return buf.value.decode(errors="replace")
+
     def release(self, sim: int):
         N.check(N.lib().fc_server_release(self._h, sim))
         self._shapes.pop(sim, None)
@@ -139,6 +155,19 @@ class Server:
         s = N.FcServerStats()
         N.check(N.lib().fc_server_get_stats(self._h, C.byref(s)))
         return {name: getattr(s, name) for name, _ in N.FcServerStats._fields_}
+
+    def class_stats(self) -> List[dict]:
+        """Statistics of each size class, with its cell bound under 'max_cells'."""
+        count = C.c_int()
+        N.check(N.lib().fc_server_class_count(self._h, C.byref(count)))
+        out = []
+        for k in range(count.value):
+            s, bound = N.FcServerStats(), C.c_longlong()
+            N.check(N.lib().fc_server_get_class_stats(self._h, k, C.byref(s), C.byref(bound)))
+            d = {name: getattr(s, name) for name, _ in N.FcServerStats._fields_}
+            d["max_cells"] = bound.value
+            out.append(d)
+        return out
 
     def step_latencies(self) -> np.ndarray:
         count = C.c_size_t()

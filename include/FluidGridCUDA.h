@@ -174,9 +174,11 @@ public:
     ProjectionResult step(double dt, int max_iterations = 200, double divergence_tolerance = 1e-6,
         StepTimings* timings = nullptr) override
     {
+        // Stage timings make every stage wait for its kernels; without them the substeps are
+        // enqueued and only the projection waits.
         fc_result r{};
         fc_timings t{};
-        check(fc_step(live(), dt, max_iterations, divergence_tolerance, &r, &t));
+        check(fc_step(live(), dt, max_iterations, divergence_tolerance, &r, timings ? &t : nullptr));
         if (timings)
         {
             *timings = {};

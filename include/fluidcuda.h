@@ -209,6 +209,10 @@ int fc_get_transport(const fc_grid* grid, int* transport);
  * cell, and max_divergence runs over the liquid only. A grid without air cells then has a
  * singular system: its coarsest factor breaks down. Set it before a batch holds the grid. */
 int fc_set_air_model(fc_grid* grid, int model);
+/* Priority of the grid's CUDA stream (cudaDeviceGetStreamPriorityRange: lower numbers run
+ * first when kernels of several streams wait for the same SMs; 0 is the default). Batches made
+ * afterwards run at the highest priority among their members. Waits for the grid's work. */
+int fc_set_stream_priority(fc_grid* grid, int priority);
 int fc_get_air_model(const fc_grid* grid, int* model);
 /* Under Dirichlet air nothing constrains the velocity between air cells, so fc_step extends the
  * liquid's face velocities into the air before each substep's transport: faces of liquid cells,
@@ -216,6 +220,14 @@ int fc_get_air_model(const fc_grid* grid, int* model);
  * mean; the faces left unknown are set to zero. No counterpart in the reference (its air is a
  * gas the projection constrains). Exposed for checks; fc_step calls it itself. */
 int fc_extend_air_velocity(fc_grid* grid);
+/* One physical substep of fc_step before its projection (FluidGridCPU.cpp:300-360 order): the
+ * air extension under Dirichlet air, transport, implicit viscosity when a component is viscous,
+ * gravity and surface tension. The kernels are enqueued on the grid's stream and the call
+ * returns without waiting for them (the viscosity solve and PLIC transport read values back and
+ * wait); the next projection of the grid (fc_project, fc_batch_project) runs after them, and
+ * errors of the enqueued kernels surface at the next call that waits. viscosity_iterations may
+ * be NULL. fc_step runs its substeps this way unless it is asked for stage timings. */
+int fc_advance_substep(fc_grid* grid, double dt, int* viscosity_iterations);
 /* FluidGridCPU::sampleVelocity (UniformCPU/FluidGridCPU.h:132, FluidGridCPU.cpp:465-471): the
  * staggered bilinear velocity at `count` world positions. positions and velocities are host
  * arrays of interleaved (x, y) pairs. */
@@ -422,9 +434,18 @@ typedef struct fc_server_stats
     long long batch_rebuilds;   /* batched solve plans built (one per change of membership) */
 } fc_server_stats;
 
-/* device_budget_bytes: device memory the simulations may hold together; max_active: slots. */
+/* device_budget_bytes: device memory the simulations may hold together; max_active: slots
+ * (both shared by all size classes). Simulations are sorted by cells into size classes, each
+ * stepped by its own worker thread in its own batched solves, so a small grid's step latency
+ * does not wait on a large grid's. fc_server_create uses three classes: up to 256 x 256 cells,
+ * up to 1024 x 1024, and larger. fc_server_create_classes takes `classes` classes with
+ * classes - 1 increasing bounds: class k holds grids of more than max_cells[k - 1] and at most
+ * max_cells[k] cells; the last class holds the rest. One class steps every simulation in
+ * lockstep. Within a class, simulations are admitted in arrival order. */
 int fc_server_create(size_t device_budget_bytes, int max_active, fc_server** out);
-/* Stops the worker; simulations still queued or running are dropped. */
+int fc_server_create_classes(size_t device_budget_bytes, int max_active, int classes, const long long* max_cells,
+    fc_server** out);
+/* Stops the workers; simulations still queued or running are dropped. */
 int fc_server_destroy(fc_server* server);
 /* Copies the description and initial state; never blocks on the GPU. A simulation that could
  * never fit the budget is rejected with FC_ERR_INVALID_ARGUMENT. */
@@ -435,10 +456,18 @@ int fc_server_wait(fc_server* server, long long id, double timeout_seconds, fc_s
 /* Final state of a finished simulation (as fc_download; NULL outputs are skipped). */
 int fc_server_download(fc_server* server, long long id, double* liquid_fraction, double* u, double* v,
     double* pressure, double* const* liquid_mass, double* const* gas_mass);
+/* The message of the call that failed a simulation (empty while it has not failed), truncated
+ * to capacity - 1 characters and terminated. */
+int fc_server_error(fc_server* server, long long id, char* text, size_t capacity);
 /* Forgets a finished simulation and its host copy of the final state. */
 int fc_server_release(fc_server* server, long long id);
+/* Statistics over all size classes (ticks: the sum of the classes' ticks). */
 int fc_server_get_stats(fc_server* server, fc_server_stats* stats);
-/* Latency of every completed time step in completion order; count receives the total. */
+int fc_server_class_count(fc_server* server, int* classes);
+/* Statistics of one size class; max_cells (may be NULL) receives its upper bound in cells. */
+int fc_server_get_class_stats(fc_server* server, int size_class, fc_server_stats* stats, long long* max_cells);
+/* Latency of every completed time step, class by class in completion order; count receives
+ * the total. */
 int fc_server_step_latencies(fc_server* server, double* ms, size_t capacity, size_t* count);
 
 #ifdef __cplusplus

@@ -58,6 +58,21 @@ def test_serving_requests_are_seeded_dam_breaks():
     assert all(s.liquid_density == 1000.0 and s.gas_density == 1.0 for s in a)
 
 
+def test_size_class_bounds_are_validated_before_any_device_call():
+    import ctypes as C
+
+    from fluidsim_b200 import FluidInvalidArgument
+    from fluidsim_b200 import _native as N
+
+    handle = C.c_void_p()
+    for classes, bounds in ((0, []), (17, [1] * 16), (3, [100, 100]), (3, [200, 100]), (2, [0]), (3, [-5, 10])):
+        arr = (C.c_longlong * max(1, len(bounds)))(*bounds)
+        with pytest.raises(FluidInvalidArgument):
+            N.check(N.lib().fc_server_create_classes(1 << 30, 4, classes, arr, C.byref(handle)))
+    with pytest.raises(FluidInvalidArgument):
+        N.check(N.lib().fc_server_create_classes(1 << 30, 4, 2, None, C.byref(handle)))
+
+
 # ----------------------------------------------------------------------------------------------
 # GPU: the serving loop through the C ABI
 # ----------------------------------------------------------------------------------------------
@@ -110,6 +125,44 @@ def test_gpu_each_result_is_the_same_alone_and_in_the_mix(precision):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("size_classes", [[48 * 48, 100 * 100], []], ids=["three_classes", "lockstep"])
+def test_gpu_size_classes_step_each_simulation_as_alone(size_classes):
+    """Grids of three size classes (two bounds) run by three workers side by side, and the same
+    mix in one lockstep class: every simulation ends exactly as it ends alone, each class counts
+    its own steps, and the classes' statistics add up to the server's."""
+    from fluidsim_b200 import scenes
+    from fluidsim_b200.serving import Server, poisson_arrivals, serve
+
+    reqs = [scenes.dam_break(n, n, seed=n, obstacles=2, velocity=0.5, cell_size=1.0 / 128.0, surface_tension=0.07)
+            for n in (24, 40, 56, 64, 90, 100, 120, 150)]
+    steps = 4
+    server = Server(1 << 34, max_active=64, size_classes=size_classes)
+    out = serve(server, reqs, poisson_arrivals(400.0, len(reqs), seed=3), steps)
+    assert all(st.state == "done" for st in out["statuses"]), [(s.name, st) for s, st in zip(reqs, out["statuses"])]
+    stats, per_class = server.stats(), server.class_stats()
+    assert len(per_class) == len(size_classes) + 1
+    bounds = list(size_classes) + [None]
+    for k, c in enumerate(per_class):
+        expect = [s for s in reqs if (k == 0 or s.cells > bounds[k - 1]) and (bounds[k] is None or s.cells <= bounds[k])]
+        assert c["steps"] == steps * len(expect)
+        assert c["cell_steps"] == steps * sum(s.cells for s in expect)
+        if bounds[k] is not None:
+            assert c["max_cells"] == bounds[k]
+    assert stats["steps"] == sum(c["steps"] for c in per_class) == steps * len(reqs)
+    assert stats["ticks"] == sum(c["ticks"] for c in per_class)
+    assert len(server.step_latencies()) == stats["steps"]
+    for scene, sim, st in zip(reqs, out["ids"], out["statuses"]):
+        assert st.state == "done" and st.steps_done == steps
+        mixed = server.download(sim)
+        alone, iterations, converged = _alone(scene, steps, "fp32")
+        assert st.iterations == iterations and st.converged == converged
+        for name in ("liquid_fraction", "u", "v", "pressure"):
+            assert np.array_equal(getattr(mixed, name), getattr(alone, name)), (scene.name, name)
+        server.release(sim)
+    server.close()
+
+
+@pytest.mark.gpu
 def test_gpu_server_rejects_what_can_never_fit():
     from fluidsim_b200 import FluidInvalidArgument, FluidLifecycleError, scenes
     from fluidsim_b200.serving import Server, grid_device_bytes
@@ -124,7 +177,16 @@ def test_gpu_server_rejects_what_can_never_fit():
     assert st.state == "done" and st.steps_done == 2
     with pytest.raises(FluidInvalidArgument):
         server.status(sim + 100)
+    assert server.error(sim) == ""
     server.release(sim)
+    # A time step that would need more capillary substeps than an int holds fails the
+    # simulation at admission (FluidGridCPU.cpp:309-320 throws there); the server keeps why.
+    import dataclasses
+
+    doomed = server.submit(dataclasses.replace(small, dt=1e12, surface_tension=0.07), 1)
+    st = server.wait(doomed, 120.0)
+    assert st.state == "failed" and "substeps" in server.error(doomed)
+    server.release(doomed)
     with pytest.raises(FluidInvalidArgument):
         server.release(sim)
     server.close()

@@ -404,16 +404,19 @@ template <> struct VecPair<double>
 };
 
 // d = (z - mean z) + beta d_old; q = A d; d.q through the grid's reduction. Warp w handles rows
-// 8w .. 8w + 7 of the tile's 64 columns (lane = column pair) in two passes of four rows: all
-// loads of a pass (six rows of z and d, four rows of weights) are issued first, then the
+// 8w .. 8w + 7 of the tile's 64 columns (lane = column pair) in four passes of two rows: all
+// loads of a pass (four rows of z and d, two rows of weights) are issued first, then the
 // directions and the operator are formed in registers; horizontal neighbours across pairs are
-// warp shuffles, and lanes 0 and 31 fetch the columns just outside the warp.
+// warp shuffles, and lanes 0 and 31 fetch the columns just outside the warp. At 64 registers
+// four CTAs fit an SM in FP32, which hides more load latency than passes of four rows at 80
+// registers and three CTAs (31.5 -> 30.2 us at 2048 x 2048).
 // Operator: FluidGridCPU.cpp:1507-1598.
 template <typename T>
-__global__ void __launch_bounds__(kVecThreads) k_direction_operator(const GridDesc* grids, const Tile* tiles, int parity)
+__global__ void __launch_bounds__(kVecThreads, sizeof(T) == 4 ? 4 : 1)
+    k_direction_operator(const GridDesc* grids, const Tile* tiles, int parity)
 {
     using P = typename VecPair<T>::type;
-    constexpr int R = 4;
+    constexpr int R = 2;
     allow_dependents();
     const Tile t = tiles[blockIdx.x];
     const GridDesc& g = grids[t.grid];
@@ -441,7 +444,7 @@ __global__ void __launch_bounds__(kVecThreads) k_direction_operator(const GridDe
         up_w = *reinterpret_cast<const P*>(down + padded_index(S, gx, t.y0 + 8 * warp - 1));
     double dot = 0.0;
 #pragma unroll 1
-    for (int pass = 0; pass < 2; ++pass)
+    for (int pass = 0; pass < 8 / R; ++pass)
     {
         const int y0 = t.y0 + 8 * warp + R * pass;
         P zz[R + 2], dd0[R + 2], w[R], dn[R];

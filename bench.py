@@ -395,7 +395,11 @@ def run_cuda(args, world, rank, local_rank):
     if not args.no_batched:
         # Every rank projects its share of the batch (placement.py); rank 0 reports.
         batched = batched_measure(args, torch, world, rank)
+        mixed = batched_measure(args, torch, world, rank, precision="mixed")
         if rank == 0:
+            batched["mixed"] = {k: mixed[k] for k in ("value", "ms_per_batch", "speedup_vs_plain", "all_converged",
+                                                      "max_iterations")}
+            batched["mixed"]["speedup_vs_fp32"] = batched["ms_per_batch"] / mixed["ms_per_batch"]
             line["batched"] = batched
     if rank == 0 and not args.no_serve:
         line["serve"] = serve_measure(args)
@@ -640,7 +644,7 @@ def viscous_measure(args, torch, flush, size=4096, steps=3, warmup=1):
     return out
 
 
-def batched_measure(args, torch, world=1, rank=0, count=256):
+def batched_measure(args, torch, world=1, rank=0, count=256, precision="fp32"):
     """Uneven grids (sides log-uniform 64..1024, aspect <= 2:1, fill 0.3-0.9, 0-8 obstacles)
     projected together, against the same grids projected one at a time. With several ranks the
     grids are placed whole on the ranks (no exchange between them) and the slowest rank's time
@@ -656,9 +660,9 @@ def batched_measure(args, torch, world=1, rank=0, count=256):
     batch_scenes = [all_scenes[i] for i in mine(assignment, rank)]
     grids, pristine = [], []
     for s in batch_scenes:
-        p = FluidGrid(s.width, s.height, s.cell_size, "fp32")
+        p = FluidGrid(s.width, s.height, s.cell_size, precision)
         scenes.upload_scene(p, s)
-        g = FluidGrid(s.width, s.height, s.cell_size, "fp32")
+        g = FluidGrid(s.width, s.height, s.cell_size, precision)
         g.configureMaterials([s.liquid_density], [s.gas_density])
         g.setObstacles(s.solid)
         pristine.append(p)
@@ -705,7 +709,8 @@ def batched_measure(args, torch, world=1, rank=0, count=256):
     batched_ms = max_over_ranks(batched_ms, dev)
     plain_ms = max_over_ranks(plain_ms, dev)
     ok = max_over_ranks(0.0 if ok else 1.0, dev) == 0.0
-    return {"value": total_cells / (batched_ms / 1e3), "unit": UNIT, "grids": count, "cells": total_cells,
+    return {"value": total_cells / (batched_ms / 1e3), "unit": UNIT, "precision": precision, "grids": count,
+            "cells": total_cells,
             "ranks": world, "ms_per_batch": batched_ms,
             "plain_one_at_a_time_cells_per_s": total_cells / (plain_ms / 1e3),
             "speedup_vs_plain": plain_ms / batched_ms, "all_converged": ok, "tail_cells": tail_cells,

@@ -57,7 +57,8 @@ __device__ __forceinline__ bool recurrence_rule_met(const SolveState& s, double 
 // one: r = b - A p in FP64 from the FP64 pressure, then a restart of the directions (iterative
 // refinement with inner FP32 PCG solves). A refresh that meets the stop rule ends the solve
 // like any verification. Measured on the 2048 x 2048 dam break under the reference's rule:
-// 85 iterations without refreshes, 61 with a ratio of 1e-4 (63 at 1e-5, 66 at 1e-6); keeping
+// 85 iterations without refreshes, 61 with a ratio of 1e-4 (63 at 1e-3 and 1e-5, 62 at 3e-3
+// and 3e-4, 66 at 1e-6); keeping
 // the directions across the refresh instead (residual replacement) gave 61 at 1e-4 and 111 at
 // 1e-5, and 96 instead of 84 with 16 obstacles at 1024 x 1024. FP64 keeps the reference's
 // schedule.

@@ -210,8 +210,10 @@ int fc_get_transport(const fc_grid* grid, int* transport);
  * singular system: its coarsest factor breaks down. Set it before a batch holds the grid. */
 int fc_set_air_model(fc_grid* grid, int model);
 /* Priority of the grid's CUDA stream (cudaDeviceGetStreamPriorityRange: lower numbers run
- * first when kernels of several streams wait for the same SMs; 0 is the default). Batches made
- * afterwards run at the highest priority among their members. Waits for the grid's work. */
+ * first when kernels of several streams wait for the same SMs; 0 is the default). Waits for the
+ * grid's work, then gives the grid a new stream of that priority (fc_get_stream returns it; the
+ * old handle is destroyed). Batches made afterwards run at the highest priority among their
+ * members. */
 int fc_set_stream_priority(fc_grid* grid, int priority);
 int fc_get_air_model(const fc_grid* grid, int* model);
 /* Under Dirichlet air nothing constrains the velocity between air cells, so fc_step extends the

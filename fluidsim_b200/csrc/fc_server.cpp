@@ -537,10 +537,27 @@ int fc_server_create_classes(size_t device_budget_bytes, int max_active, int cla
             s.lanes.back()->max_cells = k + 1 < classes ? max_cells[k] : std::numeric_limits<long long>::max();
             s.lanes.back()->priority = std::max(greatest, least - (classes - 1 - k));
         }
-        for (auto& lane : s.lanes)
+        try
         {
-            fc::Server::Lane* l = lane.get();
-            l->worker = std::thread([&s, l] { s.run(*l); });
+            for (auto& lane : s.lanes)
+            {
+                fc::Server::Lane* l = lane.get();
+                l->worker = std::thread([&s, l] { s.run(*l); });
+            }
+        }
+        catch (...)
+        {
+            // A worker that could not start: stop and join the ones that did before the server
+            // they point to goes away.
+            {
+                std::lock_guard<std::mutex> lock(s.mutex);
+                s.stop = true;
+            }
+            s.wake.notify_all();
+            for (auto& lane : s.lanes)
+                if (lane->worker.joinable())
+                    lane->worker.join();
+            fail(FC_ERR_OUT_OF_MEMORY, "could not start the server's workers");
         }
         *out = server.release();
     });

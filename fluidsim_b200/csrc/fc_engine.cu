@@ -72,6 +72,41 @@ void check(cudaError_t err, const char* what)
     }
 }
 
+// Device memory of grids and plans comes from the device's stream-ordered pool: allocations and
+// frees are ordered on the owner's stream and never synchronise the device, so tearing down one
+// grid does not wait for other threads' work (the serving loop retires simulations while other
+// size classes run; a plain free waited up to 1.4 s there). The pool keeps freed memory for
+// reuse instead of returning it at every synchronisation.
+void device_pool_setup()
+{
+    static std::mutex lock;
+    static bool done[64] = {};
+    int device = 0;
+    check(cudaGetDevice(&device), "device");
+    std::lock_guard<std::mutex> guard(lock);
+    if (device < 0 || device >= 64 || done[device])
+        return;
+    cudaMemPool_t pool;
+    check(cudaDeviceGetDefaultMemPool(&pool, device), "memory pool");
+    unsigned long long keep = ~0ull;
+    check(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep), "memory pool threshold");
+    done[device] = true;
+}
+
+template <typename P> void device_alloc(P** ptr, size_t bytes, cudaStream_t s, const char* what)
+{
+    device_pool_setup();
+    void* p = nullptr;
+    check(cudaMallocAsync(&p, bytes, s), what);
+    *ptr = static_cast<P*>(p);
+}
+
+void device_free(void* ptr, cudaStream_t s)
+{
+    if (ptr)
+        cudaFreeAsync(ptr, s);
+}
+
 inline long long launch_size(long long blocks) { return blocks; }
 inline long long launch_size(dim3 blocks) { return (long long)blocks.x * blocks.y * blocks.z; }
 
@@ -556,7 +591,7 @@ size_t allocate_grid(Grid& g, bool allocate = true)
     }
     if (!allocate)
         return total;
-    check(cudaMalloc(&g.arena, total), "grid allocation");
+    device_alloc(&g.arena, total, g.stream, "grid allocation");
     g.arena_bytes = total;
     check(cudaMemsetAsync(g.arena, 0, total, g.stream), "grid clear");
     for (size_t i = 0; i < slots.size(); ++i)
@@ -626,15 +661,15 @@ void allocate_masses(Grid& g)
     const int k = g.components();
     if (k == g.mass_capacity && g.masses)
         return;
-    cudaFree(g.masses);
-    cudaFree(g.mass_ptrs);
+    device_free(g.masses, g.stream);
+    device_free(g.mass_ptrs, g.stream);
     g.masses = nullptr;
     g.mass_ptrs = nullptr;
     g.mass_capacity = k;
     if (k > 0)
     {
-        check(cudaMalloc(&g.masses, size_t(k) * g.cells * sizeof(double)), "mass allocation");
-        check(cudaMalloc(&g.mass_ptrs, size_t(k) * sizeof(double*)), "mass pointers");
+        device_alloc(&g.masses, size_t(k) * g.cells * sizeof(double), g.stream, "mass allocation");
+        device_alloc(&g.mass_ptrs, size_t(k) * sizeof(double*), g.stream, "mass pointers");
         std::vector<double*> ptrs(k);
         for (int i = 0; i < k; ++i)
             ptrs[i] = g.masses + size_t(i) * g.cells;
@@ -896,9 +931,9 @@ struct Plan
     GridDesc* d_desc = nullptr;
     Tile* d_tiles = nullptr;
     ProjectParams* d_params = nullptr;
-    ProjectParams* h_params = nullptr; // pinned
+    ProjectParams* h_params = nullptr; // host copies (pageable)
     SolveState* d_states = nullptr;
-    SolveState* h_states = nullptr;    // pinned
+    SolveState* h_states = nullptr;
     int* d_body_count = nullptr;
     Range vec;
     Range faces; // tiles over the (W+1) x (H+1) face index space
@@ -931,13 +966,10 @@ struct Plan
             cudaGraphExecDestroy(exec);
         if (graph)
             cudaGraphDestroy(graph);
-        cudaFree(d_desc);
-        cudaFree(d_tiles);
-        cudaFree(d_params);
-        cudaFree(d_states);
-        cudaFree(d_body_count);
-        cudaFreeHost(h_params);
-        cudaFreeHost(h_states);
+        for (void* ptr : {(void*)d_desc, (void*)d_tiles, (void*)d_params, (void*)d_states, (void*)d_body_count})
+            device_free(ptr, stream);
+        delete[] h_params;
+        delete[] h_states;
         if (own_stream && stream)
             cudaStreamDestroy(stream);
     }
@@ -951,8 +983,7 @@ Grid::~Grid()
     plan.reset();
     for (void* ptr : {(void*)masses, (void*)mass_ptrs, (void*)tension_arena, (void*)visc_arena, (void*)plic_arena,
              (void*)arena})
-        if (ptr)
-            cudaFree(ptr);
+        device_free(ptr, stream);
     if (stream)
         cudaStreamDestroy(stream);
 }
@@ -1083,17 +1114,19 @@ std::unique_ptr<Plan> make_plan(const std::vector<Grid*>& grids, cudaStream_t st
                         append_tiles(tiles, i, grids[i]->levels[l].w, grids[i]->levels[l].h, tq.post_x, tq.post_y);
             });
     }
-    check(cudaMalloc(&plan->d_tiles, std::max<size_t>(1, tiles.size()) * sizeof(Tile)), "plan tiles");
+    device_alloc(&plan->d_tiles, std::max<size_t>(1, tiles.size()) * sizeof(Tile), plan->stream, "plan tiles");
     // On the plan's stream, which every kernel reading the tiles runs on (a copy on the legacy
     // default stream is not ordered with it and may return before its data lands).
     check(cudaMemcpyAsync(plan->d_tiles, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice, plan->stream),
         "plan tiles");
-    check(cudaMalloc(&plan->d_desc, n * sizeof(GridDesc)), "plan descriptors");
-    check(cudaMalloc(&plan->d_params, n * sizeof(ProjectParams)), "plan params");
-    check(cudaMalloc(&plan->d_states, n * sizeof(SolveState)), "plan states");
-    check(cudaMalloc(&plan->d_body_count, sizeof(int)), "plan counter");
-    check(cudaHostAlloc(&plan->h_params, n * sizeof(ProjectParams), cudaHostAllocDefault), "plan params");
-    check(cudaHostAlloc(&plan->h_states, n * sizeof(SolveState), cudaHostAllocDefault), "plan states");
+    device_alloc(&plan->d_desc, n * sizeof(GridDesc), plan->stream, "plan descriptors");
+    device_alloc(&plan->d_params, n * sizeof(ProjectParams), plan->stream, "plan params");
+    device_alloc(&plan->d_states, n * sizeof(SolveState), plan->stream, "plan states");
+    device_alloc(&plan->d_body_count, sizeof(int), plan->stream, "plan counter");
+    // Host copies in pageable memory: the copies into them complete before their call returns,
+    // and pinned memory would need a freeing call that synchronises the device.
+    plan->h_params = new ProjectParams[n]();
+    plan->h_states = new SolveState[n]();
     upload_descriptors(*plan);
     return plan;
 }
@@ -1701,7 +1734,7 @@ void sample_velocity(Grid& g, int count, const double* positions, double* veloci
     Plan& p = single_plan(g);
     const size_t bytes = size_t(count) * 2 * sizeof(double);
     double* d = nullptr;
-    check(cudaMalloc(&d, 2 * bytes), "sample allocation");
+    device_alloc(&d, 2 * bytes, p.stream, "sample allocation");
     try
     {
         check(cudaMemcpyAsync(d, positions, bytes, cudaMemcpyHostToDevice, p.stream), "sample upload");
@@ -1716,10 +1749,10 @@ void sample_velocity(Grid& g, int count, const double* positions, double* veloci
     }
     catch (...)
     {
-        cudaFree(d);
+        device_free(d, p.stream);
         throw;
     }
-    check(cudaFree(d), "sample free");
+    device_free(d, p.stream);
 }
 
 // FluidGridCPU::capillaryStepLimit (FluidGridCPU.cpp:843-860): half the period of the
@@ -1742,7 +1775,7 @@ void ensure_tension(Grid& g)
     tension_layout(g.cells, sizes);
     for (size_t b : sizes)
         total += b;
-    check(cudaMalloc(&g.tension_arena, total), "surface tension allocation");
+    device_alloc(&g.tension_arena, total, g.stream, "surface tension allocation");
     char* at = g.tension_arena;
     void* ptrs[6];
     for (int i = 0; i < 6; ++i)
@@ -1904,11 +1937,10 @@ ViscWork viscosity_workspace(Grid& g, cudaStream_t s)
     const size_t bytes = viscosity_layout(g, nullptr, nullptr);
     if (!g.visc_arena || g.visc_bytes < bytes)
     {
-        if (g.visc_arena)
-            cudaFree(g.visc_arena);
+        device_free(g.visc_arena, s);
         g.visc_arena = nullptr;
         g.visc_bytes = 0;
-        check(cudaMalloc(&g.visc_arena, bytes), "viscosity allocation");
+        device_alloc(&g.visc_arena, bytes, s, "viscosity allocation");
         g.visc_bytes = bytes;
         check(cudaMemsetAsync(g.visc_arena, 0, bytes, s), "viscosity clear");
     }
@@ -2095,11 +2127,10 @@ plic::PlicArrays plic_workspace(Grid& g, cudaStream_t s)
     const size_t bytes = plic_layout(g, nullptr, nullptr);
     if (!g.plic_arena || g.plic_bytes < bytes)
     {
-        if (g.plic_arena)
-            cudaFree(g.plic_arena);
+        device_free(g.plic_arena, s);
         g.plic_arena = nullptr;
         g.plic_bytes = 0;
-        check(cudaMalloc(&g.plic_arena, bytes), "transport allocation");
+        device_alloc(&g.plic_arena, bytes, s, "transport allocation");
         g.plic_bytes = bytes;
         check(cudaMemsetAsync(g.plic_arena, 0, bytes, s), "transport clear");
     }

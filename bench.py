@@ -717,15 +717,15 @@ def batched_measure(args, torch, world=1, rank=0, count=256, precision="fp32"):
             "max_iterations": max(r.iterations for r in res)}
 
 
-SERVE_CLASSES = (256 * 256, 1024 * 1024)  # the server's default size classes (cells)
+SERVE_CLASSES = (128 * 128, 256 * 256, 512 * 512, 1024 * 1024)  # the server's default size classes (cells)
 
 
 def serve_measure(args, rate=200.0, budget=150 * 10**9, precision="mixed"):
     """Serving: Poisson arrivals (mean `rate` per second) of dam breaks with surface tension
     (sigma 0.07, liquid 1000, air 1), square sides log-uniform 64..2048, each run for
     serve_steps steps of dt 1/120 to the max-norm rule at the bench tolerance, in mixed
-    precision, admitted by a device-memory budget and batched as they arrive in three size
-    classes (up to 256^2, up to 1024^2, larger cells), each stepped by its own worker. The same
+    precision, admitted by a device-memory budget and batched as they arrive in five size
+    classes (up to 128^2, 256^2, 512^2, 1024^2 cells, larger), each stepped by its own worker. The same
     simulations are then run one at a time through fc_step (the plain path, same precision).
     Step latencies are reported per size class for both. A bounded sample: serve_requests
     requests."""

@@ -565,8 +565,8 @@ int fc_server_create_classes(size_t device_budget_bytes, int max_active, int cla
 
 int fc_server_create(size_t device_budget_bytes, int max_active, fc_server** out)
 {
-    const long long bounds[2] = {256LL * 256, 1024LL * 1024};
-    return fc_server_create_classes(device_budget_bytes, max_active, 3, bounds, out);
+    const long long bounds[4] = {128LL * 128, 256LL * 256, 512LL * 512, 1024LL * 1024};
+    return fc_server_create_classes(device_budget_bytes, max_active, 5, bounds, out);
 }
 
 int fc_server_destroy(fc_server* server)

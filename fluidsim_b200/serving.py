@@ -56,7 +56,8 @@ class Server:
 
     size_classes: increasing cell-count bounds of the size classes (a class per bound plus one
     for larger grids), each stepped by its own worker; None for the library's default (up to
-    256 x 256, up to 1024 x 1024, larger); [] for one class that steps everything in lockstep."""
+    128 x 128, 256 x 256, 512 x 512, 1024 x 1024, larger); [] for one class that steps everything
+    in lockstep."""
 
     def __init__(self, device_budget_bytes: int, max_active: int = 256, size_classes: Optional[Sequence[int]] = None):
         handle = C.c_void_p()

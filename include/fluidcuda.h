@@ -439,8 +439,8 @@ typedef struct fc_server_stats
 /* device_budget_bytes: device memory the simulations may hold together; max_active: slots
  * (both shared by all size classes). Simulations are sorted by cells into size classes, each
  * stepped by its own worker thread in its own batched solves, so a small grid's step latency
- * does not wait on a large grid's. fc_server_create uses three classes: up to 256 x 256 cells,
- * up to 1024 x 1024, and larger. fc_server_create_classes takes `classes` classes with
+ * does not wait on a large grid's. fc_server_create uses five classes: up to 128 x 128 cells,
+ * up to 256 x 256, 512 x 512, 1024 x 1024, and larger. fc_server_create_classes takes `classes` classes with
  * classes - 1 increasing bounds: class k holds grids of more than max_cells[k - 1] and at most
  * max_cells[k] cells; the last class holds the rest. One class steps every simulation in
  * lockstep. Within a class, simulations are admitted in arrival order. */

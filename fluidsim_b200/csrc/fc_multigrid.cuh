@@ -316,28 +316,28 @@ template <typename T> __global__ void __launch_bounds__(kCoarseThreads) k_coarse
     }
     __syncthreads();
     // Cholesky, right-looking: at step k the pivot and column k are final; the trailing lower
-    // triangle then takes its k-th product.
+    // triangle then takes its k-th product. Every thread forms the pivot itself (the same
+    // correctly rounded square root), so a step needs two barriers: one after the column is
+    // scaled, one after the trailing update. The threads cover the trailing triangle as rows of
+    // 64 columns (kMaxCoarse), 512 / 64 rows at a time, with no index divisions; each entry takes
+    // the same operations in the same order as in the reference's column loop.
+    constexpr int kCols = kMaxCoarse, kRows = kCoarseThreads / kMaxCoarse;
+    const int trow = threadIdx.x / kCols, tcol = threadIdx.x % kCols;
     for (int k = 0; k < n; ++k)
     {
-        if (threadIdx.x == 0)
-        {
-            const double value = a[k * n + k];
-            if (!(value > 0.0) || !isfinite(value))
-                failed = 1;
-            a[k * n + k] = sqrt(value);
-        }
-        __syncthreads();
-        const double pivot = a[k * n + k];
+        const double value = a[k * n + k];
+        const double pivot = sqrt(value);
+        if (threadIdx.x == 0 && (!(value > 0.0) || !isfinite(value)))
+            failed = 1;
         for (int row = k + 1 + threadIdx.x; row < n; row += blockDim.x)
             a[row * n + k] = a[row * n + k] / pivot;
         __syncthreads();
-        const int m = n - 1 - k; // trailing rows and columns k+1 .. n-1
-        for (int e = threadIdx.x; e < m * m; e += blockDim.x)
-        {
-            const int row = k + 1 + e / m, col = k + 1 + e % m;
+        if (threadIdx.x == 0)
+            a[k * n + k] = pivot;
+        const int col = k + 1 + tcol;
+        for (int row = k + 1 + trow; row < n; row += kRows)
             if (col <= row)
                 a[row * n + col] -= a[row * n + k] * a[col * n + k];
-        }
         __syncthreads();
     }
     // Y = L^-1, right-looking forward substitution: row k of Y is final after its division;
@@ -348,12 +348,9 @@ template <typename T> __global__ void __launch_bounds__(kCoarseThreads) k_coarse
         for (int col = threadIdx.x; col <= k; col += blockDim.x)
             yi[k * n + col] = yi[k * n + col] / pivot;
         __syncthreads();
-        const int m = n - 1 - k;
-        for (int e = threadIdx.x; e < m * (k + 1); e += blockDim.x)
-        {
-            const int row = k + 1 + e / (k + 1), col = e % (k + 1);
-            yi[row * n + col] -= a[row * n + k] * yi[k * n + col];
-        }
+        if (tcol <= k)
+            for (int row = k + 1 + trow; row < n; row += kRows)
+                yi[row * n + tcol] -= a[row * n + k] * yi[k * n + tcol];
         __syncthreads();
     }
     // A^-1 = Y^T Y: entry (r, c) sums Y[k][r] Y[k][c] over k >= max(r, c).

@@ -66,6 +66,7 @@ struct SolveState
     double res_max, res_sumsq;
     double refresh_max; // FP32: recurrence max-norm that triggers a refresh from the true residual (0: none)
     double dt;          // time step of the projection in flight
+    double alpha_pending; // step length whose p += alpha d is still to be applied (p_pending)
     int iterations;
     int restarts;       // true-residual checks that failed and restarted the directions
     int refreshes;      // FP32 early restarts from the true residual (refresh_threshold)
@@ -77,6 +78,7 @@ struct SolveState
     int mg_valid;       // multigrid hierarchy and coarsest inverse are usable
     int use_mg;         // multigrid (1) or diagonal (0) preconditioner
     int nonfinite;
+    int p_pending;      // the first iteration of a pair updated r but left p += alpha d to the second
 };
 
 // Linear interpolation from a fine axis position to the two nearest coarse centres

@@ -1299,6 +1299,7 @@ template <typename T> void launch_setup(Plan& p, bool use_mg)
 template <typename T> void launch_finish(Plan& p)
 {
     cudaStream_t s = p.stream;
+    FC_LAUNCH(k_flush_pressure<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
     FC_LAUNCH(k_pressure_sum, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
     FC_LAUNCH(k_velocity_update<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
     FC_LAUNCH(k_remove_pressure_mean, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));

@@ -321,6 +321,22 @@ __device__ __forceinline__ double apply_cell_fp64(const T* right, const T* down,
            (dd(down[i - S]) * (c - x[i - S]) + dd(down[i]) * (c - x[i + S]));
 }
 
+// p + alpha d with one rounding (a fused multiply-add), the same wherever a pressure step is
+// applied (k_update, k_flush_pressure) or read as pending (k_true_residual).
+__device__ __forceinline__ double step_value(double p, double alpha, double d) { return __fma_rn(alpha, d, p); }
+
+// A p at cell i with p + alpha d in place of p: the pressure with the pending step of a pair
+// (k_update), each value formed exactly as k_update forms it.
+template <typename T>
+__device__ __forceinline__ double apply_cell_fp64_pending(const T* right, const T* down, const double* x, const T* d,
+    double alpha, long long i, int S)
+{
+    auto at = [&](long long j) { return step_value(x[j], alpha, double(d[j])); };
+    const double c = at(i);
+    return (dd(right[i - 1]) * (c - at(i - 1)) + dd(right[i]) * (c - at(i + 1))) +
+           (dd(down[i - S]) * (c - at(i - S)) + dd(down[i]) * (c - at(i + S)));
+}
+
 // True residual r = (b - mean b) - A p in FP64, stored in the working type, with its stats.
 // `initial` selects the solve's first residual (FluidGridCPU.cpp:1754-1757) versus the
 // convergence check inside the loop (:1795-1804).
@@ -337,6 +353,10 @@ __global__ void __launch_bounds__(kVecThreads) k_true_residual(const GridDesc* g
     const T* down = static_cast<const T*>(g.lev[0].down);
     T* r = static_cast<T*>(g.r);
     const double mean_b = s.mean_b;
+    // Inside a pair the pressure still lacks the first iteration's step (k_update).
+    const bool pending = !initial && s.p_pending;
+    const T* d0 = static_cast<const T*>(g.d[1]);
+    const double alpha0 = s.alpha_pending;
     double sum = 0.0, mx = 0.0, sq = 0.0;
     for (int k = 0; k < kVecCells; ++k)
     {
@@ -346,7 +366,8 @@ __global__ void __launch_bounds__(kVecThreads) k_true_residual(const GridDesc* g
         const long long i = padded_index(g.S, x, y);
         double value = 0.0;
         if (!cell_held(g, x, y))
-            value = (g.b[i] - mean_b) - apply_cell_fp64(right, down, g.p, i, g.S);
+            value = (g.b[i] - mean_b) - (pending ? apply_cell_fp64_pending(right, down, g.p, d0, alpha0, i, g.S)
+                                                 : apply_cell_fp64(right, down, g.p, i, g.S));
         const T stored = T(value);
         r[i] = stored;
         const double rv = dd(stored);
@@ -569,6 +590,14 @@ __global__ void __launch_bounds__(kVecThreads, sizeof(T) == 4 ? 4 : 1)
 // four cells per step with every load of the step issued before the arithmetic, and a CTA
 // counts its slices of a grid once; the per-slice partials and their fold are those of one CTA
 // per slice.
+//
+// The loop runs its iterations in pairs (parity 0, then 1). Nothing inside the loop reads p
+// except the true residual, so the first iteration of a pair updates only r and leaves its
+// p += alpha_0 d_0 pending (alpha_pending, p_pending); the second applies it and then its own,
+// p = (p + alpha_0 d_0) + alpha_1 d_1, the same two roundings as two separate updates. That
+// streams p (16 B per cell in FP64) once per pair instead of once per iteration. The true
+// residual reads p + alpha_0 d_0 while an update is pending (k_true_residual), and the loop's
+// exit applies a pending update (k_flush_pressure) before anything after the loop reads p.
 template <typename T> struct Quad;
 template <> struct Quad<float>
 {
@@ -582,11 +611,22 @@ template <> struct Quad<double>
 constexpr int kUpdateCtasPerSm = 2;
 
 template <typename T>
+__device__ __forceinline__ void add_step(double4& p, double alpha, const typename Quad<T>::type& d)
+{
+    p.x = step_value(p.x, alpha, double(d.x));
+    p.y = step_value(p.y, alpha, double(d.y));
+    p.z = step_value(p.z, alpha, double(d.z));
+    p.w = step_value(p.w, alpha, double(d.w));
+}
+
+template <typename T>
 __global__ void __launch_bounds__(kVecThreads, kUpdateCtasPerSm)
     k_update(const GridDesc* grids, const Tile* tiles, int count, int parity)
 {
     using Q = typename Quad<T>::type;
-    constexpr int U = 2; // quads per thread and step
+    // Quads per thread and step (FP64 takes one: its quads are twice the registers). A thread
+    // visits the same quads in the same order either way.
+    constexpr int U = sizeof(T) == 4 ? 2 : 1;
     allow_dependents();
     dependency_wait();
     __shared__ double4 total;
@@ -602,6 +642,11 @@ __global__ void __launch_bounds__(kVecThreads, kUpdateCtasPerSm)
         const T* q = static_cast<const T*>(g.q);
         T* r = static_cast<T*>(g.r);
         const double alpha = s.rz / s.dq;
+        // Second of a pair: the first's pending step (its direction is the other buffer).
+        const bool update_p = parity == 1;
+        const bool pending = update_p && s.p_pending;
+        const double alpha0 = s.alpha_pending;
+        const T* d0 = static_cast<const T*>(g.d[parity]);
         // The padded length S * (H + 2) is a multiple of 8; slices are whole quads.
         const long long quads = (long long)g.S * (g.H + 2) / 4;
         const long long per = (quads + g.vec_tiles - 1) / g.vec_tiles;
@@ -610,7 +655,7 @@ __global__ void __launch_bounds__(kVecThreads, kUpdateCtasPerSm)
         double sum = 0.0, mx = 0.0, sq = 0.0;
         for (long long base = first + threadIdx.x; base < last; base += (long long)kVecThreads * U)
         {
-            Q dv[U], qv[U], rv[U];
+            Q dv[U], d0v[U], qv[U], rv[U];
             double4 pv[U];
 #pragma unroll
             for (int u = 0; u < U; ++u)
@@ -618,10 +663,15 @@ __global__ void __launch_bounds__(kVecThreads, kUpdateCtasPerSm)
                 const long long j = base + (long long)u * kVecThreads;
                 if (j < last)
                 {
-                    dv[u] = reinterpret_cast<const Q*>(d)[j];
                     qv[u] = reinterpret_cast<const Q*>(q)[j];
                     rv[u] = reinterpret_cast<const Q*>(r)[j];
-                    pv[u] = reinterpret_cast<const double4*>(g.p)[j];
+                    if (update_p)
+                    {
+                        dv[u] = reinterpret_cast<const Q*>(d)[j];
+                        pv[u] = reinterpret_cast<const double4*>(g.p)[j];
+                        if (pending)
+                            d0v[u] = reinterpret_cast<const Q*>(d0)[j];
+                    }
                 }
             }
 #pragma unroll
@@ -630,17 +680,19 @@ __global__ void __launch_bounds__(kVecThreads, kUpdateCtasPerSm)
                 const long long j = base + (long long)u * kVecThreads;
                 if (j >= last)
                     continue;
-                double4 pp = pv[u];
-                pp.x += alpha * double(dv[u].x);
-                pp.y += alpha * double(dv[u].y);
-                pp.z += alpha * double(dv[u].z);
-                pp.w += alpha * double(dv[u].w);
+                if (update_p)
+                {
+                    double4 pp = pv[u];
+                    if (pending)
+                        add_step<T>(pp, alpha0, d0v[u]);
+                    add_step<T>(pp, alpha, dv[u]);
+                    reinterpret_cast<double4*>(g.p)[j] = pp;
+                }
                 Q rr;
                 rr.x = T(double(rv[u].x) - alpha * double(qv[u].x));
                 rr.y = T(double(rv[u].y) - alpha * double(qv[u].y));
                 rr.z = T(double(rv[u].z) - alpha * double(qv[u].z));
                 rr.w = T(double(rv[u].w) - alpha * double(qv[u].w));
-                reinterpret_cast<double4*>(g.p)[j] = pp;
                 reinterpret_cast<Q*>(r)[j] = rr;
                 const double e[4] = {double(rr.x), double(rr.y), double(rr.z), double(rr.w)};
 #pragma unroll
@@ -663,6 +715,9 @@ __global__ void __launch_bounds__(kVecThreads, kUpdateCtasPerSm)
             {
                 if (threadIdx.x == 0)
                 {
+                    // Every slice of the grid has read the pending state by now.
+                    s.p_pending = update_p ? 0 : 1;
+                    s.alpha_pending = update_p ? 0.0 : alpha;
                     s.iterations += 1;
                     const double maximum = isfinite(total.x) ? total.y : INFINITY;
                     s.sum_r = total.x;
@@ -682,6 +737,30 @@ __global__ void __launch_bounds__(kVecThreads, kUpdateCtasPerSm)
             }
             run = 0;
         }
+    }
+}
+
+// Applies a pair's pending p += alpha d at the loop's exit (see k_update), over the padded
+// array as one flat stream; p is read only after this.
+template <typename T> __global__ void __launch_bounds__(kVecThreads) k_flush_pressure(const GridDesc* grids, const Tile* tiles)
+{
+    using Q = typename Quad<T>::type;
+    const Tile t = tiles[blockIdx.x];
+    const GridDesc& g = grids[t.grid];
+    const SolveState& s = *g.state;
+    if (!s.p_pending)
+        return;
+    const T* d0 = static_cast<const T*>(g.d[1]);
+    const double alpha0 = s.alpha_pending;
+    const long long quads = (long long)g.S * (g.H + 2) / 4;
+    const long long per = (quads + g.vec_tiles - 1) / g.vec_tiles;
+    const long long first = per * t.index;
+    const long long last = min(quads, first + per);
+    for (long long j = first + threadIdx.x; j < last; j += kVecThreads)
+    {
+        double4 pp = reinterpret_cast<const double4*>(g.p)[j];
+        add_step<T>(pp, alpha0, reinterpret_cast<const Q*>(d0)[j]);
+        reinterpret_cast<double4*>(g.p)[j] = pp;
     }
 }
 

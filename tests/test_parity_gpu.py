@@ -121,6 +121,26 @@ def test_fp64_matches_restatement(oracle, size):
     assert rel_err(out.pressure, po) <= 1e-7
 
 
+@pytest.mark.parametrize("cap", [1, 2, 3, 4, 5])
+def test_iteration_cap_at_either_step_of_a_pair(oracle, cap):
+    """The PCG loop updates the pressure once per pair of iterations (the first step stays
+    pending); a solve stopped by its iteration cap after an odd or an even count must still
+    leave the pressure of every step taken: FP64 equals the restatement under the same cap."""
+    s = scenes.random_pool(96, 80, seed=cap, fill=0.55, cell_size=1.0 / 96)
+    o = oracle_grid(oracle, s)
+    ro = o.project(s.dt, cap, 1e-12)
+    uo, vo, po = o.download()
+    g = gpu_grid(s, "fp64")
+    r = g.project(s.dt, cap, 1e-12)
+    out = g.download()
+    assert r.iterations == ro.iterations == cap
+    assert not r.converged and not ro.converged
+    scale = max(1.0, np.abs(uo).max(), np.abs(vo).max())
+    assert np.abs(out.u - uo).max() <= 1e-10 * scale
+    assert np.abs(out.v - vo).max() <= 1e-10 * scale
+    assert rel_err(out.pressure, po) <= 1e-9
+
+
 @pytest.mark.parametrize("size", [(64, 64), (129, 65), (257, 193), (333, 251)])
 def test_fp32_matches_restatement(oracle, size):
     w, h = size

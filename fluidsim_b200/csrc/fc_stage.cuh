@@ -249,6 +249,12 @@ template <typename T> __device__ __forceinline__ T prolong_lerp(T w, T lo, T hi)
 // tile's entry and copy arguments are read one tile ahead: the kernel's global stores cannot
 // alias them, but the compiler cannot know that and would reload them from memory after every
 // store, which put dependent global loads on each tile's path.
+//
+// A tile whose grid's solve is done is neither computed nor copied in: the issuing thread
+// completes its barrier phase with a plain arrival instead of the boxes and records its verdict
+// in `tile_live`, which every thread reads after the phase's wait. The loop's idle passes after
+// convergence, and the finished grids of a batch, then stream nothing but the first tile's
+// boxes of each CTA (issued before the dependency wait, when no verdict is known yet).
 template <typename T, int K, typename W, int WARPS>
 __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2 : 1)
     k_smooth_pre(const GridDesc* __restrict__ grids, const Tile* __restrict__ tiles, int count, int level, int set)
@@ -265,6 +271,7 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
     static_assert(Shape::HALO % 2 == 0 && Shape::HALO / 2 >= 2 && OCX + Shape::HALO / 2 <= 31, "restriction lanes");
     __shared__ T lines[Shape::RY][32];
     __shared__ RestrictAxis<T> along_y[OCY];
+    __shared__ int tile_live; // the issuing thread's verdict on the tile it last started
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     allow_dependents();
     // TMA writes shared memory at 128-byte aligned addresses only; a misplaced staging buffer is
@@ -293,9 +300,14 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
             stage_failed_at(grids[t.grid].state);
         return;
     }
+    // The first tile's boxes complete its phase whatever its grid's state (the weights are in
+    // flight already); the verdict only decides whether it is computed.
     if (threadIdx.x == 0 && i < count)
+    {
+        tile_live = grids[t.grid].state->done == 0;
         stage_issue_data<T, W, K, true, WARPS>(issue_args(grids[t.grid], level), level, set, t.x0 - Shape::HALO,
             t.y0 - Shape::HALO, stage, &bar);
+    }
     unsigned parity = 0;
     for (; i < count; i += gridDim.x)
     {
@@ -322,16 +334,21 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
         RestrictAxis<T> row_weights{};
         if (threadIdx.x < OCY && cy0 + int(threadIdx.x) < Ch)
             row_weights = static_cast<const RestrictAxis<T>*>(Ld.rwy)[cy0 + threadIdx.x];
-        const bool done = state->done != 0;
         const double mean_r = level == 0 ? state->mean_r : 0.0;
-        // The next tile's copy arguments, for the issuing thread.
+        // The next tile's copy arguments and whether its grid still solves, for the issuing thread.
         IssueArgs na{};
+        bool next_live = false;
         if (threadIdx.x == 0 && next < count)
+        {
             na = issue_args(grids[n.grid], level);
+            next_live = grids[n.grid].state->done == 0;
+        }
         const bool ok = mbarrier_wait(&bar, parity);
         if (stage_failed(ok, state))
             return;
         parity ^= 1u;
+        // Written before the barrier inside stage_failed; rewritten only after the next one.
+        const bool done = tile_live == 0;
         Strip<T, K> s;
         if (!done)
         {
@@ -342,8 +359,14 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
         // The staging buffer is free: the next tile's boxes stream in while this one sweeps.
         if (threadIdx.x == 0 && next < count)
         {
-            fence_async_shared();
-            stage_issue<T, W, K, true, WARPS>(na, level, set, n.x0 - Shape::HALO, n.y0 - Shape::HALO, stage, &bar);
+            tile_live = next_live;
+            if (next_live)
+            {
+                fence_async_shared();
+                stage_issue<T, W, K, true, WARPS>(na, level, set, n.x0 - Shape::HALO, n.y0 - Shape::HALO, stage, &bar);
+            }
+            else
+                mbarrier_arrive(&bar);
         }
         if (done)
         {
@@ -448,6 +471,7 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
     __shared__ Edges<T, WARPS> edges;
     __shared__ double4 total;
     __shared__ double2 warp_pairs[WARPS];
+    __shared__ int tile_live; // the issuing thread's verdict on the tile it last started (k_smooth_pre)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     allow_dependents();
     // TMA writes shared memory at 128-byte aligned addresses only; a misplaced staging buffer is
@@ -476,9 +500,14 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
             stage_failed_at(grids[t.grid].state);
         return;
     }
+    // The first tile's boxes complete its phase whatever its grid's state (the weights are in
+    // flight already); the verdict only decides whether it is computed.
     if (threadIdx.x == 0 && i < count)
+    {
+        tile_live = grids[t.grid].state->done == 0;
         stage_issue_data<T, W, K, false, WARPS>(issue_args(grids[t.grid], level), level, set, t.x0 - Shape::HALO,
             t.y0 - Shape::HALO, stage, &bar);
+    }
     unsigned parity = 0;
     int run = 0; // level 0: tiles of the current grid finished since the last count
     for (; i < count; i += gridDim.x)
@@ -495,15 +524,19 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
         const int CX0 = X0 / 2 - 1, CY0 = Y0 / 2 - 1;
         const int gx = X0 + 2 * lane;
         const bool in_a = gx >= 0 && gx < Lw, in_b = gx + 1 >= 0 && gx + 1 < Lw;
-        const bool done = state->done != 0;
         const double mean_r = level == 0 ? state->mean_r : 0.0;
         IssueArgs na{};
+        bool next_live = false;
         if (threadIdx.x == 0 && next < count)
+        {
             na = issue_args(grids[n.grid], level);
+            next_live = grids[n.grid].state->done == 0;
+        }
         const bool ok = mbarrier_wait(&bar, parity);
         if (stage_failed(ok, state))
             return;
         parity ^= 1u;
+        const bool done = tile_live == 0;
         Strip<T, K> s;
         if (!done)
         {
@@ -603,8 +636,14 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
         // The staging buffer is free: the next tile's boxes stream in while this one sweeps.
         if (threadIdx.x == 0 && next < count)
         {
-            fence_async_shared();
-            stage_issue<T, W, K, false, WARPS>(na, level, set, n.x0 - Shape::HALO, n.y0 - Shape::HALO, stage, &bar);
+            tile_live = next_live;
+            if (next_live)
+            {
+                fence_async_shared();
+                stage_issue<T, W, K, false, WARPS>(na, level, set, n.x0 - Shape::HALO, n.y0 - Shape::HALO, stage, &bar);
+            }
+            else
+                mbarrier_arrive(&bar);
         }
         if (done)
         {

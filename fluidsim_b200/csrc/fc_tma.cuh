@@ -37,6 +37,14 @@ __device__ __forceinline__ void mbarrier_expect_tx(uint64_t* bar, unsigned bytes
         : "memory");
 }
 
+// One arrival with no transaction bytes: completes the phase of a barrier of count 1 that is
+// given no copies.
+__device__ __forceinline__ void mbarrier_arrive(uint64_t* bar)
+{
+    asm volatile("{\n\t.reg .b64 state;\n\tmbarrier.arrive.shared::cta.b64 state, [%0];\n\t}" ::"r"(smem_address(bar))
+                 : "memory");
+}
+
 // True once the barrier's phase with the given parity has completed; false after kWaitLimit polls.
 __device__ __forceinline__ bool mbarrier_wait(uint64_t* bar, unsigned parity)
 {

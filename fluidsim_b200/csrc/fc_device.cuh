@@ -384,6 +384,13 @@ __device__ __forceinline__ void stage_failed_at(SolveState* state)
     state->done = 1;
 }
 
+// Whether a grid's solve was done already before this kernel's dependency wait, read from L2.
+// Inside a projection the flag only rises (the set-up clears it with ordinary launches, which
+// complete before any kernel of the loop starts; the timing and tuning entry points clear it
+// with copies ordered before their launches), so a done flag read before the wait is still done
+// after it. A flag read as running may be stale and is settled after the wait.
+__device__ __forceinline__ bool done_before_wait(const SolveState* s) { return __ldcg(&s->done) != 0; }
+
 // Records a failed wait (the staged data never arrived) on the tile's grid; returns true then.
 __device__ __forceinline__ bool stage_failed(bool ok, SolveState* state)
 {
@@ -403,5 +410,13 @@ __device__ __forceinline__ bool stage_failed(bool ok, SolveState* state)
 // data no kernel of the projection writes (tiles, descriptors, face weights, transfer tables).
 __device__ __forceinline__ void dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void allow_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+// Start of a kernel that reads earlier kernels' writes from its first instruction: its own
+// successor may be scheduled at once, and it waits for its predecessors. Launched without
+// programmatic serialization, both are no-ops.
+__device__ __forceinline__ void dependent_start()
+{
+    allow_dependents();
+    dependency_wait();
+}
 
 } // namespace fc

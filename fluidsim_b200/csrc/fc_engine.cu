@@ -124,11 +124,11 @@ inline long long launch_size(dim3 blocks) { return (long long)blocks.x * blocks.
 
 // Launch with programmatic stream serialization: the kernel may be scheduled before its
 // predecessor completes and orders itself with dependency_wait() (fc_device.cuh).
-template <typename... Params, typename... Args>
-void launch_dependent(const char* name, void (*kernel)(Params...), int blocks, int threads, size_t smem,
+template <typename Blocks, typename... Params, typename... Args>
+void launch_dependent(const char* name, void (*kernel)(Params...), Blocks blocks, int threads, size_t smem,
     cudaStream_t stream, Args... args)
 {
-    if (blocks <= 0)
+    if (launch_size(blocks) <= 0)
         return;
     cudaLaunchConfig_t config = {};
     config.gridDim = dim3(blocks);
@@ -705,6 +705,7 @@ struct ProjectParams
 
 __global__ void k_init_states(const GridDesc* grids, int n, const ProjectParams* params, int* body_count)
 {
+    dependent_start();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0)
         *body_count = 0;
@@ -733,6 +734,7 @@ __global__ void k_init_states(const GridDesc* grids, int n, const ProjectParams*
 // Open (non-solid) cells define the mean-free subspace of the solve.
 __global__ void __launch_bounds__(kVecThreads) k_count_open(const GridDesc* grids, const Tile* tiles)
 {
+    dependent_start();
     const Tile t = tiles[blockIdx.x];
     const GridDesc& g = grids[t.grid];
     if (!g.solid || g.air)
@@ -771,6 +773,7 @@ __global__ void k_loop_condition(const GridDesc* grids, int n, int* body_count, 
 
 __global__ void k_gather_states(const GridDesc* grids, int n, SolveState* out)
 {
+    dependent_start();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n)
         out[i] = *grids[i].state;
@@ -1136,13 +1139,15 @@ std::unique_ptr<Plan> make_plan(const std::vector<Grid*>& grids, cudaStream_t st
 // ------------------------------------------------------------------------------------------
 
 // Density, face weights, multigrid conductances and the coarsest inverse of every grid.
+// The kernels are launched with programmatic serialization: each starts with dependent_start(),
+// so its launch overlaps the end of its predecessor.
 template <typename T> void launch_rebuild(Plan& p)
 {
     cudaStream_t s = p.stream;
-    FC_LAUNCH(k_density, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
-    FC_LAUNCH(k_coefficients<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
+    FC_LAUNCH_DEP(k_density, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
+    FC_LAUNCH_DEP(k_coefficients<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
     for (int l = 0; l + 1 < p.max_levels; ++l)
-        FC_LAUNCH(k_coarsen<T>, dim3(ceil_div(p.padded_max[l + 1], 256), p.n()), 256, 0, s, p.d_desc, l);
+        FC_LAUNCH_DEP(k_coarsen<T>, dim3(ceil_div(p.padded_max[l + 1], 256), p.n()), 256, 0, s, p.d_desc, l);
     static const bool inverse_configured = [&]
     {
         check(cudaFuncSetAttribute(k_coarse_inverse<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kCoarseInverseSmem)),
@@ -1152,12 +1157,12 @@ template <typename T> void launch_rebuild(Plan& p)
     (void)inverse_configured;
     if (p.precision == FC_PRECISION_MIXED)
         for (int l = 1; l < p.max_tail; ++l)
-            FC_LAUNCH(k_weights_half, dim3(ceil_div(p.padded_max[l], 256), p.n()), 256, 0, s, p.d_desc, l);
+            FC_LAUNCH_DEP(k_weights_half, dim3(ceil_div(p.padded_max[l], 256), p.n()), 256, 0, s, p.d_desc, l);
     // Level by level: under Dirichlet air a coarse level's held cells follow from the finer
     // level's inverse diagonal, and the coarsest factor from the level above it.
     for (int l = 0; l + 1 < p.max_levels; ++l)
-        FC_LAUNCH(k_inverse_diagonal<T>, dim3(ceil_div(p.padded_max[l], 256), p.n()), 256, 0, s, p.d_desc, l);
-    FC_LAUNCH(k_coarse_inverse<T>, p.n(), kCoarseThreads, kCoarseInverseSmem, s, p.d_desc);
+        FC_LAUNCH_DEP(k_inverse_diagonal<T>, dim3(ceil_div(p.padded_max[l], 256), p.n()), 256, 0, s, p.d_desc, l);
+    FC_LAUNCH_DEP(k_coarse_inverse<T>, p.n(), kCoarseThreads, kCoarseInverseSmem, s, p.d_desc);
 }
 
 // Resident CTAs of the persistent smoothing kernels: two per SM in FP32, one in FP64 (their
@@ -1285,13 +1290,14 @@ template <typename T> void set_kernel_attributes(Plan& p)
 template <typename T> void launch_setup(Plan& p, bool use_mg)
 {
     cudaStream_t s = p.stream;
+    // The first launch follows a copy (or starts the graph); the others follow a kernel.
     FC_LAUNCH(k_init_states, ceil_div(p.n(), 128), 128, 0, s, p.d_desc, p.n(), p.d_params, p.d_body_count);
-    FC_LAUNCH(k_count_open, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
-    FC_LAUNCH(k_rhs<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
-    FC_LAUNCH(k_rhs_stats<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
-    FC_LAUNCH(k_warm_start, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
-    FC_LAUNCH(k_remove_pressure_mean, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
-    FC_LAUNCH(k_true_residual<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec), 1);
+    FC_LAUNCH_DEP(k_count_open, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
+    FC_LAUNCH_DEP(k_rhs<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
+    FC_LAUNCH_DEP(k_rhs_stats<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
+    FC_LAUNCH_DEP(k_warm_start, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
+    FC_LAUNCH_DEP(k_remove_pressure_mean, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
+    FC_LAUNCH_DEP(k_true_residual<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec), 1);
     launch_precondition<T>(p, use_mg);
 }
 
@@ -1299,12 +1305,14 @@ template <typename T> void launch_setup(Plan& p, bool use_mg)
 template <typename T> void launch_finish(Plan& p)
 {
     cudaStream_t s = p.stream;
+    // The first launch follows the loop (a conditional node in the graph); the others follow a
+    // kernel.
     FC_LAUNCH(k_flush_pressure<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
-    FC_LAUNCH(k_pressure_sum, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
-    FC_LAUNCH(k_velocity_update<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
-    FC_LAUNCH(k_remove_pressure_mean, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
-    FC_LAUNCH(k_divergence<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
-    FC_LAUNCH(k_gather_states, ceil_div(p.n(), 128), 128, 0, s, p.d_desc, p.n(), p.d_states);
+    FC_LAUNCH_DEP(k_pressure_sum, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
+    FC_LAUNCH_DEP(k_velocity_update<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
+    FC_LAUNCH_DEP(k_remove_pressure_mean, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
+    FC_LAUNCH_DEP(k_divergence<T>, p.vec.count, kVecThreads, 0, s, p.d_desc, p.at(p.vec));
+    FC_LAUNCH_DEP(k_gather_states, ceil_div(p.n(), 128), 128, 0, s, p.d_desc, p.n(), p.d_states);
 }
 
 // Launch mechanism of the PCG loop: one CUDA graph with a device-side WHILE node (default), or

@@ -92,6 +92,7 @@ __global__ void __launch_bounds__(kVecThreads) k_precondition_diagonal(const Gri
 // the level's scale and saturated at the largest finite FP16 value (blockIdx.y = grid).
 __global__ void k_weights_half(const GridDesc* grids, int level)
 {
+    dependent_start();
     const GridDesc& g = grids[blockIdx.y];
     if (level < 1 || level >= g.tail)
         return;
@@ -136,6 +137,7 @@ template <typename T> __device__ __forceinline__ bool held_cell(const GridDesc& 
 // reciprocal are the same, so the smoothing is unchanged (PressureMultigrid.cpp:104-117).
 template <typename T> __global__ void k_inverse_diagonal(const GridDesc* grids, int level)
 {
+    dependent_start();
     const GridDesc& g = grids[blockIdx.y];
     if (level + 1 >= g.levels)
         return;
@@ -188,6 +190,7 @@ template <typename T> __global__ void k_inverse_diagonal(const GridDesc* grids, 
 // dependent chain, so the kernel needs many cells in flight rather than many cells per thread.
 template <typename T> __global__ void k_coarsen(const GridDesc* grids, int level)
 {
+    dependent_start();
     const GridDesc& g = grids[blockIdx.y];
     if (level + 1 >= g.levels)
         return;
@@ -253,6 +256,7 @@ constexpr size_t kCoarseInverseSmem = 2 * size_t(kMaxCoarse) * kMaxCoarse * size
 
 template <typename T> __global__ void __launch_bounds__(kCoarseThreads) k_coarse_inverse(const GridDesc* grids)
 {
+    dependent_start();
     const GridDesc& g = grids[blockIdx.x];
     const int last = g.levels - 1;
     const LevelDesc& l = g.lev[last];
@@ -725,6 +729,10 @@ template <typename T> __global__ void __launch_bounds__(kTailThreads) k_mg_tail(
     allow_dependents();
     const GridDesc& g = grids[blockIdx.x];
     SolveState& state = *g.state;
+    // In a batch (one CTA per grid), a grid whose solve is known to be done before the wait
+    // copies nothing in. A single grid skips the check: its load would delay the copies.
+    if (gridDim.x > 1 && done_before_wait(g.state))
+        return;
     const int first = g.tail, last = g.levels - 1;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     T* const m = tail_array<T>();

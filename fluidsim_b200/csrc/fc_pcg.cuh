@@ -98,6 +98,7 @@ __device__ __forceinline__ bool cell_held(const GridDesc& g, int x, int y)
 // FluidGridCPU.cpp:1399-1423 (rebuildDensity).
 __global__ void k_density(const GridDesc* grids, const Tile* tiles)
 {
+    dependent_start();
     FC_VEC_TILE_PROLOGUE
     const double inv_area = 1.0 / (g.dx * g.dx);
     for (int k = 0; k < kVecCells; ++k)
@@ -117,6 +118,7 @@ __global__ void k_density(const GridDesc* grids, const Tile* tiles)
 // FluidGridCPU.cpp:1154-1205 (rebuildPressureCoefficients).
 template <typename T> __global__ void k_coefficients(const GridDesc* grids, const Tile* tiles)
 {
+    dependent_start();
     FC_VEC_TILE_PROLOGUE
     const double* density = g.density;
     T* right = static_cast<T*>(g.lev[0].right);
@@ -179,6 +181,7 @@ __device__ __forceinline__ void cell_faces(const GridDesc& g, int x, int y, bool
 // FluidGridCPU.cpp:1050-1083.
 template <typename T> __global__ void __launch_bounds__(kVecThreads) k_rhs(const GridDesc* grids, const Tile* tiles)
 {
+    dependent_start();
     FC_VEC_TILE_PROLOGUE
     const double dt = g.state->dt;
     const double scale = g.dx * g.dx / dt;
@@ -209,6 +212,7 @@ template <typename T> __global__ void __launch_bounds__(kVecThreads) k_rhs(const
 // max |b - mean| and sum (b - mean)^2; decides the early exit (FluidGridCPU.cpp:1731-1740).
 template <typename T> __global__ void __launch_bounds__(kVecThreads) k_rhs_stats(const GridDesc* grids, const Tile* tiles)
 {
+    dependent_start();
     FC_VEC_TILE_PROLOGUE
     const double mean = g.state->mean_b;
     double mx = 0.0, sq = 0.0;
@@ -244,6 +248,7 @@ template <typename T> __global__ void __launch_bounds__(kVecThreads) k_rhs_stats
 // FluidGridCPU.cpp:1731-1753.
 __global__ void __launch_bounds__(kVecThreads) k_warm_start(const GridDesc* grids, const Tile* tiles)
 {
+    dependent_start();
     FC_VEC_TILE_PROLOGUE
     const bool clear = g.state->status == kNoWork;
     double sum = 0.0;
@@ -276,6 +281,7 @@ __global__ void __launch_bounds__(kVecThreads) k_warm_start(const GridDesc* grid
 // Pressure sum for the final mean removal.
 __global__ void __launch_bounds__(kVecThreads) k_pressure_sum(const GridDesc* grids, const Tile* tiles)
 {
+    dependent_start();
     FC_VEC_TILE_PROLOGUE
     if (g.state->status == kBreakdown)
         return;
@@ -298,6 +304,7 @@ __global__ void __launch_bounds__(kVecThreads) k_pressure_sum(const GridDesc* gr
 // p -= mean_p over open cells (FluidGridCPU.cpp:1466-1474, removeMean).
 __global__ void k_remove_pressure_mean(const GridDesc* grids, const Tile* tiles)
 {
+    dependent_start();
     FC_VEC_TILE_PROLOGUE
     if (g.state->status == kBreakdown)
         return;
@@ -744,6 +751,7 @@ __global__ void __launch_bounds__(kVecThreads, kUpdateCtasPerSm)
 // array as one flat stream; p is read only after this.
 template <typename T> __global__ void __launch_bounds__(kVecThreads) k_flush_pressure(const GridDesc* grids, const Tile* tiles)
 {
+    dependent_start();
     using Q = typename Quad<T>::type;
     const Tile t = tiles[blockIdx.x];
     const GridDesc& g = grids[t.grid];
@@ -768,6 +776,7 @@ template <typename T> __global__ void __launch_bounds__(kVecThreads) k_flush_pre
 // FluidGridCPU.cpp:1098-1118.
 template <typename T> __global__ void k_velocity_update(const GridDesc* grids, const Tile* tiles)
 {
+    dependent_start();
     FC_VEC_TILE_PROLOGUE
     if (g.state->status == kBreakdown)
         return;
@@ -822,6 +831,7 @@ __device__ __forceinline__ double face_ulp(double value)
 // sum of squares.
 template <typename T> __global__ void __launch_bounds__(kVecThreads) k_divergence(const GridDesc* grids, const Tile* tiles)
 {
+    dependent_start();
     FC_VEC_TILE_PROLOGUE
     const T* u = static_cast<const T*>(g.u);
     const T* v = static_cast<const T*>(g.v);

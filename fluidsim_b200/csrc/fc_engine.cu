@@ -732,7 +732,7 @@ __global__ void k_init_states(const GridDesc* grids, int n, const ProjectParams*
 }
 
 // Open (non-solid) cells define the mean-free subspace of the solve.
-__global__ void __launch_bounds__(kVecThreads) k_count_open(const GridDesc* grids, const Tile* tiles)
+__global__ void __launch_bounds__(kVecThreads) k_count_open(const GridDesc* __restrict__ grids, const Tile* __restrict__ tiles)
 {
     dependent_start();
     const Tile t = tiles[blockIdx.x];

@@ -90,7 +90,7 @@ __global__ void __launch_bounds__(kVecThreads) k_precondition_diagonal(const Gri
 
 // Mixed precision: FP16 copies of a level's face weights for the strip kernels, divided by
 // the level's scale and saturated at the largest finite FP16 value (blockIdx.y = grid).
-__global__ void k_weights_half(const GridDesc* grids, int level)
+__global__ void k_weights_half(const GridDesc* __restrict__ grids, int level)
 {
     dependent_start();
     const GridDesc& g = grids[blockIdx.y];
@@ -135,7 +135,7 @@ template <typename T> __device__ __forceinline__ bool held_cell(const GridDesc& 
 // (the FP16 copies times the level scale on mixed-precision coarse levels), 0 where the sum is
 // not positive and in the padding. The kernels formed it per region before; the sum and the
 // reciprocal are the same, so the smoothing is unchanged (PressureMultigrid.cpp:104-117).
-template <typename T> __global__ void k_inverse_diagonal(const GridDesc* grids, int level)
+template <typename T> __global__ void k_inverse_diagonal(const GridDesc* __restrict__ grids, int level)
 {
     dependent_start();
     const GridDesc& g = grids[blockIdx.y];
@@ -188,7 +188,7 @@ template <typename T> __global__ void k_inverse_diagonal(const GridDesc* grids, 
 // :104-117 (the diagonal is recomputed on the fly wherever it is needed).
 // One thread per coarse cell (blockIdx.y = grid): the FP64 divisions of a cell form a long
 // dependent chain, so the kernel needs many cells in flight rather than many cells per thread.
-template <typename T> __global__ void k_coarsen(const GridDesc* grids, int level)
+template <typename T> __global__ void k_coarsen(const GridDesc* __restrict__ grids, int level)
 {
     dependent_start();
     const GridDesc& g = grids[blockIdx.y];

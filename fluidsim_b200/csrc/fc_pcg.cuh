@@ -96,7 +96,7 @@ __device__ __forceinline__ bool cell_held(const GridDesc& g, int x, int y)
 
 // Density from component masses: sum of liquid then gas masses, times 1/dx^2.
 // FluidGridCPU.cpp:1399-1423 (rebuildDensity).
-__global__ void k_density(const GridDesc* grids, const Tile* tiles)
+__global__ void k_density(const GridDesc* __restrict__ grids, const Tile* __restrict__ tiles)
 {
     dependent_start();
     FC_VEC_TILE_PROLOGUE
@@ -116,7 +116,7 @@ __global__ void k_density(const GridDesc* grids, const Tile* tiles)
 
 // Face weights 2/(rho_a + rho_b), zero on walls and around solid cells.
 // FluidGridCPU.cpp:1154-1205 (rebuildPressureCoefficients).
-template <typename T> __global__ void k_coefficients(const GridDesc* grids, const Tile* tiles)
+template <typename T> __global__ void k_coefficients(const GridDesc* __restrict__ grids, const Tile* __restrict__ tiles)
 {
     dependent_start();
     FC_VEC_TILE_PROLOGUE
@@ -179,7 +179,7 @@ __device__ __forceinline__ void cell_faces(const GridDesc& g, int x, int y, bool
 
 // b = -(du + dv)/dx * dx^2/dt with closed faces zeroed; sums b over open cells.
 // FluidGridCPU.cpp:1050-1083.
-template <typename T> __global__ void __launch_bounds__(kVecThreads) k_rhs(const GridDesc* grids, const Tile* tiles)
+template <typename T> __global__ void __launch_bounds__(kVecThreads) k_rhs(const GridDesc* __restrict__ grids, const Tile* __restrict__ tiles)
 {
     dependent_start();
     FC_VEC_TILE_PROLOGUE
@@ -210,7 +210,7 @@ template <typename T> __global__ void __launch_bounds__(kVecThreads) k_rhs(const
 }
 
 // max |b - mean| and sum (b - mean)^2; decides the early exit (FluidGridCPU.cpp:1731-1740).
-template <typename T> __global__ void __launch_bounds__(kVecThreads) k_rhs_stats(const GridDesc* grids, const Tile* tiles)
+template <typename T> __global__ void __launch_bounds__(kVecThreads) k_rhs_stats(const GridDesc* __restrict__ grids, const Tile* __restrict__ tiles)
 {
     dependent_start();
     FC_VEC_TILE_PROLOGUE
@@ -246,7 +246,7 @@ template <typename T> __global__ void __launch_bounds__(kVecThreads) k_rhs_stats
 
 // Warm start p = 2p - p_prev, or clear both when no solve is needed; sums the prediction.
 // FluidGridCPU.cpp:1731-1753.
-__global__ void __launch_bounds__(kVecThreads) k_warm_start(const GridDesc* grids, const Tile* tiles)
+__global__ void __launch_bounds__(kVecThreads) k_warm_start(const GridDesc* __restrict__ grids, const Tile* __restrict__ tiles)
 {
     dependent_start();
     FC_VEC_TILE_PROLOGUE
@@ -279,7 +279,7 @@ __global__ void __launch_bounds__(kVecThreads) k_warm_start(const GridDesc* grid
 }
 
 // Pressure sum for the final mean removal.
-__global__ void __launch_bounds__(kVecThreads) k_pressure_sum(const GridDesc* grids, const Tile* tiles)
+__global__ void __launch_bounds__(kVecThreads) k_pressure_sum(const GridDesc* __restrict__ grids, const Tile* __restrict__ tiles)
 {
     dependent_start();
     FC_VEC_TILE_PROLOGUE
@@ -302,7 +302,7 @@ __global__ void __launch_bounds__(kVecThreads) k_pressure_sum(const GridDesc* gr
 }
 
 // p -= mean_p over open cells (FluidGridCPU.cpp:1466-1474, removeMean).
-__global__ void k_remove_pressure_mean(const GridDesc* grids, const Tile* tiles)
+__global__ void k_remove_pressure_mean(const GridDesc* __restrict__ grids, const Tile* __restrict__ tiles)
 {
     dependent_start();
     FC_VEC_TILE_PROLOGUE
@@ -348,7 +348,7 @@ __device__ __forceinline__ double apply_cell_fp64_pending(const T* right, const 
 // `initial` selects the solve's first residual (FluidGridCPU.cpp:1754-1757) versus the
 // convergence check inside the loop (:1795-1804).
 template <typename T>
-__global__ void __launch_bounds__(kVecThreads) k_true_residual(const GridDesc* grids, const Tile* tiles, int initial)
+__global__ void __launch_bounds__(kVecThreads) k_true_residual(const GridDesc* __restrict__ grids, const Tile* __restrict__ tiles, int initial)
 {
     allow_dependents();
     FC_VEC_TILE_PROLOGUE
@@ -442,7 +442,7 @@ template <> struct VecPair<double>
 // Operator: FluidGridCPU.cpp:1507-1598.
 template <typename T>
 __global__ void __launch_bounds__(kVecThreads, sizeof(T) == 4 ? 4 : 1)
-    k_direction_operator(const GridDesc* grids, const Tile* tiles, int parity)
+    k_direction_operator(const GridDesc* __restrict__ grids, const Tile* __restrict__ tiles, int parity)
 {
     using P = typename VecPair<T>::type;
     constexpr int R = 2;
@@ -628,7 +628,7 @@ __device__ __forceinline__ void add_step(double4& p, double alpha, const typenam
 
 template <typename T>
 __global__ void __launch_bounds__(kVecThreads, kUpdateCtasPerSm)
-    k_update(const GridDesc* grids, const Tile* tiles, int count, int parity)
+    k_update(const GridDesc* __restrict__ grids, const Tile* __restrict__ tiles, int count, int parity)
 {
     using Q = typename Quad<T>::type;
     // Quads per thread and step (FP64 takes one: its quads are twice the registers). A thread
@@ -749,7 +749,7 @@ __global__ void __launch_bounds__(kVecThreads, kUpdateCtasPerSm)
 
 // Applies a pair's pending p += alpha d at the loop's exit (see k_update), over the padded
 // array as one flat stream; p is read only after this.
-template <typename T> __global__ void __launch_bounds__(kVecThreads) k_flush_pressure(const GridDesc* grids, const Tile* tiles)
+template <typename T> __global__ void __launch_bounds__(kVecThreads) k_flush_pressure(const GridDesc* __restrict__ grids, const Tile* __restrict__ tiles)
 {
     dependent_start();
     using Q = typename Quad<T>::type;
@@ -774,7 +774,7 @@ template <typename T> __global__ void __launch_bounds__(kVecThreads) k_flush_pre
 
 // u -= (dp/dx) dt w on open interior faces; each cell updates its left and upper face.
 // FluidGridCPU.cpp:1098-1118.
-template <typename T> __global__ void k_velocity_update(const GridDesc* grids, const Tile* tiles)
+template <typename T> __global__ void k_velocity_update(const GridDesc* __restrict__ grids, const Tile* __restrict__ tiles)
 {
     dependent_start();
     FC_VEC_TILE_PROLOGUE
@@ -829,7 +829,7 @@ __device__ __forceinline__ double face_ulp(double value)
 // max |div u| (FluidGridCPU.cpp:1126-1152), its excess over the float rounding allowance of the
 // four faces (as UniformWebGPU's velocity_stats, FluidUniformWebGPUKernels.h:166-213), and the
 // sum of squares.
-template <typename T> __global__ void __launch_bounds__(kVecThreads) k_divergence(const GridDesc* grids, const Tile* tiles)
+template <typename T> __global__ void __launch_bounds__(kVecThreads) k_divergence(const GridDesc* __restrict__ grids, const Tile* __restrict__ tiles)
 {
     dependent_start();
     FC_VEC_TILE_PROLOGUE

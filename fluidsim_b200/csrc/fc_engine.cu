@@ -1629,8 +1629,9 @@ template <typename T> void download_velocity(Grid& g, double* host, const void* 
         return;
     FC_LAUNCH(k_to_f64<T>, std::min<int>(ceil_div(int(std::min<size_t>(count, 1 << 30)), 256), 4096), 256, 0, g.stream,
         static_cast<const T*>(device), g.staging, (long long)count);
+    // Stream order keeps the staging buffer's next writer behind this copy; the caller waits
+    // for the host buffers.
     check(cudaMemcpyAsync(host, g.staging, count * sizeof(double), cudaMemcpyDeviceToHost, g.stream), "download");
-    check(cudaStreamSynchronize(g.stream), "download");
 }
 
 int blocks_for(size_t n) { return int(std::min<size_t>((n + 255) / 256, 4096)); }
@@ -1691,7 +1692,6 @@ void download(Grid& g, double* fraction, double* u, double* v, double* pressure,
         if (dst)
             check(cudaMemcpyAsync(dst, g.masses + size_t(k) * n, n * sizeof(double), cudaMemcpyDeviceToHost, g.stream), "masses");
     }
-    check(cudaStreamSynchronize(g.stream), "download");
     dispatch(g.precision, [&](auto zero)
     {
         using T = decltype(zero);

@@ -325,6 +325,11 @@ template <typename T> __global__ void __launch_bounds__(kCoarseThreads) k_coarse
     // scaled, one after the trailing update. The threads cover the trailing triangle as rows of
     // 64 columns (kMaxCoarse), 512 / 64 rows at a time, with no index divisions; each entry takes
     // the same operations in the same order as in the reference's column loop.
+    //
+    // Y = L^-1 by right-looking forward substitution runs in the same steps: row k of Y has all
+    // its products once step k starts (steps j < k gave them), takes its division by the pivot
+    // with column k's scaling, and the rows below take its product with the trailing update.
+    // Each entry of L and Y sees the same operations in the same order as in two separate loops.
     constexpr int kCols = kMaxCoarse, kRows = kCoarseThreads / kMaxCoarse;
     const int trow = threadIdx.x / kCols, tcol = threadIdx.x % kCols;
     for (int k = 0; k < n; ++k)
@@ -335,6 +340,9 @@ template <typename T> __global__ void __launch_bounds__(kCoarseThreads) k_coarse
             failed = 1;
         for (int row = k + 1 + threadIdx.x; row < n; row += blockDim.x)
             a[row * n + k] = a[row * n + k] / pivot;
+        // Y's row k on other threads than column k's scaling (those with index >= kMaxCoarse).
+        for (int col = int(threadIdx.x) - kMaxCoarse; col >= 0 && col <= k; col += blockDim.x - kMaxCoarse)
+            yi[k * n + col] = yi[k * n + col] / pivot;
         __syncthreads();
         if (threadIdx.x == 0)
             a[k * n + k] = pivot;
@@ -342,16 +350,6 @@ template <typename T> __global__ void __launch_bounds__(kCoarseThreads) k_coarse
         for (int row = k + 1 + trow; row < n; row += kRows)
             if (col <= row)
                 a[row * n + col] -= a[row * n + k] * a[col * n + k];
-        __syncthreads();
-    }
-    // Y = L^-1, right-looking forward substitution: row k of Y is final after its division;
-    // the rows below then take its product.
-    for (int k = 0; k < n; ++k)
-    {
-        const double pivot = a[k * n + k];
-        for (int col = threadIdx.x; col <= k; col += blockDim.x)
-            yi[k * n + col] = yi[k * n + col] / pivot;
-        __syncthreads();
         if (tcol <= k)
             for (int row = k + 1 + trow; row < n; row += kRows)
                 yi[row * n + tcol] -= a[row * n + k] * yi[k * n + tcol];

@@ -251,10 +251,10 @@ template <typename T> __device__ __forceinline__ T prolong_lerp(T w, T lo, T hi)
 // store, which put dependent global loads on each tile's path.
 //
 // A tile whose grid's solve is done is neither computed nor copied in: the issuing thread
-// completes its barrier phase with a plain arrival instead of the boxes and records its verdict
+// completes its barrier phase with a plain arrival instead of the boxes and records its decision
 // in `tile_live`, which every thread reads after the phase's wait. The loop's idle passes after
 // convergence, and the finished grids of a batch, then stream nothing but the first tile's
-// boxes of each CTA (issued before the dependency wait, when no verdict is known yet).
+// boxes of each CTA (issued before the dependency wait, when no decision is known yet).
 template <typename T, int K, typename W, int WARPS>
 __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2 : 1)
     k_smooth_pre(const GridDesc* __restrict__ grids, const Tile* __restrict__ tiles, int count, int level, int set)
@@ -271,7 +271,7 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
     static_assert(Shape::HALO % 2 == 0 && Shape::HALO / 2 >= 2 && OCX + Shape::HALO / 2 <= 31, "restriction lanes");
     __shared__ T lines[Shape::RY][32];
     __shared__ RestrictAxis<T> along_y[OCY];
-    __shared__ int tile_live; // the issuing thread's verdict on the tile it last started
+    __shared__ int tile_live; // the issuing thread's decision on the tile it last started
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     allow_dependents();
     // TMA writes shared memory at 128-byte aligned addresses only; a misplaced staging buffer is
@@ -301,7 +301,7 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
         return;
     }
     // The first tile's boxes complete its phase whatever its grid's state (the weights are in
-    // flight already); the verdict only decides whether it is computed.
+    // flight already); it only decides whether the tile is computed.
     if (threadIdx.x == 0 && i < count)
     {
         tile_live = grids[t.grid].state->done == 0;
@@ -471,7 +471,7 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
     __shared__ Edges<T, WARPS> edges;
     __shared__ double4 total;
     __shared__ double2 warp_pairs[WARPS];
-    __shared__ int tile_live; // the issuing thread's verdict on the tile it last started (k_smooth_pre)
+    __shared__ int tile_live; // the issuing thread's decision on the tile it last started (k_smooth_pre)
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     allow_dependents();
     // TMA writes shared memory at 128-byte aligned addresses only; a misplaced staging buffer is
@@ -501,7 +501,7 @@ __global__ void __launch_bounds__(32 * WARPS, (sizeof(T) == 4 && WARPS == 8) ? 2
         return;
     }
     // The first tile's boxes complete its phase whatever its grid's state (the weights are in
-    // flight already); the verdict only decides whether it is computed.
+    // flight already); it only decides whether the tile is computed.
     if (threadIdx.x == 0 && i < count)
     {
         tile_live = grids[t.grid].state->done == 0;

@@ -256,7 +256,7 @@ def test_device_coefficients_are_the_references_bit_for_bit(path):
 def test_max_divergence_is_the_references_quantity(path):
     """a12: the divergence the device reports is max |(du + dv) / dx| of its own final
     velocities (FluidGridCPU.cpp:1126-1152, recomputed on the host: bit for bit), meets the
-    fixture's convergence verdict, and lies within 10 % of the fixture's value. The value after
+    fixture's convergence flag, and lies within 10 % of the fixture's value. The value after
     the solve is the stopping residual itself, which reduction order moves by a few percent
     (the FP64 restatement differs from the fixtures by up to 7.5 %)."""
     d = golden(os.path.basename(path))

@@ -89,6 +89,15 @@ __device__ __forceinline__ bool cell_held(const GridDesc& g, int x, int y)
     return cell_solid(g, x, y) || (g.air && g.air[(long long)y * g.W + x]);
 }
 
+// cell_held through the kernel's own copies of the masks: `restrict` tells the compiler that no
+// store of the kernel writes them, so their loads may be issued ahead of its stores.
+__device__ __forceinline__ bool held_at(const unsigned char* __restrict__ solid, const unsigned char* __restrict__ air,
+    int W, int x, int y)
+{
+    const long long c = (long long)y * W + x;
+    return (solid && solid[c]) || (air && air[c]);
+}
+
 #define FC_VEC_TILE_PROLOGUE                                                                       \
     const Tile t = tiles[blockIdx.x];                                                              \
     const GridDesc& g = grids[t.grid];                                                             \
@@ -215,13 +224,18 @@ template <typename T> __global__ void __launch_bounds__(kVecThreads) k_rhs_stats
     dependent_start();
     FC_VEC_TILE_PROLOGUE
     const double mean = g.state->mean_b;
+    const int W = g.W, H = g.H, S = g.S;
+    const unsigned char* __restrict__ solid = g.solid;
+    const unsigned char* __restrict__ air = g.air;
+    const double* __restrict__ rhs = g.b;
     double mx = 0.0, sq = 0.0;
+#pragma unroll
     for (int k = 0; k < kVecCells; ++k)
     {
         const int x = t.x0 + tx + 32 * (k & 1), y = t.y0 + ty + 8 * (k >> 1);
-        if (x >= g.W || y >= g.H || cell_held(g, x, y))
+        if (x >= W || y >= H || held_at(solid, air, W, x, y))
             continue;
-        const double b = g.b[padded_index(g.S, x, y)] - mean;
+        const double b = rhs[padded_index(S, x, y)] - mean;
         mx = fmax(mx, isfinite(b) ? fabs(b) : INFINITY);
         sq += b * b;
     }
@@ -251,23 +265,29 @@ __global__ void __launch_bounds__(kVecThreads) k_warm_start(const GridDesc* __re
     dependent_start();
     FC_VEC_TILE_PROLOGUE
     const bool clear = g.state->status == kNoWork;
+    const int W = g.W, H = g.H, S = g.S;
+    const unsigned char* __restrict__ solid = g.solid;
+    const unsigned char* __restrict__ air = g.air;
+    double* __restrict__ p = g.p;
+    double* __restrict__ p_prev = g.p_prev;
     double sum = 0.0;
+#pragma unroll
     for (int k = 0; k < kVecCells; ++k)
     {
         const int x = t.x0 + tx + 32 * (k & 1), y = t.y0 + ty + 8 * (k >> 1);
-        if (x >= g.W || y >= g.H)
+        if (x >= W || y >= H)
             continue;
-        const long long i = padded_index(g.S, x, y);
-        if (clear || cell_held(g, x, y))
+        const long long i = padded_index(S, x, y);
+        if (clear || held_at(solid, air, W, x, y))
         {
-            g.p[i] = 0.0;
-            g.p_prev[i] = 0.0;
+            p[i] = 0.0;
+            p_prev[i] = 0.0;
             continue;
         }
-        const double latest = g.p[i];
-        const double predicted = 2.0 * latest - g.p_prev[i];
-        g.p[i] = predicted;
-        g.p_prev[i] = latest;
+        const double latest = p[i];
+        const double predicted = 2.0 * latest - p_prev[i];
+        p[i] = predicted;
+        p_prev[i] = latest;
         sum += predicted;
     }
     __shared__ double4 total;
@@ -285,13 +305,18 @@ __global__ void __launch_bounds__(kVecThreads) k_pressure_sum(const GridDesc* __
     FC_VEC_TILE_PROLOGUE
     if (g.state->status == kBreakdown)
         return;
+    const int W = g.W, H = g.H, S = g.S;
+    const unsigned char* __restrict__ solid = g.solid;
+    const unsigned char* __restrict__ air = g.air;
+    const double* __restrict__ p = g.p;
     double sum = 0.0;
+#pragma unroll
     for (int k = 0; k < kVecCells; ++k)
     {
         const int x = t.x0 + tx + 32 * (k & 1), y = t.y0 + ty + 8 * (k >> 1);
-        if (x >= g.W || y >= g.H || cell_held(g, x, y))
+        if (x >= W || y >= H || held_at(solid, air, W, x, y))
             continue;
-        sum += g.p[padded_index(g.S, x, y)];
+        sum += p[padded_index(S, x, y)];
     }
     __shared__ double4 total;
     if (arrive_last<kVecThreads>(g, t.index, g.vec_tiles, block_reduce4<kVecThreads>(make_double4(sum, 0, 0, 0), 0), &total, 0))
@@ -309,14 +334,19 @@ __global__ void k_remove_pressure_mean(const GridDesc* __restrict__ grids, const
     if (g.state->status == kBreakdown)
         return;
     const double mean = g.state->mean_p;
+    const int W = g.W, H = g.H, S = g.S;
+    const unsigned char* __restrict__ solid = g.solid;
+    const unsigned char* __restrict__ air = g.air;
+    double* __restrict__ p = g.p;
+#pragma unroll
     for (int k = 0; k < kVecCells; ++k)
     {
         const int x = t.x0 + tx + 32 * (k & 1), y = t.y0 + ty + 8 * (k >> 1);
-        if (x >= g.W || y >= g.H)
+        if (x >= W || y >= H)
             continue;
-        const long long i = padded_index(g.S, x, y);
+        const long long i = padded_index(S, x, y);
         // Pressure inside obstacles (and in Dirichlet air) is held at zero.
-        g.p[i] = cell_held(g, x, y) ? 0.0 : g.p[i] - mean;
+        p[i] = held_at(solid, air, W, x, y) ? 0.0 : p[i] - mean;
     }
 }
 
@@ -356,25 +386,31 @@ __global__ void __launch_bounds__(kVecThreads) k_true_residual(const GridDesc* _
     dependency_wait();
     if (s.done || (!initial && !s.verify))
         return;
-    const T* right = static_cast<const T*>(g.lev[0].right);
-    const T* down = static_cast<const T*>(g.lev[0].down);
-    T* r = static_cast<T*>(g.r);
+    const T* __restrict__ right = static_cast<const T*>(g.lev[0].right);
+    const T* __restrict__ down = static_cast<const T*>(g.lev[0].down);
+    T* __restrict__ r = static_cast<T*>(g.r);
+    const double* __restrict__ rhs = g.b;
+    const double* __restrict__ p = g.p;
+    const int W = g.W, H = g.H, S = g.S;
+    const unsigned char* __restrict__ solid = g.solid;
+    const unsigned char* __restrict__ air = g.air;
     const double mean_b = s.mean_b;
     // Inside a pair the pressure still lacks the first iteration's step (k_update).
     const bool pending = !initial && s.p_pending;
-    const T* d0 = static_cast<const T*>(g.d[1]);
+    const T* __restrict__ d0 = static_cast<const T*>(g.d[1]);
     const double alpha0 = s.alpha_pending;
     double sum = 0.0, mx = 0.0, sq = 0.0;
+#pragma unroll
     for (int k = 0; k < kVecCells; ++k)
     {
         const int x = t.x0 + tx + 32 * (k & 1), y = t.y0 + ty + 8 * (k >> 1);
-        if (x >= g.W || y >= g.H)
+        if (x >= W || y >= H)
             continue;
-        const long long i = padded_index(g.S, x, y);
+        const long long i = padded_index(S, x, y);
         double value = 0.0;
-        if (!cell_held(g, x, y))
-            value = (g.b[i] - mean_b) - (pending ? apply_cell_fp64_pending(right, down, g.p, d0, alpha0, i, g.S)
-                                                 : apply_cell_fp64(right, down, g.p, i, g.S));
+        if (!held_at(solid, air, W, x, y))
+            value = (rhs[i] - mean_b) - (pending ? apply_cell_fp64_pending(right, down, p, d0, alpha0, i, S)
+                                                 : apply_cell_fp64(right, down, p, i, S));
         const T stored = T(value);
         r[i] = stored;
         const double rv = dd(stored);
@@ -780,34 +816,37 @@ template <typename T> __global__ void k_velocity_update(const GridDesc* __restri
     FC_VEC_TILE_PROLOGUE
     if (g.state->status == kBreakdown)
         return;
-    const double dt = g.state->dt;
-    T* u = static_cast<T*>(g.u);
-    T* v = static_cast<T*>(g.v);
-    const T* right = static_cast<const T*>(g.lev[0].right);
-    const T* down = static_cast<const T*>(g.lev[0].down);
+    const double dt = g.state->dt, dx = g.dx;
+    const int W = g.W, H = g.H, S = g.S;
+    T* __restrict__ u = static_cast<T*>(g.u);
+    T* __restrict__ v = static_cast<T*>(g.v);
+    const T* __restrict__ right = static_cast<const T*>(g.lev[0].right);
+    const T* __restrict__ down = static_cast<const T*>(g.lev[0].down);
+    const double* __restrict__ p = g.p;
+#pragma unroll
     for (int k = 0; k < kVecCells; ++k)
     {
         const int x = t.x0 + tx + 32 * (k & 1), y = t.y0 + ty + 8 * (k >> 1);
-        if (x >= g.W || y >= g.H)
+        if (x >= W || y >= H)
             continue;
-        const long long i = padded_index(g.S, x, y);
-        const double pc = g.p[i];
+        const long long i = padded_index(S, x, y);
+        const double pc = p[i];
         if (x > 0)
         {
             const double w = dd(right[i - 1]);
             if (w != 0.0)
             {
-                const long long f = (long long)y * (g.W + 1) + x;
-                u[f] = T(dd(u[f]) - ((pc - g.p[i - 1]) / g.dx) * dt * w);
+                const long long f = (long long)y * (W + 1) + x;
+                u[f] = T(dd(u[f]) - ((pc - p[i - 1]) / dx) * dt * w);
             }
         }
         if (y > 0)
         {
-            const double w = dd(down[i - g.S]);
+            const double w = dd(down[i - S]);
             if (w != 0.0)
             {
-                const long long f = (long long)y * g.W + x;
-                v[f] = T(dd(v[f]) - ((pc - g.p[i - g.S]) / g.dx) * dt * w);
+                const long long f = (long long)y * W + x;
+                v[f] = T(dd(v[f]) - ((pc - p[i - S]) / dx) * dt * w);
             }
         }
     }
@@ -833,29 +872,35 @@ template <typename T> __global__ void __launch_bounds__(kVecThreads) k_divergenc
 {
     dependent_start();
     FC_VEC_TILE_PROLOGUE
-    const T* u = static_cast<const T*>(g.u);
-    const T* v = static_cast<const T*>(g.v);
+    const T* __restrict__ u = static_cast<const T*>(g.u);
+    const T* __restrict__ v = static_cast<const T*>(g.v);
+    const int W = g.W, H = g.H;
+    const double dx = g.dx;
+    const bool dirichlet = g.air != nullptr;
+    const unsigned char* __restrict__ solid = g.solid;
+    const double* __restrict__ fraction = g.fraction;
     double mx = 0.0, excess = 0.0, sq = 0.0;
     int nonfinite = 0;
+#pragma unroll
     for (int k = 0; k < kVecCells; ++k)
     {
         const int x = t.x0 + tx + 32 * (k & 1), y = t.y0 + ty + 8 * (k >> 1);
-        if (x >= g.W || y >= g.H)
+        if (x >= W || y >= H)
             continue;
         // Dirichlet air: only the liquid is held divergence-free (classified from the current
         // fraction, so a check between steps needs no coefficient rebuild).
-        if (g.air && (cell_solid(g, x, y) || !(g.fraction[(long long)y * g.W + x] > 0.5)))
+        const long long iv = (long long)y * W + x;
+        if (dirichlet && ((solid && solid[iv]) || !(fraction[iv] > 0.5)))
             continue;
-        const long long iu = (long long)y * (g.W + 1) + x;
-        const long long iv = (long long)y * g.W + x;
-        const T ul = u[iu], ur = u[iu + 1], vu = v[iv], vd = v[iv + g.W];
-        const double div = ((dd(ur) - dd(ul)) + (dd(vd) - dd(vu))) / g.dx;
+        const long long iu = (long long)y * (W + 1) + x;
+        const T ul = u[iu], ur = u[iu + 1], vu = v[iv], vd = v[iv + W];
+        const double div = ((dd(ur) - dd(ul)) + (dd(vd) - dd(vu))) / dx;
         if (!isfinite(div))
         {
             nonfinite = 1;
             continue;
         }
-        const double rounding = (face_ulp(ul) + face_ulp(ur) + face_ulp(vu) + face_ulp(vd)) / g.dx;
+        const double rounding = (face_ulp(ul) + face_ulp(ur) + face_ulp(vu) + face_ulp(vd)) / dx;
         mx = fmax(mx, fabs(div));
         excess = fmax(excess, fmax(0.0, fabs(div) - rounding));
         sq += div * div;

@@ -110,16 +110,20 @@ __global__ void k_density(const GridDesc* __restrict__ grids, const Tile* __rest
     dependent_start();
     FC_VEC_TILE_PROLOGUE
     const double inv_area = 1.0 / (g.dx * g.dx);
+    const int W = g.W, H = g.H, components = g.components;
+    const double* const* __restrict__ masses = g.masses;
+    double* __restrict__ density = g.density;
+#pragma unroll
     for (int k = 0; k < kVecCells; ++k)
     {
         const int x = t.x0 + tx + 32 * (k & 1), y = t.y0 + ty + 8 * (k >> 1);
-        if (x >= g.W || y >= g.H)
+        if (x >= W || y >= H)
             continue;
-        const long long i = (long long)y * g.W + x;
+        const long long i = (long long)y * W + x;
         double total = 0.0;
-        for (int m = 0; m < g.components; ++m)
-            total += g.masses[m][i];
-        g.density[i] = total * inv_area;
+        for (int m = 0; m < components; ++m)
+            total += masses[m][i];
+        density[i] = total * inv_area;
     }
 }
 
@@ -129,24 +133,30 @@ template <typename T> __global__ void k_coefficients(const GridDesc* __restrict_
 {
     dependent_start();
     FC_VEC_TILE_PROLOGUE
-    const double* density = g.density;
-    T* right = static_cast<T*>(g.lev[0].right);
-    T* down = static_cast<T*>(g.lev[0].down);
+    const double* __restrict__ density = g.density;
+    T* __restrict__ right = static_cast<T*>(g.lev[0].right);
+    T* __restrict__ down = static_cast<T*>(g.lev[0].down);
+    const int W = g.W, H = g.H, S = g.S;
+    const unsigned char* __restrict__ solid_mask = g.solid;
+    unsigned char* __restrict__ air = g.air;
+    const double* __restrict__ fraction = g.fraction;
+    auto solid_at = [&](int sx, int sy) { return solid_mask && solid_mask[(long long)sy * W + sx]; };
+#pragma unroll
     for (int k = 0; k < kVecCells; ++k)
     {
         const int x = t.x0 + tx + 32 * (k & 1), y = t.y0 + ty + 8 * (k >> 1);
-        if (x >= g.W || y >= g.H)
+        if (x >= W || y >= H)
             continue;
-        const long long c = (long long)y * g.W + x;
-        const long long i = padded_index(g.S, x, y);
-        const bool solid = cell_solid(g, x, y);
-        if (g.air)
-            g.air[c] = !solid && !(g.fraction[c] > 0.5); // FluidGridCPU.cpp:1321-1322: liquid is f > 0.5
+        const long long c = (long long)y * W + x;
+        const long long i = padded_index(S, x, y);
+        const bool solid = solid_at(x, y);
+        if (air)
+            air[c] = !solid && !(fraction[c] > 0.5); // FluidGridCPU.cpp:1321-1322: liquid is f > 0.5
         double wr = 0.0, wd = 0.0;
-        if (x + 1 < g.W && !solid && !cell_solid(g, x + 1, y))
+        if (x + 1 < W && !solid && !solid_at(x + 1, y))
             wr = 2.0 / (density[c] + density[c + 1]);
-        if (y + 1 < g.H && !solid && !cell_solid(g, x, y + 1))
-            wd = 2.0 / (density[c] + density[c + g.W]);
+        if (y + 1 < H && !solid && !solid_at(x, y + 1))
+            wd = 2.0 / (density[c] + density[c + W]);
         right[i] = T(wr);
         down[i] = T(wd);
     }
@@ -155,22 +165,21 @@ template <typename T> __global__ void k_coefficients(const GridDesc* __restrict_
 // Closed faces (outer walls, and faces of solid cells) read as zero; the thread of the cell on
 // the low side of a face writes the zero. Returns the four face velocities of cell (x, y).
 template <typename T>
-__device__ __forceinline__ void cell_faces(const GridDesc& g, int x, int y, bool write_closed, double& ul, double& ur,
-    double& vu, double& vd)
+__device__ __forceinline__ void cell_faces(T* __restrict__ u, T* __restrict__ v, const unsigned char* __restrict__ solid,
+    int W, int H, int x, int y, bool write_closed, double& ul, double& ur, double& vu, double& vd)
 {
-    T* u = static_cast<T*>(g.u);
-    T* v = static_cast<T*>(g.v);
-    const long long iu = (long long)y * (g.W + 1) + x;
-    const long long iv = (long long)y * g.W + x;
-    const bool solid = cell_solid(g, x, y);
-    const bool closed_l = x == 0 || solid || cell_solid(g, x - 1, y);
-    const bool closed_r = x + 1 == g.W || solid || cell_solid(g, x + 1, y);
-    const bool closed_u = y == 0 || solid || cell_solid(g, x, y - 1);
-    const bool closed_d = y + 1 == g.H || solid || cell_solid(g, x, y + 1);
+    const long long iu = (long long)y * (W + 1) + x;
+    const long long iv = (long long)y * W + x;
+    auto solid_at = [&](int sx, int sy) { return solid && solid[(long long)sy * W + sx]; };
+    const bool here = solid_at(x, y);
+    const bool closed_l = x == 0 || here || solid_at(x - 1, y);
+    const bool closed_r = x + 1 == W || here || solid_at(x + 1, y);
+    const bool closed_u = y == 0 || here || solid_at(x, y - 1);
+    const bool closed_d = y + 1 == H || here || solid_at(x, y + 1);
     ul = closed_l ? 0.0 : dd(u[iu]);
     ur = closed_r ? 0.0 : dd(u[iu + 1]);
     vu = closed_u ? 0.0 : dd(v[iv]);
-    vd = closed_d ? 0.0 : dd(v[iv + g.W]);
+    vd = closed_d ? 0.0 : dd(v[iv + W]);
     if (write_closed)
     {
         // Each closed face is zeroed by exactly one cell: the left/upper face by this cell when
@@ -178,7 +187,7 @@ __device__ __forceinline__ void cell_faces(const GridDesc& g, int x, int y, bool
         if (closed_r)
             u[iu + 1] = T(0);
         if (closed_d)
-            v[iv + g.W] = T(0);
+            v[iv + W] = T(0);
         if (x == 0)
             u[iu] = T(0);
         if (y == 0)
@@ -193,21 +202,29 @@ template <typename T> __global__ void __launch_bounds__(kVecThreads) k_rhs(const
     dependent_start();
     FC_VEC_TILE_PROLOGUE
     const double dt = g.state->dt;
-    const double scale = g.dx * g.dx / dt;
+    const double dx = g.dx;
+    const double scale = dx * dx / dt;
+    const int W = g.W, H = g.H, S = g.S;
+    T* __restrict__ u = static_cast<T*>(g.u);
+    T* __restrict__ v = static_cast<T*>(g.v);
+    const unsigned char* __restrict__ solid = g.solid;
+    const unsigned char* __restrict__ air = g.air;
+    double* __restrict__ rhs = g.b;
     double sum = 0.0;
+#pragma unroll
     for (int k = 0; k < kVecCells; ++k)
     {
         const int x = t.x0 + tx + 32 * (k & 1), y = t.y0 + ty + 8 * (k >> 1);
-        if (x >= g.W || y >= g.H)
+        if (x >= W || y >= H)
             continue;
         double ul, ur, vu, vd;
-        cell_faces<T>(g, x, y, true, ul, ur, vu, vd);
+        cell_faces<T>(u, v, solid, W, H, x, y, true, ul, ur, vu, vd);
         const double du = ur - ul;
         const double dv = vd - vu;
-        double b = -(du + dv) / g.dx * scale;
-        if (cell_held(g, x, y))
+        double b = -(du + dv) / dx * scale;
+        if (held_at(solid, air, W, x, y))
             b = 0.0;
-        g.b[padded_index(g.S, x, y)] = b;
+        rhs[padded_index(S, x, y)] = b;
         sum += b;
     }
     __shared__ double4 total;

@@ -83,60 +83,63 @@ __device__ __forceinline__ void trace_back(const T* u, const T* v, int W, int H,
 // New face velocities into u_next / v_next. The tiles cover the (W+1) x (H+1) face index space:
 // point (i, j) is u face (i, j) when j < H and v face (i, j) when i < W.
 template <typename T>
-__global__ void k_advect_velocity(const GridDesc* grids, const Tile* tiles, double s, double half, T* u_next,
-    T* v_next)
+__global__ void k_advect_velocity(const GridDesc* __restrict__ grids, const Tile* __restrict__ tiles, double s,
+    double half, T* __restrict__ u_next, T* __restrict__ v_next)
 {
     const Tile t = tiles[blockIdx.x];
     const GridDesc& g = grids[t.grid];
-    const T* u = static_cast<const T*>(g.u);
-    const T* v = static_cast<const T*>(g.v);
+    // The current velocities are read only; the new ones go to other arrays.
+    const T* __restrict__ u = static_cast<const T*>(g.u);
+    const T* __restrict__ v = static_cast<const T*>(g.v);
+    const int W = g.W, H = g.H;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     for (int k = 0; k < kVecCells; ++k)
     {
         const int i = t.x0 + tx + 32 * (k & 1), j = t.y0 + ty + 8 * (k >> 1);
-        if (i <= g.W && j < g.H)
+        if (i <= W && j < H)
         {
             double value = 0.0;
-            if (i > 0 && i < g.W)
+            if (i > 0 && i < W)
             {
                 double bx, by;
-                trace_back(u, v, g.W, g.H, s, half, double(i), __dadd_rn(double(j), 0.5), bx, by);
-                value = sample_clamped(u, g.W + 1, g.H, bx, __dsub_rn(by, 0.5));
+                trace_back(u, v, W, H, s, half, double(i), __dadd_rn(double(j), 0.5), bx, by);
+                value = sample_clamped(u, W + 1, H, bx, __dsub_rn(by, 0.5));
             }
-            u_next[(long long)j * (g.W + 1) + i] = T(value);
+            u_next[(long long)j * (W + 1) + i] = T(value);
         }
-        if (i < g.W && j <= g.H)
+        if (i < W && j <= H)
         {
             double value = 0.0;
-            if (j > 0 && j < g.H)
+            if (j > 0 && j < H)
             {
                 double bx, by;
-                trace_back(u, v, g.W, g.H, s, half, __dadd_rn(double(i), 0.5), double(j), bx, by);
-                value = sample_clamped(v, g.W, g.H + 1, __dsub_rn(bx, 0.5), by);
+                trace_back(u, v, W, H, s, half, __dadd_rn(double(i), 0.5), double(j), bx, by);
+                value = sample_clamped(v, W, H + 1, __dsub_rn(bx, 0.5), by);
             }
-            v_next[(long long)j * g.W + i] = T(value);
+            v_next[(long long)j * W + i] = T(value);
         }
     }
 }
 
 // One cell-centred FP64 field (liquid fraction or a component mass) into `next`.
 template <typename T>
-__global__ void k_advect_cells(const GridDesc* grids, const Tile* tiles, double s, double half, const double* field,
-    double* next)
+__global__ void k_advect_cells(const GridDesc* __restrict__ grids, const Tile* __restrict__ tiles, double s, double half,
+    const double* __restrict__ field, double* __restrict__ next)
 {
     const Tile t = tiles[blockIdx.x];
     const GridDesc& g = grids[t.grid];
-    const T* u = static_cast<const T*>(g.u);
-    const T* v = static_cast<const T*>(g.v);
+    const T* __restrict__ u = static_cast<const T*>(g.u);
+    const T* __restrict__ v = static_cast<const T*>(g.v);
+    const int W = g.W, H = g.H;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     for (int k = 0; k < kVecCells; ++k)
     {
         const int i = t.x0 + tx + 32 * (k & 1), j = t.y0 + ty + 8 * (k >> 1);
-        if (i >= g.W || j >= g.H)
+        if (i >= W || j >= H)
             continue;
         double bx, by;
-        trace_back(u, v, g.W, g.H, s, half, __dadd_rn(double(i), 0.5), __dadd_rn(double(j), 0.5), bx, by);
-        next[(long long)j * g.W + i] = sample_clamped(field, g.W, g.H, __dsub_rn(bx, 0.5), __dsub_rn(by, 0.5));
+        trace_back(u, v, W, H, s, half, __dadd_rn(double(i), 0.5), __dadd_rn(double(j), 0.5), bx, by);
+        next[(long long)j * W + i] = sample_clamped(field, W, H, __dsub_rn(bx, 0.5), __dsub_rn(by, 0.5));
     }
 }
 
